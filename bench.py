@@ -1,0 +1,290 @@
+"""Benchmark of the CHAPSim2 per-timestep hot path on B200.
+
+Metric: Mcell-RK3-substeps/s (cells x substeps / s / 1e6), whole job.
+Workload: the periodic turbulent channel, 128 x 96 x 128 cells, tanh
+stretching beta = 1.5, Re_b = 2800, constant mass flux, FP64, CD2 operators
+(the only accuracy whose operators are consistent with the FISHPACK 2nd-order
+Poisson solver), synthetic Poiseuille + seeded noise initial
+field, dt from CFL 0.8 frozen.
+
+One "step" is one RK3 time step (3 substeps) replayed from captured CUDA
+graphs with all state resident in HBM.  The per-step working set (~40 FP64
+fields of 12.6 MB) exceeds the 126 MB L2, so no L2 flush is inserted.
+
+--impl reference times the CPU restatement of the reference's path (the
+oracle; the Fortran/MPI reference cannot be built in this image) on all host
+cores, one substep of the same workload per step.
+
+Multi-GPU (torchrun): independent replicas, one channel per GPU, no
+collective on the data path ("replicas only"); value is the sum over ranks,
+time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from chapsim2_b200 import config as C  # noqa: E402
+from chapsim2_b200 import initial as I  # noqa: E402
+
+METRIC = "Mcell-RK3-substeps/s on 1 B200: mixed+MLP vs plain FP64 at ≤1e-5 L2; HBM frac"
+UNIT = "Mcell-substeps/s"
+# compulsory traffic per cell per RK3 substep, flow-only FP64 (30 words)
+BYTES_PER_CELL_SUBSTEP_FP64 = 240.0
+
+
+def workload(nc=(128, 96, 128), iacc=C.IACCU_CD2):
+    cfg = C.channel(nc=nc, iacc=iacc)
+    fields = I.channel_fields(cfg)
+    cfg.dt = I.cfl_dt(cfg, *fields[:3], cfl=0.8)
+    return cfg, fields
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "", 1).isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+        dist = tdist
+    return world, rank, local, dist
+
+
+def max_over_ranks(dist, v):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_time_oracle(cfg, fields, nsub):
+    """Oracle (CPU restatement) on all host threads: seconds for nsub substeps after the initial step."""
+    from oracle import pyoracle as po
+    o = po.Oracle(cfg)
+    o.set_fields(*fields)
+    o.substep(0)
+    t0 = time.perf_counter()
+    for i in range(nsub):
+        o.substep(1 + i % 3)
+    return time.perf_counter() - t0
+
+
+def run_reference(args, cfg, fields, world, rank, dist):
+    if rank != 0:
+        return None
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    cpu_time_oracle(cfg, fields, args.warmup)
+    t = cpu_time_oracle(cfg, fields, args.steps)
+    value = cfg.ncell * args.steps / t / 1e6
+    sample = f"{args.steps} substeps of the {cfg.nc[0]}x{cfg.nc[1]}x{cfg.nc[2]} channel (CD2, FP64)"
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"channel {cfg.nc[0]}x{cfg.nc[1]}x{cfg.nc[2]} flow-only, beta=1.5, Re_b=2800, CD2",
+                   "step": "one RK3 substep", "cells": cfg.ncell},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def roofline(prof, peak, peak_kind):
+    by = {}
+    for r in prof:
+        k = ("line_op", "fft", "ysolve", "elementwise")[r["kind"]]
+        a = by.setdefault(k, {"ms": 0.0, "bytes": 0.0, "n": 0})
+        a["ms"] += r["ms"]
+        a["bytes"] += r["bytes"]
+        a["n"] += 1
+    dom = max(by, key=lambda k: by[k]["ms"])
+    a = by[dom]
+    achieved = a["bytes"] / (a["ms"] * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get(dom)
+    return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+            "bytes_per_launch": a["bytes"] / a["n"], "ms_per_launch": a["ms"] / a["n"], "launches": a["n"],
+            "share_of_substep": a["ms"] / sum(v["ms"] for v in by.values()),
+            "classes": {k: {"ms": v["ms"], "launches": v["n"]} for k, v in by.items()}}
+
+
+def run_ours(args, cfg, fields, world, rank, local, dist):
+    from chapsim2_b200 import solver as S
+    g = S.Solver(cfg, device=local)
+    g.set_fields(*fields)
+    g.Solve_momentum_eq(0)
+    g.step(args.warmup)
+    g.sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(dist)
+    l0 = g.kernel_launches()
+    ms = g.time_steps(args.steps)
+    l1 = g.kernel_launches()
+    barrier(dist)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(dist, ms)
+    sub = 3 * args.steps
+    value = world * cfg.ncell * sub / (ms_max * 1e-3) / 1e6
+    diag = g.diagnostics()
+
+    # end to end through the host-array drop-in: pinned host fields in/out every substep
+    shp = cfg.shapes()
+    host = [g.pinned(s) for s in shp]
+    cur = g.get_fields()[:4]
+    for h, a in zip(host, cur):
+        h[...] = a
+    barrier(dist)
+    ms_e2e = g.time_steps_host(args.steps, *host)
+    barrier(dist)
+    ms_e2e = max_over_ranks(dist, ms_e2e)
+    field_bytes = sum(int(np.prod(s)) for s in shp) * 8
+    e2e = {"value": world * cfg.ncell * sub / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": 3 * field_bytes, "d2h_bytes_per_step": 3 * field_bytes,
+           "path": "chs_momentum_substep_host semantics: fields H2D, graph substep, fields D2H, x3 per step"}
+
+    peak, peak_kind = measured_peaks()
+    prof = g.profile_substep(1)
+    rl = roofline(prof, peak, peak_kind)
+    step_model = {"bytes_per_cell_substep": BYTES_PER_CELL_SUBSTEP_FP64,
+                  "achieved_gbs": BYTES_PER_CELL_SUBSTEP_FP64 * cfg.ncell * sub / (ms * 1e-3) / 1e9}
+    step_model["frac"] = step_model["achieved_gbs"] / peak
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"channel {cfg.nc[0]}x{cfg.nc[1]}x{cfg.nc[2]} flow-only, beta=1.5, Re_b=2800, CD2",
+                   "step": "one RK3 step (3 substeps), CUDA-graph replay",
+                   "cells": cfg.ncell, "dt": cfg.dt, "precision": "fp64",
+                   "l2": "working set ~40 FP64 fields x 12.6 MB per step > 126 MB L2; no flush",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": rl, "step_model": step_model, "e2e": e2e,
+        "gpu_launches": l1 - l0, "clocks": clk,
+        "diagnostics": {"max_div": diag["max_div"], "bulk_u": diag["bulk_u"], "bulk_ke": diag["bulk_ke"],
+                        "nan": diag["nan_flag"]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        nsub = 6
+        t = cpu_time_oracle(cfg, fields, nsub)
+        out["cpu_baseline"] = {"value": cfg.ncell * nsub / t / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+                               "sample": f"{nsub} substeps of the same channel (oracle, OpenMP)"}
+    g.close()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nc", type=int, nargs=3, default=[128, 96, 128])
+    ap.add_argument("--iacc", type=int, default=C.IACCU_CD2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    cfg, fields = workload(tuple(args.nc), args.iacc)
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        out = run_reference(args, cfg, fields, world, rank, None)
+        if out is not None:
+            print(json.dumps(out))
+        return
+    world, rank, local, dist = dist_setup(args.gpus)
+    out = run_ours(args, cfg, fields, world, rank, local, dist)
+    if rank == 0:
+        print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

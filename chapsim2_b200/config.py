@@ -1,0 +1,161 @@
+"""Domain configuration mirroring CHAPSim2's input parameters and set-up.
+
+Codes follow src/modules.f90 (boundary conditions :223-229, accuracies
+:248-251, stretching :207-212, FFT libraries :169-173).  Geometry follows
+src/geometry.f90:151-269 and :410-530; boundary-condition reassignment follows
+src/bc_general.f90:137-248 and src/input_general.f90:405-460.
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# boundary-condition codes (src/modules.f90:223-229)
+IBC_INTERIOR, IBC_PERIODIC, IBC_SYMMETRIC, IBC_ASYMMETRIC, IBC_DIRICHLET, IBC_NEUMANN, IBC_INTRPL = range(7)
+# accuracy codes (src/modules.f90:248-251)
+IACCU_CD2, IACCU_CD4, IACCU_CP4, IACCU_CP6 = 1, 2, 3, 4
+# stretching (src/modules.f90:207-212)
+ISTRET_NO, ISTRET_CENTRE, ISTRET_2SIDES, ISTRET_BOTTOM, ISTRET_TOP = 0, 1, 2, 3, 4
+# Poisson solvers (src/modules.f90:169-170)
+FFT_FISHPACK_2DFFT, FFT_2DECOMP_3DFFT = 2, 3
+# flow driving (src/modules.f90:260-264)
+IDRVF_NO, IDRVF_X_MASSFLUX = 0, 1
+# variable slots of the nominal bc table
+V_QX, V_QY, V_QZ, V_PR, V_TM = range(5)
+
+
+@dataclass
+class DomainConfig:
+    """One CHAPSim2 domain: grid, boundary conditions, schemes and time step."""
+    nc: tuple
+    lxx: float
+    lyt: float
+    lyb: float
+    lzz: float
+    istret: int = ISTRET_NO
+    rstret: float = 0.0
+    iacc: int = IACCU_CP6
+    ifft: int = FFT_FISHPACK_2DFFT
+    idriven: int = IDRVF_NO
+    ren: float = 1600.0
+    dt: float = 1.0e-3
+    # nominal bc codes [dir x,y,z][var qx,qy,qz,pr,Tm][side]
+    nominal_bc: np.ndarray = field(default_factory=lambda: np.full((3, 5, 2), IBC_PERIODIC, np.int32))
+    # constant y-wall values [var][side] (fbcy_const, src/input_general.f90:420-424)
+    fbcy_const: np.ndarray = field(default_factory=lambda: np.zeros((5, 2)))
+    name: str = "domain"
+
+    @property
+    def periodic_y(self):
+        return bool(np.any(self.nominal_bc[1] == IBC_PERIODIC))
+
+    @property
+    def stretch_y(self):
+        return self.istret != ISTRET_NO
+
+    @property
+    def np_(self):
+        """Point counts per direction: nc for periodic directions, nc + 1 otherwise."""
+        n = list(self.nc)
+        if not self.periodic_y:
+            n[1] = self.nc[1] + 1
+        return tuple(n)
+
+    def shapes(self):
+        """numpy (C-order, k-j-i) shapes of qx, qy, qz, p."""
+        nc, n = self.nc, self.np_
+        return ((nc[2], nc[1], n[0]), (nc[2], n[1], nc[0]), (n[2], nc[1], nc[0]), (nc[2], nc[1], nc[0]))
+
+    @property
+    def ncell(self):
+        return int(self.nc[0]) * int(self.nc[1]) * int(self.nc[2])
+
+
+def taylor_green(n=64, iacc=IACCU_CP6, dt=1.0e-3, ren=1600.0):
+    """3D Taylor-Green vortex box: triply periodic, uniform, 3D-FFT Poisson.
+
+    The reference forces the box to x, z in [0, 2 pi], y in [-pi, pi]
+    (src/input_general.f90:376-382).
+    """
+    return DomainConfig(nc=(n, n, n), lxx=2 * np.pi, lyt=np.pi, lyb=-np.pi, lzz=2 * np.pi, iacc=iacc,
+                        ifft=FFT_2DECOMP_3DFFT, idriven=IDRVF_NO, ren=ren, dt=dt, name=f"tgv{n}")
+
+
+def channel(nc=(128, 96, 128), rstret=0.075, ren=2800.0, iacc=IACCU_CP6, dt=None, lxx=4 * np.pi,
+            lzz=4 * np.pi / 3):
+    """Periodic turbulent channel with no-slip y walls and constant mass flux.
+
+    Stretching is the reference's tanh mapping with beta = 20 * rstret
+    (src/geometry.f90:237); rstret = 0.075 is beta = 1.5.  tanh stretching
+    selects the FISHPACK Poisson path (src/input_general.f90:552).
+    """
+    bc = np.full((3, 5, 2), IBC_PERIODIC, np.int32)
+    bc[1, V_QX] = IBC_DIRICHLET
+    bc[1, V_QY] = IBC_DIRICHLET
+    bc[1, V_QZ] = IBC_DIRICHLET
+    bc[1, V_PR] = IBC_NEUMANN
+    bc[1, V_TM] = IBC_DIRICHLET
+    cfg = DomainConfig(nc=tuple(nc), lxx=lxx, lyt=1.0, lyb=-1.0, lzz=lzz, istret=ISTRET_2SIDES, rstret=rstret,
+                       iacc=iacc, ifft=FFT_FISHPACK_2DFFT, idriven=IDRVF_X_MASSFLUX, ren=ren,
+                       dt=dt if dt is not None else 1.0e-3, nominal_bc=bc, name=f"channel{nc[0]}x{nc[1]}x{nc[2]}")
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# geometry (src/geometry.f90)
+# ---------------------------------------------------------------------------
+def _tanh_mapping(cfg, node, n):
+    if node:
+        shift, delta_eta = 0.0, 1.0 / (n - 1)
+    else:
+        shift, delta_eta = 0.5 / n, 1.0 / n
+    eta = shift + np.arange(n) * delta_eta
+    gamma, delta, ymin, ymax = {ISTRET_2SIDES: (0.5, 0.5, -1.0, 1.0), ISTRET_BOTTOM: (-1.0, 1.0, 0.0, 1.0),
+                                ISTRET_TOP: (1.0, 0.0, 0.0, 1.0)}[cfg.istret]
+    beta = cfg.rstret * 20.0
+    mm = np.tanh(beta * gamma)
+    y = np.tanh(beta * (eta - delta)) / mm
+    m1 = 1.0 - y * y * mm * mm
+    small = (m1 < 1e-20) & (m1 > -1e-20)
+    m1 = np.where(small, 1.0, mm / beta / np.where(small, 1.0, m1))
+    ff = (cfg.lyt - cfg.lyb) / (ymax - ymin)
+    return (y - ymin) * ff + cfg.lyb, m1 / ff
+
+
+def geometry(cfg):
+    """Return dict with h(3), yp(np_geo), yc(nc), mppt, mpcc (yMapping(:,1))."""
+    nc = cfg.nc
+    h = np.array([cfg.lxx / nc[0], (cfg.lyt - cfg.lyb) / nc[1], cfg.lzz / nc[2]])
+    if cfg.stretch_y:
+        h[1] = 1.0 / nc[1]
+        yp, mppt = _tanh_mapping(cfg, True, nc[1] + 1)
+        yc, mpcc = _tanh_mapping(cfg, False, nc[1])
+    else:
+        yp = np.arange(nc[1] + 1) * h[1] + cfg.lyb
+        yc = np.arange(nc[1]) * h[1] + h[1] * 0.5 + cfg.lyb
+        mppt = np.ones(nc[1] + 1)
+        mpcc = np.ones(nc[1])
+    return dict(h=h, yp=yp, yc=yc, mppt=mppt, mpcc=mpcc)
+
+
+def calculated_bcs(cfg):
+    """Apply config_calc_basic_ibc (src/bc_general.f90:137-184) to the nominal table.
+
+    Returns (ibc[3][5][2], fbcy_const[5][2]).
+    """
+    ibc = np.array(cfg.nominal_bc, np.int32, copy=True)
+    fb = np.array(cfg.fbcy_const, np.float64, copy=True)
+    for n in range(2):
+        if ibc[0, V_QX, n] == IBC_SYMMETRIC:
+            ibc[0, V_QX, n] = IBC_ASYMMETRIC
+        if ibc[1, V_QY, n] == IBC_SYMMETRIC:
+            ibc[1, V_QY, n] = IBC_ASYMMETRIC
+        if ibc[2, V_QZ, n] == IBC_SYMMETRIC:
+            ibc[2, V_QZ, n] = IBC_ASYMMETRIC
+        if ibc[0, V_QX, n] == IBC_DIRICHLET:
+            ibc[0, V_PR, n] = IBC_NEUMANN
+        if ibc[1, V_QY, n] == IBC_DIRICHLET:
+            ibc[1, V_PR, n] = IBC_NEUMANN
+            fb[V_PR, n] = 0.0
+        if ibc[2, V_QZ, n] == IBC_DIRICHLET:
+            ibc[2, V_PR, n] = IBC_NEUMANN
+    return ibc, fb

@@ -1,0 +1,692 @@
+// sm_100a kernels of the CHAPSim2 hot path: batched compact line operators,
+// Stockham FFTs, the FISHPACK y-tridiagonal solve, spectral division and the
+// elementwise/reduction kernels of the RK3 substep.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <stdexcept>
+
+#include "chs_kernels.cuh"
+
+namespace chs {
+
+// ===========================================================================
+// Compact line operator
+//
+// One CTA owns LT consecutive lines.  The tile is staged into shared memory
+// with coalesced loads (rows for x, LT consecutive i for y and z), the input
+// expression is evaluated on the fly, then one thread per line builds the RHS
+// with a sliding 5-point register window and runs the Thomas forward sweep
+// in place, followed by the backward sweep and the cyclic closure.  The store
+// phase applies the cyclic correction, the y metric, the Neumann overrides and
+// the output accumulation, again coalesced.
+// ===========================================================================
+template <int DIR>
+struct LineAddr {
+  int64_t nlines;
+  int n1, n2;
+  __device__ __forceinline__ int64_t at(int64_t L, int p, int n) const {
+    if (DIR == 0) return L * n + p;
+    if (DIR == 1) {
+      int64_t k = L / n1, i = L - k * n1;
+      return (k * n + p) * n1 + i;
+    }
+    int64_t j = L / n1, i = L - j * n1;
+    return ((int64_t)p * n2 + j) * n1 + i;
+  }
+};
+
+__device__ __forceinline__ double eval_expr(const LineIO& io, int64_t a) {
+  double A = io.A[a];
+  switch (io.emode) {
+    case E_A: return io.s * A;
+    case E_AB: return io.s * (A * io.B[a]);
+    case E_ApB: return io.s * (A + io.c1 * io.B[a]);
+    default: return io.s * (A + io.c1 * io.B[a]) * io.C[a];
+  }
+}
+
+template <int FAM>
+struct Bulk;
+// r1*(f[i+o0] + sgn f[i+o1]) + r2*(f[i+o2] + sgn f[i+o3]); window w[k] = f[i-2+k]
+template <> struct Bulk<M1P2C> {
+  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
+    return r1 * (w[2] + w[3]) + r2 * (w[1] + w[4]);
+  }
+};
+template <> struct Bulk<M1C2P> {
+  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
+    return r1 * (w[2] + w[1]) + r2 * (w[3] + w[0]);
+  }
+};
+template <> struct Bulk<D1C2C> {
+  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
+    return r1 * (w[3] - w[1]) + r2 * (w[4] - w[0]);
+  }
+};
+template <> struct Bulk<D1P2P> {
+  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
+    return r1 * (w[3] - w[1]) + r2 * (w[4] - w[0]);
+  }
+};
+template <> struct Bulk<D1C2P> {
+  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
+    return r1 * (w[2] - w[1]) + r2 * (w[3] - w[0]);
+  }
+};
+template <> struct Bulk<D1P2C> {
+  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
+    return r1 * (w[3] - w[2]) + r2 * (w[4] - w[1]);
+  }
+};
+
+template <int DIR, int FAM>
+__global__ void __launch_bounds__(256) line_op_kernel(const __grid_constant__ OpPlan P,
+                                                      const __grid_constant__ LineIO io,
+                                                      const double* __restrict__ table, int64_t nlines, int LT) {
+  extern __shared__ double smem[];
+  const int nin = P.nin, nout = P.nout;
+  const int nmax = nin > nout ? nin : nout;
+  const int ld = LT + 1;
+  double* s = smem;                    // [nmax][ld]
+  double* sa = s + (size_t)nmax * ld;  // LHS a
+  double* sc = sa + nmax;              // LHS c'
+  double* sd = sc + nmax;              // LHS 1/pivot
+  double* sx = sd + nmax;              // cyclic correction x1
+  double* sm = sx + nmax;              // y metric
+  LineAddr<DIR> ad{nlines, io.n1, io.n2};
+  const int64_t L0 = (int64_t)blockIdx.x * LT;
+  const int nt = blockDim.x;
+
+  // ---- stage the tile
+  const int tot_in = LT * nin;
+  for (int e = threadIdx.x; e < tot_in; e += nt) {
+    int l, p;
+    if (DIR == 0) { l = e / nin; p = e - l * nin; }
+    else { p = e / LT; l = e - p * LT; }
+    const int64_t L = L0 + l;
+    double v = 0.0;
+    if (L < nlines) v = eval_expr(io, ad.at(L, p, nin));
+    s[p * ld + l] = v;
+  }
+  for (int p = threadIdx.x; p < nout; p += nt) {
+    if (P.tdma) {
+      sa[p] = table[P.la + p];
+      sc[p] = table[P.lc + p];
+      sd[p] = table[P.ld + p];
+      sx[p] = table[P.lx1 + p];
+    }
+    if (P.lmap >= 0) sm[p] = table[P.lmap + p];
+  }
+  __syncthreads();
+
+  // ---- one thread per line: RHS + Thomas
+  const int l = threadIdx.x;
+  const int64_t L = L0 + l;
+  if (l < LT && L < nlines) {
+    double* col = s + l;
+    const double dd = P.dd;
+    double sv[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      double v = 0.0;
+      if (k < P.nspec) {
+        const SpecialRow& R = P.sp[k];
+        for (int t = 0; t < R.nt; ++t) v += R.w[t] * col[R.idx[t] * ld];
+        for (int u = 0; u < 4; ++u)
+          if (R.wb[u] != 0.0) v += R.wb[u] * io.fbc[u * nlines + L];
+      }
+      sv[k] = v * dd;
+    }
+    const int nsw = (P.tdma == 2) ? nout - 1 : nout;
+    double w[5];
+    w[0] = 0.0;
+    w[1] = 0.0;
+    w[2] = col[0];
+    w[3] = col[ld];
+    double yprev = 0.0;
+    for (int i = 0; i < nout; ++i) {
+      w[4] = (i + 2 < nin) ? col[(i + 2) * ld] : 0.0;
+      double r;
+      if (i >= P.b_lo && i <= P.b_hi) {
+        r = Bulk<FAM>::f(w, P.r1, P.r2) * dd;
+      } else {
+        r = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (k < P.nspec && P.sp[k].row == i) r = sv[k];
+      }
+      double y = r;
+      if (P.tdma && i < nsw) {
+        y = (i == 0) ? r / P.b1 : (r - sa[i] * yprev) * sd[i];
+        yprev = y;
+      }
+      col[i * ld] = y;
+      w[0] = w[1]; w[1] = w[2]; w[2] = w[3]; w[3] = w[4];
+    }
+    if (P.tdma) {
+      double xn = col[(nsw - 1) * ld];
+      for (int i = nsw - 2; i >= 0; --i) {
+        const double x = col[i * ld] - sc[i] * xn;
+        col[i * ld] = x;
+        xn = x;
+      }
+      if (P.tdma == 2) {
+        const double rn = col[(nout - 1) * ld];
+        col[(nout - 1) * ld] = (rn - P.cn * col[0] - P.an * col[(nout - 2) * ld]) * P.inv_den;
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- store
+  const int tot_out = LT * nout;
+  for (int e = threadIdx.x; e < tot_out; e += nt) {
+    int ll, p;
+    if (DIR == 0) { ll = e / nout; p = e - ll * nout; }
+    else { p = e / LT; ll = e - p * LT; }
+    const int64_t LL = L0 + ll;
+    if (LL >= nlines) continue;
+    double v = s[p * ld + ll];
+    if (P.tdma == 2 && p < nout - 1) v += sx[p] * s[(nout - 1) * ld + ll];
+    if (P.lmap >= 0) v *= sm[p];
+    if (P.neu1 && p == 0) v = io.fbc[LL];
+    if (P.neu2 && p == nout - 1) v = io.fbc[nlines + LL];
+    const int64_t a = ad.at(LL, p, nout);
+    io.out[a] = io.accumulate ? io.out[a] + io.g * v : io.g * v;
+  }
+}
+
+template <int DIR>
+static void launch_dir(const OpPlan& P, const LineIO& io, const double* table, cudaStream_t st, int64_t nlines,
+                       int LT, size_t shm) {
+  dim3 grid((unsigned)((nlines + LT - 1) / LT));
+  dim3 block(256);
+  switch (P.fam) {
+#define CHS_CASE(F)                                                                                   \
+  case F:                                                                                             \
+    cudaFuncSetAttribute(line_op_kernel<DIR, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm); \
+    line_op_kernel<DIR, F><<<grid, block, shm, st>>>(P, io, table, nlines, LT);                       \
+    break;
+    CHS_CASE(D1C2C)
+    CHS_CASE(D1P2P)
+    CHS_CASE(D1C2P)
+    CHS_CASE(D1P2C)
+    CHS_CASE(M1C2P)
+    CHS_CASE(M1P2C)
+#undef CHS_CASE
+    default: throw std::runtime_error("bad family");
+  }
+}
+
+void launch_line_op(int d, const OpPlan& P, const LineIO& io, const double* table, cudaStream_t st) {
+  int n_in3[3] = {io.n1, io.n2, io.n3};
+  if (n_in3[d] != P.nin) throw std::runtime_error("line operator: input extent does not match the plan");
+  const int64_t nlines = num_lines(d, io.n1, io.n2, io.n3);
+  const int nmax = P.nin > P.nout ? P.nin : P.nout;
+  const int LT = nmax <= 200 ? 64 : 32;
+  const size_t shm = ((size_t)nmax * (LT + 1) + 5 * (size_t)nmax) * sizeof(double);
+  if (d == 0) launch_dir<0>(P, io, table, st, nlines, LT, shm);
+  else if (d == 1) launch_dir<1>(P, io, table, st, nlines, LT, shm);
+  else launch_dir<2>(P, io, table, st, nlines, LT, shm);
+}
+
+// ===========================================================================
+// Stockham FFT in shared memory (radix 2, 3, 4), several lines per CTA
+// ===========================================================================
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+
+// one radix-R butterfly column of a Stockham stage
+template <int R>
+__device__ __forceinline__ void stockham_bfly(const double2* in, double2* out, int j, int n, int ns,
+                                              const double2* tw, int sign) {
+  double2 v[R];
+  const int stride = n / R;
+  const int k = j % ns;
+  const int tstep = n / (ns * R);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    double2 x = in[j + r * stride];
+    if (r > 0 && k > 0) {
+      double2 t = tw[(k * r * tstep) % n];
+      if (sign > 0) t.y = -t.y;
+      x = cmul(x, t);
+    }
+    v[r] = x;
+  }
+  const double sg = (double)sign;
+  if (R == 2) {
+    double2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if (R == 4) {
+    double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    double2 b0 = cadd(v[1], v[3]), b1 = csub(v[1], v[3]);
+    double2 ib1 = make_double2(-sg * b1.y, sg * b1.x);  // (i*sign) * b1
+    v[0] = cadd(a0, b0);
+    v[2] = csub(a0, b0);
+    v[1] = cadd(a1, ib1);
+    v[3] = csub(a1, ib1);
+  } else {  // R == 3
+    const double h = 0.86602540378443864676;  // sqrt(3)/2
+    double2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+    double2 m = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
+    double2 it2 = make_double2(-sg * h * t2.y, sg * h * t2.x);
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(m, it2);
+    v[2] = csub(m, it2);
+  }
+  const int idxd = (j / ns) * ns * R + k;
+#pragma unroll
+  for (int r = 0; r < R; ++r) out[idxd + r * ns] = v[r];
+}
+
+// FFT of `nl` lines of length n stored contiguously in buf0 (line stride n); result in buf0 or buf1
+// (returned).  All threads of the CTA take part.
+__device__ double2* smem_fft(double2* buf0, double2* buf1, int nl, const FftPlan& fp, int sign) {
+  const int n = fp.n;
+  int ns = 1;
+  double2* in = buf0;
+  double2* out = buf1;
+  for (int s = 0; s < fp.nst; ++s) {
+    const int R = fp.radix[s];
+    const int nb = n / R;
+    for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
+      const int line = t / nb, j = t - line * nb;
+      const double2* li = in + line * n;
+      double2* lo = out + line * n;
+      if (R == 4) stockham_bfly<4>(li, lo, j, n, ns, fp.tw, sign);
+      else if (R == 2) stockham_bfly<2>(li, lo, j, n, ns, fp.tw, sign);
+      else stockham_bfly<3>(li, lo, j, n, ns, fp.tw, sign);
+    }
+    __syncthreads();
+    ns *= R;
+    double2* tmp = in; in = out; out = tmp;
+  }
+  return in;
+}
+
+static int fft_lines_per_cta(int n) {
+  int l = 2048 / n;
+  if (l < 1) l = 1;
+  if (l > 32) l = 32;
+  return l;
+}
+
+// real rows -> half spectra; two real rows per complex transform
+__global__ void rfft_x_kernel(const __grid_constant__ FftPlan fp, const double* __restrict__ in,
+                              double2* __restrict__ out, int nrows, int lpc) {
+  extern __shared__ double2 sh[];
+  const int n = fp.n, nh = n / 2 + 1;
+  double2* b0 = sh;
+  double2* b1 = sh + (size_t)lpc * n;
+  const int pair0 = blockIdx.x * lpc;
+  for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
+    const int l = t / n, p = t - l * n;
+    const int ra = 2 * (pair0 + l), rb = ra + 1;
+    double a = 0.0, b = 0.0;
+    if (ra < nrows) a = in[(int64_t)ra * n + p];
+    if (rb < nrows) b = in[(int64_t)rb * n + p];
+    b0[t] = make_double2(a, b);
+  }
+  __syncthreads();
+  double2* r = smem_fft(b0, b1, lpc, fp, -1);
+  for (int t = threadIdx.x; t < lpc * nh; t += blockDim.x) {
+    const int l = t / nh, k = t - l * nh;
+    const int ra = 2 * (pair0 + l), rb = ra + 1;
+    const double2 z = r[l * n + k];
+    double2 zc = r[l * n + ((n - k) % n)];
+    zc.y = -zc.y;
+    const double2 xa = make_double2(0.5 * (z.x + zc.x), 0.5 * (z.y + zc.y));
+    const double2 d = csub(z, zc);
+    const double2 xb = make_double2(0.5 * d.y, -0.5 * d.x);
+    if (ra < nrows) out[(int64_t)ra * nh + k] = xa;
+    if (rb < nrows) out[(int64_t)rb * nh + k] = xb;
+  }
+}
+
+__global__ void irfft_x_kernel(const __grid_constant__ FftPlan fp, const double2* __restrict__ in,
+                               double* __restrict__ out, int nrows, double scale, int lpc) {
+  extern __shared__ double2 sh[];
+  const int n = fp.n, nh = n / 2 + 1;
+  double2* b0 = sh;
+  double2* b1 = sh + (size_t)lpc * n;
+  const int pair0 = blockIdx.x * lpc;
+  for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
+    const int l = t / n, k = t - l * n;
+    const int ra = 2 * (pair0 + l), rb = ra + 1;
+    const bool hi = k > n / 2;
+    const int kk = hi ? n - k : k;
+    double2 xa = make_double2(0.0, 0.0), xb = make_double2(0.0, 0.0);
+    if (ra < nrows) xa = in[(int64_t)ra * nh + kk];
+    if (rb < nrows) xb = in[(int64_t)rb * nh + kk];
+    if (kk == 0 || 2 * kk == n) { xa.y = 0.0; xb.y = 0.0; }
+    if (hi) { xa.y = -xa.y; xb.y = -xb.y; }
+    b0[t] = make_double2(xa.x - xb.y, xa.y + xb.x);  // xa + i*xb
+  }
+  __syncthreads();
+  double2* r = smem_fft(b0, b1, lpc, fp, +1);
+  for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
+    const int l = t / n, p = t - l * n;
+    const int ra = 2 * (pair0 + l), rb = ra + 1;
+    const double2 z = r[t];
+    if (ra < nrows) out[(int64_t)ra * n + p] = z.x * scale;
+    if (rb < nrows) out[(int64_t)rb * n + p] = z.y * scale;
+  }
+}
+
+__global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __restrict__ data, int na, int nb,
+                                 int64_t bstride, int64_t stride, int sign, int lpc) {
+  extern __shared__ double2 sh[];
+  const int n = fp.n;
+  double2* b0 = sh;
+  double2* b1 = sh + (size_t)lpc * n;
+  const int64_t g0 = (int64_t)blockIdx.x * lpc;
+  const int64_t nlines = (int64_t)na * nb;
+  for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
+    const int p = t / lpc, l = t - p * lpc;
+    const int64_t g = g0 + l;
+    double2 v = make_double2(0.0, 0.0);
+    if (g < nlines) {
+      const int64_t b = g / na, a = g - b * na;
+      v = data[a + b * bstride + p * stride];
+    }
+    b0[l * n + p] = v;
+  }
+  __syncthreads();
+  double2* r = smem_fft(b0, b1, lpc, fp, sign);
+  for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
+    const int p = t / lpc, l = t - p * lpc;
+    const int64_t g = g0 + l;
+    if (g < nlines) {
+      const int64_t b = g / na, a = g - b * na;
+      data[a + b * bstride + p * stride] = r[l * n + p];
+    }
+  }
+}
+
+void launch_rfft_x(const FftPlan& fp, const double* in, double2* out, int nrows, cudaStream_t st) {
+  const int lpc = fft_lines_per_cta(fp.n);
+  const int npairs = (nrows + 1) / 2;
+  const size_t shm = 2 * (size_t)lpc * fp.n * sizeof(double2);
+  cudaFuncSetAttribute(rfft_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  rfft_x_kernel<<<(npairs + lpc - 1) / lpc, 256, shm, st>>>(fp, in, out, nrows, lpc);
+}
+
+void launch_irfft_x(const FftPlan& fp, const double2* in, double* out, int nrows, double scale, cudaStream_t st) {
+  const int lpc = fft_lines_per_cta(fp.n);
+  const int npairs = (nrows + 1) / 2;
+  const size_t shm = 2 * (size_t)lpc * fp.n * sizeof(double2);
+  cudaFuncSetAttribute(irfft_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  irfft_x_kernel<<<(npairs + lpc - 1) / lpc, 256, shm, st>>>(fp, in, out, nrows, scale, lpc);
+}
+
+void launch_cfft_axis(const FftPlan& fp, double2* data, int na, int nb, int64_t bstride, int64_t stride, int sign,
+                      cudaStream_t st) {
+  const int lpc = fft_lines_per_cta(fp.n);
+  const int64_t nlines = (int64_t)na * nb;
+  const size_t shm = 2 * (size_t)lpc * fp.n * sizeof(double2);
+  cudaFuncSetAttribute(cfft_axis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  cfft_axis_kernel<<<(unsigned)((nlines + lpc - 1) / lpc), 256, shm, st>>>(fp, data, na, nb, bstride, stride, sign,
+                                                                            lpc);
+}
+
+// ===========================================================================
+// FISHPACK y solve: TRID0 (src/poisson_fishpack.f90:20-57) per (kx, kz) on complex data
+// laid out (kz, j, kx) with kx fastest.
+// ===========================================================================
+__global__ void ysolve_kernel(double2* __restrict__ data, int nxh, int ny, int nz, const double* __restrict__ pa,
+                              const double* __restrict__ pb, const double* __restrict__ pc,
+                              const double* __restrict__ lamx, const double* __restrict__ lamz) {
+  extern __shared__ double sD[];  // [ny][blockDim]
+  const int t = threadIdx.x;
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + t;
+  if (g >= (int64_t)nxh * nz) return;
+  const int kz = (int)(g / nxh), kx = (int)(g - (int64_t)kz * nxh);
+  const double lx = lamx[kx], lz = lamz[kz];
+  double* D = sD + t;
+  const int bd = blockDim.x;
+  double2* T = data + (int64_t)kz * ny * nxh + kx;
+  const int64_t js = nxh;
+  double bb = (pb[0] + lx) + lz;
+  double Z = 1.0 / bb;
+  D[0] = pc[0] * Z;
+  double2 tp = T[0];
+  tp.x *= Z; tp.y *= Z;
+  T[0] = tp;
+  for (int j = 1; j < ny - 1; ++j) {
+    bb = (pb[j] + lx) + lz;
+    Z = 1.0 / (bb - pa[j] * D[(j - 1) * bd]);
+    D[j * bd] = pc[j] * Z;
+    double2 v = T[j * js];
+    v.x = (v.x - pa[j] * tp.x) * Z;
+    v.y = (v.y - pa[j] * tp.y) * Z;
+    T[j * js] = v;
+    tp = v;
+  }
+  bb = (pb[ny - 1] + lx) + lz;
+  Z = bb - pa[ny - 1] * D[(ny - 2) * bd];
+  double2 v = T[(ny - 1) * js];
+  if (fabs(Z) > 1.0e-10) {
+    v.x = (v.x - pa[ny - 1] * tp.x) / Z;
+    v.y = (v.y - pa[ny - 1] * tp.y) / Z;
+  } else {
+    v.x = 0.0;
+    v.y = 0.0;
+  }
+  T[(ny - 1) * js] = v;
+  for (int j = ny - 2; j >= 0; --j) {
+    double2 u = T[j * js];
+    u.x = u.x - D[j * bd] * v.x;
+    u.y = u.y - D[j * bd] * v.y;
+    T[j * js] = u;
+    v = u;
+  }
+}
+
+void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* pa, const double* pb, const double* pc,
+                   const double* lamx, const double* lamz, cudaStream_t st) {
+  const int bs = 64;
+  const int64_t n = (int64_t)nxh * nz;
+  const size_t shm = (size_t)ny * bs * sizeof(double);
+  cudaFuncSetAttribute(ysolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  ysolve_kernel<<<(unsigned)((n + bs - 1) / bs), bs, shm, st>>>(data, nxh, ny, nz, pa, pb, pc, lamx, lamz);
+}
+
+__global__ void spectral_divide_kernel(double2* __restrict__ data, int nxh, int ny, int nz,
+                                       const double* __restrict__ k2x, const double* __restrict__ k2y,
+                                       const double* __restrict__ k2z, double norm) {
+  const int64_t n = (int64_t)nxh * ny * nz;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+    const int kx = (int)(g % nxh);
+    const int64_t r = g / nxh;
+    const int j = (int)(r % ny);
+    const int k = (int)(r / ny);
+    double2 v = data[g];
+    v.x *= norm;
+    v.y *= norm;
+    const double kk = k2x[kx] + k2y[j] + k2z[k];
+    if (kk < 1.0e-16) { v.x = 0.0; v.y = 0.0; }
+    else { v.x = v.x / (-kk); v.y = v.y / (-kk); }
+    data[g] = v;
+  }
+}
+
+void launch_spectral_divide(double2* data, int nxh, int ny, int nz, const double* k2x, const double* k2y,
+                            const double* k2z, double norm, cudaStream_t st) {
+  spectral_divide_kernel<<<148 * 8, 256, 0, st>>>(data, nxh, ny, nz, k2x, k2y, k2z, norm);
+}
+
+// ===========================================================================
+// elementwise and reductions
+// ===========================================================================
+__global__ void fractional_step_kernel(double* __restrict__ rhs1, double* __restrict__ rhs0,
+                                       const double* __restrict__ pfc, int64_t n, double dt, double gam, double zeta,
+                                       double alpha) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double cur = rhs1[i], last = rhs0[i];
+    double tot = gam * cur + zeta * last;
+    rhs0[i] = cur;
+    tot = tot + alpha * pfc[i];
+    rhs1[i] = dt * tot;
+  }
+}
+void launch_fractional_step(double* rhs1, double* rhs0, const double* pfc, int64_t n, double dt, double gam,
+                            double zeta, double alpha, cudaStream_t st) {
+  fractional_step_kernel<<<148 * 8, 256, 0, st>>>(rhs1, rhs0, pfc, n, dt, gam, zeta, alpha);
+}
+
+__global__ void weighted_partial_kernel(const double* __restrict__ a, const double* __restrict__ wy, int n1, int n2,
+                                        int n3, double* __restrict__ partial) {
+  __shared__ double red[256];
+  const int64_t n = (int64_t)n1 * n2 * n3;
+  double acc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int j = (int)((i / n1) % n2);
+    acc += a[i] * wy[j];
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+__global__ void finalize_mean_kernel(const double* __restrict__ partial, int npart, double* __restrict__ out,
+                                     double vol) {
+  __shared__ double red[256];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < npart; i += blockDim.x) acc += partial[i];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = red[0] / vol;
+}
+void launch_weighted_mean(const double* a, const double* wy, int n1, int n2, int n3, double* partial, int npart,
+                          double* out, double vol, cudaStream_t st) {
+  weighted_partial_kernel<<<npart, 256, 0, st>>>(a, wy, n1, n2, n3, partial);
+  finalize_mean_kernel<<<1, 256, 0, st>>>(partial, npart, out, vol);
+}
+
+__global__ void update_q_kernel(double* __restrict__ q, const double* __restrict__ rhs, const double* __restrict__ sub,
+                                int64_t n) {
+  const double s = sub ? sub[0] : 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    q[i] = q[i] + (rhs[i] - s);
+}
+void launch_update_q(double* q, const double* rhs, const double* sub, int64_t n, cudaStream_t st) {
+  update_q_kernel<<<148 * 8, 256, 0, st>>>(q, rhs, sub, n);
+}
+
+__global__ void set_yrows_kernel(double* __restrict__ a, int n1, int n2, int n3, int s0, double v0, int s1, double v1) {
+  const int64_t n = (int64_t)n1 * n3;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = g / n1, i = g - k * n1;
+    if (s0) a[(k * n2 + 0) * n1 + i] = v0;
+    if (s1) a[(k * n2 + (n2 - 1)) * n1 + i] = v1;
+  }
+}
+void launch_set_yrows(double* a, int n1, int n2, int n3, int s0, double v0, int s1, double v1, cudaStream_t st) {
+  set_yrows_kernel<<<148, 256, 0, st>>>(a, n1, n2, n3, s0, v0, s1, v1);
+}
+
+__global__ void fbcy_const_kernel(double* __restrict__ fbc, int64_t nl, double v0, double v1) {
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < nl; g += (int64_t)gridDim.x * blockDim.x) {
+    fbc[g] = v0;
+    fbc[nl + g] = v1;
+    fbc[2 * nl + g] = v0;
+    fbc[3 * nl + g] = v1;
+  }
+}
+void launch_fbcy_const(double* fbc, int n1, int n3, double v0, double v1, cudaStream_t st) {
+  fbcy_const_kernel<<<148, 256, 0, st>>>(fbc, (int64_t)n1 * n3, v0, v1);
+}
+
+// planes [4][n1*n3] from the wall rows of (n1, n2, n3) arrays: v = s*(A + c1*B)*C, C optional (else c2)
+__global__ void fbcy_extract_kernel(double* __restrict__ fbc, const double* __restrict__ A,
+                                    const double* __restrict__ B, const double* __restrict__ C, double c1, double s,
+                                    double c2, int n1, int n2, int n3) {
+  const int64_t nl = (int64_t)n1 * n3;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < nl; g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = g / n1, i = g - k * n1;
+    for (int side = 0; side < 2; ++side) {
+      const int64_t a = (k * n2 + (side == 0 ? 0 : n2 - 1)) * n1 + i;
+      double v = A[a];
+      if (B) v = v + c1 * B[a];
+      v = v * s;
+      v = C ? v * C[a] : v * c2;
+      fbc[side * nl + g] = v;
+      fbc[(side + 2) * nl + g] = v;
+    }
+  }
+}
+void launch_fbcy_extract(double* fbc, const double* A, const double* B, const double* C, double c1, double s,
+                         double c2, int n1, int n2, int n3, cudaStream_t st) {
+  fbcy_extract_kernel<<<148, 256, 0, st>>>(fbc, A, B, C, c1, s, c2, n1, n2, n3);
+}
+
+__global__ void axpby_kernel(double* __restrict__ out, const double* __restrict__ a, double sa,
+                             const double* __restrict__ b, double sb, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double v = sa * a[i];
+    if (b) v += sb * b[i];
+    out[i] = v;
+  }
+}
+void launch_axpby(double* out, const double* a, double sa, const double* b, double sb, int64_t n, cudaStream_t st) {
+  axpby_kernel<<<148 * 8, 256, 0, st>>>(out, a, sa, b, sb, n);
+}
+
+__global__ void absmax_partial_kernel(const double* __restrict__ a, int64_t n, double* __restrict__ partial) {
+  __shared__ double red[256];
+  __shared__ int bad[256];
+  double m = 0.0;
+  int nanf = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = a[i];
+    if (!isfinite(v)) nanf = 1;
+    else m = fmax(m, fabs(v));
+  }
+  red[threadIdx.x] = m;
+  bad[threadIdx.x] = nanf;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+      bad[threadIdx.x] |= bad[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { partial[2 * blockIdx.x] = red[0]; partial[2 * blockIdx.x + 1] = (double)bad[0]; }
+}
+__global__ void absmax_final_kernel(const double* __restrict__ partial, int npart, double* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double m = 0.0, b = 0.0;
+    for (int i = 0; i < npart; ++i) { m = fmax(m, partial[2 * i]); b = fmax(b, partial[2 * i + 1]); }
+    out[0] = m;
+    out[1] = b;
+  }
+}
+void launch_absmax(const double* a, int64_t n, double* partial, int npart, double* out, cudaStream_t st) {
+  absmax_partial_kernel<<<npart, 256, 0, st>>>(a, n, partial);
+  absmax_final_kernel<<<1, 32, 0, st>>>(partial, npart, out);
+}
+
+__global__ void ke_density_kernel(double* __restrict__ out, const double* __restrict__ u, const double* __restrict__ v,
+                                  const double* __restrict__ w, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = 0.5 * (u[i] * u[i] + v[i] * v[i] + w[i] * w[i]);
+}
+void launch_ke_density(double* out, const double* u, const double* v, const double* w, int64_t n, cudaStream_t st) {
+  ke_density_kernel<<<148 * 8, 256, 0, st>>>(out, u, v, w, n);
+}
+
+}  // namespace chs

@@ -1,0 +1,85 @@
+// Device kernels of the B200 CHAPSim2 hot path (declarations and launch helpers).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "chs_plan.h"
+
+namespace chs {
+
+// Input expression of a line operator, evaluated while a tile is staged:
+//   E_A     f = s * A
+//   E_AB    f = s * (A * B)
+//   E_ApB   f = s * (A + c1 * B)
+//   E_ApBC  f = s * (A + c1 * B) * C
+enum InMode { E_A = 0, E_AB = 1, E_ApB = 2, E_ApBC = 3 };
+
+struct LineIO {
+  const double* A;
+  const double* B;
+  const double* C;
+  int emode;
+  double s, c1;
+  const double* fbc;  // boundary values, layout [4][nlines] (line order of the kernel), or null
+  double* out;
+  int accumulate;     // 0: out = g * r ; 1: out += g * r
+  double g;
+  int n1, n2, n3;     // extents of the INPUT array (x fastest)
+};
+
+// Launch one plan over all lines of direction d.  `table` holds the LHS/mapping arrays.
+void launch_line_op(int d, const OpPlan& plan, const LineIO& io, const double* table, cudaStream_t st);
+
+// number of lines of a direction for an input array of extents n1 x n2 x n3
+inline int64_t num_lines(int d, int n1, int n2, int n3) {
+  return d == 0 ? (int64_t)n2 * n3 : (d == 1 ? (int64_t)n1 * n3 : (int64_t)n1 * n2);
+}
+
+// ---- Poisson building blocks (double2 = complex) ----
+struct FftPlan {
+  int n;            // transform length (2^a 3^b)
+  int nst;          // number of radix stages
+  int radix[16];
+  const double2* tw;  // exp(-2 pi i m / n), m = 0..n-1 (device)
+};
+
+// real x-lines (rows of length nx) -> half spectra (rows of nx/2+1), scaled by `scale`
+void launch_rfft_x(const FftPlan& fp, const double* in, double2* out, int nrows, cudaStream_t st);
+// half spectra -> real x-lines, scaled by `scale`
+void launch_irfft_x(const FftPlan& fp, const double2* in, double* out, int nrows, double scale, cudaStream_t st);
+// complex FFT along a strided axis: element (line, p) at base(line) + p*stride,
+// line = a + na*b with base = a + b*bstride (a fastest); sign -1 forward, +1 backward
+void launch_cfft_axis(const FftPlan& fp, double2* data, int na, int nb, int64_t bstride, int64_t stride, int sign,
+                      cudaStream_t st);
+// y tridiagonal solve per (kx, kz) of the FISHPACK path (TRID0 with the singular-pivot pin)
+void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* pa, const double* pb, const double* pc,
+                   const double* lamx, const double* lamz, cudaStream_t st);
+// 3D spectral division by -(kx'^2 + ky'^2 + kz'^2) (zero mode -> 0), with normalisation
+void launch_spectral_divide(double2* data, int nxh, int ny, int nz, const double* k2x, const double* k2y,
+                            const double* k2z, double norm, cudaStream_t st);
+
+// ---- elementwise and reductions ----
+// rhs1 <- dt*(gamma*rhs1 + zeta*rhs0 + alpha*pfc); rhs0 <- old rhs1
+void launch_fractional_step(double* rhs1, double* rhs0, const double* pfc, int64_t n, double dt, double gam,
+                            double zeta, double alpha, cudaStream_t st);
+// weighted sum over (n1, n2, n3) with weight w[j] -> partial sums; finalize writes out[0] = sum/vol
+void launch_weighted_mean(const double* a, const double* wy, int n1, int n2, int n3, double* partial, int npart,
+                          double* out, double vol, cudaStream_t st);
+// q <- q + rhs - (sub ? *sub : 0)
+void launch_update_q(double* q, const double* rhs, const double* sub, int64_t n, cudaStream_t st);
+// set rows j = 0 and j = n2-1 of an (n1, n2, n3) array to v0 / v1 (flags select sides)
+void launch_set_yrows(double* a, int n1, int n2, int n3, int s0, double v0, int s1, double v1, cudaStream_t st);
+// fbc planes [4][n1*n3] for y-lines: constant wall values
+void launch_fbcy_const(double* fbc, int n1, int n3, double v0, double v1, cudaStream_t st);
+// fbc planes from the first/last y rows of `a` (extract_dirichlet_fbcy): out = s*(A_wall + c1*B_wall)*C
+void launch_fbcy_extract(double* fbc, const double* A, const double* B, const double* C, double c1, double s,
+                         double c2, int n1, int n2, int n3, cudaStream_t st);
+// out = a * s
+void launch_axpby(double* out, const double* a, double sa, const double* b, double sb, int64_t n, cudaStream_t st);
+// max |a| and NaN flag into out[0], out[1] (two-pass with partials)
+void launch_absmax(const double* a, int64_t n, double* partial, int npart, double* out, cudaStream_t st);
+// 0.5*(u^2+v^2+w^2) over ccc
+void launch_ke_density(double* out, const double* u, const double* v, const double* w, int64_t n, cudaStream_t st);
+
+}  // namespace chs

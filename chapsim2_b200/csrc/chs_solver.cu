@@ -1,0 +1,1111 @@
+// Handle, device state and the RK3 substep of the B200 CHAPSim2 hot path,
+// behind the C ABI of include/chapsim_gpu.h.
+//
+// Substep structure (Solve_momentum_eq, src/eq_momentum2.f90:1799-1932):
+//   1. derived velocity quantities (interpolations/derivatives, :347-508),
+//   2. momentum RHS terms accumulated straight into mx/my/mz and px/py/pz
+//      (x :796-966, y :978-1242, z :1262-1457), products evaluated while the
+//      operator tiles are staged,
+//   3. fractional step (:35-71), mass-flux driving (:1547-1562),
+//   4. q += rhs, wall enforcement (src/bc_dirichlet.f90:461-516),
+//   5. Poisson RHS (:1663-1718), Poisson solve, p += phi, projection (:1577-1660).
+// All state stays in HBM; the substep is captured once into a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/chapsim_gpu.h"
+#include "chs_kernels.cuh"
+#include "chs_plan.h"
+
+using namespace chs;
+
+namespace {
+
+enum { V_QX = 0, V_QY = 1, V_QZ = 2, V_PR = 3, V_TM = 4 };
+enum { JSELF = 0, JGRAD = 1, JPROD = 2 };
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define CK(x)                                                                                     \
+  do {                                                                                            \
+    cudaError_t e_ = (x);                                                                         \
+    if (e_ != cudaSuccess) throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+// build_bc_symm_operation (src/bc_general.f90:455-509)
+void symm_op(const int ibc[2], int mbc[2][3], const int* jbc) {
+  for (int i = 0; i < 2; ++i) mbc[i][0] = mbc[i][1] = mbc[i][2] = ibc[i];
+  for (int i = 0; i < 2; ++i) {
+    if (jbc) {
+      const int a = ibc[i], b = jbc[i];
+      if ((a == BC_SYMMETRIC || a == BC_ASYMMETRIC) && (b == BC_SYMMETRIC || b == BC_ASYMMETRIC)) {
+        mbc[i][JPROD] = (a == b) ? BC_SYMMETRIC : BC_ASYMMETRIC;
+      } else if (a != b) {
+        if (a == BC_DIRICHLET) mbc[i][0] = mbc[i][1] = mbc[i][2] = a;
+        if (b == BC_DIRICHLET) mbc[i][0] = mbc[i][1] = mbc[i][2] = b;
+      }
+    } else {
+      if (ibc[i] == BC_SYMMETRIC) { mbc[i][JGRAD] = BC_ASYMMETRIC; }
+      else if (ibc[i] == BC_ASYMMETRIC) { mbc[i][JGRAD] = BC_SYMMETRIC; mbc[i][JPROD] = BC_SYMMETRIC; }
+    }
+  }
+}
+struct Pair { int v[2]; };
+Pair prod_of(const int a[2], const int b[2]) {
+  int m[2][3];
+  symm_op(a, m, b);
+  return Pair{{m[0][JPROD], m[1][JPROD]}};
+}
+Pair tau_of(const int var[2], const int ftp[2]) {
+  int m[2][3];
+  symm_op(var, m, nullptr);
+  int g[2] = {m[0][JGRAD], m[1][JGRAD]};
+  return prod_of(ftp, g);
+}
+
+// complex FFT plan: radix 4s, then 2, then 3s
+FftPlan make_fft(int n, std::vector<double2>& tw_host) {
+  FftPlan fp{};
+  fp.n = n;
+  int m = n;
+  fp.nst = 0;
+  while (m % 4 == 0) { fp.radix[fp.nst++] = 4; m /= 4; }
+  while (m % 2 == 0) { fp.radix[fp.nst++] = 2; m /= 2; }
+  while (m % 3 == 0) { fp.radix[fp.nst++] = 3; m /= 3; }
+  if (m != 1) throw std::runtime_error("FFT length must be of the form 2^a 3^b");
+  tw_host.resize(n);
+  const double pi = 3.141592653589793238462643383279502884;
+  for (int k = 0; k < n; ++k) tw_host[k] = make_double2(std::cos(2.0 * pi * k / n), -std::sin(2.0 * pi * k / n));
+  return fp;
+}
+
+}  // namespace
+
+struct chs_handle {
+  // configuration
+  int nc[3], np[3];
+  bool periodic_y, stretch_y;
+  int iacc, ifft, idriven;
+  double h[3];
+  double dt, rre, sigma2p;
+  double tGamma[4], tZeta[4], tAlpha[4];
+  int ibc[3][5][2];
+  double fbcy[5][2];
+  Pair mbcx_cov1, mbcy_cov1, mbcz_cov1, mbcx_tau1, mbcy_tau1, mbcz_tau1;
+  Pair mbcx_cov2, mbcy_cov2, mbcz_cov2, mbcx_tau2, mbcy_tau2, mbcz_tau2;
+  Pair mbcx_cov3, mbcy_cov3, mbcz_cov3, mbcx_tau3, mbcy_tau3, mbcz_tau3;
+  bool fbcy_velo = false;
+  std::vector<double> mpcc, mppt;
+
+  // device
+  int device = 0;
+  cudaStream_t st = nullptr;
+  PlanBook book;
+  std::map<std::tuple<int, int, int, int, int>, OpPlan> plans;
+  double* table = nullptr;
+  std::vector<void*> allocs;
+  long long launches = 0;
+  std::string err;
+
+  size_t n_pcc, n_cpc, n_ccp, n_ccc, n_ppc, n_pcp, n_cpp;
+  double *qx, *qy, *qz, *pres, *pcor;
+  double *mx0, *my0, *mz0, *mx, *my, *mz, *px, *py, *pz;
+  double *qxix, *qxdx, *qxdy, *qxiy, *qxiz, *qxdz;
+  double *qydx, *qyix, *qydy, *qyiy, *qydz, *qyiz;
+  double *qzdx, *qzix, *qziy, *qzdy, *qziz, *qzdz;
+  double *div, *qxdx_cpc, *qydy_cpc, *qzdz_cpc;
+  double *fb_qx, *fb_qy, *fb_qz, *fb_pr, *fb_mpr, *fb_conv2, *fb_visc2, *fb_maxp;
+  double *wy, *partial, *scal;
+  double vol = 0.0;
+  int npart = 0;
+  // Poisson
+  FftPlan fx{}, fy{}, fz{};
+  double2* spec = nullptr;
+  double *lamx = nullptr, *lamz = nullptr, *pa = nullptr, *pb = nullptr, *pc = nullptr;
+  double *k2x = nullptr, *k2y = nullptr, *k2z = nullptr;
+  // graphs per substep (1..3) and for a whole step
+  cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
+  long long kernels_per_sub[4] = {0, 0, 0, 0};
+  bool capturing = false;
+  // per-kernel profiling (chs_profile_substep)
+  bool profiling = false;
+  struct Rec { int kind, dir; double bytes; cudaEvent_t e0, e1; };
+  std::vector<Rec> recs;
+  cudaEvent_t prof_begin() {
+    cudaEvent_t e = nullptr;
+    if (profiling) { CK(cudaEventCreate(&e)); CK(cudaEventRecord(e, st)); }
+    return e;
+  }
+  void prof_end(cudaEvent_t e0, int kind, int dir, double bytes) {
+    if (!profiling) return;
+    cudaEvent_t e1;
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e1, st));
+    recs.push_back(Rec{kind, dir, bytes, e0, e1});
+  }
+
+  template <class T>
+  T* dalloc(size_t n) {
+    void* p = nullptr;
+    CK(cudaMalloc(&p, n * sizeof(T) + 64));
+    CK(cudaMemsetAsync(p, 0, n * sizeof(T) + 64, st));
+    allocs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  const OpPlan& plan(int d, int fam, Pair bc, bool has_fbc) {
+    auto key = std::make_tuple(d, fam, bc.v[0], bc.v[1], has_fbc ? 1 : 0);
+    auto it = plans.find(key);
+    if (it != plans.end()) return it->second;
+    if (capturing) throw std::runtime_error("operator plan missing from the prepared set");
+    OpPlan p = book.make(d, fam, bc.v, has_fbc);
+    return plans.emplace(key, p).first->second;
+  }
+};
+
+namespace {
+
+Pair P2(const int v[2]) { return Pair{{v[0], v[1]}}; }
+void upload_table(chs_handle* H);
+
+struct Src {
+  const double* A;
+  const double* B = nullptr;
+  const double* C = nullptr;
+  int mode = E_A;
+  double s = 1.0, c1 = 0.0;
+};
+Src src(const double* a, double s = 1.0) { Src x; x.A = a; x.s = s; return x; }
+Src prod(const double* a, const double* b, double s) { Src x; x.A = a; x.B = b; x.mode = E_AB; x.s = s; return x; }
+Src lin(const double* a, const double* b, double c1, double s) {
+  Src x; x.A = a; x.B = b; x.c1 = c1; x.mode = E_ApB; x.s = s; return x;
+}
+
+// run one operator: direction d, family fam, operation bc, boundary planes fbc (null = absent)
+void run_op(chs_handle* H, int d, int fam, Pair bc, const double* fbc, const Src& in, const int n_in[3], double* out,
+            bool accumulate, double g) {
+  const size_t tsz = H->book.table.size();
+  const OpPlan& P = H->plan(d, fam, bc, fbc != nullptr);
+  if (H->book.table.size() != tsz) upload_table(H);
+  LineIO io{};
+  io.A = in.A; io.B = in.B; io.C = in.C; io.emode = in.mode; io.s = in.s; io.c1 = in.c1;
+  io.fbc = fbc;
+  io.out = out;
+  io.accumulate = accumulate ? 1 : 0;
+  io.g = g;
+  io.n1 = n_in[0]; io.n2 = n_in[1]; io.n3 = n_in[2];
+  const double nin_tot = (double)n_in[0] * n_in[1] * n_in[2];
+  const double nout_tot = nin_tot / P.nin * P.nout;
+  const int narr = 1 + (in.B ? 1 : 0) + (in.C ? 1 : 0);
+  const double bytes = 8.0 * (narr * nin_tot + (accumulate ? 2.0 : 1.0) * nout_tot);
+  cudaEvent_t e0 = H->prof_begin();
+  launch_line_op(d, P, io, H->table, H->st);
+  H->prof_end(e0, 0, d, bytes);
+  H->launches++;
+}
+
+// profile wrapper for the other kernel classes
+#define PROF(H, kind, bytes, ...)                       \
+  do {                                                   \
+    cudaEvent_t e0_ = (H)->prof_begin();                 \
+    __VA_ARGS__;                                         \
+    (H)->prof_end(e0_, kind, -1, (bytes));               \
+  } while (0)
+
+void build_bcs(chs_handle* H, const chs_config* c) {
+  std::memcpy(H->ibc, c->nominal_bc, sizeof(H->ibc));
+  std::memcpy(H->fbcy, c->fbcy_const, sizeof(H->fbcy));
+  for (int n = 0; n < 2; ++n) {  // config_calc_basic_ibc (src/bc_general.f90:141-184)
+    if (H->ibc[0][V_QX][n] == BC_SYMMETRIC) H->ibc[0][V_QX][n] = BC_ASYMMETRIC;
+    if (H->ibc[1][V_QY][n] == BC_SYMMETRIC) H->ibc[1][V_QY][n] = BC_ASYMMETRIC;
+    if (H->ibc[2][V_QZ][n] == BC_SYMMETRIC) H->ibc[2][V_QZ][n] = BC_ASYMMETRIC;
+    if (H->ibc[0][V_QX][n] == BC_DIRICHLET) H->ibc[0][V_PR][n] = BC_NEUMANN;
+    if (H->ibc[1][V_QY][n] == BC_DIRICHLET) { H->ibc[1][V_PR][n] = BC_NEUMANN; H->fbcy[V_PR][n] = 0.0; }
+    if (H->ibc[2][V_QZ][n] == BC_DIRICHLET) H->ibc[2][V_PR][n] = BC_NEUMANN;
+  }
+  for (int n = 0; n < 2; ++n)
+    for (int v = 0; v < 5; ++v)
+      if (H->ibc[0][v][n] != BC_PERIODIC || H->ibc[2][v][n] != BC_PERIODIC)
+        throw std::invalid_argument("x and z must be periodic (channel / Taylor-Green configurations)");
+  int ftp[3][2];
+  for (int d = 0; d < 3; ++d)
+    for (int n = 0; n < 2; ++n)
+      ftp[d][n] = H->ibc[d][V_TM][n] == BC_NEUMANN ? BC_DIRICHLET : H->ibc[d][V_TM][n];
+  auto& B = H->ibc;
+  // config_calc_eqs_ibc (src/bc_general.f90:512-677)
+  H->mbcx_cov1 = prod_of(B[0][V_QX], B[0][V_QX]);
+  H->mbcy_cov1 = prod_of(B[1][V_QY], B[1][V_QX]);
+  H->mbcz_cov1 = prod_of(B[2][V_QZ], B[2][V_QX]);
+  H->mbcx_tau1 = tau_of(B[0][V_QX], ftp[0]);
+  H->mbcy_tau1 = tau_of(B[1][V_QX], ftp[1]);
+  H->mbcz_tau1 = tau_of(B[2][V_QX], ftp[2]);
+  H->mbcx_cov2 = prod_of(B[0][V_QX], B[0][V_QY]);
+  H->mbcy_cov2 = prod_of(B[1][V_QY], B[1][V_QY]);
+  H->mbcz_cov2 = prod_of(B[2][V_QZ], B[2][V_QY]);
+  H->mbcx_tau2 = tau_of(B[0][V_QY], ftp[0]);
+  H->mbcy_tau2 = tau_of(B[1][V_QY], ftp[1]);
+  H->mbcz_tau2 = tau_of(B[2][V_QY], ftp[2]);
+  H->mbcx_cov3 = prod_of(B[0][V_QX], B[0][V_QZ]);
+  H->mbcy_cov3 = prod_of(B[1][V_QY], B[1][V_QZ]);
+  H->mbcz_cov3 = prod_of(B[2][V_QZ], B[2][V_QZ]);
+  H->mbcx_tau3 = tau_of(B[0][V_QZ], ftp[0]);
+  H->mbcy_tau3 = tau_of(B[1][V_QZ], ftp[1]);
+  H->mbcz_tau3 = tau_of(B[2][V_QZ], ftp[2]);
+  H->fbcy_velo = false;
+  for (int v = V_QX; v <= V_QZ; ++v)
+    for (int n = 0; n < 2; ++n)
+      if (B[1][v][n] == BC_DIRICHLET || B[1][v][n] == BC_INTERIOR) H->fbcy_velo = true;
+  if (H->periodic_y && H->fbcy_velo) throw std::invalid_argument("inconsistent y boundary conditions");
+}
+
+// operator-plan geometry (host only): ghost spacings and y metric of the 1D wrappers
+// (src/basics_operations2.f90:2739-3950)
+void setup_book(chs_handle* H, const chs_config* c) {
+  const int nc1 = H->nc[1], np1 = H->np[1];
+  std::vector<double> yp(c->yp, c->yp + nc1 + 1), yc(c->yc, c->yc + nc1);
+  std::vector<double> mppt(c->ymap_pt, c->ymap_pt + nc1 + 1), mpcc(c->ymap_cc, c->ymap_cc + nc1);
+  H->mpcc = mpcc;
+  H->mppt = mppt;
+  PlanBook& bk = H->book;
+  bk.iacc = H->iacc;
+  for (int d : {0, 2}) {
+    auto& G = bk.dir[d];
+    G.nc = H->nc[d]; G.np = H->np[d]; G.periodic = true; G.dd = 1.0 / H->h[d];
+    const double hh = H->h[d];
+    G.dp_c[0] = hh; G.dp_c[2] = hh * 2.0; G.dp_c[1] = hh; G.dp_c[3] = hh * 2.0;
+    G.dp_p[0] = hh * 2.0; G.dp_p[2] = hh * 4.0; G.dp_p[1] = hh * 2.0; G.dp_p[3] = hh * 4.0;
+  }
+  auto& G = bk.dir[1];
+  G.nc = nc1; G.np = np1; G.periodic = H->periodic_y; G.dd = 1.0 / H->h[1];
+  G.dp_c[0] = (yc[0] - yp[0]) * 2.0;
+  G.dp_c[2] = (yc[1] - yp[0]) * 2.0;
+  G.dp_c[1] = (yp[np1 - 1] - yc[nc1 - 1]) * 2.0;
+  G.dp_c[3] = (yp[np1 - 1] - yc[nc1 - 2]) * 2.0;
+  G.dp_p[0] = (yp[1] - yp[0]) * 2.0;
+  G.dp_p[2] = (yp[2] - yp[0]) * 2.0;
+  G.dp_p[1] = (yp[np1 - 1] - yp[np1 - 2]) * 2.0;
+  G.dp_p[3] = (yp[np1 - 1] - yp[np1 - 3]) * 2.0;
+  if (H->stretch_y) {
+    G.map_cc = bk.add_array(mpcc);
+    G.map_pt = bk.add_array(std::vector<double>(mppt.begin(), mppt.begin() + np1));
+  }
+}
+
+// scalars, boundary conditions and plan geometry (no device work)
+void setup_host(chs_handle* H, const chs_config* c) {
+  for (int d = 0; d < 3; ++d) {
+    if (c->nc[d] < 8) throw std::invalid_argument("at least 8 cells per direction are required");
+    H->nc[d] = c->nc[d];
+  }
+  H->periodic_y = false;
+  for (int v = 0; v < 5; ++v)
+    for (int n = 0; n < 2; ++n)
+      if (c->nominal_bc[1][v][n] == BC_PERIODIC) H->periodic_y = true;
+  H->np[0] = H->nc[0];
+  H->np[1] = H->periodic_y ? H->nc[1] : H->nc[1] + 1;
+  H->np[2] = H->nc[2];
+  H->stretch_y = c->istret != 0;
+  H->iacc = c->iacc;
+  H->ifft = c->ifft;
+  H->idriven = c->idriven;
+  if (H->iacc < 1 || H->iacc > 4) throw std::invalid_argument("iacc must be 1..4");
+  if (H->ifft != 2 && H->ifft != 3) throw std::invalid_argument("ifft must be 2 or 3");
+  if (H->ifft == 2 && H->periodic_y) throw std::invalid_argument("FISHPACK Poisson needs non-periodic y");
+  if (H->ifft == 3 && !H->periodic_y) throw std::invalid_argument("3D-FFT Poisson needs periodic y");
+  if (c->precision != CHS_FP64) throw std::invalid_argument("only the FP64 path is available in this build");
+  H->h[0] = c->lxx / H->nc[0];
+  H->h[2] = c->lzz / H->nc[2];
+  H->h[1] = H->stretch_y ? 1.0 / H->nc[1] : (c->lyt - c->lyb) / H->nc[1];
+  H->dt = c->dt;
+  H->rre = 1.0 / c->ren;
+  H->sigma2p = 1.0;
+  // RK3 constants (src/input_general.f90:851-886)
+  H->tGamma[0] = 1.0; H->tGamma[1] = 8.0 / 15.0; H->tGamma[2] = 5.0 / 12.0; H->tGamma[3] = 3.0 * 0.25;
+  H->tZeta[0] = 0.0; H->tZeta[1] = 0.0; H->tZeta[2] = -17.0 / 60.0; H->tZeta[3] = -5.0 / 12.0;
+  for (int i = 0; i < 4; ++i) H->tAlpha[i] = H->tGamma[i] + H->tZeta[i];
+  build_bcs(H, c);
+  setup_book(H, c);
+}
+
+// device buffers and Poisson tables
+void setup_device(chs_handle* H, const chs_config* c) {
+  const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2], np1 = H->np[1];
+  const std::vector<double>& mpcc = H->mpcc;
+  const std::vector<double>& mppt = H->mppt;
+  CK(cudaStreamCreateWithFlags(&H->st, cudaStreamNonBlocking));
+  H->n_pcc = (size_t)H->np[0] * nc1 * nc2;
+  H->n_cpc = (size_t)nc0 * np1 * nc2;
+  H->n_ccp = (size_t)nc0 * nc1 * H->np[2];
+  H->n_ccc = (size_t)nc0 * nc1 * nc2;
+  H->n_ppc = (size_t)H->np[0] * np1 * nc2;
+  H->n_pcp = (size_t)H->np[0] * nc1 * H->np[2];
+  H->n_cpp = (size_t)nc0 * np1 * H->np[2];
+  H->qx = H->dalloc<double>(H->n_pcc); H->qy = H->dalloc<double>(H->n_cpc); H->qz = H->dalloc<double>(H->n_ccp);
+  H->pres = H->dalloc<double>(H->n_ccc); H->pcor = H->dalloc<double>(H->n_ccc);
+  H->mx0 = H->dalloc<double>(H->n_pcc); H->my0 = H->dalloc<double>(H->n_cpc); H->mz0 = H->dalloc<double>(H->n_ccp);
+  H->mx = H->dalloc<double>(H->n_pcc); H->my = H->dalloc<double>(H->n_cpc); H->mz = H->dalloc<double>(H->n_ccp);
+  H->px = H->dalloc<double>(H->n_pcc); H->py = H->dalloc<double>(H->n_cpc); H->pz = H->dalloc<double>(H->n_ccp);
+  H->qxix = H->dalloc<double>(H->n_ccc); H->qxdx = H->dalloc<double>(H->n_ccc);
+  H->qxdy = H->dalloc<double>(H->n_ppc); H->qxiy = H->dalloc<double>(H->n_ppc);
+  H->qxiz = H->dalloc<double>(H->n_pcp); H->qxdz = H->dalloc<double>(H->n_pcp);
+  H->qydx = H->dalloc<double>(H->n_ppc); H->qyix = H->dalloc<double>(H->n_ppc);
+  H->qydy = H->dalloc<double>(H->n_ccc); H->qyiy = H->dalloc<double>(H->n_ccc);
+  H->qydz = H->dalloc<double>(H->n_cpp); H->qyiz = H->dalloc<double>(H->n_cpp);
+  H->qzdx = H->dalloc<double>(H->n_pcp); H->qzix = H->dalloc<double>(H->n_pcp);
+  H->qziy = H->dalloc<double>(H->n_cpp); H->qzdy = H->dalloc<double>(H->n_cpp);
+  H->qziz = H->dalloc<double>(H->n_ccc); H->qzdz = H->dalloc<double>(H->n_ccc);
+  H->div = H->dalloc<double>(H->n_ccc);
+  if (H->fbcy_velo) {
+    H->qxdx_cpc = H->dalloc<double>(H->n_cpc);
+    H->qydy_cpc = H->dalloc<double>(H->n_cpc);
+    H->qzdz_cpc = H->dalloc<double>(H->n_cpc);
+  }
+  const size_t nl = (size_t)nc0 * nc2;  // y lines (x and z are periodic: np = nc)
+  H->fb_qx = H->dalloc<double>(4 * nl); H->fb_qy = H->dalloc<double>(4 * nl); H->fb_qz = H->dalloc<double>(4 * nl);
+  H->fb_pr = H->dalloc<double>(4 * nl); H->fb_mpr = H->dalloc<double>(4 * nl);
+  H->fb_conv2 = H->dalloc<double>(4 * nl); H->fb_visc2 = H->dalloc<double>(4 * nl);
+  H->fb_maxp = H->dalloc<double>(4 * nl);
+  launch_fbcy_const(H->fb_qx, nc0, nc2, H->fbcy[V_QX][0], H->fbcy[V_QX][1], H->st);
+  launch_fbcy_const(H->fb_qy, nc0, nc2, H->fbcy[V_QY][0], H->fbcy[V_QY][1], H->st);
+  launch_fbcy_const(H->fb_qz, nc0, nc2, H->fbcy[V_QZ][0], H->fbcy[V_QZ][1], H->st);
+  launch_fbcy_const(H->fb_pr, nc0, nc2, H->fbcy[V_PR][0], H->fbcy[V_PR][1], H->st);
+  launch_fbcy_const(H->fb_mpr, nc0, nc2, -H->fbcy[V_PR][0], -H->fbcy[V_PR][1], H->st);
+  launch_fbcy_const(H->fb_conv2, nc0, nc2, -H->fbcy[V_QY][0] * H->fbcy[V_QY][0],
+                    -H->fbcy[V_QY][1] * H->fbcy[V_QY][1], H->st);
+  launch_fbcy_const(H->fb_maxp, nc0, nc2, kMaxp, kMaxp, H->st);
+  H->launches += 7;
+
+  // volume weights dy(j)*dx*dz (src/tools_general.f90:1229-1253)
+  std::vector<double> wy(nc1);
+  H->vol = 0.0;
+  for (int j = 0; j < nc1; ++j) {
+    double dy = H->h[1];
+    if (H->stretch_y) dy = H->h[1] / mpcc[j];
+    wy[j] = dy * H->h[0] * H->h[2];
+    H->vol += wy[j] * (double)H->np[0] * (double)nc2;
+  }
+  H->wy = H->dalloc<double>(nc1);
+  CK(cudaMemcpyAsync(H->wy, wy.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice, H->st));
+  H->npart = 148 * 4;
+  H->partial = H->dalloc<double>(2 * H->npart);
+  H->scal = H->dalloc<double>(16);
+
+  // Poisson tables
+  std::vector<double2> tw;
+  const int nxh = nc0 / 2 + 1;
+  H->fx = make_fft(nc0, tw);
+  {
+    double2* d = H->dalloc<double2>(tw.size());
+    CK(cudaMemcpyAsync(d, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, H->st));
+    H->fx.tw = d;
+  }
+  H->fz = make_fft(nc2, tw);
+  {
+    double2* d = H->dalloc<double2>(tw.size());
+    CK(cudaMemcpyAsync(d, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, H->st));
+    H->fz.tw = d;
+  }
+  H->spec = H->dalloc<double2>((size_t)nxh * nc1 * nc2);
+  const double pi = 2.0 * std::asin(1.0);
+  if (H->ifft == 2) {
+    if (nc0 % 2 || nc2 % 2) throw std::invalid_argument("FISHPACK path needs even nx and nz");
+    // fishpack_root_1D eigenvalues (src/poisson_fishpack.f90:60-110), one per complex mode
+    auto roots = [&](int N, double c1, std::vector<double>& lam) {
+      const double dxr = pi / (2.0 * (double)N);
+      lam.assign(N, 0.0);
+      for (int k = 0; k < N; ++k) {
+        const int kk = k <= N / 2 ? k : N - k;
+        if (kk == 0) lam[k] = 0.0;
+        else if (2 * kk == N) lam[k] = -4.0 * c1;
+        else {
+          const double s = std::sin(double(2 * kk) * dxr);
+          lam[k] = -4.0 * c1 * s * s;
+        }
+      }
+    };
+    std::vector<double> lx, lz;
+    roots(nc0, 1.0 / (H->h[0] * H->h[0]), lx);
+    roots(nc2, 1.0 / (H->h[2] * H->h[2]), lz);
+    lx.resize(nxh);
+    H->lamx = H->dalloc<double>(nxh);
+    H->lamz = H->dalloc<double>(nc2);
+    CK(cudaMemcpyAsync(H->lamx, lx.data(), nxh * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    CK(cudaMemcpyAsync(H->lamz, lz.data(), nc2 * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    // y coefficients (src/poisson_fishpack.f90:312-323), Cartesian
+    const double h2r = 1.0 / (H->h[1] * H->h[1]);
+    std::vector<double> a(nc1), b(nc1), cc(nc1);
+    for (int j = 0; j < nc1; ++j) {
+      a[j] = h2r * mpcc[j] * mppt[j] * 1.0 * 1.0;
+      cc[j] = h2r * mpcc[j] * mppt[j + 1] * 1.0 * 1.0;
+    }
+    for (int j = 0; j < nc1; ++j) b[j] = -(a[j] + cc[j]);
+    b[0] = b[0] + a[0]; a[0] = 0.0;
+    b[nc1 - 1] = b[nc1 - 1] + cc[nc1 - 1]; cc[nc1 - 1] = 0.0;
+    H->pa = H->dalloc<double>(nc1); H->pb = H->dalloc<double>(nc1); H->pc = H->dalloc<double>(nc1);
+    CK(cudaMemcpyAsync(H->pa, a.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    CK(cudaMemcpyAsync(H->pb, b.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    CK(cudaMemcpyAsync(H->pc, cc.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice, H->st));
+  } else {
+    H->fy = make_fft(nc1, tw);
+    double2* d = H->dalloc<double2>(tw.size());
+    CK(cudaMemcpyAsync(d, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, H->st));
+    H->fy.tw = d;
+    // modified wavenumbers of the periodic C2P derivative (src/poisson_1stderivcomp.f90:2448-2503)
+    const CoefSet& cs = coef(D1C2P, H->iacc);
+    const double alc = cs.lhs[2][0][BC_PERIODIC];
+    auto k2 = [&](int n, double len, double dh) {
+      const double ac = cs.rhs[2][0][BC_PERIODIC] / dh, bc = cs.rhs[2][1][BC_PERIODIC] / dh;
+      std::vector<double> v(n, 0.0);
+      for (int i = 1; i <= n / 2 + 1; ++i) {
+        const double w = 2.0 * pi * double(i - 1) / double(n);
+        double wp = ac * 2.0 * dh * std::sin(w * 0.5) + bc * 2.0 * dh * std::sin(3.0 * 0.5 * w);
+        wp = wp / (1.0 + 2.0 * alc * std::cos(w));
+        const double q = double(n) * wp / len;
+        v[i - 1] = q * q;
+      }
+      for (int i = n / 2 + 2; i <= n; ++i) v[i - 1] = v[n - i + 1];
+      return v;
+    };
+    auto kx = k2(nc0, c->lxx, H->h[0]);
+    auto ky = k2(nc1, c->lyt - c->lyb, H->h[1]);
+    auto kz = k2(nc2, c->lzz, H->h[2]);
+    kx.resize(nxh);
+    H->k2x = H->dalloc<double>(nxh); H->k2y = H->dalloc<double>(nc1); H->k2z = H->dalloc<double>(nc2);
+    CK(cudaMemcpyAsync(H->k2x, kx.data(), nxh * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    CK(cudaMemcpyAsync(H->k2y, ky.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    CK(cudaMemcpyAsync(H->k2z, kz.data(), nc2 * sizeof(double), cudaMemcpyHostToDevice, H->st));
+  }
+}
+
+void drop_graphs(chs_handle* H) {
+  for (auto& g : H->gexec)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+// plans are created lazily; the table must be on the device before any launch.  Captured
+// graphs hold the table pointer, so they are dropped when the table moves.
+void upload_table(chs_handle* H) {
+  drop_graphs(H);
+  if (H->table) { CK(cudaFreeAsync(H->table, H->st)); H->table = nullptr; }
+  const size_t n = H->book.table.size() + 4;
+  CK(cudaMallocAsync(&H->table, n * sizeof(double), H->st));
+  CK(cudaMemcpyAsync(H->table, H->book.table.data(), H->book.table.size() * sizeof(double), cudaMemcpyHostToDevice,
+                     H->st));
+}
+
+void poisson_device(chs_handle* H, double* rhs) {
+  const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
+  const int nxh = nc0 / 2 + 1;
+  cudaStream_t st = H->st;
+  const double nreal = (double)nc0 * nc1 * nc2, nspec = (double)nxh * nc1 * nc2;
+  const double b_r2c = 8.0 * nreal + 16.0 * nspec, b_c2c = 32.0 * nspec;
+  PROF(H, 1, b_r2c, launch_rfft_x(H->fx, rhs, H->spec, nc1 * nc2, st));
+  if (H->ifft == 2) {
+    // fishpack_fft_simple (src/poisson_fishpack.f90:354-490)
+    PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, H->spec, nxh, nc1, nxh, (int64_t)nxh * nc1, -1, st));
+    PROF(H, 2, b_c2c, launch_ysolve(H->spec, nxh, nc1, nc2, H->pa, H->pb, H->pc, H->lamx, H->lamz, st));
+    PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, H->spec, nxh, nc1, nxh, (int64_t)nxh * nc1, +1, st));
+    PROF(H, 1, b_r2c, launch_irfft_x(H->fx, H->spec, rhs, nc1 * nc2, 1.0 / ((double)nc0 * (double)nc2), st));
+    H->launches += 5;
+  } else {
+    // poisson_000 (src/poisson_1stderivcomp.f90:1016-1195)
+    PROF(H, 1, b_c2c, launch_cfft_axis(H->fy, H->spec, nxh, nc2, (int64_t)nxh * nc1, nxh, -1, st));
+    PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, H->spec, nxh, nc1, nxh, (int64_t)nxh * nc1, -1, st));
+    PROF(H, 3, b_c2c, launch_spectral_divide(H->spec, nxh, nc1, nc2, H->k2x, H->k2y, H->k2z,
+                                             1.0 / ((double)nc0 * (double)nc1 * (double)nc2), st));
+    PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, H->spec, nxh, nc1, nxh, (int64_t)nxh * nc1, +1, st));
+    PROF(H, 1, b_c2c, launch_cfft_axis(H->fy, H->spec, nxh, nc2, (int64_t)nxh * nc1, nxh, +1, st));
+    PROF(H, 1, b_r2c, launch_irfft_x(H->fx, H->spec, rhs, nc1 * nc2, 1.0, st));
+    H->launches += 7;
+  }
+}
+
+// the substep body (enqueued on H->st; capturable)
+void substep_body(chs_handle* H, int isub) {
+  cudaStream_t st = H->st;
+  const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
+  const int np0 = H->np[0], np1 = H->np[1], np2 = H->np[2];
+  const int s_pcc[3] = {np0, nc1, nc2}, s_cpc[3] = {nc0, np1, nc2}, s_ccp[3] = {nc0, nc1, np2};
+  const int s_ccc[3] = {nc0, nc1, nc2}, s_ppc[3] = {np0, np1, nc2}, s_pcp[3] = {np0, nc1, np2};
+  const int s_cpp[3] = {nc0, np1, np2};
+  const auto& B = H->ibc;
+  const Pair bx_qx = P2(B[0][V_QX]), by_qx = P2(B[1][V_QX]), bz_qx = P2(B[2][V_QX]);
+  const Pair bx_qy = P2(B[0][V_QY]), by_qy = P2(B[1][V_QY]), bz_qy = P2(B[2][V_QY]);
+  const Pair bx_qz = P2(B[0][V_QZ]), by_qz = P2(B[1][V_QZ]), bz_qz = P2(B[2][V_QZ]);
+  const Pair bx_pr = P2(B[0][V_PR]), by_pr = P2(B[1][V_PR]), bz_pr = P2(B[2][V_PR]);
+  const double* any = H->fb_maxp;  // periodic x/z never read their boundary planes
+  const double* fyqx = H->periodic_y ? nullptr : H->fb_qx;
+  const double* fyqy = H->periodic_y ? nullptr : H->fb_qy;
+  const double* fyqz = H->periodic_y ? nullptr : H->fb_qz;
+  const double* fypr = H->periodic_y ? nullptr : H->fb_pr;
+  const double* fympr = H->periodic_y ? nullptr : H->fb_mpr;
+  const double rre = H->rre, third = 1.0 / 3.0;
+
+  // ---- 1. derived quantities (src/eq_momentum2.f90:347-508)
+  run_op(H, 0, M1P2C, bx_qx, any, src(H->qx), s_pcc, H->qxix, false, 1.0);
+  run_op(H, 0, D1P2C, bx_qx, any, src(H->qx), s_pcc, H->qxdx, false, 1.0);
+  run_op(H, 1, D1C2P, by_qx, fyqx, src(H->qx), s_pcc, H->qxdy, false, 1.0);
+  run_op(H, 1, M1C2P, by_qx, fyqx, src(H->qx), s_pcc, H->qxiy, false, 1.0);
+  run_op(H, 2, M1C2P, bz_qx, any, src(H->qx), s_pcc, H->qxiz, false, 1.0);
+  run_op(H, 2, D1C2P, bz_qx, any, src(H->qx), s_pcc, H->qxdz, false, 1.0);
+  run_op(H, 0, D1C2P, bx_qy, any, src(H->qy), s_cpc, H->qydx, false, 1.0);
+  run_op(H, 0, M1C2P, bx_qy, any, src(H->qy), s_cpc, H->qyix, false, 1.0);
+  run_op(H, 1, D1P2C, by_qy, nullptr, src(H->qy), s_cpc, H->qydy, false, 1.0);
+  run_op(H, 1, M1P2C, by_qy, fyqy, src(H->qy), s_cpc, H->qyiy, false, 1.0);
+  run_op(H, 2, D1C2P, bz_qy, any, src(H->qy), s_cpc, H->qydz, false, 1.0);
+  run_op(H, 2, M1C2P, bz_qy, any, src(H->qy), s_cpc, H->qyiz, false, 1.0);
+  run_op(H, 0, D1C2P, bx_qz, any, src(H->qz), s_ccp, H->qzdx, false, 1.0);
+  run_op(H, 0, M1C2P, bx_qz, any, src(H->qz), s_ccp, H->qzix, false, 1.0);
+  run_op(H, 1, M1C2P, by_qz, fyqz, src(H->qz), s_ccp, H->qziy, false, 1.0);
+  run_op(H, 1, D1C2P, by_qz, fyqz, src(H->qz), s_ccp, H->qzdy, false, 1.0);
+  run_op(H, 2, M1P2C, bz_qz, any, src(H->qz), s_ccp, H->qziz, false, 1.0);
+  run_op(H, 2, D1P2C, bz_qz, nullptr, src(H->qz), s_ccp, H->qzdz, false, 1.0);
+  // div = qxdx + qydy + qzdz (:512-534)
+  PROF(H, 3, 24.0 * H->n_ccc, launch_axpby(H->div, H->qxdx, 1.0, H->qydy, 1.0, (int64_t)H->n_ccc, st));
+  PROF(H, 3, 24.0 * H->n_ccc, launch_axpby(H->div, H->div, 1.0, H->qzdz, 1.0, (int64_t)H->n_ccc, st));
+  H->launches += 2;
+  if (H->fbcy_velo) {
+    // wall divergence for the y-viscous boundary value (:374-442, :537-546)
+    run_op(H, 0, D1P2C, bx_qx, nullptr, src(H->qxiy), s_ppc, H->qxdx_cpc, false, 1.0);
+    run_op(H, 1, D1C2P, by_qy, fyqy, src(H->qyiy), s_ccc, H->qydy_cpc, false, 1.0);
+    run_op(H, 2, D1P2C, bz_qz, nullptr, src(H->qziy), s_cpp, H->qzdz_cpc, false, 1.0);
+    // fbcy_div = walls of (qxdx + qydy + qzdz)_cpc; visc2 bc = (qydy_cpc - div/3) * 2 (:1156-1171)
+    PROF(H, 3, 24.0 * H->n_cpc,
+         launch_axpby(H->qxdx_cpc, H->qxdx_cpc, 1.0, H->qydy_cpc, 1.0, (int64_t)H->n_cpc, st));
+    PROF(H, 3, 24.0 * H->n_cpc,
+         launch_axpby(H->qxdx_cpc, H->qxdx_cpc, 1.0, H->qzdz_cpc, 1.0, (int64_t)H->n_cpc, st));
+    PROF(H, 3, 48.0 * nc0 * nc2,
+         launch_fbcy_extract(H->fb_visc2, H->qydy_cpc, H->qxdx_cpc, nullptr, -third, 1.0, 2.0, nc0, np1, nc2, st));
+    H->launches += 3;
+  }
+
+  // ---- 2. x-momentum (:796-966)
+  run_op(H, 0, D1C2P, H->mbcx_cov1, any, prod(H->qxix, H->qxix, -1.0), s_ccc, H->mx, false, 1.0);
+  run_op(H, 1, D1P2C, H->mbcy_cov1, nullptr, prod(H->qyix, H->qxiy, -1.0), s_ppc, H->mx, true, 1.0);
+  run_op(H, 2, D1P2C, H->mbcz_cov1, nullptr, prod(H->qzix, H->qxiz, -1.0), s_pcp, H->mx, true, 1.0);
+  run_op(H, 0, D1C2P, bx_pr, any, src(H->pres, -1.0), s_ccc, H->px, false, 1.0);
+  run_op(H, 0, D1C2P, H->mbcx_tau1, any, lin(H->qxdx, H->div, -third, 2.0), s_ccc, H->mx, true, rre);
+  run_op(H, 1, D1P2C, H->mbcy_tau1, nullptr, lin(H->qxdy, H->qydx, 1.0, 1.0), s_ppc, H->mx, true, rre);
+  run_op(H, 2, D1P2C, H->mbcz_tau1, nullptr, lin(H->qxdz, H->qzdx, 1.0, 1.0), s_pcp, H->mx, true, rre);
+  // y-momentum (:978-1242)
+  run_op(H, 0, D1P2C, H->mbcx_cov2, nullptr, prod(H->qxiy, H->qyix, -1.0), s_ppc, H->my, false, 1.0);
+  run_op(H, 1, D1C2P, H->mbcy_cov2, H->fbcy_velo ? H->fb_conv2 : H->fb_maxp, prod(H->qyiy, H->qyiy, -1.0), s_ccc,
+         H->my, true, 1.0);
+  run_op(H, 2, D1P2C, H->mbcz_cov2, nullptr, prod(H->qyiz, H->qziy, -1.0), s_cpp, H->my, true, 1.0);
+  run_op(H, 1, D1C2P, by_pr, fympr, src(H->pres, -1.0), s_ccc, H->py, false, 1.0);
+  run_op(H, 0, D1P2C, H->mbcx_tau2, nullptr, lin(H->qxdy, H->qydx, 1.0, 1.0), s_ppc, H->my, true, rre);
+  run_op(H, 1, D1C2P, H->mbcy_tau2, H->fbcy_velo ? H->fb_visc2 : H->fb_maxp, lin(H->qydy, H->div, -third, 2.0), s_ccc,
+         H->my, true, rre);
+  run_op(H, 2, D1P2C, H->mbcz_tau2, nullptr, lin(H->qzdy, H->qydz, 1.0, 1.0), s_cpp, H->my, true, rre);
+  // z-momentum (:1262-1457)
+  run_op(H, 0, D1P2C, H->mbcx_cov3, nullptr, prod(H->qxiz, H->qzix, -1.0), s_pcp, H->mz, false, 1.0);
+  run_op(H, 1, D1P2C, H->mbcy_cov3, nullptr, prod(H->qyiz, H->qziy, -1.0), s_cpp, H->mz, true, 1.0);
+  run_op(H, 2, D1C2P, H->mbcz_cov3, any, prod(H->qziz, H->qziz, -1.0), s_ccc, H->mz, true, 1.0);
+  run_op(H, 2, D1C2P, bz_pr, any, src(H->pres, -1.0), s_ccc, H->pz, false, 1.0);
+  run_op(H, 0, D1P2C, H->mbcx_tau3, nullptr, lin(H->qxdz, H->qzdx, 1.0, 1.0), s_pcp, H->mz, true, rre);
+  run_op(H, 1, D1P2C, H->mbcy_tau3, nullptr, lin(H->qzdy, H->qydz, 1.0, 1.0), s_cpp, H->mz, true, rre);
+  run_op(H, 2, D1C2P, H->mbcz_tau3, any, lin(H->qzdz, H->div, -third, 2.0), s_ccc, H->mz, true, rre);
+
+  // ---- 3. fractional step, mass flux
+  PROF(H, 3, 40.0 * H->n_pcc,
+       launch_fractional_step(H->mx, H->mx0, H->px, (int64_t)H->n_pcc, H->dt, H->tGamma[isub], H->tZeta[isub],
+                              H->tAlpha[isub], st));
+  PROF(H, 3, 40.0 * H->n_cpc,
+       launch_fractional_step(H->my, H->my0, H->py, (int64_t)H->n_cpc, H->dt, H->tGamma[isub], H->tZeta[isub],
+                              H->tAlpha[isub], st));
+  PROF(H, 3, 40.0 * H->n_ccp,
+       launch_fractional_step(H->mz, H->mz0, H->pz, (int64_t)H->n_ccp, H->dt, H->tGamma[isub], H->tZeta[isub],
+                              H->tAlpha[isub], st));
+  H->launches += 3;
+  const double* bulk = nullptr;
+  if (H->idriven == 1) {
+    PROF(H, 3, 8.0 * H->n_pcc,
+         launch_weighted_mean(H->mx, H->wy, np0, nc1, nc2, H->partial, H->npart, H->scal + 0, H->vol, st));
+    bulk = H->scal + 0;
+    H->launches += 2;
+  }
+  // ---- 4. q += rhs, walls
+  PROF(H, 3, 24.0 * H->n_pcc, launch_update_q(H->qx, H->mx, bulk, (int64_t)H->n_pcc, st));
+  PROF(H, 3, 24.0 * H->n_cpc, launch_update_q(H->qy, H->my, nullptr, (int64_t)H->n_cpc, st));
+  PROF(H, 3, 24.0 * H->n_ccp, launch_update_q(H->qz, H->mz, nullptr, (int64_t)H->n_ccp, st));
+  H->launches += 3;
+  const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
+  if (w0 || w1) {
+    PROF(H, 3, 16.0 * nc0 * nc2,
+         launch_set_yrows(H->qy, nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+    H->launches++;
+  }
+  // ---- 5. Poisson RHS, solve, pressure and projection
+  const double coeff = 1.0 / (H->tAlpha[isub] * H->sigma2p * H->dt);
+  run_op(H, 0, D1P2C, bx_qx, any, src(H->qx), s_pcc, H->pcor, false, coeff);
+  run_op(H, 1, D1P2C, by_qy, nullptr, src(H->qy), s_cpc, H->pcor, true, coeff);
+  run_op(H, 2, D1P2C, bz_qz, nullptr, src(H->qz), s_ccp, H->pcor, true, coeff);
+  poisson_device(H, H->pcor);
+  PROF(H, 3, 24.0 * H->n_ccc, launch_axpby(H->pres, H->pres, 1.0, H->pcor, 1.0, (int64_t)H->n_ccc, st));
+  H->launches++;
+  const double f = H->dt * H->tAlpha[isub] * H->sigma2p;
+  run_op(H, 0, D1C2P, bx_pr, any, src(H->pcor), s_ccc, H->qx, true, -f);
+  run_op(H, 1, D1C2P, by_pr, fypr, src(H->pcor), s_ccc, H->qy, true, -f);
+  run_op(H, 2, D1C2P, bz_pr, any, src(H->pcor), s_ccc, H->qz, true, -f);
+  if (w0 || w1) {
+    PROF(H, 3, 16.0 * nc0 * nc2,
+         launch_set_yrows(H->qy, nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+    H->launches++;
+  }
+}
+
+// Prepare every plan the substep uses (plans are host objects; the table must be final
+// before the graph is captured).
+void prepare_plans(chs_handle* H) {
+  // dry run on a null stream is not possible; instead enumerate through a throw-away pass that
+  // only builds plans: run_op builds the plan before launching, so a capture-free first substep
+  // would launch kernels.  Plans are built here explicitly in the same order.
+  struct Rec { int d, fam; Pair bc; bool f; };
+  const auto& B = H->ibc;
+  const bool y = !H->periodic_y;
+  std::vector<Rec> r = {
+      {0, M1P2C, P2(B[0][V_QX]), true}, {0, D1P2C, P2(B[0][V_QX]), true}, {1, D1C2P, P2(B[1][V_QX]), y},
+      {1, M1C2P, P2(B[1][V_QX]), y}, {2, M1C2P, P2(B[2][V_QX]), true}, {2, D1C2P, P2(B[2][V_QX]), true},
+      {0, D1C2P, P2(B[0][V_QY]), true}, {0, M1C2P, P2(B[0][V_QY]), true}, {1, D1P2C, P2(B[1][V_QY]), false},
+      {1, M1P2C, P2(B[1][V_QY]), y}, {2, D1C2P, P2(B[2][V_QY]), true}, {2, M1C2P, P2(B[2][V_QY]), true},
+      {0, D1C2P, P2(B[0][V_QZ]), true}, {0, M1C2P, P2(B[0][V_QZ]), true}, {1, M1C2P, P2(B[1][V_QZ]), y},
+      {1, D1C2P, P2(B[1][V_QZ]), y}, {2, M1P2C, P2(B[2][V_QZ]), true}, {2, D1P2C, P2(B[2][V_QZ]), false},
+      {0, D1C2P, H->mbcx_cov1, true}, {1, D1P2C, H->mbcy_cov1, false}, {2, D1P2C, H->mbcz_cov1, false},
+      {0, D1C2P, P2(B[0][V_PR]), true}, {0, D1C2P, H->mbcx_tau1, true}, {1, D1P2C, H->mbcy_tau1, false},
+      {2, D1P2C, H->mbcz_tau1, false}, {0, D1P2C, H->mbcx_cov2, false}, {1, D1C2P, H->mbcy_cov2, true},
+      {2, D1P2C, H->mbcz_cov2, false}, {1, D1C2P, P2(B[1][V_PR]), y}, {0, D1P2C, H->mbcx_tau2, false},
+      {1, D1C2P, H->mbcy_tau2, true}, {2, D1P2C, H->mbcz_tau2, false}, {0, D1P2C, H->mbcx_cov3, false},
+      {1, D1P2C, H->mbcy_cov3, false}, {2, D1C2P, H->mbcz_cov3, true}, {2, D1C2P, P2(B[2][V_PR]), true},
+      {0, D1P2C, H->mbcx_tau3, false}, {1, D1P2C, H->mbcy_tau3, false}, {2, D1C2P, H->mbcz_tau3, true},
+      {0, D1P2C, P2(B[0][V_QX]), true}, {1, D1P2C, P2(B[1][V_QY]), false}, {2, D1P2C, P2(B[2][V_QZ]), false},
+      {0, D1C2P, P2(B[0][V_PR]), true}, {1, D1C2P, P2(B[1][V_PR]), y}, {2, D1C2P, P2(B[2][V_PR]), true},
+      {0, M1P2C, P2(B[0][V_QX]), true}, {1, M1P2C, P2(B[1][V_QY]), y}, {2, M1P2C, P2(B[2][V_QZ]), true},
+  };
+  if (H->fbcy_velo) {
+    r.push_back({0, D1P2C, P2(B[0][V_QX]), false});
+    r.push_back({1, D1C2P, P2(B[1][V_QY]), true});
+    r.push_back({2, D1P2C, P2(B[2][V_QZ]), false});
+  }
+  for (const auto& x : r) H->plan(x.d, x.fam, x.bc, x.f);
+  upload_table(H);
+}
+
+void set_err(chs_handle* H, const char* fmt, ...) {
+  if (!H) return;
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  H->err = buf;
+}
+
+int guard(chs_handle* H, const std::function<void()>& f) {
+  try {
+    f();
+    return CHS_OK;
+  } catch (const CudaError& e) {
+    set_err(H, "%s", e.what());
+    return CHS_ERR_CUDA;
+  } catch (const std::invalid_argument& e) {
+    set_err(H, "%s", e.what());
+    return CHS_ERR_ARG;
+  } catch (const std::exception& e) {
+    set_err(H, "%s", e.what());
+    return CHS_ERR_ARG;
+  }
+}
+
+double* field_ptr(chs_handle* H, int field, size_t* n) {
+  switch (field) {
+    case CHS_QX: *n = H->n_pcc; return H->qx;
+    case CHS_QY: *n = H->n_cpc; return H->qy;
+    case CHS_QZ: *n = H->n_ccp; return H->qz;
+    case CHS_PRES: *n = H->n_ccc; return H->pres;
+    case CHS_PCOR: *n = H->n_ccc; return H->pcor;
+    case CHS_MX_RHS0: *n = H->n_pcc; return H->mx0;
+    case CHS_MY_RHS0: *n = H->n_cpc; return H->my0;
+    case CHS_MZ_RHS0: *n = H->n_ccp; return H->mz0;
+    default: throw std::invalid_argument("unknown field id");
+  }
+}
+
+void capture_graphs(chs_handle* H) {
+  for (int isub = 1; isub <= 3; ++isub) {
+    cudaGraph_t g;
+    const long long before = H->launches;
+    CK(cudaStreamBeginCapture(H->st, cudaStreamCaptureModeThreadLocal));
+    H->capturing = true;
+    try {
+      substep_body(H, isub);
+    } catch (...) {
+      H->capturing = false;
+      cudaStreamEndCapture(H->st, &g);
+      throw;
+    }
+    H->capturing = false;
+    CK(cudaStreamEndCapture(H->st, &g));
+    H->kernels_per_sub[isub] = H->launches - before;
+    H->launches = before;
+    CK(cudaGraphInstantiate(&H->gexec[isub], g, 0));
+    CK(cudaGraphDestroy(g));
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int chs_create(const chs_config* cfg, int device, chs_handle** out) {
+  if (!cfg || !out) return CHS_ERR_ARG;
+  chs_handle* H = new chs_handle();
+  int rc = guard(H, [&] {
+    setup_host(H, cfg);  // validates the configuration before any device work
+    if (device >= 0) CK(cudaSetDevice(device));
+    CK(cudaGetDevice(&H->device));
+    setup_device(H, cfg);
+    prepare_plans(H);
+    CK(cudaStreamSynchronize(H->st));
+  });
+  if (rc != CHS_OK) {
+    std::fprintf(stderr, "chs_create: %s\n", H->err.c_str());
+    chs_destroy(H);
+    *out = nullptr;
+    return rc;
+  }
+  *out = H;
+  return CHS_OK;
+}
+
+int chs_destroy(chs_handle* H) {
+  if (!H) return CHS_OK;
+  if (H->st) cudaStreamSynchronize(H->st);
+  drop_graphs(H);
+  if (H->table) cudaFree(H->table);
+  for (void* p : H->allocs) cudaFree(p);
+  if (H->st) cudaStreamDestroy(H->st);
+  delete H;
+  return CHS_OK;
+}
+
+int chs_upload_field(chs_handle* H, int field, const double* host, size_t n) {
+  if (!H || !host) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    size_t m;
+    double* d = field_ptr(H, field, &m);
+    if (n != m) throw std::invalid_argument("field size mismatch");
+    CK(cudaMemcpyAsync(d, host, n * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    CK(cudaStreamSynchronize(H->st));
+  });
+}
+
+int chs_download_field(chs_handle* H, int field, double* host, size_t n) {
+  if (!H || !host) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    size_t m;
+    double* d = field_ptr(H, field, &m);
+    if (n != m) throw std::invalid_argument("field size mismatch");
+    CK(cudaMemcpyAsync(host, d, n * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+  });
+}
+
+int chs_momentum_substep(chs_handle* H, int isub) {
+  if (!H) return CHS_ERR_ARG;
+  if (isub < 0 || isub > 3) { set_err(H, "isub must be 0..3"); return CHS_ERR_ARG; }
+  return guard(H, [&] {
+    if (isub >= 1 && H->gexec[isub]) {
+      CK(cudaGraphLaunch(H->gexec[isub], H->st));
+      H->launches += H->kernels_per_sub[isub];
+    } else {
+      substep_body(H, isub);
+    }
+    CK(cudaGetLastError());
+  });
+}
+
+int chs_step(chs_handle* H, int nsteps) {
+  if (!H) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    if (!H->gexec[1]) capture_graphs(H);
+    for (int s = 0; s < nsteps; ++s)
+      for (int isub = 1; isub <= 3; ++isub) {
+        CK(cudaGraphLaunch(H->gexec[isub], H->st));
+        H->launches += H->kernels_per_sub[isub];
+      }
+    CK(cudaGetLastError());
+  });
+}
+
+int chs_momentum_substep_host(chs_handle* H, int isub, double* qx, double* qy, double* qz, double* pres) {
+  if (!H || !qx || !qy || !qz || !pres) return CHS_ERR_ARG;
+  if (isub < 0 || isub > 3) { set_err(H, "isub must be 0..3"); return CHS_ERR_ARG; }
+  return guard(H, [&] {
+    CK(cudaMemcpyAsync(H->qx, qx, H->n_pcc * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    CK(cudaMemcpyAsync(H->qy, qy, H->n_cpc * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    CK(cudaMemcpyAsync(H->qz, qz, H->n_ccp * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    CK(cudaMemcpyAsync(H->pres, pres, H->n_ccc * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    if (isub >= 1) {
+      if (!H->gexec[1]) capture_graphs(H);
+      CK(cudaGraphLaunch(H->gexec[isub], H->st));
+      H->launches += H->kernels_per_sub[isub];
+    } else {
+      substep_body(H, isub);
+    }
+    CK(cudaMemcpyAsync(qx, H->qx, H->n_pcc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaMemcpyAsync(qy, H->qy, H->n_cpc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaMemcpyAsync(qz, H->qz, H->n_ccp * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaMemcpyAsync(pres, H->pres, H->n_ccc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+  });
+}
+
+int chs_time_steps(chs_handle* H, int nsteps, float* ms) {
+  if (!H || !ms || nsteps < 0) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    if (!H->gexec[1]) capture_graphs(H);
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, H->st));
+    for (int s = 0; s < nsteps; ++s)
+      for (int isub = 1; isub <= 3; ++isub) {
+        CK(cudaGraphLaunch(H->gexec[isub], H->st));
+        H->launches += H->kernels_per_sub[isub];
+      }
+    CK(cudaEventRecord(b, H->st));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  });
+}
+
+int chs_time_steps_host(chs_handle* H, int nsteps, double* qx, double* qy, double* qz, double* pres, float* ms) {
+  if (!H || !ms || !qx || !qy || !qz || !pres || nsteps < 0) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    if (!H->gexec[1]) capture_graphs(H);
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, H->st));
+    for (int s = 0; s < nsteps; ++s)
+      for (int isub = 1; isub <= 3; ++isub) {
+        CK(cudaMemcpyAsync(H->qx, qx, H->n_pcc * sizeof(double), cudaMemcpyHostToDevice, H->st));
+        CK(cudaMemcpyAsync(H->qy, qy, H->n_cpc * sizeof(double), cudaMemcpyHostToDevice, H->st));
+        CK(cudaMemcpyAsync(H->qz, qz, H->n_ccp * sizeof(double), cudaMemcpyHostToDevice, H->st));
+        CK(cudaMemcpyAsync(H->pres, pres, H->n_ccc * sizeof(double), cudaMemcpyHostToDevice, H->st));
+        CK(cudaGraphLaunch(H->gexec[isub], H->st));
+        H->launches += H->kernels_per_sub[isub];
+        CK(cudaMemcpyAsync(qx, H->qx, H->n_pcc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+        CK(cudaMemcpyAsync(qy, H->qy, H->n_cpc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+        CK(cudaMemcpyAsync(qz, H->qz, H->n_ccp * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+        CK(cudaMemcpyAsync(pres, H->pres, H->n_ccc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+      }
+    CK(cudaEventRecord(b, H->st));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  });
+}
+
+void* chs_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+  return p;
+}
+
+void chs_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+int chs_profile_substep(chs_handle* H, int isub, chs_kprof* out, int max, int* n) {
+  if (!H || !out || !n || isub < 0 || isub > 3) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    H->recs.clear();
+    H->profiling = true;
+    try {
+      substep_body(H, isub);
+    } catch (...) {
+      H->profiling = false;
+      throw;
+    }
+    H->profiling = false;
+    CK(cudaStreamSynchronize(H->st));
+    int k = 0;
+    for (auto& r : H->recs) {
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, r.e0, r.e1));
+      if (k < max) out[k] = chs_kprof{r.kind, r.dir, r.bytes, ms};
+      ++k;
+      cudaEventDestroy(r.e0);
+      cudaEventDestroy(r.e1);
+    }
+    H->recs.clear();
+    *n = k;
+  });
+}
+
+int chs_poisson_solve(chs_handle* H, double* rhs) {
+  if (!H || !rhs) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    CK(cudaMemcpyAsync(H->pcor, rhs, H->n_ccc * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    poisson_device(H, H->pcor);
+    CK(cudaMemcpyAsync(rhs, H->pcor, H->n_ccc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+  });
+}
+
+int chs_poisson_solve_device(chs_handle* H, double* d_rhs) {
+  if (!H || !d_rhs) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    poisson_device(H, d_rhs);
+    CK(cudaGetLastError());
+  });
+}
+
+int chs_diagnostics(chs_handle* H, chs_diag* out) {
+  if (!H || !out) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
+    const int s_pcc[3] = {H->np[0], nc1, nc2}, s_cpc[3] = {nc0, H->np[1], nc2}, s_ccp[3] = {nc0, nc1, H->np[2]};
+    const Pair bx = P2(H->ibc[0][V_QX]), by = P2(H->ibc[1][V_QY]), bz = P2(H->ibc[2][V_QZ]);
+    // divergence (Get_divergence_flow, src/eq_continuity.f90:91-161) into `div`
+    run_op(H, 0, D1P2C, bx, H->fb_maxp, src(H->qx), s_pcc, H->div, false, 1.0);
+    run_op(H, 1, D1P2C, by, nullptr, src(H->qy), s_cpc, H->div, true, 1.0);
+    run_op(H, 2, D1P2C, bz, nullptr, src(H->qz), s_ccp, H->div, true, 1.0);
+    launch_absmax(H->div, (int64_t)H->n_ccc, H->partial, H->npart, H->scal + 2, H->st);
+    // kinetic energy of the P2C-interpolated velocities (src/io_monitor.f90:209-241)
+    run_op(H, 0, M1P2C, bx, H->fb_maxp, src(H->qx), s_pcc, H->qxix, false, 1.0);
+    run_op(H, 1, M1P2C, by, H->periodic_y ? nullptr : H->fb_qy, src(H->qy), s_cpc, H->qyiy, false, 1.0);
+    run_op(H, 2, M1P2C, bz, H->fb_maxp, src(H->qz), s_ccp, H->qziz, false, 1.0);
+    launch_ke_density(H->qxdx, H->qxix, H->qyiy, H->qziz, (int64_t)H->n_ccc, H->st);
+    launch_weighted_mean(H->qxdx, H->wy, nc0, nc1, nc2, H->partial, H->npart, H->scal + 4, H->vol, H->st);
+    launch_weighted_mean(H->qx, H->wy, H->np[0], nc1, nc2, H->partial, H->npart, H->scal + 5, H->vol, H->st);
+    H->launches += 7;
+    double s[8];
+    CK(cudaMemcpyAsync(s, H->scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+    out->max_div = s[2];
+    out->nan_flag = s[3] != 0.0 ? 1 : 0;
+    out->bulk_ke = s[4];
+    out->bulk_u = s[5];
+    out->last_bulk_rhs = s[0];
+  });
+}
+
+int chs_op3d(chs_handle* H, int dir, int fam, int ibc1, int ibc2, const double* fbc2d, const double* in,
+             const int nin3[3], double* out) {
+  if (!H || !in || !out || !nin3 || dir < 0 || dir > 2 || fam < 0 || fam > 5) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    const int n1 = nin3[0], n2 = nin3[1], n3 = nin3[2];
+    const size_t nin = (size_t)n1 * n2 * n3;
+    int o[3] = {n1, n2, n3};
+    o[dir] = fam_p_output(fam) ? H->np[dir] : H->nc[dir];
+    const size_t nout = (size_t)o[0] * o[1] * o[2];
+    const int64_t nl = num_lines(dir, n1, n2, n3);
+    Pair bc{{ibc1, ibc2}};
+    const size_t before = H->book.table.size();
+    H->plan(dir, fam, bc, fbc2d != nullptr);
+    if (H->book.table.size() != before) upload_table(H);
+    double *din, *dout, *dfbc = nullptr;
+    CK(cudaMallocAsync(&din, nin * sizeof(double), H->st));
+    CK(cudaMallocAsync(&dout, nout * sizeof(double), H->st));
+    CK(cudaMemcpyAsync(din, in, nin * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    std::vector<double> fb;
+    if (fbc2d) {
+      // reference layouts fbcx(4,n2,n3) / fbcy(n1,4,n3) / fbcz(n1,n2,4) -> [4][lines]
+      fb.resize(4 * nl);
+      for (int64_t L = 0; L < nl; ++L)
+        for (int u = 0; u < 4; ++u) {
+          size_t src_i;
+          if (dir == 0) src_i = (size_t)L * 4 + u;
+          else if (dir == 1) { int64_t k = L / n1, i = L - k * n1; src_i = (size_t)(k * 4 + u) * n1 + i; }
+          else { int64_t j = L / n1, i = L - j * n1; src_i = (size_t)(u * n2 + j) * n1 + i; }
+          fb[u * nl + L] = fbc2d[src_i];
+        }
+      CK(cudaMallocAsync(&dfbc, fb.size() * sizeof(double), H->st));
+      CK(cudaMemcpyAsync(dfbc, fb.data(), fb.size() * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    }
+    run_op(H, dir, fam, bc, dfbc, src(din), nin3, dout, false, 1.0);
+    CK(cudaMemcpyAsync(out, dout, nout * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+    cudaFreeAsync(din, H->st);
+    cudaFreeAsync(dout, H->st);
+    if (dfbc) cudaFreeAsync(dfbc, H->st);
+    CK(cudaStreamSynchronize(H->st));
+  });
+}
+
+// Host-only inspection of one operator plan (no device work).  Layout of buf:
+// [0..15] fam nin nout b_lo b_hi off0..3 sgn r1 r2 dd nspec tdma b1
+// [16..19] an cn inv_den neu1*2+neu2
+// [20 + 26*s ..] special row s: row nt idx[10] w[10] wb[4]  (s < 4)
+// [128 ..] a c' d x1 map (nout each; zeros when absent)
+int chs_plan_inspect(const chs_config* cfg, int dir, int fam, int ibc1, int ibc2, int has_fbc, double* buf,
+                     size_t len) {
+  if (!cfg || !buf || dir < 0 || dir > 2 || fam < 0 || fam > 5) return CHS_ERR_ARG;
+  chs_handle H;
+  try {
+    setup_host(&H, cfg);
+    int bc[2] = {ibc1, ibc2};
+    OpPlan P = H.book.make(dir, fam, bc, has_fbc != 0);
+    const int n = P.nout;
+    if (len < (size_t)(128 + 5 * n)) return CHS_ERR_ARG;
+    for (size_t i = 0; i < len; ++i) buf[i] = 0.0;
+    double hd[20] = {(double)P.fam, (double)P.nin, (double)P.nout, (double)P.b_lo, (double)P.b_hi,
+                     (double)P.off[0], (double)P.off[1], (double)P.off[2], (double)P.off[3], P.sgn, P.r1, P.r2,
+                     P.dd, (double)P.nspec, (double)P.tdma, P.b1, P.an, P.cn, P.inv_den,
+                     (double)(P.neu1 * 2 + P.neu2)};
+    for (int i = 0; i < 20; ++i) buf[i] = hd[i];
+    for (int k = 0; k < P.nspec; ++k) {
+      double* o = buf + 20 + 26 * k;
+      o[0] = P.sp[k].row;
+      o[1] = P.sp[k].nt;
+      for (int t = 0; t < P.sp[k].nt; ++t) { o[2 + t] = P.sp[k].idx[t]; o[12 + t] = P.sp[k].w[t]; }
+      for (int u = 0; u < 4; ++u) o[22 + u] = P.sp[k].wb[u];
+    }
+    const std::vector<double>& T = H.book.table;
+    double* arr = buf + 128;
+    for (int i = 0; i < n; ++i) {
+      if (P.tdma) {
+        arr[i] = T[P.la + i];
+        arr[n + i] = T[P.lc + i];
+        arr[2 * n + i] = T[P.ld + i];
+        arr[3 * n + i] = T[P.lx1 + i];
+      }
+      if (P.lmap >= 0) arr[4 * n + i] = T[P.lmap + i];
+    }
+    return CHS_OK;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "chs_plan_inspect: %s\n", e.what());
+    return CHS_ERR_ARG;
+  }
+}
+
+int chs_sync(chs_handle* H) {
+  if (!H) return CHS_ERR_ARG;
+  return guard(H, [&] { CK(cudaStreamSynchronize(H->st)); });
+}
+
+long long chs_kernel_launches(const chs_handle* H) { return H ? H->launches : 0; }
+
+int chs_last_error(const chs_handle* H, char* buf, size_t len) {
+  if (!H || !buf || len == 0) return CHS_ERR_ARG;
+  std::snprintf(buf, len, "%s", H->err.c_str());
+  return CHS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,46 @@
+"""Run a few substeps of the channel (or Taylor-Green) case for profilers.
+
+Launches every kernel individually (no graph replay), so a profiler sees one
+launch per operator.  Example:
+    python chapsim2_b200/profile_case.py --nc 128 96 128 --substeps 3
+"""
+import argparse
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+from chapsim2_b200 import config as C  # noqa: E402
+from chapsim2_b200 import initial as I  # noqa: E402
+from chapsim2_b200 import solver as S  # noqa: E402
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="channel", choices=["channel", "tgv"])
+    ap.add_argument("--nc", type=int, nargs=3, default=[128, 96, 128])
+    ap.add_argument("--iacc", type=int, default=C.IACCU_CD2)
+    ap.add_argument("--substeps", type=int, default=3)
+    a = ap.parse_args()
+    if a.case == "channel":
+        cfg = C.channel(nc=tuple(a.nc), iacc=a.iacc)
+        f = I.channel_fields(cfg)
+        cfg.dt = I.cfl_dt(cfg, *f[:3], cfl=0.8)
+    else:
+        cfg = C.taylor_green(a.nc[0], iacc=a.iacc)
+        f = I.taylor_green_fields(cfg)
+    g = S.Solver(cfg)
+    g.set_fields(*f)
+    g.Solve_momentum_eq(0)
+    for i in range(a.substeps):
+        g.Solve_momentum_eq(1 + i % 3)
+    d = g.diagnostics()
+    print(f"{a.case} {cfg.nc} iacc={a.iacc}: {a.substeps} substeps, launches={g.kernel_launches()}, "
+          f"max_div={d['max_div']:.3e}, nan={d['nan_flag']}")
+    g.close()
+    if d["nan_flag"]:
+        sys.exit(1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,266 @@
+"""ctypes binding of libchapsim_gpu.so, mirroring the reference's Fortran interface.
+
+The calls follow the routines that src/chapsim.f90 drives each time step:
+``Solve_momentum_eq(isub)`` (src/eq_momentum2.f90:1799), ``solve_fft_poisson``
+(src/poisson_interface.f90:119) and the post-step checks.  There is no CPU
+fallback: if the CUDA library is missing or no GPU is present the calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import config as C
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libchapsim_gpu.so")
+
+CHS_QX, CHS_QY, CHS_QZ, CHS_PRES, CHS_PCOR, CHS_MX_RHS0, CHS_MY_RHS0, CHS_MZ_RHS0 = range(8)
+CHS_FP64, CHS_MIXED = 0, 1
+_D = ctypes.POINTER(ctypes.c_double)
+
+
+class ChsConfig(ctypes.Structure):
+    _fields_ = [
+        ("nc", ctypes.c_int * 3),
+        ("iacc", ctypes.c_int),
+        ("istret", ctypes.c_int),
+        ("ifft", ctypes.c_int),
+        ("idriven", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("lxx", ctypes.c_double), ("lyt", ctypes.c_double), ("lyb", ctypes.c_double), ("lzz", ctypes.c_double),
+        ("rstret", ctypes.c_double), ("dt", ctypes.c_double), ("ren", ctypes.c_double),
+        ("nominal_bc", ctypes.c_int * 30),
+        ("fbcy_const", ctypes.c_double * 10),
+        ("yp", _D), ("yc", _D), ("ymap_pt", _D), ("ymap_cc", _D),
+    ]
+
+
+class ChsDiag(ctypes.Structure):
+    _fields_ = [("max_div", ctypes.c_double), ("bulk_ke", ctypes.c_double), ("bulk_u", ctypes.c_double),
+                ("last_bulk_rhs", ctypes.c_double), ("nan_flag", ctypes.c_int)]
+
+
+EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field", "chs_momentum_substep",
+            "chs_step", "chs_poisson_solve", "chs_poisson_solve_device", "chs_diagnostics", "chs_op3d",
+            "chs_plan_inspect", "chs_sync", "chs_kernel_launches", "chs_last_error", "chs_momentum_substep_host",
+            "chs_time_steps", "chs_time_steps_host", "chs_host_alloc", "chs_host_free", "chs_profile_substep"]
+
+
+class ChsKprof(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("dir", ctypes.c_int), ("bytes", ctypes.c_double), ("ms", ctypes.c_float)]
+
+_lib = None
+
+
+def load():
+    """Load the in-tree CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run chapsim2_b200/build.py (no CPU fallback exists)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.chs_create.argtypes = [ctypes.POINTER(ChsConfig), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.chs_destroy.argtypes = [ctypes.c_void_p]
+    L.chs_upload_field.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_size_t]
+    L.chs_download_field.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_size_t]
+    L.chs_momentum_substep.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.chs_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.chs_poisson_solve.argtypes = [ctypes.c_void_p, _D]
+    L.chs_poisson_solve_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.chs_diagnostics.argtypes = [ctypes.c_void_p, ctypes.POINTER(ChsDiag)]
+    L.chs_op3d.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D,
+                           ctypes.POINTER(ctypes.c_int), _D]
+    L.chs_plan_inspect.argtypes = [ctypes.POINTER(ChsConfig), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, _D, ctypes.c_size_t]
+    L.chs_sync.argtypes = [ctypes.c_void_p]
+    L.chs_kernel_launches.restype = ctypes.c_longlong
+    L.chs_kernel_launches.argtypes = [ctypes.c_void_p]
+    L.chs_last_error.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    L.chs_momentum_substep_host.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D, _D]
+    L.chs_time_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.chs_time_steps_host.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D, _D, ctypes.POINTER(ctypes.c_float)]
+    L.chs_host_alloc.restype = ctypes.c_void_p
+    L.chs_host_alloc.argtypes = [ctypes.c_size_t]
+    L.chs_host_free.argtypes = [ctypes.c_void_p]
+    L.chs_profile_substep.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ChsKprof), ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int)]
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_D)
+
+
+def make_config(cfg, precision=CHS_FP64):
+    """Fill a ChsConfig from a DomainConfig; returns (struct, keep-alive arrays)."""
+    g = C.geometry(cfg)
+    keep = [np.ascontiguousarray(g[k], np.float64) for k in ("yp", "yc", "mppt", "mpcc")]
+    s = ChsConfig()
+    for d in range(3):
+        s.nc[d] = int(cfg.nc[d])
+    s.iacc, s.istret, s.ifft, s.idriven = int(cfg.iacc), int(cfg.istret), int(cfg.ifft), int(cfg.idriven)
+    s.precision = int(precision)
+    s.lxx, s.lyt, s.lyb, s.lzz = float(cfg.lxx), float(cfg.lyt), float(cfg.lyb), float(cfg.lzz)
+    s.rstret, s.dt, s.ren = float(cfg.rstret), float(cfg.dt), float(cfg.ren)
+    nb = np.ascontiguousarray(cfg.nominal_bc, np.int32).ravel()
+    for i in range(30):
+        s.nominal_bc[i] = int(nb[i])
+    fb = np.ascontiguousarray(cfg.fbcy_const, np.float64).ravel()
+    for i in range(10):
+        s.fbcy_const[i] = float(fb[i])
+    s.yp, s.yc, s.ymap_pt, s.ymap_cc = [_ptr(a) for a in keep]
+    return s, keep
+
+
+def plan_inspect(cfg, d, fam, ibc, has_fbc):
+    """Host-only view of one operator plan (dict of numpy arrays)."""
+    L = load()
+    s, keep = make_config(cfg)
+    n = cfg.np_[d] if fam in (1, 2, 4) else cfg.nc[d]
+    buf = np.zeros(128 + 5 * n + 8)
+    rc = L.chs_plan_inspect(ctypes.byref(s), d, fam, int(ibc[0]), int(ibc[1]), int(bool(has_fbc)), _ptr(buf),
+                            buf.size)
+    if rc != 0:
+        raise RuntimeError(f"chs_plan_inspect failed ({rc})")
+    h = buf[:20]
+    p = dict(fam=int(h[0]), nin=int(h[1]), nout=int(h[2]), b_lo=int(h[3]), b_hi=int(h[4]),
+             off=[int(x) for x in h[5:9]], sgn=h[9], r1=h[10], r2=h[11], dd=h[12], nspec=int(h[13]),
+             tdma=int(h[14]), b1=h[15], an=h[16], cn=h[17], inv_den=h[18], neu1=int(h[19]) // 2,
+             neu2=int(h[19]) % 2)
+    rows = []
+    for k in range(p["nspec"]):
+        o = buf[20 + 26 * k: 46 + 26 * k]
+        nt = int(o[1])
+        rows.append(dict(row=int(o[0]), idx=o[2:2 + nt].astype(int), w=o[12:12 + nt].copy(), wb=o[22:26].copy()))
+    p["rows"] = rows
+    arr = buf[128:128 + 5 * n]
+    p["a"], p["c"], p["d"], p["x1"], p["map"] = [arr[i * n:(i + 1) * n].copy() for i in range(5)]
+    return p
+
+
+class Solver:
+    """One domain resident on the GPU (a chs_handle)."""
+
+    def __init__(self, cfg, device=0, precision=CHS_FP64):
+        self.cfg = cfg
+        self.L = load()
+        self._s, self._keep = make_config(cfg, precision)
+        h = ctypes.c_void_p()
+        rc = self.L.chs_create(ctypes.byref(self._s), int(device), ctypes.byref(h))
+        if rc != 0 or not h.value:
+            raise RuntimeError(f"chs_create failed with status {rc}")
+        self.h = h
+        self.shapes = cfg.shapes()
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.chs_destroy(self.h)
+            self.h = None
+        for p in self.__dict__.pop("_pinned", []):
+            self.L.chs_host_free(p)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != 0:
+            buf = ctypes.create_string_buffer(1024)
+            self.L.chs_last_error(self.h, buf, 1024)
+            raise RuntimeError(f"{what} failed ({rc}): {buf.value.decode()}")
+
+    # ---- state
+    def upload(self, field, a):
+        a = np.ascontiguousarray(a, np.float64)
+        self._check(self.L.chs_upload_field(self.h, field, _ptr(a), a.size), "chs_upload_field")
+
+    def download(self, field):
+        shp = {CHS_QX: 0, CHS_MX_RHS0: 0, CHS_QY: 1, CHS_MY_RHS0: 1, CHS_QZ: 2, CHS_MZ_RHS0: 2,
+               CHS_PRES: 3, CHS_PCOR: 3}[field]
+        a = np.zeros(self.shapes[shp])
+        self._check(self.L.chs_download_field(self.h, field, _ptr(a), a.size), "chs_download_field")
+        return a
+
+    def set_fields(self, qx, qy, qz, p):
+        for f, a in ((CHS_QX, qx), (CHS_QY, qy), (CHS_QZ, qz), (CHS_PRES, p)):
+            self.upload(f, a)
+
+    def get_fields(self):
+        return tuple(self.download(f) for f in (CHS_QX, CHS_QY, CHS_QZ, CHS_PRES, CHS_PCOR))
+
+    # ---- reference-facing calls
+    def Solve_momentum_eq(self, isub):
+        """One RK3 substep (isub 1..3) or the initial Euler step (isub 0)."""
+        self._check(self.L.chs_momentum_substep(self.h, int(isub)), "chs_momentum_substep")
+
+    def step(self, nsteps=1):
+        self._check(self.L.chs_step(self.h, int(nsteps)), "chs_step")
+
+    def solve_fft_poisson(self, rhs):
+        r = np.array(rhs, np.float64, copy=True, order="C")
+        self._check(self.L.chs_poisson_solve(self.h, _ptr(r)), "chs_poisson_solve")
+        return r
+
+    def diagnostics(self):
+        d = ChsDiag()
+        self._check(self.L.chs_diagnostics(self.h, ctypes.byref(d)), "chs_diagnostics")
+        return dict(max_div=d.max_div, bulk_ke=d.bulk_ke, bulk_u=d.bulk_u, last_bulk_rhs=d.last_bulk_rhs,
+                    nan_flag=d.nan_flag)
+
+    def op3d(self, d, fam, ibc, fi, fbc2d=None):
+        fi = np.ascontiguousarray(fi, np.float64)
+        nin = (ctypes.c_int * 3)(fi.shape[2], fi.shape[1], fi.shape[0])
+        nout = [fi.shape[2], fi.shape[1], fi.shape[0]]
+        nout[d] = self.cfg.np_[d] if fam in (1, 2, 4) else self.cfg.nc[d]
+        fo = np.zeros((nout[2], nout[1], nout[0]))
+        fb = None if fbc2d is None else np.ascontiguousarray(fbc2d, np.float64)
+        self._check(self.L.chs_op3d(self.h, d, fam, int(ibc[0]), int(ibc[1]), _ptr(fb), _ptr(fi), nin, _ptr(fo)),
+                    "chs_op3d")
+        return fo
+
+    def Solve_momentum_eq_host(self, isub, qx, qy, qz, p):
+        """Drop-in substep on host arrays (updated in place)."""
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (qx, qy, qz, p)]
+        for a, s in zip(arrs, self.shapes):
+            assert a.shape == s
+        self._check(self.L.chs_momentum_substep_host(self.h, int(isub), *[_ptr(a) for a in arrs]),
+                    "chs_momentum_substep_host")
+        return arrs
+
+    def time_steps(self, nsteps):
+        ms = ctypes.c_float()
+        self._check(self.L.chs_time_steps(self.h, int(nsteps), ctypes.byref(ms)), "chs_time_steps")
+        return float(ms.value)
+
+    def pinned(self, shape):
+        """numpy view of a page-locked host buffer (freed with the Solver)."""
+        n = int(np.prod(shape))
+        p = self.L.chs_host_alloc(n * 8)
+        if not p:
+            raise RuntimeError("chs_host_alloc failed")
+        self.__dict__.setdefault("_pinned", []).append(p)
+        buf = (ctypes.c_double * n).from_address(p)
+        return np.ndarray(shape, np.float64, buffer=buf)
+
+    def time_steps_host(self, nsteps, qx, qy, qz, p):
+        ms = ctypes.c_float()
+        self._check(self.L.chs_time_steps_host(self.h, int(nsteps), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(p),
+                                               ctypes.byref(ms)), "chs_time_steps_host")
+        return float(ms.value)
+
+    def profile_substep(self, isub=1, maxk=512):
+        arr = (ChsKprof * maxk)()
+        n = ctypes.c_int()
+        self._check(self.L.chs_profile_substep(self.h, int(isub), arr, maxk, ctypes.byref(n)), "chs_profile_substep")
+        return [dict(kind=arr[i].kind, dir=arr[i].dir, bytes=arr[i].bytes, ms=arr[i].ms) for i in range(n.value)]
+
+    def sync(self):
+        self._check(self.L.chs_sync(self.h), "chs_sync")
+
+    def kernel_launches(self):
+        return int(self.L.chs_kernel_launches(self.h))

@@ -1,0 +1,162 @@
+/*
+ * chapsim_gpu.h -- C ABI of the B200 (sm_100a) CHAPSim2 per-timestep hot path.
+ *
+ * The library owns all device state of one domain (velocity, pressure, RK3
+ * history, work arrays), resident in HBM across steps.  Host arrays use the
+ * reference's Fortran x-pencil layout: column-major, x fastest, full domain.
+ * Every entry point returns 0 on success and a non-zero chs_status otherwise;
+ * chs_last_error() returns the message.  A handle is bound to one CUDA stream
+ * and must be used from one host thread at a time.
+ *
+ * Each entry point names the reference routine it replaces (file:line in
+ * weiwangstfc/CHAPSim2).
+ */
+#ifndef CHAPSIM_GPU_H
+#define CHAPSIM_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct chs_handle chs_handle;
+
+enum chs_status {
+  CHS_OK = 0,
+  CHS_ERR_ARG = 1,       /* invalid argument or unsupported configuration */
+  CHS_ERR_CUDA = 2,      /* CUDA runtime error */
+  CHS_ERR_STATE = 3,     /* call not valid in the current state */
+  CHS_ERR_NUMERIC = 4    /* NaN/Inf detected in the solution */
+};
+
+/* field identifiers for upload/download */
+enum chs_field {
+  CHS_QX = 0, CHS_QY = 1, CHS_QZ = 2, CHS_PRES = 3, CHS_PCOR = 4,
+  CHS_MX_RHS0 = 5, CHS_MY_RHS0 = 6, CHS_MZ_RHS0 = 7
+};
+
+/* precision of the path */
+enum chs_precision { CHS_FP64 = 0, CHS_MIXED = 1 };
+
+/*
+ * Domain configuration: the scalars of t_domain/t_flow that the momentum and
+ * Poisson routines read (src/modules.f90:412-653), the nominal boundary codes
+ * as read from [boundary] (src/input_general.f90:399-424) and the y geometry
+ * built by Buildup_geometry_mesh_info (src/geometry.f90:410-530).
+ */
+typedef struct chs_config {
+  int nc[3];                /* cells in x, y, z */
+  int iacc;                 /* 1 CD2, 2 CD4, 3 CP4, 4 CP6 (src/modules.f90:248-251) */
+  int istret;               /* 0 none, 2 two-sided, 3 bottom, 4 top */
+  int ifft;                 /* 2 FISHPACK x/z-FFT + y-TDMA, 3 3D FFT (src/modules.f90:169-170) */
+  int idriven;              /* 0 none, 1 constant x mass flux */
+  int precision;            /* chs_precision */
+  double lxx, lyt, lyb, lzz;
+  double rstret, dt, ren;
+  int nominal_bc[3][5][2];  /* [x,y,z][qx,qy,qz,p,T][side] bc codes (src/modules.f90:223-229) */
+  double fbcy_const[5][2];  /* constant y-wall values [qx,qy,qz,p,T][side] */
+  const double* yp;         /* nc[1]+1 node coordinates */
+  const double* yc;         /* nc[1] centre coordinates */
+  const double* ymap_pt;    /* yMappingpt(:,1), nc[1]+1 */
+  const double* ymap_cc;    /* yMappingcc(:,1), nc[1] */
+} chs_config;
+
+typedef struct chs_diag {
+  double max_div;      /* max |div u| over the domain (Check_element_mass_conservation, src/eq_continuity.f90:337-397) */
+  double bulk_ke;      /* bulk kinetic energy (write_monitor_total, src/io_monitor.f90:209-241) */
+  double bulk_u;       /* volume-averaged qx */
+  double last_bulk_rhs;/* last mass-flux correction removed from mx_rhs */
+  int nan_flag;        /* 1 if a NaN/Inf was found */
+} chs_diag;
+
+/* Replaces initialise_fft / Prepare_LHS_coeffs_for_operations / allocation
+ * (src/chapsim.f90:79-97, src/poisson_interface.f90:102-116,
+ * src/basics_operations2.f90:1600-1800).  device < 0 uses the current device. */
+int chs_create(const chs_config* cfg, int device, chs_handle** out);
+int chs_destroy(chs_handle* h);
+
+/* Copy one field between host (Fortran layout) and the handle's device state.
+ * n is the element count and must equal the field's staggered size. */
+int chs_upload_field(chs_handle* h, int field, const double* host, size_t n);
+int chs_download_field(chs_handle* h, int field, double* host, size_t n);
+
+/* Replaces Solve_momentum_eq(fl, dm, isub) (src/eq_momentum2.f90:1799-1932):
+ * momentum RHS, RK3 fractional step, mass-flux driving, Poisson solve,
+ * pressure update, projection.  isub = 0 is the initial Euler step
+ * (src/chapsim.f90:135), isub = 1..3 the RK3 substeps. */
+int chs_momentum_substep(chs_handle* h, int isub);
+
+/* nsteps full RK3 steps (3 substeps each) of the time loop
+ * (src/chapsim.f90:243-309), replayed from a captured CUDA graph. */
+int chs_step(chs_handle* h, int nsteps);
+
+/* Replaces solve_fft_poisson(rhs_xpencil, dm) (src/poisson_interface.f90:119-149)
+ * on a host buffer of nc[0]*nc[1]*nc[2] values, in place. */
+int chs_poisson_solve(chs_handle* h, double* rhs_inout);
+
+/* Drop-in for Solve_momentum_eq with host-owned arrays (the Fortran x-pencil
+ * arrays fl%qx, fl%qy, fl%qz, fl%pres): uploads them, runs the substep and
+ * copies the updated fields back (in place).  Pinned host memory
+ * (chs_host_alloc) makes the copies asynchronous DMA. */
+int chs_momentum_substep_host(chs_handle* h, int isub, double* qx, double* qy, double* qz, double* pres);
+
+/* Time nsteps RK3 steps replayed from the captured graphs with CUDA events
+ * recorded on the handle's stream; *ms = elapsed device time. */
+int chs_time_steps(chs_handle* h, int nsteps, float* ms);
+
+/* Time nsteps RK3 steps of chs_momentum_substep_host (host->device copies,
+ * substep, device->host copies, three times per step) with CUDA events on the
+ * handle's stream; *ms = elapsed device time including the copies. */
+int chs_time_steps_host(chs_handle* h, int nsteps, double* qx, double* qy, double* qz, double* pres, float* ms);
+
+/* Page-locked host buffers for the host-array entry points. */
+void* chs_host_alloc(size_t bytes);
+void chs_host_free(void* p);
+
+/* Per-kernel profile of one substep (not graph-replayed): for each launch, its
+ * class (0 line op, 1 FFT, 2 y solve, 3 elementwise/reduction), direction
+ * (-1 if none), algorithmic bytes moved and CUDA-event duration. */
+typedef struct chs_kprof {
+  int kind;
+  int dir;
+  double bytes;
+  float ms;
+} chs_kprof;
+int chs_profile_substep(chs_handle* h, int isub, chs_kprof* out, int max, int* n);
+
+/* Same as chs_poisson_solve on a device buffer (no host copies). */
+int chs_poisson_solve_device(chs_handle* h, double* d_rhs_inout);
+
+/* Post-step checks (src/chapsim.f90:326-356): divergence, bulk KE, NaN scan. */
+int chs_diagnostics(chs_handle* h, chs_diag* out);
+
+/* One compact operator Get_{x,y,z}_{midp,1der}_{C2P,P2C,C2C,P2P}_3D
+ * (src/basics_operations2.f90:3952-4800) on host arrays.
+ * dir 0/1/2; fam 0 d1C2C, 1 d1P2P, 2 d1C2P, 3 d1P2C, 4 m1C2P, 5 m1P2C;
+ * nin3 = input extents (x,y,z); fbc2d, when non-NULL, holds the 4 boundary
+ * planes in the reference layout fbcx(4,n2,n3) / fbcy(n1,4,n3) / fbcz(n1,n2,4). */
+int chs_op3d(chs_handle* h, int dir, int fam, int ibc1, int ibc2, const double* fbc2d,
+             const double* in, const int nin3[3], double* out);
+
+/* Host-only inspection of the operator plan that chs_op3d / the substep would use
+ * (test support; no counterpart in the reference, no device work).  Writes the
+ * bulk stencil, boundary rows, pre-factorised LHS and y metric into buf
+ * (len >= 128 + 5*nout doubles); see chs_solver.cu for the layout. */
+int chs_plan_inspect(const chs_config* cfg, int dir, int fam, int ibc1, int ibc2, int has_fbc, double* buf,
+                     size_t len);
+
+/* Block until all work queued on the handle's stream is done. */
+int chs_sync(chs_handle* h);
+
+/* Number of kernels the handle launched since creation (all entry points). */
+long long chs_kernel_launches(const chs_handle* h);
+
+/* Last error message (NUL-terminated, truncated to len). */
+int chs_last_error(const chs_handle* h, char* buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHAPSIM_GPU_H */
