@@ -21,193 +21,228 @@ namespace chs {
 // phase applies the cyclic correction, the y metric, the Neumann overrides and
 // the output accumulation, again coalesced.
 // ===========================================================================
-template <int DIR>
-struct LineAddr {
-  int64_t nlines;
-  int n1, n2;
-  __device__ __forceinline__ int64_t at(int64_t L, int p, int n) const {
-    if (DIR == 0) return L * n + p;
-    if (DIR == 1) {
-      int64_t k = L / n1, i = L - k * n1;
-      return (k * n + p) * n1 + i;
-    }
-    int64_t j = L / n1, i = L - j * n1;
-    return ((int64_t)p * n2 + j) * n1 + i;
-  }
-};
+// exact input reads of the bulk stencil of each family, rows i (0-based), column stride ld
+template <int FAM, typename T>
+__device__ __forceinline__ T bulk_at(const T* col, int ld, int i, T r1, T r2) {
+  if (FAM == M1P2C) return r1 * (col[i * ld] + col[(i + 1) * ld]) + r2 * (col[(i - 1) * ld] + col[(i + 2) * ld]);
+  if (FAM == M1C2P) return r1 * (col[i * ld] + col[(i - 1) * ld]) + r2 * (col[(i + 1) * ld] + col[(i - 2) * ld]);
+  if (FAM == D1C2C || FAM == D1P2P)
+    return r1 * (col[(i + 1) * ld] - col[(i - 1) * ld]) + r2 * (col[(i + 2) * ld] - col[(i - 2) * ld]);
+  if (FAM == D1C2P) return r1 * (col[i * ld] - col[(i - 1) * ld]) + r2 * (col[(i + 1) * ld] - col[(i - 2) * ld]);
+  return r1 * (col[(i + 1) * ld] - col[i * ld]) + r2 * (col[(i + 2) * ld] - col[(i - 1) * ld]);  // D1P2C
+}
 
-__device__ __forceinline__ double eval_expr(const LineIO& io, int64_t a) {
-  double A = io.A[a];
-  switch (io.emode) {
-    case E_A: return io.s * A;
-    case E_AB: return io.s * (A * io.B[a]);
-    case E_ApB: return io.s * (A + io.c1 * io.B[a]);
-    default: return io.s * (A + io.c1 * io.B[a]) * io.C[a];
+// boundary row of the plan evaluated from the staged column
+template <typename T>
+__device__ __forceinline__ T special_at(const SpecialRow& R, const T* col, int ld, const T* fbc, int nlines, int L) {
+  T v = T(0);
+  for (int t = 0; t < R.nt; ++t) v += T(R.w[t]) * col[R.idx[t] * ld];
+  for (int u = 0; u < 4; ++u)
+    if (R.wb[u] != 0.0) v += T(R.wb[u]) * fbc[u * nlines + L];
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T eval_term(const TermT<T>& t, int64_t a) {
+  switch (t.mode) {
+    case T_X: return T(t.s) * t.X[a];
+    case T_XY: return T(t.s) * (t.X[a] * t.Y[a]);
+    case T_XpY: return T(t.s) * (t.X[a] + T(t.c) * t.Y[a]);
+    default: return T(0);
   }
 }
 
-template <int FAM>
-struct Bulk;
-// r1*(f[i+o0] + sgn f[i+o1]) + r2*(f[i+o2] + sgn f[i+o3]); window w[k] = f[i-2+k]
-template <> struct Bulk<M1P2C> {
-  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
-    return r1 * (w[2] + w[3]) + r2 * (w[1] + w[4]);
-  }
-};
-template <> struct Bulk<M1C2P> {
-  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
-    return r1 * (w[2] + w[1]) + r2 * (w[3] + w[0]);
-  }
-};
-template <> struct Bulk<D1C2C> {
-  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
-    return r1 * (w[3] - w[1]) + r2 * (w[4] - w[0]);
-  }
-};
-template <> struct Bulk<D1P2P> {
-  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
-    return r1 * (w[3] - w[1]) + r2 * (w[4] - w[0]);
-  }
-};
-template <> struct Bulk<D1C2P> {
-  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
-    return r1 * (w[2] - w[1]) + r2 * (w[3] - w[0]);
-  }
-};
-template <> struct Bulk<D1P2C> {
-  static __device__ __forceinline__ double f(const double* w, double r1, double r2) {
-    return r1 * (w[3] - w[2]) + r2 * (w[4] - w[1]);
-  }
-};
+template <typename T>
+__device__ __forceinline__ T eval_expr(const LineIOT<T>& io, int64_t a) {
+  T v = eval_term(io.t[0], a);
+  if (io.t[1].mode != T_NONE) v += eval_term(io.t[1], a);
+  return v;
+}
 
-template <int DIR, int FAM>
+// address of (line L, position 0) of an array whose direction-DIR extent is n
+template <int DIR>
+__device__ __forceinline__ int64_t line_base(int L, int n, int n1) {
+  if (DIR == 0) return (int64_t)L * n;
+  if (DIR == 1) {
+    const int k = L / n1, i = L - k * n1;
+    return (int64_t)k * n * n1 + i;
+  }
+  return (int64_t)L;  // DIR == 2: L = i + n1*j
+}
+template <int DIR>
+__device__ __forceinline__ int64_t pos_stride(int n1, int n2) {
+  return DIR == 0 ? 1 : (DIR == 1 ? (int64_t)n1 : (int64_t)n1 * n2);
+}
+
+template <typename T, int DIR, int FAM>
 __global__ void __launch_bounds__(256) line_op_kernel(const __grid_constant__ OpPlan P,
-                                                      const __grid_constant__ LineIO io,
-                                                      const double* __restrict__ table, int64_t nlines, int LT) {
-  extern __shared__ double smem[];
+                                                      const __grid_constant__ LineIOT<T> io,
+                                                      const double* __restrict__ table, int nlines, int LT) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s = reinterpret_cast<T*>(smem_raw);
   const int nin = P.nin, nout = P.nout;
   const int nmax = nin > nout ? nin : nout;
   const int ld = LT + 1;
-  double* s = smem;                    // [nmax][ld]
-  double* sa = s + (size_t)nmax * ld;  // LHS a
-  double* sc = sa + nmax;              // LHS c'
-  double* sd = sc + nmax;              // LHS 1/pivot
-  double* sx = sd + nmax;              // cyclic correction x1
-  double* sm = sx + nmax;              // y metric
-  LineAddr<DIR> ad{nlines, io.n1, io.n2};
-  const int64_t L0 = (int64_t)blockIdx.x * LT;
+  T* sa = s + (size_t)nmax * ld;  // LHS a
+  T* sc = sa + nmax;              // LHS c'
+  T* sd = sc + nmax;              // LHS 1/pivot
+  T* sx = sd + nmax;              // cyclic correction x1
+  T* sm = sx + nmax;              // y metric
+  const int L0 = blockIdx.x * LT;
   const int nt = blockDim.x;
+  const int tid = threadIdx.x;
+  const int64_t ps = pos_stride<DIR>(io.n1, io.n2);
 
   // ---- stage the tile
-  const int tot_in = LT * nin;
-  for (int e = threadIdx.x; e < tot_in; e += nt) {
-    int l, p;
-    if (DIR == 0) { l = e / nin; p = e - l * nin; }
-    else { p = e / LT; l = e - p * LT; }
-    const int64_t L = L0 + l;
-    double v = 0.0;
-    if (L < nlines) v = eval_expr(io, ad.at(L, p, nin));
-    s[p * ld + l] = v;
-  }
-  for (int p = threadIdx.x; p < nout; p += nt) {
-    if (P.tdma) {
-      sa[p] = table[P.la + p];
-      sc[p] = table[P.lc + p];
-      sd[p] = table[P.ld + p];
-      sx[p] = table[P.lx1 + p];
+  if (DIR == 0) {
+    // LT consecutive rows are one contiguous run of LT*nin values
+    const int tot = LT * nin;
+    const int64_t g0 = (int64_t)L0 * nin;
+    const int64_t gmax = (int64_t)nlines * nin;
+    for (int e = tid; e < tot; e += nt) {
+      const int l = e / nin, p = e - l * nin;
+      T v = T(0);
+      if (g0 + e < gmax) v = eval_expr(io, g0 + e);
+      s[p * ld + l] = v;
     }
-    if (P.lmap >= 0) sm[p] = table[P.lmap + p];
+  } else {
+    // each thread owns one line of the tile (nt is a multiple of LT)
+    const int l = tid % LT;
+    const int L = L0 + l;
+    const bool ok = L < nlines;
+    const int64_t base = ok ? line_base<DIR>(L, nin, io.n1) : 0;
+    for (int p = tid / LT; p < nin; p += nt / LT) s[p * ld + l] = ok ? eval_expr(io, base + p * ps) : T(0);
+  }
+  for (int p = tid; p < nout; p += nt) {
+    if (P.tdma) {
+      sa[p] = T(table[P.la + p]);
+      sc[p] = T(table[P.lc + p]);
+      sd[p] = T(table[P.ld + p]);
+      sx[p] = T(table[P.lx1 + p]);
+    }
+    if (P.lmap >= 0) sm[p] = T(table[P.lmap + p]);
   }
   __syncthreads();
 
-  // ---- one thread per line: RHS + Thomas
-  const int l = threadIdx.x;
-  const int64_t L = L0 + l;
-  if (l < LT && L < nlines) {
-    double* col = s + l;
-    const double dd = P.dd;
-    double sv[4];
+  const T dd = T(P.dd), r1 = T(P.r1), r2 = T(P.r2);
+  if (P.tdma) {
+    // ---- compact scheme: one thread per line builds the RHS (5-point register window) and runs
+    // the Thomas forward sweep in place, then the backward sweep and the cyclic closure
+    const int l = tid;
+    const int L = L0 + l;
+    if (l < LT && L < nlines) {
+      T* col = s + l;
+      T sv[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      double v = 0.0;
-      if (k < P.nspec) {
-        const SpecialRow& R = P.sp[k];
-        for (int t = 0; t < R.nt; ++t) v += R.w[t] * col[R.idx[t] * ld];
-        for (int u = 0; u < 4; ++u)
-          if (R.wb[u] != 0.0) v += R.wb[u] * io.fbc[u * nlines + L];
-      }
-      sv[k] = v * dd;
-    }
-    const int nsw = (P.tdma == 2) ? nout - 1 : nout;
-    double w[5];
-    w[0] = 0.0;
-    w[1] = 0.0;
-    w[2] = col[0];
-    w[3] = col[ld];
-    double yprev = 0.0;
-    for (int i = 0; i < nout; ++i) {
-      w[4] = (i + 2 < nin) ? col[(i + 2) * ld] : 0.0;
-      double r;
-      if (i >= P.b_lo && i <= P.b_hi) {
-        r = Bulk<FAM>::f(w, P.r1, P.r2) * dd;
-      } else {
-        r = 0.0;
+      for (int k = 0; k < 4; ++k) sv[k] = k < P.nspec ? special_at(P.sp[k], col, ld, io.fbc, nlines, L) * dd : T(0);
+      const int nsw = (P.tdma == 2) ? nout - 1 : nout;
+      T w0 = T(0), w1 = T(0), w2 = col[0], w3 = col[ld], w4;
+      T yprev = T(0);
+      const T b1 = T(P.b1);
+      for (int i = 0; i < nout; ++i) {
+        w4 = (i + 2 < nin) ? col[(i + 2) * ld] : T(0);
+        T r;
+        if (i >= P.b_lo && i <= P.b_hi) {
+          if (FAM == M1P2C) r = r1 * (w2 + w3) + r2 * (w1 + w4);
+          else if (FAM == M1C2P) r = r1 * (w2 + w1) + r2 * (w3 + w0);
+          else if (FAM == D1C2C || FAM == D1P2P) r = r1 * (w3 - w1) + r2 * (w4 - w0);
+          else if (FAM == D1C2P) r = r1 * (w2 - w1) + r2 * (w3 - w0);
+          else r = r1 * (w3 - w2) + r2 * (w4 - w1);
+          r = r * dd;
+        } else {
+          r = T(0);
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-          if (k < P.nspec && P.sp[k].row == i) r = sv[k];
+          for (int k = 0; k < 4; ++k)
+            if (k < P.nspec && P.sp[k].row == i) r = sv[k];
+        }
+        T y = r;
+        if (i < nsw) {
+          y = (i == 0) ? r / b1 : (r - sa[i] * yprev) * sd[i];
+          yprev = y;
+        }
+        col[i * ld] = y;
+        w0 = w1; w1 = w2; w2 = w3; w3 = w4;
       }
-      double y = r;
-      if (P.tdma && i < nsw) {
-        y = (i == 0) ? r / P.b1 : (r - sa[i] * yprev) * sd[i];
-        yprev = y;
-      }
-      col[i * ld] = y;
-      w[0] = w[1]; w[1] = w[2]; w[2] = w[3]; w[3] = w[4];
-    }
-    if (P.tdma) {
-      double xn = col[(nsw - 1) * ld];
+      T xn = col[(nsw - 1) * ld];
       for (int i = nsw - 2; i >= 0; --i) {
-        const double x = col[i * ld] - sc[i] * xn;
+        const T x = col[i * ld] - sc[i] * xn;
         col[i * ld] = x;
         xn = x;
       }
       if (P.tdma == 2) {
-        const double rn = col[(nout - 1) * ld];
-        col[(nout - 1) * ld] = (rn - P.cn * col[0] - P.an * col[(nout - 2) * ld]) * P.inv_den;
+        const T rn = col[(nout - 1) * ld];
+        col[(nout - 1) * ld] = (rn - T(P.cn) * col[0] - T(P.an) * col[(nout - 2) * ld]) * T(P.inv_den);
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- store (explicit schemes compute every row here, in parallel)
+  auto finish = [&](int l, int p, int L) -> T {
+    T v;
+    if (P.tdma) {
+      v = s[p * ld + l];
+      if (P.tdma == 2 && p < nout - 1) v += sx[p] * s[(nout - 1) * ld + l];
+    } else {
+      const T* col = s + l;
+      if (p >= P.b_lo && p <= P.b_hi) {
+        v = bulk_at<FAM>(col, ld, p, r1, r2) * dd;
+      } else {
+        v = T(0);
+        for (int k = 0; k < P.nspec; ++k)
+          if (P.sp[k].row == p) v = special_at(P.sp[k], col, ld, io.fbc, nlines, L) * dd;
+      }
+    }
+    if (P.lmap >= 0) v *= sm[p];
+    if (P.neu1 && p == 0) v = io.fbc[L];
+    if (P.neu2 && p == nout - 1) v = io.fbc[nlines + L];
+    return v;
+  };
+  const T g = T(io.g);
+  if (DIR == 0) {
+    const int tot = LT * nout;
+    const int64_t g0 = (int64_t)L0 * nout;
+    for (int e = tid; e < tot; e += nt) {
+      const int l = e / nout, p = e - l * nout;
+      const int L = L0 + l;
+      if (L >= nlines) break;
+      const T v = finish(l, p, L);
+      const int64_t a = g0 + e;
+      io.out[a] = io.accumulate ? io.out[a] + g * v : g * v;
+    }
+  } else {
+    const int l = tid % LT;
+    const int L = L0 + l;
+    if (L < nlines) {
+      const int64_t base = line_base<DIR>(L, nout, io.n1);
+      for (int p = tid / LT; p < nout; p += nt / LT) {
+        const T v = finish(l, p, L);
+        const int64_t a = base + p * ps;
+        io.out[a] = io.accumulate ? io.out[a] + g * v : g * v;
       }
     }
   }
-  __syncthreads();
-
-  // ---- store
-  const int tot_out = LT * nout;
-  for (int e = threadIdx.x; e < tot_out; e += nt) {
-    int ll, p;
-    if (DIR == 0) { ll = e / nout; p = e - ll * nout; }
-    else { p = e / LT; ll = e - p * LT; }
-    const int64_t LL = L0 + ll;
-    if (LL >= nlines) continue;
-    double v = s[p * ld + ll];
-    if (P.tdma == 2 && p < nout - 1) v += sx[p] * s[(nout - 1) * ld + ll];
-    if (P.lmap >= 0) v *= sm[p];
-    if (P.neu1 && p == 0) v = io.fbc[LL];
-    if (P.neu2 && p == nout - 1) v = io.fbc[nlines + LL];
-    const int64_t a = ad.at(LL, p, nout);
-    io.out[a] = io.accumulate ? io.out[a] + io.g * v : io.g * v;
-  }
 }
 
-template <int DIR>
-static void launch_dir(const OpPlan& P, const LineIO& io, const double* table, cudaStream_t st, int64_t nlines,
+constexpr int kLineSmemMax = 200 * 1024;
+
+template <typename T, int DIR>
+static void launch_dir(const OpPlan& P, const LineIOT<T>& io, const double* table, cudaStream_t st, int nlines,
                        int LT, size_t shm) {
   dim3 grid((unsigned)((nlines + LT - 1) / LT));
   dim3 block(256);
   switch (P.fam) {
 #define CHS_CASE(F)                                                                                   \
-  case F:                                                                                             \
-    cudaFuncSetAttribute(line_op_kernel<DIR, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm); \
-    line_op_kernel<DIR, F><<<grid, block, shm, st>>>(P, io, table, nlines, LT);                       \
-    break;
+  case F: {                                                                                           \
+    static bool attr_set = false;                                                                     \
+    if (!attr_set) {                                                                                  \
+      cudaFuncSetAttribute(line_op_kernel<T, DIR, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                           kLineSmemMax);                                                             \
+      attr_set = true;                                                                                \
+    }                                                                                                 \
+    line_op_kernel<T, DIR, F><<<grid, block, shm, st>>>(P, io, table, nlines, LT);                    \
+    break;                                                                                            \
+  }
     CHS_CASE(D1C2C)
     CHS_CASE(D1P2P)
     CHS_CASE(D1C2P)
@@ -219,16 +254,29 @@ static void launch_dir(const OpPlan& P, const LineIO& io, const double* table, c
   }
 }
 
-void launch_line_op(int d, const OpPlan& P, const LineIO& io, const double* table, cudaStream_t st) {
+template <typename T>
+void launch_line_op_t(int d, const OpPlan& P, const LineIOT<T>& io, const double* table, cudaStream_t st) {
   int n_in3[3] = {io.n1, io.n2, io.n3};
   if (n_in3[d] != P.nin) throw std::runtime_error("line operator: input extent does not match the plan");
-  const int64_t nlines = num_lines(d, io.n1, io.n2, io.n3);
+  const int64_t nl = num_lines(d, io.n1, io.n2, io.n3);
+  if (nl > 0x7fffffff) throw std::runtime_error("line operator: too many lines");
+  const int nlines = (int)nl;
   const int nmax = P.nin > P.nout ? P.nin : P.nout;
-  const int LT = nmax <= 200 ? 64 : 32;
-  const size_t shm = ((size_t)nmax * (LT + 1) + 5 * (size_t)nmax) * sizeof(double);
-  if (d == 0) launch_dir<0>(P, io, table, st, nlines, LT, shm);
-  else if (d == 1) launch_dir<1>(P, io, table, st, nlines, LT, shm);
-  else launch_dir<2>(P, io, table, st, nlines, LT, shm);
+  // 64 lines per CTA while the tile fits in ~110 KB (two CTAs per SM), fewer for long lines
+  int LT = 64;
+  while (LT > 16 && ((size_t)nmax * (LT + 1) + 5 * (size_t)nmax) * sizeof(T) > 110 * 1024) LT /= 2;
+  const size_t shm = ((size_t)nmax * (LT + 1) + 5 * (size_t)nmax) * sizeof(T);
+  if (shm > (size_t)kLineSmemMax) throw std::runtime_error("line operator: line too long for the shared-memory tile");
+  if (d == 0) launch_dir<T, 0>(P, io, table, st, nlines, LT, shm);
+  else if (d == 1) launch_dir<T, 1>(P, io, table, st, nlines, LT, shm);
+  else launch_dir<T, 2>(P, io, table, st, nlines, LT, shm);
+}
+
+void launch_line_op(int d, const OpPlan& P, const LineIO& io, const double* table, cudaStream_t st) {
+  launch_line_op_t<double>(d, P, io, table, st);
+}
+void launch_line_op(int d, const OpPlan& P, const LineIOT<float>& io, const double* table, cudaStream_t st) {
+  launch_line_op_t<float>(d, P, io, table, st);
 }
 
 // ===========================================================================
@@ -439,62 +487,85 @@ void launch_cfft_axis(const FftPlan& fp, double2* data, int na, int nb, int64_t 
 // FISHPACK y solve: TRID0 (src/poisson_fishpack.f90:20-57) per (kx, kz) on complex data
 // laid out (kz, j, kx) with kx fastest.
 // ===========================================================================
-__global__ void ysolve_kernel(double2* __restrict__ data, int nxh, int ny, int nz, const double* __restrict__ pa,
-                              const double* __restrict__ pb, const double* __restrict__ pc,
-                              const double* __restrict__ lamx, const double* __restrict__ lamz) {
-  extern __shared__ double sD[];  // [ny][blockDim]
-  const int t = threadIdx.x;
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + t;
-  if (g >= (int64_t)nxh * nz) return;
-  const int kz = (int)(g / nxh), kx = (int)(g - (int64_t)kz * nxh);
-  const double lx = lamx[kx], lz = lamz[kz];
-  double* D = sD + t;
-  const int bd = blockDim.x;
-  double2* T = data + (int64_t)kz * ny * nxh + kx;
-  const int64_t js = nxh;
-  double bb = (pb[0] + lx) + lz;
-  double Z = 1.0 / bb;
-  D[0] = pc[0] * Z;
-  double2 tp = T[0];
-  tp.x *= Z; tp.y *= Z;
-  T[0] = tp;
-  for (int j = 1; j < ny - 1; ++j) {
-    bb = (pb[j] + lx) + lz;
-    Z = 1.0 / (bb - pa[j] * D[(j - 1) * bd]);
-    D[j * bd] = pc[j] * Z;
-    double2 v = T[j * js];
-    v.x = (v.x - pa[j] * tp.x) * Z;
-    v.y = (v.y - pa[j] * tp.y) * Z;
-    T[j * js] = v;
-    tp = v;
+// One CTA per `lt` consecutive (kx, kz) columns: the columns are staged in shared memory with
+// coalesced row loads by all threads, swept by `lt` threads (one column each), and written back.
+__global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data, int nxh, int ny, int nz,
+                                                     const double* __restrict__ pa, const double* __restrict__ pb,
+                                                     const double* __restrict__ pc, const double* __restrict__ lamx,
+                                                     const double* __restrict__ lamz, int lt) {
+  extern __shared__ __align__(16) double2 sT[];  // [ny][lt] right-hand sides / solution
+  double* sD = reinterpret_cast<double*>(sT + (size_t)ny * lt);  // [ny][lt] forward-sweep factors
+  const int tid = threadIdx.x;
+  const int l = tid % lt;
+  const int64_t nl = (int64_t)nxh * nz;
+  const int64_t g = (int64_t)blockIdx.x * lt + l;
+  const bool ok = g < nl;
+  const int kz = ok ? (int)(g / nxh) : 0;
+  const int kx = ok ? (int)(g - (int64_t)kz * nxh) : 0;
+  double2* col = data + (int64_t)kz * ny * nxh + kx;
+  const int jstep = blockDim.x / lt;
+  if (ok)
+    for (int j = tid / lt; j < ny; j += jstep) sT[j * lt + l] = col[(int64_t)j * nxh];
+  __syncthreads();
+  if (tid < lt && ok) {
+    double2* T = sT + l;
+    double* D = sD + l;
+    const double lx = lamx[kx], lz = lamz[kz];
+    double bb = (pb[0] + lx) + lz;
+    double Z = 1.0 / bb;
+    D[0] = pc[0] * Z;
+    double2 tp = T[0];
+    tp.x *= Z; tp.y *= Z;
+    T[0] = tp;
+    for (int j = 1; j < ny - 1; ++j) {
+      bb = (pb[j] + lx) + lz;
+      Z = 1.0 / (bb - pa[j] * D[(j - 1) * lt]);
+      D[j * lt] = pc[j] * Z;
+      double2 v = T[j * lt];
+      v.x = (v.x - pa[j] * tp.x) * Z;
+      v.y = (v.y - pa[j] * tp.y) * Z;
+      T[j * lt] = v;
+      tp = v;
+    }
+    bb = (pb[ny - 1] + lx) + lz;
+    Z = bb - pa[ny - 1] * D[(ny - 2) * lt];
+    double2 v = T[(ny - 1) * lt];
+    // TRID0's singular-pivot pin: the last unknown is set to zero when the pivot vanishes
+    if (fabs(Z) > 1.0e-10) {
+      v.x = (v.x - pa[ny - 1] * tp.x) / Z;
+      v.y = (v.y - pa[ny - 1] * tp.y) / Z;
+    } else {
+      v.x = 0.0;
+      v.y = 0.0;
+    }
+    T[(ny - 1) * lt] = v;
+    for (int j = ny - 2; j >= 0; --j) {
+      double2 u = T[j * lt];
+      u.x = u.x - D[j * lt] * v.x;
+      u.y = u.y - D[j * lt] * v.y;
+      T[j * lt] = u;
+      v = u;
+    }
   }
-  bb = (pb[ny - 1] + lx) + lz;
-  Z = bb - pa[ny - 1] * D[(ny - 2) * bd];
-  double2 v = T[(ny - 1) * js];
-  if (fabs(Z) > 1.0e-10) {
-    v.x = (v.x - pa[ny - 1] * tp.x) / Z;
-    v.y = (v.y - pa[ny - 1] * tp.y) / Z;
-  } else {
-    v.x = 0.0;
-    v.y = 0.0;
-  }
-  T[(ny - 1) * js] = v;
-  for (int j = ny - 2; j >= 0; --j) {
-    double2 u = T[j * js];
-    u.x = u.x - D[j * bd] * v.x;
-    u.y = u.y - D[j * bd] * v.y;
-    T[j * js] = u;
-    v = u;
-  }
+  __syncthreads();
+  if (ok)
+    for (int j = tid / lt; j < ny; j += jstep) col[(int64_t)j * nxh] = sT[j * lt + l];
 }
 
 void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* pa, const double* pb, const double* pc,
                    const double* lamx, const double* lamz, cudaStream_t st) {
-  const int bs = 64;
+  if (ny < 2) throw std::runtime_error("ysolve: ny must be at least 2");
+  int lt = 32;
+  while (lt > 4 && (size_t)ny * lt * 24 > 110 * 1024) lt /= 2;
+  const size_t shm = (size_t)ny * lt * 24;
+  if (shm > 200 * 1024) throw std::runtime_error("ysolve: ny too large for the shared-memory tile");
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(ysolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
+  }
   const int64_t n = (int64_t)nxh * nz;
-  const size_t shm = (size_t)ny * bs * sizeof(double);
-  cudaFuncSetAttribute(ysolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-  ysolve_kernel<<<(unsigned)((n + bs - 1) / bs), bs, shm, st>>>(data, nxh, ny, nz, pa, pb, pc, lamx, lamz);
+  ysolve_kernel<<<(unsigned)((n + lt - 1) / lt), 128, shm, st>>>(data, nxh, ny, nz, pa, pb, pc, lamx, lamz, lt);
 }
 
 __global__ void spectral_divide_kernel(double2* __restrict__ data, int nxh, int ny, int nz,

@@ -9,27 +9,35 @@
 namespace chs {
 
 // Input expression of a line operator, evaluated while a tile is staged:
-//   E_A     f = s * A
-//   E_AB    f = s * (A * B)
-//   E_ApB   f = s * (A + c1 * B)
-//   E_ApBC  f = s * (A + c1 * B) * C
-enum InMode { E_A = 0, E_AB = 1, E_ApB = 2, E_ApBC = 3 };
+// f = term0 + term1, each term one of
+//   T_X     s * X
+//   T_XY    s * (X * Y)
+//   T_XpY   s * (X + c * Y)
+enum TermMode { T_NONE = 0, T_X = 1, T_XY = 2, T_XpY = 3 };
 
-struct LineIO {
-  const double* A;
-  const double* B;
-  const double* C;
-  int emode;
-  double s, c1;
-  const double* fbc;  // boundary values, layout [4][nlines] (line order of the kernel), or null
-  double* out;
+template <typename T>
+struct TermT {
+  const T* X;
+  const T* Y;
+  int mode;
+  double s, c;
+};
+using Term = TermT<double>;
+
+template <typename T>
+struct LineIOT {
+  TermT<T> t[2];
+  const T* fbc;       // boundary values, layout [4][nlines] (line order of the kernel), or null
+  T* out;
   int accumulate;     // 0: out = g * r ; 1: out += g * r
   double g;
   int n1, n2, n3;     // extents of the INPUT array (x fastest)
 };
+using LineIO = LineIOT<double>;
 
 // Launch one plan over all lines of direction d.  `table` holds the LHS/mapping arrays.
 void launch_line_op(int d, const OpPlan& plan, const LineIO& io, const double* table, cudaStream_t st);
+void launch_line_op(int d, const OpPlan& plan, const LineIOT<float>& io, const double* table, cudaStream_t st);
 
 // number of lines of a direction for an input array of extents n1 x n2 x n3
 inline int64_t num_lines(int d, int n1, int n2, int n3) {

@@ -126,7 +126,7 @@ struct chs_handle {
   double *qydx, *qyix, *qydy, *qyiy, *qydz, *qyiz;
   double *qzdx, *qzix, *qziy, *qzdy, *qziz, *qzdz;
   double *div, *qxdx_cpc, *qydy_cpc, *qzdz_cpc;
-  double *fb_qx, *fb_qy, *fb_qz, *fb_pr, *fb_mpr, *fb_conv2, *fb_visc2, *fb_maxp;
+  double *fb_qx, *fb_qy, *fb_qz, *fb_pr, *fb_mpr, *fb_conv2, *fb_visc2, *fb_comb, *fb_maxp;
   double *wy, *partial, *scal;
   double vol = 0.0;
   int npart = 0;
@@ -179,17 +179,26 @@ namespace {
 Pair P2(const int v[2]) { return Pair{{v[0], v[1]}}; }
 void upload_table(chs_handle* H);
 
+// input expression: up to two terms (see LineIO)
 struct Src {
-  const double* A;
-  const double* B = nullptr;
-  const double* C = nullptr;
-  int mode = E_A;
-  double s = 1.0, c1 = 0.0;
+  Term t[2] = {{nullptr, nullptr, T_NONE, 0.0, 0.0}, {nullptr, nullptr, T_NONE, 0.0, 0.0}};
+  int narrays() const {
+    int n = 0;
+    for (const auto& x : t) n += (x.X ? 1 : 0) + (x.Y ? 1 : 0);
+    return n;
+  }
 };
-Src src(const double* a, double s = 1.0) { Src x; x.A = a; x.s = s; return x; }
-Src prod(const double* a, const double* b, double s) { Src x; x.A = a; x.B = b; x.mode = E_AB; x.s = s; return x; }
+Src src(const double* a, double s = 1.0) { Src x; x.t[0] = Term{a, nullptr, T_X, s, 0.0}; return x; }
+Src prod(const double* a, const double* b, double s) { Src x; x.t[0] = Term{a, b, T_XY, s, 0.0}; return x; }
 Src lin(const double* a, const double* b, double c1, double s) {
-  Src x; x.A = a; x.B = b; x.c1 = c1; x.mode = E_ApB; x.s = s; return x;
+  Src x; x.t[0] = Term{a, b, T_XpY, s, c1}; return x;
+}
+// a + w * b, for two single-term expressions
+Src plus(const Src& a, const Src& b, double w) {
+  Src x = a;
+  x.t[1] = b.t[0];
+  x.t[1].s *= w;
+  return x;
 }
 
 // run one operator: direction d, family fam, operation bc, boundary planes fbc (null = absent)
@@ -199,7 +208,8 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const double* fbc, const Src
   const OpPlan& P = H->plan(d, fam, bc, fbc != nullptr);
   if (H->book.table.size() != tsz) upload_table(H);
   LineIO io{};
-  io.A = in.A; io.B = in.B; io.C = in.C; io.emode = in.mode; io.s = in.s; io.c1 = in.c1;
+  io.t[0] = in.t[0];
+  io.t[1] = in.t[1];
   io.fbc = fbc;
   io.out = out;
   io.accumulate = accumulate ? 1 : 0;
@@ -207,7 +217,7 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const double* fbc, const Src
   io.n1 = n_in[0]; io.n2 = n_in[1]; io.n3 = n_in[2];
   const double nin_tot = (double)n_in[0] * n_in[1] * n_in[2];
   const double nout_tot = nin_tot / P.nin * P.nout;
-  const int narr = 1 + (in.B ? 1 : 0) + (in.C ? 1 : 0);
+  const int narr = in.narrays();
   const double bytes = 8.0 * (narr * nin_tot + (accumulate ? 2.0 : 1.0) * nout_tot);
   cudaEvent_t e0 = H->prof_begin();
   launch_line_op(d, P, io, H->table, H->st);
@@ -222,6 +232,22 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const double* fbc, const Src
     __VA_ARGS__;                                         \
     (H)->prof_end(e0_, kind, -1, (bytes));               \
   } while (0)
+
+// op(a; fbc1) + w*op(b; fbc2).  When both terms use the same plan the sum runs as one launch
+// on the combined input (the operator is linear in its input and boundary values); fcomb must
+// then hold fbc1 + w*fbc2 when the two planes differ.
+void run_pair(chs_handle* H, int d, int fam, Pair bc1, const double* f1, const Src& a, Pair bc2, const double* f2,
+              const Src& b, double w, const int n_in[3], double* out, bool accumulate, const double* fcomb) {
+  const bool same = bc1.v[0] == bc2.v[0] && bc1.v[1] == bc2.v[1] && ((f1 == nullptr) == (f2 == nullptr)) &&
+                    (f1 == f2 || fcomb != nullptr);
+  if (same) {
+    const double* f = (f1 == f2) ? f1 : fcomb;
+    run_op(H, d, fam, bc1, f, plus(a, b, w), n_in, out, accumulate, 1.0);
+  } else {
+    run_op(H, d, fam, bc1, f1, a, n_in, out, accumulate, 1.0);
+    run_op(H, d, fam, bc2, f2, b, n_in, out, true, w);
+  }
+}
 
 void build_bcs(chs_handle* H, const chs_config* c) {
   std::memcpy(H->ibc, c->nominal_bc, sizeof(H->ibc));
@@ -375,6 +401,7 @@ void setup_device(chs_handle* H, const chs_config* c) {
   H->fb_qx = H->dalloc<double>(4 * nl); H->fb_qy = H->dalloc<double>(4 * nl); H->fb_qz = H->dalloc<double>(4 * nl);
   H->fb_pr = H->dalloc<double>(4 * nl); H->fb_mpr = H->dalloc<double>(4 * nl);
   H->fb_conv2 = H->dalloc<double>(4 * nl); H->fb_visc2 = H->dalloc<double>(4 * nl);
+  H->fb_comb = H->dalloc<double>(4 * nl);
   H->fb_maxp = H->dalloc<double>(4 * nl);
   launch_fbcy_const(H->fb_qx, nc0, nc2, H->fbcy[V_QX][0], H->fbcy[V_QX][1], H->st);
   launch_fbcy_const(H->fb_qy, nc0, nc2, H->fbcy[V_QY][0], H->fbcy[V_QY][1], H->st);
@@ -590,32 +617,39 @@ void substep_body(chs_handle* H, int isub) {
     H->launches += 3;
   }
 
-  // ---- 2. x-momentum (:796-966)
-  run_op(H, 0, D1C2P, H->mbcx_cov1, any, prod(H->qxix, H->qxix, -1.0), s_ccc, H->mx, false, 1.0);
-  run_op(H, 1, D1P2C, H->mbcy_cov1, nullptr, prod(H->qyix, H->qxiy, -1.0), s_ppc, H->mx, true, 1.0);
-  run_op(H, 2, D1P2C, H->mbcz_cov1, nullptr, prod(H->qzix, H->qxiz, -1.0), s_pcp, H->mx, true, 1.0);
+  // ---- 2. momentum RHS.  The convection and diffusion terms of one direction share the
+  // operator (same family and boundary pair), and the operator is linear in its input and
+  // boundary values, so op(conv) + rre*op(diff) runs as op(conv + rre*diff) in one launch.
+  // x-momentum (:796-966)
+  run_pair(H, 0, D1C2P, H->mbcx_cov1, any, prod(H->qxix, H->qxix, -1.0), H->mbcx_tau1, any,
+           lin(H->qxdx, H->div, -third, 2.0), rre, s_ccc, H->mx, false, nullptr);
+  run_pair(H, 1, D1P2C, H->mbcy_cov1, nullptr, prod(H->qyix, H->qxiy, -1.0), H->mbcy_tau1, nullptr,
+           lin(H->qxdy, H->qydx, 1.0, 1.0), rre, s_ppc, H->mx, true, nullptr);
+  run_pair(H, 2, D1P2C, H->mbcz_cov1, nullptr, prod(H->qzix, H->qxiz, -1.0), H->mbcz_tau1, nullptr,
+           lin(H->qxdz, H->qzdx, 1.0, 1.0), rre, s_pcp, H->mx, true, nullptr);
   run_op(H, 0, D1C2P, bx_pr, any, src(H->pres, -1.0), s_ccc, H->px, false, 1.0);
-  run_op(H, 0, D1C2P, H->mbcx_tau1, any, lin(H->qxdx, H->div, -third, 2.0), s_ccc, H->mx, true, rre);
-  run_op(H, 1, D1P2C, H->mbcy_tau1, nullptr, lin(H->qxdy, H->qydx, 1.0, 1.0), s_ppc, H->mx, true, rre);
-  run_op(H, 2, D1P2C, H->mbcz_tau1, nullptr, lin(H->qxdz, H->qzdx, 1.0, 1.0), s_pcp, H->mx, true, rre);
   // y-momentum (:978-1242)
-  run_op(H, 0, D1P2C, H->mbcx_cov2, nullptr, prod(H->qxiy, H->qyix, -1.0), s_ppc, H->my, false, 1.0);
-  run_op(H, 1, D1C2P, H->mbcy_cov2, H->fbcy_velo ? H->fb_conv2 : H->fb_maxp, prod(H->qyiy, H->qyiy, -1.0), s_ccc,
-         H->my, true, 1.0);
-  run_op(H, 2, D1P2C, H->mbcz_cov2, nullptr, prod(H->qyiz, H->qziy, -1.0), s_cpp, H->my, true, 1.0);
+  run_pair(H, 0, D1P2C, H->mbcx_cov2, nullptr, prod(H->qxiy, H->qyix, -1.0), H->mbcx_tau2, nullptr,
+           lin(H->qxdy, H->qydx, 1.0, 1.0), rre, s_ppc, H->my, false, nullptr);
+  if (H->fbcy_velo) {
+    PROF(H, 3, 24.0 * 4 * nc0 * nc2,
+         launch_axpby(H->fb_comb, H->fb_conv2, 1.0, H->fb_visc2, rre, (int64_t)4 * nc0 * nc2, st));
+    H->launches++;
+  }
+  run_pair(H, 1, D1C2P, H->mbcy_cov2, H->fbcy_velo ? H->fb_conv2 : H->fb_maxp, prod(H->qyiy, H->qyiy, -1.0),
+           H->mbcy_tau2, H->fbcy_velo ? H->fb_visc2 : H->fb_maxp, lin(H->qydy, H->div, -third, 2.0), rre, s_ccc,
+           H->my, true, H->fb_comb);
+  run_pair(H, 2, D1P2C, H->mbcz_cov2, nullptr, prod(H->qyiz, H->qziy, -1.0), H->mbcz_tau2, nullptr,
+           lin(H->qzdy, H->qydz, 1.0, 1.0), rre, s_cpp, H->my, true, nullptr);
   run_op(H, 1, D1C2P, by_pr, fympr, src(H->pres, -1.0), s_ccc, H->py, false, 1.0);
-  run_op(H, 0, D1P2C, H->mbcx_tau2, nullptr, lin(H->qxdy, H->qydx, 1.0, 1.0), s_ppc, H->my, true, rre);
-  run_op(H, 1, D1C2P, H->mbcy_tau2, H->fbcy_velo ? H->fb_visc2 : H->fb_maxp, lin(H->qydy, H->div, -third, 2.0), s_ccc,
-         H->my, true, rre);
-  run_op(H, 2, D1P2C, H->mbcz_tau2, nullptr, lin(H->qzdy, H->qydz, 1.0, 1.0), s_cpp, H->my, true, rre);
   // z-momentum (:1262-1457)
-  run_op(H, 0, D1P2C, H->mbcx_cov3, nullptr, prod(H->qxiz, H->qzix, -1.0), s_pcp, H->mz, false, 1.0);
-  run_op(H, 1, D1P2C, H->mbcy_cov3, nullptr, prod(H->qyiz, H->qziy, -1.0), s_cpp, H->mz, true, 1.0);
-  run_op(H, 2, D1C2P, H->mbcz_cov3, any, prod(H->qziz, H->qziz, -1.0), s_ccc, H->mz, true, 1.0);
+  run_pair(H, 0, D1P2C, H->mbcx_cov3, nullptr, prod(H->qxiz, H->qzix, -1.0), H->mbcx_tau3, nullptr,
+           lin(H->qxdz, H->qzdx, 1.0, 1.0), rre, s_pcp, H->mz, false, nullptr);
+  run_pair(H, 1, D1P2C, H->mbcy_cov3, nullptr, prod(H->qyiz, H->qziy, -1.0), H->mbcy_tau3, nullptr,
+           lin(H->qzdy, H->qydz, 1.0, 1.0), rre, s_cpp, H->mz, true, nullptr);
+  run_pair(H, 2, D1C2P, H->mbcz_cov3, any, prod(H->qziz, H->qziz, -1.0), H->mbcz_tau3, any,
+           lin(H->qzdz, H->div, -third, 2.0), rre, s_ccc, H->mz, true, nullptr);
   run_op(H, 2, D1C2P, bz_pr, any, src(H->pres, -1.0), s_ccc, H->pz, false, 1.0);
-  run_op(H, 0, D1P2C, H->mbcx_tau3, nullptr, lin(H->qxdz, H->qzdx, 1.0, 1.0), s_pcp, H->mz, true, rre);
-  run_op(H, 1, D1P2C, H->mbcy_tau3, nullptr, lin(H->qzdy, H->qydz, 1.0, 1.0), s_cpp, H->mz, true, rre);
-  run_op(H, 2, D1C2P, H->mbcz_tau3, any, lin(H->qzdz, H->div, -third, 2.0), s_ccc, H->mz, true, rre);
 
   // ---- 3. fractional step, mass flux
   PROF(H, 3, 40.0 * H->n_pcc,

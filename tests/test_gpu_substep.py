@@ -25,8 +25,12 @@ def _pair(cfg, fields):
 def _compare(o, g, tol):
     ref = o.get_fields()
     got = g.get_fields()
-    for name, a, b in zip(("qx", "qy", "qz", "p", "pcor"), got, ref):
+    for name, a, b in zip(("qx", "qy", "qz", "p"), got[:4], ref[:4]):
         assert rel(a, b) < tol, (name, rel(a, b))
+    # phi solves L phi = div(u*)/(alpha dt), where div(u*) cancels to round-off level; its error is
+    # measured on the pressure scale
+    err = np.linalg.norm(got[4] - ref[4]) / max(np.linalg.norm(ref[3]), 1e-300)
+    assert err < tol, ("pcor", err)
 
 
 @pytest.mark.parametrize("acc", [1, 3, 4])
