@@ -74,6 +74,8 @@ __device__ __forceinline__ int64_t pos_stride(int n1, int n2) {
   return DIR == 0 ? 1 : (DIR == 1 ? (int64_t)n1 : (int64_t)n1 * n2);
 }
 
+constexpr int kStageBatch = 8;
+
 template <typename T, int DIR, int FAM>
 __global__ void __launch_bounds__(256) line_op_kernel(const __grid_constant__ OpPlan P,
                                                       const __grid_constant__ LineIOT<T> io,
@@ -93,17 +95,28 @@ __global__ void __launch_bounds__(256) line_op_kernel(const __grid_constant__ Op
   const int tid = threadIdx.x;
   const int64_t ps = pos_stride<DIR>(io.n1, io.n2);
 
-  // ---- stage the tile
+  // ---- stage the tile; loads are issued in batches of kStageBatch per thread so that enough
+  // of them are in flight to cover HBM latency
   if (DIR == 0) {
     // LT consecutive rows are one contiguous run of LT*nin values
     const int tot = LT * nin;
     const int64_t g0 = (int64_t)L0 * nin;
     const int64_t gmax = (int64_t)nlines * nin;
-    for (int e = tid; e < tot; e += nt) {
-      const int l = e / nin, p = e - l * nin;
-      T v = T(0);
-      if (g0 + e < gmax) v = eval_expr(io, g0 + e);
-      s[p * ld + l] = v;
+    for (int e0 = tid; e0 < tot; e0 += kStageBatch * nt) {
+      T v[kStageBatch];
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const int e = e0 + u * nt;
+        v[u] = (e < tot && g0 + e < gmax) ? eval_expr(io, g0 + e) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const int e = e0 + u * nt;
+        if (e < tot) {
+          const int l = e / nin, p = e - l * nin;
+          s[p * ld + l] = v[u];
+        }
+      }
     }
   } else {
     // each thread owns one line of the tile (nt is a multiple of LT)
@@ -111,7 +124,20 @@ __global__ void __launch_bounds__(256) line_op_kernel(const __grid_constant__ Op
     const int L = L0 + l;
     const bool ok = L < nlines;
     const int64_t base = ok ? line_base<DIR>(L, nin, io.n1) : 0;
-    for (int p = tid / LT; p < nin; p += nt / LT) s[p * ld + l] = ok ? eval_expr(io, base + p * ps) : T(0);
+    const int step = nt / LT;
+    for (int p0 = tid / LT; p0 < nin; p0 += kStageBatch * step) {
+      T v[kStageBatch];
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const int p = p0 + u * step;
+        v[u] = (ok && p < nin) ? eval_expr(io, base + p * ps) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < kStageBatch; ++u) {
+        const int p = p0 + u * step;
+        if (p < nin) s[p * ld + l] = v[u];
+      }
+    }
   }
   for (int p = tid; p < nout; p += nt) {
     if (P.tdma) {
@@ -262,9 +288,10 @@ void launch_line_op_t(int d, const OpPlan& P, const LineIOT<T>& io, const double
   if (nl > 0x7fffffff) throw std::runtime_error("line operator: too many lines");
   const int nlines = (int)nl;
   const int nmax = P.nin > P.nout ? P.nin : P.nout;
-  // 64 lines per CTA while the tile fits in ~110 KB (two CTAs per SM), fewer for long lines
+  // up to 64 lines per CTA, fewer while the tile exceeds ~45 KB so that four or more CTAs
+  // (32+ warps) stay resident per SM
   int LT = 64;
-  while (LT > 16 && ((size_t)nmax * (LT + 1) + 5 * (size_t)nmax) * sizeof(T) > 110 * 1024) LT /= 2;
+  while (LT > 16 && ((size_t)nmax * (LT + 1) + 5 * (size_t)nmax) * sizeof(T) > 45 * 1024) LT /= 2;
   const size_t shm = ((size_t)nmax * (LT + 1) + 5 * (size_t)nmax) * sizeof(T);
   if (shm > (size_t)kLineSmemMax) throw std::runtime_error("line operator: line too long for the shared-memory tile");
   if (d == 0) launch_dir<T, 0>(P, io, table, st, nlines, LT, shm);
