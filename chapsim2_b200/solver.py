@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(_HERE, "libchapsim_gpu.so")
 
 CHS_QX, CHS_QY, CHS_QZ, CHS_PRES, CHS_PCOR, CHS_MX_RHS0, CHS_MY_RHS0, CHS_MZ_RHS0 = range(8)
 CHS_FP64, CHS_MIXED = 0, 1
+CHS_OK, CHS_ERR_ARG, CHS_ERR_CUDA, CHS_ERR_STATE, CHS_ERR_NUMERIC = range(5)
 _D = ctypes.POINTER(ctypes.c_double)
 
 
@@ -44,7 +45,8 @@ class ChsDiag(ctypes.Structure):
 EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field", "chs_momentum_substep",
             "chs_step", "chs_poisson_solve", "chs_poisson_solve_device", "chs_diagnostics", "chs_op3d",
             "chs_plan_inspect", "chs_sync", "chs_kernel_launches", "chs_last_error", "chs_momentum_substep_host",
-            "chs_time_steps", "chs_time_steps_host", "chs_host_alloc", "chs_host_free", "chs_profile_substep"]
+            "chs_time_steps", "chs_time_steps_host", "chs_host_alloc", "chs_host_free", "chs_profile_substep",
+            "chs_poisson_periodic_static"]
 
 
 class ChsKprof(ctypes.Structure):
@@ -86,8 +88,24 @@ def load():
     L.chs_host_free.argtypes = [ctypes.c_void_p]
     L.chs_profile_substep.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ChsKprof), ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int)]
+    L.chs_poisson_periodic_static.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_void_p,
+                                              ctypes.c_char_p, ctypes.c_size_t]
     _lib = L
     return L
+
+
+def poisson_periodic_static(d_rhs, nc, lengths, iacc, stream=None):
+    """Periodic Poisson solve in place on a device array (address d_rhs) with no device allocation.
+
+    Returns (status, message); status 0 is success.
+    """
+    L = load()
+    n = (ctypes.c_int * 3)(*[int(v) for v in nc])
+    ln = (ctypes.c_double * 3)(*[float(v) for v in lengths])
+    err = ctypes.create_string_buffer(512)
+    rc = L.chs_poisson_periodic_static(ctypes.c_void_p(d_rhs), n, ln, int(iacc), stream, err, 512)
+    return rc, err.value.decode()
 
 
 def _ptr(a):

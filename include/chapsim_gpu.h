@@ -155,6 +155,34 @@ long long chs_kernel_launches(const chs_handle* h);
 /* Last error message (NUL-terminated, truncated to len). */
 int chs_last_error(const chs_handle* h, char* buf, size_t len);
 
+/* Periodic 3D pressure Poisson solve that allocates nothing.  No counterpart in
+ * the reference (it is the spectral solve of poisson_000,
+ * src/poisson_1stderivcomp.f90:1016-1195, without a handle).
+ *
+ * For callers that cannot allocate device memory (a host code whose device
+ * memory is owned by its own pool, or a fixed-footprint deployment): solves
+ * L phi = rhs in place on the caller's device array d_rhs (nc[0]*nc[1]*nc[2]
+ * doubles, x fastest) for a box of edge lengths len[3], periodic in x, y and z,
+ * with the modified wavenumbers of the C2P derivative of scheme iacc (1 CD2,
+ * 2 CD4, 3 CP4, 4 CP6).  The result equals chs_poisson_solve_device on a handle
+ * of the same grid and scheme.  Kernels run on `stream` (a cudaStream_t; NULL
+ * is the legacy default stream).
+ *
+ * Work memory is a fixed module-level device array of 16 MiB + 144 KiB, so the
+ * limits are (nc[0]/2+1)*nc[1]*nc[2] <= 1048576 complex values and each nc[d]
+ * <= 4096, each of the form 2^a 3^b; larger grids return CHS_ERR_ARG with a
+ * message.  Nothing in it needs to start at zero: every value is written before
+ * it is read.  The first call on a device, and any call whose nc, len or iacc
+ * differ from the previous call's, does set-up: it writes the FFT and
+ * wavenumber tables with a host-to-device copy on `stream` and synchronizes
+ * that stream, so make such a call before any stream capture.  All calls on one
+ * device share the one work array: calls that overlap in time (on different
+ * streams, or from threads that do not order them) race and corrupt each other;
+ * order them on one stream.  Errors are written to err (errlen bytes, may be
+ * NULL) and returned as chs_status. */
+int chs_poisson_periodic_static(double* d_rhs, const int nc[3], const double len[3], int iacc, void* stream,
+                                char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif
