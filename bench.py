@@ -248,6 +248,29 @@ def run_ours(args, cfg, fields, world, rank, local, dist):
         "diagnostics": {"max_div": diag["max_div"], "bulk_u": diag["bulk_u"], "bulk_ke": diag["bulk_ke"],
                         "nan": diag["nan_flag"]},
     }
+    # the mixed-precision form on the same workload and step count (FP32 fields/operators,
+    # FP64 Poisson, mass-flux mean and checks)
+    m = S.Solver(cfg, device=local, precision=S.CHS_MIXED)
+    m.set_fields(*fields)
+    m.Solve_momentum_eq(0)
+    m.step(args.warmup)
+    m.sync()
+    barrier(dist)
+    ms_m = m.time_steps(args.steps)
+    barrier(dist)
+    ms_m = max_over_ranks(dist, ms_m)
+    m.step(args.steps)  # matches the FP64 handle's e2e steps
+    sh = cfg.shapes()[0]
+    pm = m.get_fields()[0].reshape(sh).mean(axis=(0, 2))
+    pd = g.get_fields()[0].reshape(sh).mean(axis=(0, 2))
+    out["forms"] = {
+        "fp64": {"value": value, "ms_per_step": ms_max / args.steps},
+        "mixed": {"value": world * cfg.ncell * sub / (ms_m * 1e-3) / 1e6, "ms_per_step": ms_m / args.steps,
+                  "speedup_vs_fp64": ms_max / ms_m,
+                  "u_mean_profile_rel_l2_vs_fp64": float(np.linalg.norm(pm - pd) / np.linalg.norm(pd)),
+                  "steps_compared": 1 + args.warmup + 2 * args.steps},
+    }
+    m.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         nsub = 6

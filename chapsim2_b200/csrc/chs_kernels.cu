@@ -250,6 +250,110 @@ __global__ void __launch_bounds__(256) line_op_kernel(const __grid_constant__ Op
   }
 }
 
+// ---------------------------------------------------------------------------
+// Explicit operators (no line solve): one thread per output value, flattened over the output
+// array in memory order so that loads and stores are coalesced.  Neighbour values along the
+// line come from L1/L2; every row is independent.
+// ---------------------------------------------------------------------------
+template <int FAM, typename T, typename F>
+__device__ __forceinline__ T bulk_fn(const F& f, int i, T r1, T r2) {
+  T v;
+  if (FAM == M1P2C) v = r1 * (f(i) + f(i + 1));
+  else if (FAM == M1C2P) v = r1 * (f(i) + f(i - 1));
+  else if (FAM == D1C2C || FAM == D1P2P) v = r1 * (f(i + 1) - f(i - 1));
+  else if (FAM == D1C2P) v = r1 * (f(i) - f(i - 1));
+  else v = r1 * (f(i + 1) - f(i));  // D1P2C
+  if (r2 != T(0)) {
+    if (FAM == M1P2C) v += r2 * (f(i - 1) + f(i + 2));
+    else if (FAM == M1C2P) v += r2 * (f(i + 1) + f(i - 2));
+    else if (FAM == D1C2C || FAM == D1P2P) v += r2 * (f(i + 2) - f(i - 2));
+    else if (FAM == D1C2P) v += r2 * (f(i + 1) - f(i - 2));
+    else v += r2 * (f(i + 2) - f(i - 1));
+  }
+  return v;
+}
+
+template <typename T, int DIR, int FAM>
+__global__ void __launch_bounds__(256) stencil_op_kernel(const __grid_constant__ OpPlan P,
+                                                         const __grid_constant__ LineIOT<T> io,
+                                                         const double* __restrict__ table, int nlines, int m1,
+                                                         int m2) {
+  // output array (m1, m2, m3), x fastest: blockIdx.y is the outermost index k, the x grid
+  // covers the (i, j) plane
+  const int nin = P.nin, nout = P.nout;
+  const int plane = m1 * m2;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= plane) return;
+  const int k = blockIdx.y;
+  const int j = q / m1;
+  const int i = q - j * m1;
+  int p, L;
+  int64_t ibase, istride;
+  if (DIR == 0) {
+    p = i;
+    L = j + m2 * k;
+    ibase = (int64_t)L * nin;
+    istride = 1;
+  } else if (DIR == 1) {
+    p = j;
+    L = i + m1 * k;
+    ibase = (int64_t)k * nin * m1 + i;
+    istride = m1;
+  } else {
+    p = k;
+    L = q;
+    ibase = q;
+    istride = plane;
+  }
+  const int64_t o = (int64_t)plane * k + q;
+  const T dd = T(P.dd), r1 = T(P.r1), r2 = T(P.r2), g = T(io.g);
+  auto f = [&](int qq) -> T { return eval_expr(io, ibase + (int64_t)qq * istride); };
+  T v;
+  if (p >= P.b_lo && p <= P.b_hi) {
+    v = bulk_fn<FAM>(f, p, r1, r2) * dd;
+  } else {
+    v = T(0);
+    for (int s = 0; s < P.nspec; ++s) {
+      if (P.sp[s].row != p) continue;
+      const SpecialRow& R = P.sp[s];
+      T acc = T(0);
+      for (int t = 0; t < R.nt; ++t) acc += T(R.w[t]) * f(R.idx[t]);
+      for (int u = 0; u < 4; ++u)
+        if (R.wb[u] != 0.0) acc += T(R.wb[u]) * io.fbc[u * nlines + L];
+      v = acc * dd;
+    }
+  }
+  if (P.lmap >= 0) v *= T(table[P.lmap + p]);
+  if (P.neu1 && p == 0) v = io.fbc[L];
+  if (P.neu2 && p == nout - 1) v = io.fbc[nlines + L];
+  io.out[o] = io.accumulate ? io.out[o] + g * v : g * v;
+}
+
+template <typename T, int DIR>
+static void launch_stencil_dir(const OpPlan& P, const LineIOT<T>& io, const double* table, cudaStream_t st,
+                               int nlines) {
+  int m[3] = {io.n1, io.n2, io.n3};
+  m[DIR] = P.nout;
+  if ((int64_t)m[0] * m[1] > 0x7fffffff || m[2] > 65535)
+    throw std::runtime_error("explicit operator: array extents out of range");
+  const int plane = m[0] * m[1];
+  dim3 grid((unsigned)((plane + 255) / 256), (unsigned)m[2]);
+  switch (P.fam) {
+#define CHS_CASE(F)                                                                                 \
+  case F:                                                                                           \
+    stencil_op_kernel<T, DIR, F><<<grid, 256, 0, st>>>(P, io, table, nlines, m[0], m[1]);           \
+    break;
+    CHS_CASE(D1C2C)
+    CHS_CASE(D1P2P)
+    CHS_CASE(D1C2P)
+    CHS_CASE(D1P2C)
+    CHS_CASE(M1C2P)
+    CHS_CASE(M1P2C)
+#undef CHS_CASE
+    default: throw std::runtime_error("bad family");
+  }
+}
+
 constexpr int kLineSmemMax = 200 * 1024;
 
 template <typename T, int DIR>
@@ -287,6 +391,13 @@ void launch_line_op_t(int d, const OpPlan& P, const LineIOT<T>& io, const double
   const int64_t nl = num_lines(d, io.n1, io.n2, io.n3);
   if (nl > 0x7fffffff) throw std::runtime_error("line operator: too many lines");
   const int nlines = (int)nl;
+  if (!P.tdma) {
+    // explicit scheme: every output row is independent
+    if (d == 0) launch_stencil_dir<T, 0>(P, io, table, st, nlines);
+    else if (d == 1) launch_stencil_dir<T, 1>(P, io, table, st, nlines);
+    else launch_stencil_dir<T, 2>(P, io, table, st, nlines);
+    return;
+  }
   const int nmax = P.nin > P.nout ? P.nin : P.nout;
   // up to 64 lines per CTA, fewer while the tile exceeds ~45 KB so that four or more CTAs
   // (32+ warps) stay resident per SM
@@ -392,21 +503,34 @@ static int fft_lines_per_cta(int n) {
   return l;
 }
 
-// real rows -> half spectra; two real rows per complex transform
-__global__ void rfft_x_kernel(const __grid_constant__ FftPlan fp, const double* __restrict__ in,
+// real rows -> half spectra; two real rows per complex transform (rows of type R, FP64 transform)
+template <typename R>
+__global__ void rfft_x_kernel(const __grid_constant__ FftPlan fp, const R* __restrict__ in,
                               double2* __restrict__ out, int nrows, int lpc) {
   extern __shared__ double2 sh[];
   const int n = fp.n, nh = n / 2 + 1;
   double2* b0 = sh;
   double2* b1 = sh + (size_t)lpc * n;
   const int pair0 = blockIdx.x * lpc;
-  for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
-    const int l = t / n, p = t - l * n;
-    const int ra = 2 * (pair0 + l), rb = ra + 1;
-    double a = 0.0, b = 0.0;
-    if (ra < nrows) a = in[(int64_t)ra * n + p];
-    if (rb < nrows) b = in[(int64_t)rb * n + p];
-    b0[t] = make_double2(a, b);
+  for (int t0 = threadIdx.x; t0 < lpc * n; t0 += 4 * blockDim.x) {
+    double a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = t0 + u * blockDim.x;
+      a[u] = 0.0;
+      b[u] = 0.0;
+      if (t < lpc * n) {
+        const int l = t / n, p = t - l * n;
+        const int ra = 2 * (pair0 + l), rb = ra + 1;
+        if (ra < nrows) a[u] = (double)in[(int64_t)ra * n + p];
+        if (rb < nrows) b[u] = (double)in[(int64_t)rb * n + p];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < lpc * n) b0[t] = make_double2(a[u], b[u]);
+    }
   }
   __syncthreads();
   double2* r = smem_fft(b0, b1, lpc, fp, -1);
@@ -424,24 +548,42 @@ __global__ void rfft_x_kernel(const __grid_constant__ FftPlan fp, const double* 
   }
 }
 
+template <typename R>
 __global__ void irfft_x_kernel(const __grid_constant__ FftPlan fp, const double2* __restrict__ in,
-                               double* __restrict__ out, int nrows, double scale, int lpc) {
+                               R* __restrict__ out, int nrows, double scale, int lpc) {
   extern __shared__ double2 sh[];
   const int n = fp.n, nh = n / 2 + 1;
   double2* b0 = sh;
   double2* b1 = sh + (size_t)lpc * n;
   const int pair0 = blockIdx.x * lpc;
-  for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
-    const int l = t / n, k = t - l * n;
-    const int ra = 2 * (pair0 + l), rb = ra + 1;
-    const bool hi = k > n / 2;
-    const int kk = hi ? n - k : k;
-    double2 xa = make_double2(0.0, 0.0), xb = make_double2(0.0, 0.0);
-    if (ra < nrows) xa = in[(int64_t)ra * nh + kk];
-    if (rb < nrows) xb = in[(int64_t)rb * nh + kk];
-    if (kk == 0 || 2 * kk == n) { xa.y = 0.0; xb.y = 0.0; }
-    if (hi) { xa.y = -xa.y; xb.y = -xb.y; }
-    b0[t] = make_double2(xa.x - xb.y, xa.y + xb.x);  // xa + i*xb
+  for (int t0 = threadIdx.x; t0 < lpc * n; t0 += 4 * blockDim.x) {
+    double2 xa[4], xb[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = t0 + u * blockDim.x;
+      xa[u] = make_double2(0.0, 0.0);
+      xb[u] = make_double2(0.0, 0.0);
+      if (t < lpc * n) {
+        const int l = t / n, k = t - l * n;
+        const int ra = 2 * (pair0 + l), rb = ra + 1;
+        const int kk = k > n / 2 ? n - k : k;
+        if (ra < nrows) xa[u] = in[(int64_t)ra * nh + kk];
+        if (rb < nrows) xb[u] = in[(int64_t)rb * nh + kk];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < lpc * n) {
+        const int k = t % n;
+        const bool hi = k > n / 2;
+        const int kk = hi ? n - k : k;
+        double2 A = xa[u], B = xb[u];
+        if (kk == 0 || 2 * kk == n) { A.y = 0.0; B.y = 0.0; }
+        if (hi) { A.y = -A.y; B.y = -B.y; }
+        b0[t] = make_double2(A.x - B.y, A.y + B.x);  // xa + i*xb
+      }
+    }
   }
   __syncthreads();
   double2* r = smem_fft(b0, b1, lpc, fp, +1);
@@ -449,8 +591,8 @@ __global__ void irfft_x_kernel(const __grid_constant__ FftPlan fp, const double2
     const int l = t / n, p = t - l * n;
     const int ra = 2 * (pair0 + l), rb = ra + 1;
     const double2 z = r[t];
-    if (ra < nrows) out[(int64_t)ra * n + p] = z.x * scale;
-    if (rb < nrows) out[(int64_t)rb * n + p] = z.y * scale;
+    if (ra < nrows) out[(int64_t)ra * n + p] = R(z.x * scale);
+    if (rb < nrows) out[(int64_t)rb * n + p] = R(z.y * scale);
   }
 }
 
@@ -462,15 +604,29 @@ __global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __
   double2* b1 = sh + (size_t)lpc * n;
   const int64_t g0 = (int64_t)blockIdx.x * lpc;
   const int64_t nlines = (int64_t)na * nb;
-  for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
-    const int p = t / lpc, l = t - p * lpc;
-    const int64_t g = g0 + l;
-    double2 v = make_double2(0.0, 0.0);
-    if (g < nlines) {
-      const int64_t b = g / na, a = g - b * na;
-      v = data[a + b * bstride + p * stride];
+  for (int t0 = threadIdx.x; t0 < lpc * n; t0 += 4 * blockDim.x) {
+    double2 v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = t0 + u * blockDim.x;
+      v[u] = make_double2(0.0, 0.0);
+      if (t < lpc * n) {
+        const int p = t / lpc, l = t - p * lpc;
+        const int64_t g = g0 + l;
+        if (g < nlines) {
+          const int64_t b = g / na, a = g - b * na;
+          v[u] = data[a + b * bstride + p * stride];
+        }
+      }
     }
-    b0[l * n + p] = v;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < lpc * n) {
+        const int p = t / lpc, l = t - p * lpc;
+        b0[l * n + p] = v[u];
+      }
+    }
   }
   __syncthreads();
   double2* r = smem_fft(b0, b1, lpc, fp, sign);
@@ -484,21 +640,27 @@ __global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __
   }
 }
 
-void launch_rfft_x(const FftPlan& fp, const double* in, double2* out, int nrows, cudaStream_t st) {
+template <typename R>
+void launch_rfft_x(const FftPlan& fp, const R* in, double2* out, int nrows, cudaStream_t st) {
   const int lpc = fft_lines_per_cta(fp.n);
   const int npairs = (nrows + 1) / 2;
   const size_t shm = 2 * (size_t)lpc * fp.n * sizeof(double2);
-  cudaFuncSetAttribute(rfft_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-  rfft_x_kernel<<<(npairs + lpc - 1) / lpc, 256, shm, st>>>(fp, in, out, nrows, lpc);
+  cudaFuncSetAttribute(rfft_x_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  rfft_x_kernel<R><<<(npairs + lpc - 1) / lpc, 256, shm, st>>>(fp, in, out, nrows, lpc);
 }
 
-void launch_irfft_x(const FftPlan& fp, const double2* in, double* out, int nrows, double scale, cudaStream_t st) {
+template <typename R>
+void launch_irfft_x(const FftPlan& fp, const double2* in, R* out, int nrows, double scale, cudaStream_t st) {
   const int lpc = fft_lines_per_cta(fp.n);
   const int npairs = (nrows + 1) / 2;
   const size_t shm = 2 * (size_t)lpc * fp.n * sizeof(double2);
-  cudaFuncSetAttribute(irfft_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-  irfft_x_kernel<<<(npairs + lpc - 1) / lpc, 256, shm, st>>>(fp, in, out, nrows, scale, lpc);
+  cudaFuncSetAttribute(irfft_x_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  irfft_x_kernel<R><<<(npairs + lpc - 1) / lpc, 256, shm, st>>>(fp, in, out, nrows, scale, lpc);
 }
+template void launch_rfft_x<double>(const FftPlan&, const double*, double2*, int, cudaStream_t);
+template void launch_rfft_x<float>(const FftPlan&, const float*, double2*, int, cudaStream_t);
+template void launch_irfft_x<double>(const FftPlan&, const double2*, double*, int, double, cudaStream_t);
+template void launch_irfft_x<float>(const FftPlan&, const double2*, float*, int, double, cudaStream_t);
 
 void launch_cfft_axis(const FftPlan& fp, double2* data, int na, int nb, int64_t bstride, int64_t stride, int sign,
                       cudaStream_t st) {
@@ -514,14 +676,51 @@ void launch_cfft_axis(const FftPlan& fp, double2* data, int na, int nb, int64_t 
 // FISHPACK y solve: TRID0 (src/poisson_fishpack.f90:20-57) per (kx, kz) on complex data
 // laid out (kz, j, kx) with kx fastest.
 // ===========================================================================
+// The forward-sweep factors of TRID0 depend only on (kx, kz), not on the right-hand side, so
+// they are computed once: Zr[j] = 1/pivot_j (j < ny-1), D[j] = c_j * Zr[j], and for the last
+// row the pivot itself, or 0 when it is pinned (|pivot| <= 1e-10).  Layout (kz, j, kx) like the
+// spectrum.  The arithmetic is TRID0's, in its order, so the solve is bitwise the same.
+__global__ void ysolve_factor_kernel(double* __restrict__ Zr, double* __restrict__ D, int nxh, int ny, int nz,
+                                     const double* __restrict__ pa, const double* __restrict__ pb,
+                                     const double* __restrict__ pc, const double* __restrict__ lamx,
+                                     const double* __restrict__ lamz) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (int64_t)nxh * nz) return;
+  const int kz = (int)(g / nxh), kx = (int)(g - (int64_t)kz * nxh);
+  const double lx = lamx[kx], lz = lamz[kz];
+  const int64_t base = (int64_t)kz * ny * nxh + kx;
+  double bb = (pb[0] + lx) + lz;
+  double Z = 1.0 / bb;
+  double d = pc[0] * Z;
+  Zr[base] = Z;
+  D[base] = d;
+  for (int j = 1; j < ny - 1; ++j) {
+    bb = (pb[j] + lx) + lz;
+    Z = 1.0 / (bb - pa[j] * d);
+    d = pc[j] * Z;
+    Zr[base + (int64_t)j * nxh] = Z;
+    D[base + (int64_t)j * nxh] = d;
+  }
+  bb = (pb[ny - 1] + lx) + lz;
+  Z = bb - pa[ny - 1] * d;
+  Zr[base + (int64_t)(ny - 1) * nxh] = fabs(Z) > 1.0e-10 ? Z : 0.0;
+  D[base + (int64_t)(ny - 1) * nxh] = 0.0;
+}
+
+void launch_ysolve_factor(double* Zr, double* D, int nxh, int ny, int nz, const double* pa, const double* pb,
+                          const double* pc, const double* lamx, const double* lamz, cudaStream_t st) {
+  if (ny < 2) throw std::runtime_error("ysolve: ny must be at least 2");
+  const int64_t n = (int64_t)nxh * nz;
+  ysolve_factor_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(Zr, D, nxh, ny, nz, pa, pb, pc, lamx, lamz);
+}
+
 // One CTA per `lt` consecutive (kx, kz) columns: the columns are staged in shared memory with
-// coalesced row loads by all threads, swept by `lt` threads (one column each), and written back.
+// coalesced row loads by all threads, swept by `lt` threads (one column each) with the
+// precomputed factors, and written back.
 __global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data, int nxh, int ny, int nz,
-                                                     const double* __restrict__ pa, const double* __restrict__ pb,
-                                                     const double* __restrict__ pc, const double* __restrict__ lamx,
-                                                     const double* __restrict__ lamz, int lt) {
+                                                     const double* __restrict__ Zr, const double* __restrict__ D,
+                                                     const double* __restrict__ pa, int lt) {
   extern __shared__ __align__(16) double2 sT[];  // [ny][lt] right-hand sides / solution
-  double* sD = reinterpret_cast<double*>(sT + (size_t)ny * lt);  // [ny][lt] forward-sweep factors
   const int tid = threadIdx.x;
   const int l = tid % lt;
   const int64_t nl = (int64_t)nxh * nz;
@@ -529,47 +728,59 @@ __global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data,
   const bool ok = g < nl;
   const int kz = ok ? (int)(g / nxh) : 0;
   const int kx = ok ? (int)(g - (int64_t)kz * nxh) : 0;
-  double2* col = data + (int64_t)kz * ny * nxh + kx;
+  const int64_t base = (int64_t)kz * ny * nxh + kx;
+  double2* col = data + base;
   const int jstep = blockDim.x / lt;
-  if (ok)
-    for (int j = tid / lt; j < ny; j += jstep) sT[j * lt + l] = col[(int64_t)j * nxh];
+  if (ok) {
+    for (int j0 = tid / lt; j0 < ny; j0 += 8 * jstep) {
+      double2 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int j = j0 + u * jstep;
+        if (j < ny) v[u] = col[(int64_t)j * nxh];
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int j = j0 + u * jstep;
+        if (j < ny) sT[j * lt + l] = v[u];
+      }
+    }
+  }
   __syncthreads();
   if (tid < lt && ok) {
     double2* T = sT + l;
-    double* D = sD + l;
-    const double lx = lamx[kx], lz = lamz[kz];
-    double bb = (pb[0] + lx) + lz;
-    double Z = 1.0 / bb;
-    D[0] = pc[0] * Z;
+    const double* zr = Zr + base;
+    const double* dd = D + base;
     double2 tp = T[0];
+    double Z = zr[0];
     tp.x *= Z; tp.y *= Z;
     T[0] = tp;
+#pragma unroll 4
     for (int j = 1; j < ny - 1; ++j) {
-      bb = (pb[j] + lx) + lz;
-      Z = 1.0 / (bb - pa[j] * D[(j - 1) * lt]);
-      D[j * lt] = pc[j] * Z;
+      const double z = zr[(int64_t)j * nxh], a = pa[j];
       double2 v = T[j * lt];
-      v.x = (v.x - pa[j] * tp.x) * Z;
-      v.y = (v.y - pa[j] * tp.y) * Z;
+      v.x = (v.x - a * tp.x) * z;
+      v.y = (v.y - a * tp.y) * z;
       T[j * lt] = v;
       tp = v;
     }
-    bb = (pb[ny - 1] + lx) + lz;
-    Z = bb - pa[ny - 1] * D[(ny - 2) * lt];
+    const double zl = zr[(int64_t)(ny - 1) * nxh];
     double2 v = T[(ny - 1) * lt];
-    // TRID0's singular-pivot pin: the last unknown is set to zero when the pivot vanishes
-    if (fabs(Z) > 1.0e-10) {
-      v.x = (v.x - pa[ny - 1] * tp.x) / Z;
-      v.y = (v.y - pa[ny - 1] * tp.y) / Z;
+    // TRID0's singular-pivot pin: the last unknown is zero when the pivot vanishes
+    if (zl != 0.0) {
+      v.x = (v.x - pa[ny - 1] * tp.x) / zl;
+      v.y = (v.y - pa[ny - 1] * tp.y) / zl;
     } else {
       v.x = 0.0;
       v.y = 0.0;
     }
     T[(ny - 1) * lt] = v;
+#pragma unroll 4
     for (int j = ny - 2; j >= 0; --j) {
+      const double d = dd[(int64_t)j * nxh];
       double2 u = T[j * lt];
-      u.x = u.x - D[j * lt] * v.x;
-      u.y = u.y - D[j * lt] * v.y;
+      u.x = u.x - d * v.x;
+      u.y = u.y - d * v.y;
       T[j * lt] = u;
       v = u;
     }
@@ -579,12 +790,12 @@ __global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data,
     for (int j = tid / lt; j < ny; j += jstep) col[(int64_t)j * nxh] = sT[j * lt + l];
 }
 
-void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* pa, const double* pb, const double* pc,
-                   const double* lamx, const double* lamz, cudaStream_t st) {
+void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* Zr, const double* D, const double* pa,
+                   cudaStream_t st) {
   if (ny < 2) throw std::runtime_error("ysolve: ny must be at least 2");
   int lt = 32;
-  while (lt > 4 && (size_t)ny * lt * 24 > 110 * 1024) lt /= 2;
-  const size_t shm = (size_t)ny * lt * 24;
+  while (lt > 4 && (size_t)ny * lt * 16 > 110 * 1024) lt /= 2;
+  const size_t shm = (size_t)ny * lt * 16;
   if (shm > 200 * 1024) throw std::runtime_error("ysolve: ny too large for the shared-memory tile");
   static bool attr_set = false;
   if (!attr_set) {
@@ -592,7 +803,7 @@ void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* pa, con
     attr_set = true;
   }
   const int64_t n = (int64_t)nxh * nz;
-  ysolve_kernel<<<(unsigned)((n + lt - 1) / lt), 128, shm, st>>>(data, nxh, ny, nz, pa, pb, pc, lamx, lamz, lt);
+  ysolve_kernel<<<(unsigned)((n + lt - 1) / lt), 128, shm, st>>>(data, nxh, ny, nz, Zr, D, pa, lt);
 }
 
 __global__ void spectral_divide_kernel(double2* __restrict__ data, int nxh, int ny, int nz,
@@ -620,32 +831,36 @@ void launch_spectral_divide(double2* data, int nxh, int ny, int nz, const double
 }
 
 // ===========================================================================
-// elementwise and reductions
+// elementwise and reductions.  Field arrays are T (double, or float in the mixed-precision
+// form); scalars, reduction accumulators and results stay double.
 // ===========================================================================
-__global__ void fractional_step_kernel(double* __restrict__ rhs1, double* __restrict__ rhs0,
-                                       const double* __restrict__ pfc, int64_t n, double dt, double gam, double zeta,
-                                       double alpha) {
+template <typename T>
+__global__ void fractional_step_kernel(T* __restrict__ rhs1, T* __restrict__ rhs0, const T* __restrict__ pfc,
+                                       int64_t n, double dt, double gam, double zeta, double alpha) {
+  const T tdt = T(dt), tg = T(gam), tz = T(zeta), ta = T(alpha);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double cur = rhs1[i], last = rhs0[i];
-    double tot = gam * cur + zeta * last;
+    const T cur = rhs1[i], last = rhs0[i];
+    T tot = tg * cur + tz * last;
     rhs0[i] = cur;
-    tot = tot + alpha * pfc[i];
-    rhs1[i] = dt * tot;
+    tot = tot + ta * pfc[i];
+    rhs1[i] = tdt * tot;
   }
 }
-void launch_fractional_step(double* rhs1, double* rhs0, const double* pfc, int64_t n, double dt, double gam,
-                            double zeta, double alpha, cudaStream_t st) {
-  fractional_step_kernel<<<148 * 8, 256, 0, st>>>(rhs1, rhs0, pfc, n, dt, gam, zeta, alpha);
+template <typename T>
+void launch_fractional_step(T* rhs1, T* rhs0, const T* pfc, int64_t n, double dt, double gam, double zeta,
+                            double alpha, cudaStream_t st) {
+  fractional_step_kernel<T><<<148 * 8, 256, 0, st>>>(rhs1, rhs0, pfc, n, dt, gam, zeta, alpha);
 }
 
-__global__ void weighted_partial_kernel(const double* __restrict__ a, const double* __restrict__ wy, int n1, int n2,
+template <typename T>
+__global__ void weighted_partial_kernel(const T* __restrict__ a, const double* __restrict__ wy, int n1, int n2,
                                         int n3, double* __restrict__ partial) {
   __shared__ double red[256];
   const int64_t n = (int64_t)n1 * n2 * n3;
   double acc = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int j = (int)((i / n1) % n2);
-    acc += a[i] * wy[j];
+    acc += (double)a[i] * wy[j];
   }
   red[threadIdx.x] = acc;
   __syncthreads();
@@ -668,80 +883,122 @@ __global__ void finalize_mean_kernel(const double* __restrict__ partial, int npa
   }
   if (threadIdx.x == 0) out[0] = red[0] / vol;
 }
-void launch_weighted_mean(const double* a, const double* wy, int n1, int n2, int n3, double* partial, int npart,
+template <typename T>
+void launch_weighted_mean(const T* a, const double* wy, int n1, int n2, int n3, double* partial, int npart,
                           double* out, double vol, cudaStream_t st) {
-  weighted_partial_kernel<<<npart, 256, 0, st>>>(a, wy, n1, n2, n3, partial);
+  weighted_partial_kernel<T><<<npart, 256, 0, st>>>(a, wy, n1, n2, n3, partial);
   finalize_mean_kernel<<<1, 256, 0, st>>>(partial, npart, out, vol);
 }
 
-__global__ void update_q_kernel(double* __restrict__ q, const double* __restrict__ rhs, const double* __restrict__ sub,
+template <typename T>
+__global__ void update_q_kernel(T* __restrict__ q, const T* __restrict__ rhs, const double* __restrict__ sub,
                                 int64_t n) {
-  const double s = sub ? sub[0] : 0.0;
+  const T s = sub ? T(sub[0]) : T(0);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     q[i] = q[i] + (rhs[i] - s);
 }
-void launch_update_q(double* q, const double* rhs, const double* sub, int64_t n, cudaStream_t st) {
-  update_q_kernel<<<148 * 8, 256, 0, st>>>(q, rhs, sub, n);
+template <typename T>
+void launch_update_q(T* q, const T* rhs, const double* sub, int64_t n, cudaStream_t st) {
+  update_q_kernel<T><<<148 * 8, 256, 0, st>>>(q, rhs, sub, n);
 }
 
-__global__ void set_yrows_kernel(double* __restrict__ a, int n1, int n2, int n3, int s0, double v0, int s1, double v1) {
+template <typename T>
+__global__ void set_yrows_kernel(T* __restrict__ a, int n1, int n2, int n3, int s0, double v0, int s1, double v1) {
   const int64_t n = (int64_t)n1 * n3;
   for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
     const int64_t k = g / n1, i = g - k * n1;
-    if (s0) a[(k * n2 + 0) * n1 + i] = v0;
-    if (s1) a[(k * n2 + (n2 - 1)) * n1 + i] = v1;
+    if (s0) a[(k * n2 + 0) * n1 + i] = T(v0);
+    if (s1) a[(k * n2 + (n2 - 1)) * n1 + i] = T(v1);
   }
 }
-void launch_set_yrows(double* a, int n1, int n2, int n3, int s0, double v0, int s1, double v1, cudaStream_t st) {
-  set_yrows_kernel<<<148, 256, 0, st>>>(a, n1, n2, n3, s0, v0, s1, v1);
+template <typename T>
+void launch_set_yrows(T* a, int n1, int n2, int n3, int s0, double v0, int s1, double v1, cudaStream_t st) {
+  set_yrows_kernel<T><<<148, 256, 0, st>>>(a, n1, n2, n3, s0, v0, s1, v1);
 }
 
-__global__ void fbcy_const_kernel(double* __restrict__ fbc, int64_t nl, double v0, double v1) {
+template <typename T>
+__global__ void fbcy_const_kernel(T* __restrict__ fbc, int64_t nl, double v0, double v1) {
   for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < nl; g += (int64_t)gridDim.x * blockDim.x) {
-    fbc[g] = v0;
-    fbc[nl + g] = v1;
-    fbc[2 * nl + g] = v0;
-    fbc[3 * nl + g] = v1;
+    fbc[g] = T(v0);
+    fbc[nl + g] = T(v1);
+    fbc[2 * nl + g] = T(v0);
+    fbc[3 * nl + g] = T(v1);
   }
 }
-void launch_fbcy_const(double* fbc, int n1, int n3, double v0, double v1, cudaStream_t st) {
-  fbcy_const_kernel<<<148, 256, 0, st>>>(fbc, (int64_t)n1 * n3, v0, v1);
+template <typename T>
+void launch_fbcy_const(T* fbc, int n1, int n3, double v0, double v1, cudaStream_t st) {
+  fbcy_const_kernel<T><<<148, 256, 0, st>>>(fbc, (int64_t)n1 * n3, v0, v1);
 }
 
 // planes [4][n1*n3] from the wall rows of (n1, n2, n3) arrays: v = s*(A + c1*B)*C, C optional (else c2)
-__global__ void fbcy_extract_kernel(double* __restrict__ fbc, const double* __restrict__ A,
-                                    const double* __restrict__ B, const double* __restrict__ C, double c1, double s,
-                                    double c2, int n1, int n2, int n3) {
+template <typename T>
+__global__ void fbcy_extract_kernel(T* __restrict__ fbc, const T* __restrict__ A, const T* __restrict__ B,
+                                    const T* __restrict__ C, double c1, double s, double c2, int n1, int n2, int n3) {
   const int64_t nl = (int64_t)n1 * n3;
   for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < nl; g += (int64_t)gridDim.x * blockDim.x) {
     const int64_t k = g / n1, i = g - k * n1;
     for (int side = 0; side < 2; ++side) {
       const int64_t a = (k * n2 + (side == 0 ? 0 : n2 - 1)) * n1 + i;
-      double v = A[a];
-      if (B) v = v + c1 * B[a];
-      v = v * s;
-      v = C ? v * C[a] : v * c2;
+      T v = A[a];
+      if (B) v = v + T(c1) * B[a];
+      v = v * T(s);
+      v = C ? v * C[a] : v * T(c2);
       fbc[side * nl + g] = v;
       fbc[(side + 2) * nl + g] = v;
     }
   }
 }
-void launch_fbcy_extract(double* fbc, const double* A, const double* B, const double* C, double c1, double s,
-                         double c2, int n1, int n2, int n3, cudaStream_t st) {
-  fbcy_extract_kernel<<<148, 256, 0, st>>>(fbc, A, B, C, c1, s, c2, n1, n2, n3);
+template <typename T>
+void launch_fbcy_extract(T* fbc, const T* A, const T* B, const T* C, double c1, double s, double c2, int n1, int n2,
+                         int n3, cudaStream_t st) {
+  fbcy_extract_kernel<T><<<148, 256, 0, st>>>(fbc, A, B, C, c1, s, c2, n1, n2, n3);
 }
 
-__global__ void axpby_kernel(double* __restrict__ out, const double* __restrict__ a, double sa,
-                             const double* __restrict__ b, double sb, int64_t n) {
+template <typename T>
+__global__ void axpby_kernel(T* __restrict__ out, const T* __restrict__ a, double sa, const T* __restrict__ b,
+                             double sb, int64_t n) {
+  const T ta = T(sa), tb = T(sb);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    double v = sa * a[i];
-    if (b) v += sb * b[i];
+    T v = ta * a[i];
+    if (b) v += tb * b[i];
     out[i] = v;
   }
 }
-void launch_axpby(double* out, const double* a, double sa, const double* b, double sb, int64_t n, cudaStream_t st) {
-  axpby_kernel<<<148 * 8, 256, 0, st>>>(out, a, sa, b, sb, n);
+template <typename T>
+void launch_axpby(T* out, const T* a, double sa, const T* b, double sb, int64_t n, cudaStream_t st) {
+  axpby_kernel<T><<<148 * 8, 256, 0, st>>>(out, a, sa, b, sb, n);
 }
+
+// conversion between the double host layout and a float device field
+__global__ void convert_kernel_d2f(float* __restrict__ out, const double* __restrict__ in, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+__global__ void convert_kernel_f2d(double* __restrict__ out, const float* __restrict__ in, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+void launch_convert(float* out, const double* in, int64_t n, cudaStream_t st) {
+  convert_kernel_d2f<<<148 * 8, 256, 0, st>>>(out, in, n);
+}
+void launch_convert(double* out, const float* in, int64_t n, cudaStream_t st) {
+  convert_kernel_f2d<<<148 * 8, 256, 0, st>>>(out, in, n);
+}
+
+#define CHS_INST_ELEM(T)                                                                                      \
+  template void launch_fractional_step<T>(T*, T*, const T*, int64_t, double, double, double, double,          \
+                                          cudaStream_t);                                                      \
+  template void launch_weighted_mean<T>(const T*, const double*, int, int, int, double*, int, double*, double, \
+                                        cudaStream_t);                                                        \
+  template void launch_update_q<T>(T*, const T*, const double*, int64_t, cudaStream_t);                       \
+  template void launch_set_yrows<T>(T*, int, int, int, int, double, int, double, cudaStream_t);               \
+  template void launch_fbcy_const<T>(T*, int, int, double, double, cudaStream_t);                             \
+  template void launch_fbcy_extract<T>(T*, const T*, const T*, const T*, double, double, double, int, int, int, \
+                                       cudaStream_t);                                                         \
+  template void launch_axpby<T>(T*, const T*, double, const T*, double, int64_t, cudaStream_t);
+CHS_INST_ELEM(double)
+CHS_INST_ELEM(float)
+#undef CHS_INST_ELEM
 
 __global__ void absmax_partial_kernel(const double* __restrict__ a, int64_t n, double* __restrict__ partial) {
   __shared__ double red[256];

@@ -52,39 +52,55 @@ struct FftPlan {
   const double2* tw;  // exp(-2 pi i m / n), m = 0..n-1 (device)
 };
 
-// real x-lines (rows of length nx) -> half spectra (rows of nx/2+1), scaled by `scale`
-void launch_rfft_x(const FftPlan& fp, const double* in, double2* out, int nrows, cudaStream_t st);
-// half spectra -> real x-lines, scaled by `scale`
-void launch_irfft_x(const FftPlan& fp, const double2* in, double* out, int nrows, double scale, cudaStream_t st);
+// real x-lines (rows of length nx, R = double or float) -> FP64 half spectra (rows of nx/2+1)
+template <typename R>
+void launch_rfft_x(const FftPlan& fp, const R* in, double2* out, int nrows, cudaStream_t st);
+// FP64 half spectra -> real x-lines, scaled by `scale`
+template <typename R>
+void launch_irfft_x(const FftPlan& fp, const double2* in, R* out, int nrows, double scale, cudaStream_t st);
 // complex FFT along a strided axis: element (line, p) at base(line) + p*stride,
 // line = a + na*b with base = a + b*bstride (a fastest); sign -1 forward, +1 backward
 void launch_cfft_axis(const FftPlan& fp, double2* data, int na, int nb, int64_t bstride, int64_t stride, int sign,
                       cudaStream_t st);
+// forward-sweep factors of the FISHPACK y solve per (kx, kz), computed once (layout (kz, j, kx))
+void launch_ysolve_factor(double* Zr, double* D, int nxh, int ny, int nz, const double* pa, const double* pb,
+                          const double* pc, const double* lamx, const double* lamz, cudaStream_t st);
 // y tridiagonal solve per (kx, kz) of the FISHPACK path (TRID0 with the singular-pivot pin)
-void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* pa, const double* pb, const double* pc,
-                   const double* lamx, const double* lamz, cudaStream_t st);
+void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* Zr, const double* D, const double* pa,
+                   cudaStream_t st);
 // 3D spectral division by -(kx'^2 + ky'^2 + kz'^2) (zero mode -> 0), with normalisation
 void launch_spectral_divide(double2* data, int nxh, int ny, int nz, const double* k2x, const double* k2y,
                             const double* k2z, double norm, cudaStream_t st);
 
-// ---- elementwise and reductions ----
+// ---- elementwise and reductions (T = double, or float in the mixed-precision form) ----
 // rhs1 <- dt*(gamma*rhs1 + zeta*rhs0 + alpha*pfc); rhs0 <- old rhs1
-void launch_fractional_step(double* rhs1, double* rhs0, const double* pfc, int64_t n, double dt, double gam,
-                            double zeta, double alpha, cudaStream_t st);
-// weighted sum over (n1, n2, n3) with weight w[j] -> partial sums; finalize writes out[0] = sum/vol
-void launch_weighted_mean(const double* a, const double* wy, int n1, int n2, int n3, double* partial, int npart,
+template <typename T>
+void launch_fractional_step(T* rhs1, T* rhs0, const T* pfc, int64_t n, double dt, double gam, double zeta,
+                            double alpha, cudaStream_t st);
+// weighted sum over (n1, n2, n3) with weight w[j] (double accumulation) -> partial sums;
+// finalize writes out[0] = sum/vol
+template <typename T>
+void launch_weighted_mean(const T* a, const double* wy, int n1, int n2, int n3, double* partial, int npart,
                           double* out, double vol, cudaStream_t st);
 // q <- q + rhs - (sub ? *sub : 0)
-void launch_update_q(double* q, const double* rhs, const double* sub, int64_t n, cudaStream_t st);
+template <typename T>
+void launch_update_q(T* q, const T* rhs, const double* sub, int64_t n, cudaStream_t st);
 // set rows j = 0 and j = n2-1 of an (n1, n2, n3) array to v0 / v1 (flags select sides)
-void launch_set_yrows(double* a, int n1, int n2, int n3, int s0, double v0, int s1, double v1, cudaStream_t st);
+template <typename T>
+void launch_set_yrows(T* a, int n1, int n2, int n3, int s0, double v0, int s1, double v1, cudaStream_t st);
 // fbc planes [4][n1*n3] for y-lines: constant wall values
-void launch_fbcy_const(double* fbc, int n1, int n3, double v0, double v1, cudaStream_t st);
+template <typename T>
+void launch_fbcy_const(T* fbc, int n1, int n3, double v0, double v1, cudaStream_t st);
 // fbc planes from the first/last y rows of `a` (extract_dirichlet_fbcy): out = s*(A_wall + c1*B_wall)*C
-void launch_fbcy_extract(double* fbc, const double* A, const double* B, const double* C, double c1, double s,
-                         double c2, int n1, int n2, int n3, cudaStream_t st);
-// out = a * s
-void launch_axpby(double* out, const double* a, double sa, const double* b, double sb, int64_t n, cudaStream_t st);
+template <typename T>
+void launch_fbcy_extract(T* fbc, const T* A, const T* B, const T* C, double c1, double s, double c2, int n1, int n2,
+                         int n3, cudaStream_t st);
+// out = sa*a + sb*b (b optional)
+template <typename T>
+void launch_axpby(T* out, const T* a, double sa, const T* b, double sb, int64_t n, cudaStream_t st);
+// float <-> double field conversion
+void launch_convert(float* out, const double* in, int64_t n, cudaStream_t st);
+void launch_convert(double* out, const float* in, int64_t n, cudaStream_t st);
 // max |a| and NaN flag into out[0], out[1] (two-pass with partials)
 void launch_absmax(const double* a, int64_t n, double* partial, int npart, double* out, cudaStream_t st);
 // 0.5*(u^2+v^2+w^2) over ccc

@@ -98,6 +98,7 @@ struct chs_handle {
   int nc[3], np[3];
   bool periodic_y, stretch_y;
   int iacc, ifft, idriven;
+  bool mixed = false;  // FP32 fields and operators, FP64 Poisson / mass flux / diagnostics
   double h[3];
   double dt, rre, sigma2p;
   double tGamma[4], tZeta[4], tAlpha[4];
@@ -128,12 +129,14 @@ struct chs_handle {
   double *div, *qxdx_cpc, *qydy_cpc, *qzdz_cpc;
   double *fb_qx, *fb_qy, *fb_qz, *fb_pr, *fb_mpr, *fb_conv2, *fb_visc2, *fb_comb, *fb_maxp;
   double *wy, *partial, *scal;
+  double* stage = nullptr;  // mixed precision: FP64 staging for host transfers
   double vol = 0.0;
   int npart = 0;
   // Poisson
   FftPlan fx{}, fy{}, fz{};
   double2* spec = nullptr;
   double *lamx = nullptr, *lamz = nullptr, *pa = nullptr, *pb = nullptr, *pc = nullptr;
+  double *yzr = nullptr, *yd = nullptr;  // precomputed y-solve factors
   double *k2x = nullptr, *k2y = nullptr, *k2z = nullptr;
   // graphs per substep (1..3) and for a whole step
   cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -179,35 +182,44 @@ namespace {
 Pair P2(const int v[2]) { return Pair{{v[0], v[1]}}; }
 void upload_table(chs_handle* H);
 
-// input expression: up to two terms (see LineIO)
-struct Src {
-  Term t[2] = {{nullptr, nullptr, T_NONE, 0.0, 0.0}, {nullptr, nullptr, T_NONE, 0.0, 0.0}};
+template <class T>
+struct Id { using type = T; };
+
+// input expression: up to two terms (see LineIOT)
+template <typename T>
+struct SrcT {
+  TermT<T> t[2] = {{nullptr, nullptr, T_NONE, 0.0, 0.0}, {nullptr, nullptr, T_NONE, 0.0, 0.0}};
   int narrays() const {
     int n = 0;
     for (const auto& x : t) n += (x.X ? 1 : 0) + (x.Y ? 1 : 0);
     return n;
   }
 };
-Src src(const double* a, double s = 1.0) { Src x; x.t[0] = Term{a, nullptr, T_X, s, 0.0}; return x; }
-Src prod(const double* a, const double* b, double s) { Src x; x.t[0] = Term{a, b, T_XY, s, 0.0}; return x; }
-Src lin(const double* a, const double* b, double c1, double s) {
-  Src x; x.t[0] = Term{a, b, T_XpY, s, c1}; return x;
+template <typename T>
+SrcT<T> src(const T* a, double s = 1.0) { SrcT<T> x; x.t[0] = TermT<T>{a, nullptr, T_X, s, 0.0}; return x; }
+template <typename T>
+SrcT<T> prod(const T* a, const T* b, double s) { SrcT<T> x; x.t[0] = TermT<T>{a, b, T_XY, s, 0.0}; return x; }
+template <typename T>
+SrcT<T> lin(const T* a, const T* b, double c1, double s) {
+  SrcT<T> x; x.t[0] = TermT<T>{a, b, T_XpY, s, c1}; return x;
 }
 // a + w * b, for two single-term expressions
-Src plus(const Src& a, const Src& b, double w) {
-  Src x = a;
+template <typename T>
+SrcT<T> plus(const SrcT<T>& a, const SrcT<T>& b, double w) {
+  SrcT<T> x = a;
   x.t[1] = b.t[0];
   x.t[1].s *= w;
   return x;
 }
 
 // run one operator: direction d, family fam, operation bc, boundary planes fbc (null = absent)
-void run_op(chs_handle* H, int d, int fam, Pair bc, const double* fbc, const Src& in, const int n_in[3], double* out,
-            bool accumulate, double g) {
+template <typename T>
+void run_op(chs_handle* H, int d, int fam, Pair bc, const typename Id<T>::type* fbc, const SrcT<T>& in,
+            const int n_in[3], T* out, bool accumulate, double g) {
   const size_t tsz = H->book.table.size();
   const OpPlan& P = H->plan(d, fam, bc, fbc != nullptr);
   if (H->book.table.size() != tsz) upload_table(H);
-  LineIO io{};
+  LineIOT<T> io{};
   io.t[0] = in.t[0];
   io.t[1] = in.t[1];
   io.fbc = fbc;
@@ -218,7 +230,7 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const double* fbc, const Src
   const double nin_tot = (double)n_in[0] * n_in[1] * n_in[2];
   const double nout_tot = nin_tot / P.nin * P.nout;
   const int narr = in.narrays();
-  const double bytes = 8.0 * (narr * nin_tot + (accumulate ? 2.0 : 1.0) * nout_tot);
+  const double bytes = (double)sizeof(T) * (narr * nin_tot + (accumulate ? 2.0 : 1.0) * nout_tot);
   cudaEvent_t e0 = H->prof_begin();
   launch_line_op(d, P, io, H->table, H->st);
   H->prof_end(e0, 0, d, bytes);
@@ -236,16 +248,18 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const double* fbc, const Src
 // op(a; fbc1) + w*op(b; fbc2).  When both terms use the same plan the sum runs as one launch
 // on the combined input (the operator is linear in its input and boundary values); fcomb must
 // then hold fbc1 + w*fbc2 when the two planes differ.
-void run_pair(chs_handle* H, int d, int fam, Pair bc1, const double* f1, const Src& a, Pair bc2, const double* f2,
-              const Src& b, double w, const int n_in[3], double* out, bool accumulate, const double* fcomb) {
+template <typename T>
+void run_pair(chs_handle* H, int d, int fam, Pair bc1, const typename Id<T>::type* f1, const SrcT<T>& a, Pair bc2,
+              const typename Id<T>::type* f2, const SrcT<T>& b, double w, const int n_in[3], T* out, bool accumulate,
+              const typename Id<T>::type* fcomb) {
   const bool same = bc1.v[0] == bc2.v[0] && bc1.v[1] == bc2.v[1] && ((f1 == nullptr) == (f2 == nullptr)) &&
                     (f1 == f2 || fcomb != nullptr);
   if (same) {
-    const double* f = (f1 == f2) ? f1 : fcomb;
-    run_op(H, d, fam, bc1, f, plus(a, b, w), n_in, out, accumulate, 1.0);
+    const T* f = (f1 == f2) ? f1 : fcomb;
+    run_op<T>(H, d, fam, bc1, f, plus(a, b, w), n_in, out, accumulate, 1.0);
   } else {
-    run_op(H, d, fam, bc1, f1, a, n_in, out, accumulate, 1.0);
-    run_op(H, d, fam, bc2, f2, b, n_in, out, true, w);
+    run_op<T>(H, d, fam, bc1, f1, a, n_in, out, accumulate, 1.0);
+    run_op<T>(H, d, fam, bc2, f2, b, n_in, out, true, w);
   }
 }
 
@@ -349,7 +363,8 @@ void setup_host(chs_handle* H, const chs_config* c) {
   if (H->ifft != 2 && H->ifft != 3) throw std::invalid_argument("ifft must be 2 or 3");
   if (H->ifft == 2 && H->periodic_y) throw std::invalid_argument("FISHPACK Poisson needs non-periodic y");
   if (H->ifft == 3 && !H->periodic_y) throw std::invalid_argument("3D-FFT Poisson needs periodic y");
-  if (c->precision != CHS_FP64) throw std::invalid_argument("only the FP64 path is available in this build");
+  if (c->precision != CHS_FP64 && c->precision != CHS_MIXED) throw std::invalid_argument("unknown precision mode");
+  H->mixed = c->precision == CHS_MIXED;
   H->h[0] = c->lxx / H->nc[0];
   H->h[2] = c->lzz / H->nc[2];
   H->h[1] = H->stretch_y ? 1.0 / H->nc[1] : (c->lyt - c->lyb) / H->nc[1];
@@ -403,14 +418,22 @@ void setup_device(chs_handle* H, const chs_config* c) {
   H->fb_conv2 = H->dalloc<double>(4 * nl); H->fb_visc2 = H->dalloc<double>(4 * nl);
   H->fb_comb = H->dalloc<double>(4 * nl);
   H->fb_maxp = H->dalloc<double>(4 * nl);
-  launch_fbcy_const(H->fb_qx, nc0, nc2, H->fbcy[V_QX][0], H->fbcy[V_QX][1], H->st);
-  launch_fbcy_const(H->fb_qy, nc0, nc2, H->fbcy[V_QY][0], H->fbcy[V_QY][1], H->st);
-  launch_fbcy_const(H->fb_qz, nc0, nc2, H->fbcy[V_QZ][0], H->fbcy[V_QZ][1], H->st);
-  launch_fbcy_const(H->fb_pr, nc0, nc2, H->fbcy[V_PR][0], H->fbcy[V_PR][1], H->st);
-  launch_fbcy_const(H->fb_mpr, nc0, nc2, -H->fbcy[V_PR][0], -H->fbcy[V_PR][1], H->st);
-  launch_fbcy_const(H->fb_conv2, nc0, nc2, -H->fbcy[V_QY][0] * H->fbcy[V_QY][0],
-                    -H->fbcy[V_QY][1] * H->fbcy[V_QY][1], H->st);
-  launch_fbcy_const(H->fb_maxp, nc0, nc2, kMaxp, kMaxp, H->st);
+  auto fill = [&](double* p, double v0, double v1) {
+    if (H->mixed) launch_fbcy_const(reinterpret_cast<float*>(p), nc0, nc2, v0, v1, H->st);
+    else launch_fbcy_const(p, nc0, nc2, v0, v1, H->st);
+  };
+  fill(H->fb_qx, H->fbcy[V_QX][0], H->fbcy[V_QX][1]);
+  fill(H->fb_qy, H->fbcy[V_QY][0], H->fbcy[V_QY][1]);
+  fill(H->fb_qz, H->fbcy[V_QZ][0], H->fbcy[V_QZ][1]);
+  fill(H->fb_pr, H->fbcy[V_PR][0], H->fbcy[V_PR][1]);
+  fill(H->fb_mpr, -H->fbcy[V_PR][0], -H->fbcy[V_PR][1]);
+  fill(H->fb_conv2, -H->fbcy[V_QY][0] * H->fbcy[V_QY][0], -H->fbcy[V_QY][1] * H->fbcy[V_QY][1]);
+  fill(H->fb_maxp, kMaxp, kMaxp);
+  if (H->mixed) {
+    size_t m = H->n_pcc;
+    for (size_t v : {H->n_cpc, H->n_ccp, H->n_ccc}) m = v > m ? v : m;
+    H->stage = H->dalloc<double>(m);
+  }
   H->launches += 7;
 
   // volume weights dy(j)*dx*dz (src/tools_general.f90:1229-1253)
@@ -483,6 +506,10 @@ void setup_device(chs_handle* H, const chs_config* c) {
     CK(cudaMemcpyAsync(H->pa, a.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice, H->st));
     CK(cudaMemcpyAsync(H->pb, b.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice, H->st));
     CK(cudaMemcpyAsync(H->pc, cc.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    H->yzr = H->dalloc<double>((size_t)nxh * nc1 * nc2);
+    H->yd = H->dalloc<double>((size_t)nxh * nc1 * nc2);
+    launch_ysolve_factor(H->yzr, H->yd, nxh, nc1, nc2, H->pa, H->pb, H->pc, H->lamx, H->lamz, H->st);
+    H->launches++;
   } else {
     H->fy = make_fft(nc1, tw);
     double2* d = H->dalloc<double2>(tw.size());
@@ -531,17 +558,18 @@ void upload_table(chs_handle* H) {
                      H->st));
 }
 
-void poisson_device(chs_handle* H, double* rhs) {
+template <typename T>
+void poisson_device(chs_handle* H, T* rhs) {
   const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
   const int nxh = nc0 / 2 + 1;
   cudaStream_t st = H->st;
   const double nreal = (double)nc0 * nc1 * nc2, nspec = (double)nxh * nc1 * nc2;
-  const double b_r2c = 8.0 * nreal + 16.0 * nspec, b_c2c = 32.0 * nspec;
+  const double b_r2c = (double)sizeof(T) * nreal + 16.0 * nspec, b_c2c = 32.0 * nspec;
   PROF(H, 1, b_r2c, launch_rfft_x(H->fx, rhs, H->spec, nc1 * nc2, st));
   if (H->ifft == 2) {
     // fishpack_fft_simple (src/poisson_fishpack.f90:354-490)
     PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, H->spec, nxh, nc1, nxh, (int64_t)nxh * nc1, -1, st));
-    PROF(H, 2, b_c2c, launch_ysolve(H->spec, nxh, nc1, nc2, H->pa, H->pb, H->pc, H->lamx, H->lamz, st));
+    PROF(H, 2, 48.0 * nspec, launch_ysolve(H->spec, nxh, nc1, nc2, H->yzr, H->yd, H->pa, st));
     PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, H->spec, nxh, nc1, nxh, (int64_t)nxh * nc1, +1, st));
     PROF(H, 1, b_r2c, launch_irfft_x(H->fx, H->spec, rhs, nc1 * nc2, 1.0 / ((double)nc0 * (double)nc2), st));
     H->launches += 5;
@@ -558,8 +586,10 @@ void poisson_device(chs_handle* H, double* rhs) {
   }
 }
 
-// the substep body (enqueued on H->st; capturable)
-void substep_body(chs_handle* H, int isub) {
+// the substep body (enqueued on H->st; capturable); T is the field type
+template <typename T>
+void substep_body_t(chs_handle* H, int isub) {
+  auto A = [](double* p) { return reinterpret_cast<T*>(p); };
   cudaStream_t st = H->st;
   const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
   const int np0 = H->np[0], np1 = H->np[1], np2 = H->np[2];
@@ -571,49 +601,49 @@ void substep_body(chs_handle* H, int isub) {
   const Pair bx_qy = P2(B[0][V_QY]), by_qy = P2(B[1][V_QY]), bz_qy = P2(B[2][V_QY]);
   const Pair bx_qz = P2(B[0][V_QZ]), by_qz = P2(B[1][V_QZ]), bz_qz = P2(B[2][V_QZ]);
   const Pair bx_pr = P2(B[0][V_PR]), by_pr = P2(B[1][V_PR]), bz_pr = P2(B[2][V_PR]);
-  const double* any = H->fb_maxp;  // periodic x/z never read their boundary planes
-  const double* fyqx = H->periodic_y ? nullptr : H->fb_qx;
-  const double* fyqy = H->periodic_y ? nullptr : H->fb_qy;
-  const double* fyqz = H->periodic_y ? nullptr : H->fb_qz;
-  const double* fypr = H->periodic_y ? nullptr : H->fb_pr;
-  const double* fympr = H->periodic_y ? nullptr : H->fb_mpr;
+  const T* any = A(H->fb_maxp);  // periodic x/z never read their boundary planes
+  const T* fyqx = H->periodic_y ? nullptr : A(H->fb_qx);
+  const T* fyqy = H->periodic_y ? nullptr : A(H->fb_qy);
+  const T* fyqz = H->periodic_y ? nullptr : A(H->fb_qz);
+  const T* fypr = H->periodic_y ? nullptr : A(H->fb_pr);
+  const T* fympr = H->periodic_y ? nullptr : A(H->fb_mpr);
   const double rre = H->rre, third = 1.0 / 3.0;
 
   // ---- 1. derived quantities (src/eq_momentum2.f90:347-508)
-  run_op(H, 0, M1P2C, bx_qx, any, src(H->qx), s_pcc, H->qxix, false, 1.0);
-  run_op(H, 0, D1P2C, bx_qx, any, src(H->qx), s_pcc, H->qxdx, false, 1.0);
-  run_op(H, 1, D1C2P, by_qx, fyqx, src(H->qx), s_pcc, H->qxdy, false, 1.0);
-  run_op(H, 1, M1C2P, by_qx, fyqx, src(H->qx), s_pcc, H->qxiy, false, 1.0);
-  run_op(H, 2, M1C2P, bz_qx, any, src(H->qx), s_pcc, H->qxiz, false, 1.0);
-  run_op(H, 2, D1C2P, bz_qx, any, src(H->qx), s_pcc, H->qxdz, false, 1.0);
-  run_op(H, 0, D1C2P, bx_qy, any, src(H->qy), s_cpc, H->qydx, false, 1.0);
-  run_op(H, 0, M1C2P, bx_qy, any, src(H->qy), s_cpc, H->qyix, false, 1.0);
-  run_op(H, 1, D1P2C, by_qy, nullptr, src(H->qy), s_cpc, H->qydy, false, 1.0);
-  run_op(H, 1, M1P2C, by_qy, fyqy, src(H->qy), s_cpc, H->qyiy, false, 1.0);
-  run_op(H, 2, D1C2P, bz_qy, any, src(H->qy), s_cpc, H->qydz, false, 1.0);
-  run_op(H, 2, M1C2P, bz_qy, any, src(H->qy), s_cpc, H->qyiz, false, 1.0);
-  run_op(H, 0, D1C2P, bx_qz, any, src(H->qz), s_ccp, H->qzdx, false, 1.0);
-  run_op(H, 0, M1C2P, bx_qz, any, src(H->qz), s_ccp, H->qzix, false, 1.0);
-  run_op(H, 1, M1C2P, by_qz, fyqz, src(H->qz), s_ccp, H->qziy, false, 1.0);
-  run_op(H, 1, D1C2P, by_qz, fyqz, src(H->qz), s_ccp, H->qzdy, false, 1.0);
-  run_op(H, 2, M1P2C, bz_qz, any, src(H->qz), s_ccp, H->qziz, false, 1.0);
-  run_op(H, 2, D1P2C, bz_qz, nullptr, src(H->qz), s_ccp, H->qzdz, false, 1.0);
+  run_op(H, 0, M1P2C, bx_qx, any, src(A(H->qx)), s_pcc, A(H->qxix), false, 1.0);
+  run_op(H, 0, D1P2C, bx_qx, any, src(A(H->qx)), s_pcc, A(H->qxdx), false, 1.0);
+  run_op(H, 1, D1C2P, by_qx, fyqx, src(A(H->qx)), s_pcc, A(H->qxdy), false, 1.0);
+  run_op(H, 1, M1C2P, by_qx, fyqx, src(A(H->qx)), s_pcc, A(H->qxiy), false, 1.0);
+  run_op(H, 2, M1C2P, bz_qx, any, src(A(H->qx)), s_pcc, A(H->qxiz), false, 1.0);
+  run_op(H, 2, D1C2P, bz_qx, any, src(A(H->qx)), s_pcc, A(H->qxdz), false, 1.0);
+  run_op(H, 0, D1C2P, bx_qy, any, src(A(H->qy)), s_cpc, A(H->qydx), false, 1.0);
+  run_op(H, 0, M1C2P, bx_qy, any, src(A(H->qy)), s_cpc, A(H->qyix), false, 1.0);
+  run_op(H, 1, D1P2C, by_qy, nullptr, src(A(H->qy)), s_cpc, A(H->qydy), false, 1.0);
+  run_op(H, 1, M1P2C, by_qy, fyqy, src(A(H->qy)), s_cpc, A(H->qyiy), false, 1.0);
+  run_op(H, 2, D1C2P, bz_qy, any, src(A(H->qy)), s_cpc, A(H->qydz), false, 1.0);
+  run_op(H, 2, M1C2P, bz_qy, any, src(A(H->qy)), s_cpc, A(H->qyiz), false, 1.0);
+  run_op(H, 0, D1C2P, bx_qz, any, src(A(H->qz)), s_ccp, A(H->qzdx), false, 1.0);
+  run_op(H, 0, M1C2P, bx_qz, any, src(A(H->qz)), s_ccp, A(H->qzix), false, 1.0);
+  run_op(H, 1, M1C2P, by_qz, fyqz, src(A(H->qz)), s_ccp, A(H->qziy), false, 1.0);
+  run_op(H, 1, D1C2P, by_qz, fyqz, src(A(H->qz)), s_ccp, A(H->qzdy), false, 1.0);
+  run_op(H, 2, M1P2C, bz_qz, any, src(A(H->qz)), s_ccp, A(H->qziz), false, 1.0);
+  run_op(H, 2, D1P2C, bz_qz, nullptr, src(A(H->qz)), s_ccp, A(H->qzdz), false, 1.0);
   // div = qxdx + qydy + qzdz (:512-534)
-  PROF(H, 3, 24.0 * H->n_ccc, launch_axpby(H->div, H->qxdx, 1.0, H->qydy, 1.0, (int64_t)H->n_ccc, st));
-  PROF(H, 3, 24.0 * H->n_ccc, launch_axpby(H->div, H->div, 1.0, H->qzdz, 1.0, (int64_t)H->n_ccc, st));
+  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, launch_axpby(A(H->div), A(H->qxdx), 1.0, A(H->qydy), 1.0, (int64_t)H->n_ccc, st));
+  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, launch_axpby(A(H->div), A(H->div), 1.0, A(H->qzdz), 1.0, (int64_t)H->n_ccc, st));
   H->launches += 2;
   if (H->fbcy_velo) {
     // wall divergence for the y-viscous boundary value (:374-442, :537-546)
-    run_op(H, 0, D1P2C, bx_qx, nullptr, src(H->qxiy), s_ppc, H->qxdx_cpc, false, 1.0);
-    run_op(H, 1, D1C2P, by_qy, fyqy, src(H->qyiy), s_ccc, H->qydy_cpc, false, 1.0);
-    run_op(H, 2, D1P2C, bz_qz, nullptr, src(H->qziy), s_cpp, H->qzdz_cpc, false, 1.0);
+    run_op(H, 0, D1P2C, bx_qx, nullptr, src(A(H->qxiy)), s_ppc, A(H->qxdx_cpc), false, 1.0);
+    run_op(H, 1, D1C2P, by_qy, fyqy, src(A(H->qyiy)), s_ccc, A(H->qydy_cpc), false, 1.0);
+    run_op(H, 2, D1P2C, bz_qz, nullptr, src(A(H->qziy)), s_cpp, A(H->qzdz_cpc), false, 1.0);
     // fbcy_div = walls of (qxdx + qydy + qzdz)_cpc; visc2 bc = (qydy_cpc - div/3) * 2 (:1156-1171)
-    PROF(H, 3, 24.0 * H->n_cpc,
-         launch_axpby(H->qxdx_cpc, H->qxdx_cpc, 1.0, H->qydy_cpc, 1.0, (int64_t)H->n_cpc, st));
-    PROF(H, 3, 24.0 * H->n_cpc,
-         launch_axpby(H->qxdx_cpc, H->qxdx_cpc, 1.0, H->qzdz_cpc, 1.0, (int64_t)H->n_cpc, st));
-    PROF(H, 3, 48.0 * nc0 * nc2,
-         launch_fbcy_extract(H->fb_visc2, H->qydy_cpc, H->qxdx_cpc, nullptr, -third, 1.0, 2.0, nc0, np1, nc2, st));
+    PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc,
+         launch_axpby(A(H->qxdx_cpc), A(H->qxdx_cpc), 1.0, A(H->qydy_cpc), 1.0, (int64_t)H->n_cpc, st));
+    PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc,
+         launch_axpby(A(H->qxdx_cpc), A(H->qxdx_cpc), 1.0, A(H->qzdz_cpc), 1.0, (int64_t)H->n_cpc, st));
+    PROF(H, 3, 48.0 / 8.0 * sizeof(T) * nc0 * nc2,
+         launch_fbcy_extract<T>(A(H->fb_visc2), A(H->qydy_cpc), A(H->qxdx_cpc), nullptr, -third, 1.0, 2.0, nc0, np1, nc2, st));
     H->launches += 3;
   }
 
@@ -621,82 +651,87 @@ void substep_body(chs_handle* H, int isub) {
   // operator (same family and boundary pair), and the operator is linear in its input and
   // boundary values, so op(conv) + rre*op(diff) runs as op(conv + rre*diff) in one launch.
   // x-momentum (:796-966)
-  run_pair(H, 0, D1C2P, H->mbcx_cov1, any, prod(H->qxix, H->qxix, -1.0), H->mbcx_tau1, any,
-           lin(H->qxdx, H->div, -third, 2.0), rre, s_ccc, H->mx, false, nullptr);
-  run_pair(H, 1, D1P2C, H->mbcy_cov1, nullptr, prod(H->qyix, H->qxiy, -1.0), H->mbcy_tau1, nullptr,
-           lin(H->qxdy, H->qydx, 1.0, 1.0), rre, s_ppc, H->mx, true, nullptr);
-  run_pair(H, 2, D1P2C, H->mbcz_cov1, nullptr, prod(H->qzix, H->qxiz, -1.0), H->mbcz_tau1, nullptr,
-           lin(H->qxdz, H->qzdx, 1.0, 1.0), rre, s_pcp, H->mx, true, nullptr);
-  run_op(H, 0, D1C2P, bx_pr, any, src(H->pres, -1.0), s_ccc, H->px, false, 1.0);
+  run_pair(H, 0, D1C2P, H->mbcx_cov1, any, prod(A(H->qxix), A(H->qxix), -1.0), H->mbcx_tau1, any,
+           lin(A(H->qxdx), A(H->div), -third, 2.0), rre, s_ccc, A(H->mx), false, nullptr);
+  run_pair(H, 1, D1P2C, H->mbcy_cov1, nullptr, prod(A(H->qyix), A(H->qxiy), -1.0), H->mbcy_tau1, nullptr,
+           lin(A(H->qxdy), A(H->qydx), 1.0, 1.0), rre, s_ppc, A(H->mx), true, nullptr);
+  run_pair(H, 2, D1P2C, H->mbcz_cov1, nullptr, prod(A(H->qzix), A(H->qxiz), -1.0), H->mbcz_tau1, nullptr,
+           lin(A(H->qxdz), A(H->qzdx), 1.0, 1.0), rre, s_pcp, A(H->mx), true, nullptr);
+  run_op(H, 0, D1C2P, bx_pr, any, src(A(H->pres), -1.0), s_ccc, A(H->px), false, 1.0);
   // y-momentum (:978-1242)
-  run_pair(H, 0, D1P2C, H->mbcx_cov2, nullptr, prod(H->qxiy, H->qyix, -1.0), H->mbcx_tau2, nullptr,
-           lin(H->qxdy, H->qydx, 1.0, 1.0), rre, s_ppc, H->my, false, nullptr);
+  run_pair(H, 0, D1P2C, H->mbcx_cov2, nullptr, prod(A(H->qxiy), A(H->qyix), -1.0), H->mbcx_tau2, nullptr,
+           lin(A(H->qxdy), A(H->qydx), 1.0, 1.0), rre, s_ppc, A(H->my), false, nullptr);
   if (H->fbcy_velo) {
-    PROF(H, 3, 24.0 * 4 * nc0 * nc2,
-         launch_axpby(H->fb_comb, H->fb_conv2, 1.0, H->fb_visc2, rre, (int64_t)4 * nc0 * nc2, st));
+    PROF(H, 3, 24.0 / 8.0 * sizeof(T) * 4 * nc0 * nc2,
+         launch_axpby(A(H->fb_comb), A(H->fb_conv2), 1.0, A(H->fb_visc2), rre, (int64_t)4 * nc0 * nc2, st));
     H->launches++;
   }
-  run_pair(H, 1, D1C2P, H->mbcy_cov2, H->fbcy_velo ? H->fb_conv2 : H->fb_maxp, prod(H->qyiy, H->qyiy, -1.0),
-           H->mbcy_tau2, H->fbcy_velo ? H->fb_visc2 : H->fb_maxp, lin(H->qydy, H->div, -third, 2.0), rre, s_ccc,
-           H->my, true, H->fb_comb);
-  run_pair(H, 2, D1P2C, H->mbcz_cov2, nullptr, prod(H->qyiz, H->qziy, -1.0), H->mbcz_tau2, nullptr,
-           lin(H->qzdy, H->qydz, 1.0, 1.0), rre, s_cpp, H->my, true, nullptr);
-  run_op(H, 1, D1C2P, by_pr, fympr, src(H->pres, -1.0), s_ccc, H->py, false, 1.0);
+  run_pair(H, 1, D1C2P, H->mbcy_cov2, H->fbcy_velo ? A(H->fb_conv2) : A(H->fb_maxp), prod(A(H->qyiy), A(H->qyiy), -1.0),
+           H->mbcy_tau2, H->fbcy_velo ? A(H->fb_visc2) : A(H->fb_maxp), lin(A(H->qydy), A(H->div), -third, 2.0), rre, s_ccc,
+           A(H->my), true, A(H->fb_comb));
+  run_pair(H, 2, D1P2C, H->mbcz_cov2, nullptr, prod(A(H->qyiz), A(H->qziy), -1.0), H->mbcz_tau2, nullptr,
+           lin(A(H->qzdy), A(H->qydz), 1.0, 1.0), rre, s_cpp, A(H->my), true, nullptr);
+  run_op(H, 1, D1C2P, by_pr, fympr, src(A(H->pres), -1.0), s_ccc, A(H->py), false, 1.0);
   // z-momentum (:1262-1457)
-  run_pair(H, 0, D1P2C, H->mbcx_cov3, nullptr, prod(H->qxiz, H->qzix, -1.0), H->mbcx_tau3, nullptr,
-           lin(H->qxdz, H->qzdx, 1.0, 1.0), rre, s_pcp, H->mz, false, nullptr);
-  run_pair(H, 1, D1P2C, H->mbcy_cov3, nullptr, prod(H->qyiz, H->qziy, -1.0), H->mbcy_tau3, nullptr,
-           lin(H->qzdy, H->qydz, 1.0, 1.0), rre, s_cpp, H->mz, true, nullptr);
-  run_pair(H, 2, D1C2P, H->mbcz_cov3, any, prod(H->qziz, H->qziz, -1.0), H->mbcz_tau3, any,
-           lin(H->qzdz, H->div, -third, 2.0), rre, s_ccc, H->mz, true, nullptr);
-  run_op(H, 2, D1C2P, bz_pr, any, src(H->pres, -1.0), s_ccc, H->pz, false, 1.0);
+  run_pair(H, 0, D1P2C, H->mbcx_cov3, nullptr, prod(A(H->qxiz), A(H->qzix), -1.0), H->mbcx_tau3, nullptr,
+           lin(A(H->qxdz), A(H->qzdx), 1.0, 1.0), rre, s_pcp, A(H->mz), false, nullptr);
+  run_pair(H, 1, D1P2C, H->mbcy_cov3, nullptr, prod(A(H->qyiz), A(H->qziy), -1.0), H->mbcy_tau3, nullptr,
+           lin(A(H->qzdy), A(H->qydz), 1.0, 1.0), rre, s_cpp, A(H->mz), true, nullptr);
+  run_pair(H, 2, D1C2P, H->mbcz_cov3, any, prod(A(H->qziz), A(H->qziz), -1.0), H->mbcz_tau3, any,
+           lin(A(H->qzdz), A(H->div), -third, 2.0), rre, s_ccc, A(H->mz), true, nullptr);
+  run_op(H, 2, D1C2P, bz_pr, any, src(A(H->pres), -1.0), s_ccc, A(H->pz), false, 1.0);
 
   // ---- 3. fractional step, mass flux
-  PROF(H, 3, 40.0 * H->n_pcc,
-       launch_fractional_step(H->mx, H->mx0, H->px, (int64_t)H->n_pcc, H->dt, H->tGamma[isub], H->tZeta[isub],
+  PROF(H, 3, 40.0 / 8.0 * sizeof(T) * H->n_pcc,
+       launch_fractional_step(A(H->mx), A(H->mx0), A(H->px), (int64_t)H->n_pcc, H->dt, H->tGamma[isub], H->tZeta[isub],
                               H->tAlpha[isub], st));
-  PROF(H, 3, 40.0 * H->n_cpc,
-       launch_fractional_step(H->my, H->my0, H->py, (int64_t)H->n_cpc, H->dt, H->tGamma[isub], H->tZeta[isub],
+  PROF(H, 3, 40.0 / 8.0 * sizeof(T) * H->n_cpc,
+       launch_fractional_step(A(H->my), A(H->my0), A(H->py), (int64_t)H->n_cpc, H->dt, H->tGamma[isub], H->tZeta[isub],
                               H->tAlpha[isub], st));
-  PROF(H, 3, 40.0 * H->n_ccp,
-       launch_fractional_step(H->mz, H->mz0, H->pz, (int64_t)H->n_ccp, H->dt, H->tGamma[isub], H->tZeta[isub],
+  PROF(H, 3, 40.0 / 8.0 * sizeof(T) * H->n_ccp,
+       launch_fractional_step(A(H->mz), A(H->mz0), A(H->pz), (int64_t)H->n_ccp, H->dt, H->tGamma[isub], H->tZeta[isub],
                               H->tAlpha[isub], st));
   H->launches += 3;
   const double* bulk = nullptr;
   if (H->idriven == 1) {
-    PROF(H, 3, 8.0 * H->n_pcc,
-         launch_weighted_mean(H->mx, H->wy, np0, nc1, nc2, H->partial, H->npart, H->scal + 0, H->vol, st));
+    PROF(H, 3, 8.0 / 8.0 * sizeof(T) * H->n_pcc,
+         launch_weighted_mean(A(H->mx), H->wy, np0, nc1, nc2, H->partial, H->npart, H->scal + 0, H->vol, st));
     bulk = H->scal + 0;
     H->launches += 2;
   }
   // ---- 4. q += rhs, walls
-  PROF(H, 3, 24.0 * H->n_pcc, launch_update_q(H->qx, H->mx, bulk, (int64_t)H->n_pcc, st));
-  PROF(H, 3, 24.0 * H->n_cpc, launch_update_q(H->qy, H->my, nullptr, (int64_t)H->n_cpc, st));
-  PROF(H, 3, 24.0 * H->n_ccp, launch_update_q(H->qz, H->mz, nullptr, (int64_t)H->n_ccp, st));
+  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_pcc, launch_update_q(A(H->qx), A(H->mx), bulk, (int64_t)H->n_pcc, st));
+  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc, launch_update_q(A(H->qy), A(H->my), nullptr, (int64_t)H->n_cpc, st));
+  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccp, launch_update_q(A(H->qz), A(H->mz), nullptr, (int64_t)H->n_ccp, st));
   H->launches += 3;
   const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
   if (w0 || w1) {
-    PROF(H, 3, 16.0 * nc0 * nc2,
-         launch_set_yrows(H->qy, nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+    PROF(H, 3, 16.0 / 8.0 * sizeof(T) * nc0 * nc2,
+         launch_set_yrows(A(H->qy), nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
     H->launches++;
   }
   // ---- 5. Poisson RHS, solve, pressure and projection
   const double coeff = 1.0 / (H->tAlpha[isub] * H->sigma2p * H->dt);
-  run_op(H, 0, D1P2C, bx_qx, any, src(H->qx), s_pcc, H->pcor, false, coeff);
-  run_op(H, 1, D1P2C, by_qy, nullptr, src(H->qy), s_cpc, H->pcor, true, coeff);
-  run_op(H, 2, D1P2C, bz_qz, nullptr, src(H->qz), s_ccp, H->pcor, true, coeff);
-  poisson_device(H, H->pcor);
-  PROF(H, 3, 24.0 * H->n_ccc, launch_axpby(H->pres, H->pres, 1.0, H->pcor, 1.0, (int64_t)H->n_ccc, st));
+  run_op(H, 0, D1P2C, bx_qx, any, src(A(H->qx)), s_pcc, A(H->pcor), false, coeff);
+  run_op(H, 1, D1P2C, by_qy, nullptr, src(A(H->qy)), s_cpc, A(H->pcor), true, coeff);
+  run_op(H, 2, D1P2C, bz_qz, nullptr, src(A(H->qz)), s_ccp, A(H->pcor), true, coeff);
+  poisson_device<T>(H, A(H->pcor));
+  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, launch_axpby(A(H->pres), A(H->pres), 1.0, A(H->pcor), 1.0, (int64_t)H->n_ccc, st));
   H->launches++;
   const double f = H->dt * H->tAlpha[isub] * H->sigma2p;
-  run_op(H, 0, D1C2P, bx_pr, any, src(H->pcor), s_ccc, H->qx, true, -f);
-  run_op(H, 1, D1C2P, by_pr, fypr, src(H->pcor), s_ccc, H->qy, true, -f);
-  run_op(H, 2, D1C2P, bz_pr, any, src(H->pcor), s_ccc, H->qz, true, -f);
+  run_op(H, 0, D1C2P, bx_pr, any, src(A(H->pcor)), s_ccc, A(H->qx), true, -f);
+  run_op(H, 1, D1C2P, by_pr, fypr, src(A(H->pcor)), s_ccc, A(H->qy), true, -f);
+  run_op(H, 2, D1C2P, bz_pr, any, src(A(H->pcor)), s_ccc, A(H->qz), true, -f);
   if (w0 || w1) {
-    PROF(H, 3, 16.0 * nc0 * nc2,
-         launch_set_yrows(H->qy, nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+    PROF(H, 3, 16.0 / 8.0 * sizeof(T) * nc0 * nc2,
+         launch_set_yrows(A(H->qy), nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
     H->launches++;
   }
+}
+
+void substep_body(chs_handle* H, int isub) {
+  if (H->mixed) substep_body_t<float>(H, isub);
+  else substep_body_t<double>(H, isub);
 }
 
 // Prepare every plan the substep uses (plans are host objects; the table must be final
@@ -775,6 +810,26 @@ double* field_ptr(chs_handle* H, int field, size_t* n) {
   }
 }
 
+// host (double) -> device field, converting to float in the mixed form (stream-ordered)
+void h2d_field(chs_handle* H, double* dev, const double* host, size_t n) {
+  if (!H->mixed) {
+    CK(cudaMemcpyAsync(dev, host, n * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    return;
+  }
+  CK(cudaMemcpyAsync(H->stage, host, n * sizeof(double), cudaMemcpyHostToDevice, H->st));
+  launch_convert(reinterpret_cast<float*>(dev), H->stage, (int64_t)n, H->st);
+  H->launches++;
+}
+void d2h_field(chs_handle* H, double* host, const double* dev, size_t n) {
+  if (!H->mixed) {
+    CK(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    return;
+  }
+  launch_convert(H->stage, reinterpret_cast<const float*>(dev), (int64_t)n, H->st);
+  H->launches++;
+  CK(cudaMemcpyAsync(host, H->stage, n * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+}
+
 void capture_graphs(chs_handle* H) {
   for (int isub = 1; isub <= 3; ++isub) {
     cudaGraph_t g;
@@ -839,7 +894,7 @@ int chs_upload_field(chs_handle* H, int field, const double* host, size_t n) {
     size_t m;
     double* d = field_ptr(H, field, &m);
     if (n != m) throw std::invalid_argument("field size mismatch");
-    CK(cudaMemcpyAsync(d, host, n * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    h2d_field(H, d, host, n);
     CK(cudaStreamSynchronize(H->st));
   });
 }
@@ -850,7 +905,7 @@ int chs_download_field(chs_handle* H, int field, double* host, size_t n) {
     size_t m;
     double* d = field_ptr(H, field, &m);
     if (n != m) throw std::invalid_argument("field size mismatch");
-    CK(cudaMemcpyAsync(host, d, n * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    d2h_field(H, host, d, n);
     CK(cudaStreamSynchronize(H->st));
   });
 }
@@ -886,10 +941,10 @@ int chs_momentum_substep_host(chs_handle* H, int isub, double* qx, double* qy, d
   if (!H || !qx || !qy || !qz || !pres) return CHS_ERR_ARG;
   if (isub < 0 || isub > 3) { set_err(H, "isub must be 0..3"); return CHS_ERR_ARG; }
   return guard(H, [&] {
-    CK(cudaMemcpyAsync(H->qx, qx, H->n_pcc * sizeof(double), cudaMemcpyHostToDevice, H->st));
-    CK(cudaMemcpyAsync(H->qy, qy, H->n_cpc * sizeof(double), cudaMemcpyHostToDevice, H->st));
-    CK(cudaMemcpyAsync(H->qz, qz, H->n_ccp * sizeof(double), cudaMemcpyHostToDevice, H->st));
-    CK(cudaMemcpyAsync(H->pres, pres, H->n_ccc * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    h2d_field(H, H->qx, qx, H->n_pcc);
+    h2d_field(H, H->qy, qy, H->n_cpc);
+    h2d_field(H, H->qz, qz, H->n_ccp);
+    h2d_field(H, H->pres, pres, H->n_ccc);
     if (isub >= 1) {
       if (!H->gexec[1]) capture_graphs(H);
       CK(cudaGraphLaunch(H->gexec[isub], H->st));
@@ -897,10 +952,10 @@ int chs_momentum_substep_host(chs_handle* H, int isub, double* qx, double* qy, d
     } else {
       substep_body(H, isub);
     }
-    CK(cudaMemcpyAsync(qx, H->qx, H->n_pcc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
-    CK(cudaMemcpyAsync(qy, H->qy, H->n_cpc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
-    CK(cudaMemcpyAsync(qz, H->qz, H->n_ccp * sizeof(double), cudaMemcpyDeviceToHost, H->st));
-    CK(cudaMemcpyAsync(pres, H->pres, H->n_ccc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    d2h_field(H, qx, H->qx, H->n_pcc);
+    d2h_field(H, qy, H->qy, H->n_cpc);
+    d2h_field(H, qz, H->qz, H->n_ccp);
+    d2h_field(H, pres, H->pres, H->n_ccc);
     CK(cudaStreamSynchronize(H->st));
   });
 }
@@ -936,16 +991,16 @@ int chs_time_steps_host(chs_handle* H, int nsteps, double* qx, double* qy, doubl
     CK(cudaEventRecord(a, H->st));
     for (int s = 0; s < nsteps; ++s)
       for (int isub = 1; isub <= 3; ++isub) {
-        CK(cudaMemcpyAsync(H->qx, qx, H->n_pcc * sizeof(double), cudaMemcpyHostToDevice, H->st));
-        CK(cudaMemcpyAsync(H->qy, qy, H->n_cpc * sizeof(double), cudaMemcpyHostToDevice, H->st));
-        CK(cudaMemcpyAsync(H->qz, qz, H->n_ccp * sizeof(double), cudaMemcpyHostToDevice, H->st));
-        CK(cudaMemcpyAsync(H->pres, pres, H->n_ccc * sizeof(double), cudaMemcpyHostToDevice, H->st));
+        h2d_field(H, H->qx, qx, H->n_pcc);
+        h2d_field(H, H->qy, qy, H->n_cpc);
+        h2d_field(H, H->qz, qz, H->n_ccp);
+        h2d_field(H, H->pres, pres, H->n_ccc);
         CK(cudaGraphLaunch(H->gexec[isub], H->st));
         H->launches += H->kernels_per_sub[isub];
-        CK(cudaMemcpyAsync(qx, H->qx, H->n_pcc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
-        CK(cudaMemcpyAsync(qy, H->qy, H->n_cpc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
-        CK(cudaMemcpyAsync(qz, H->qz, H->n_ccp * sizeof(double), cudaMemcpyDeviceToHost, H->st));
-        CK(cudaMemcpyAsync(pres, H->pres, H->n_ccc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+        d2h_field(H, qx, H->qx, H->n_pcc);
+        d2h_field(H, qy, H->qy, H->n_cpc);
+        d2h_field(H, qz, H->qz, H->n_ccp);
+        d2h_field(H, pres, H->pres, H->n_ccc);
       }
     CK(cudaEventRecord(b, H->st));
     CK(cudaEventSynchronize(b));
@@ -995,9 +1050,11 @@ int chs_profile_substep(chs_handle* H, int isub, chs_kprof* out, int max, int* n
 int chs_poisson_solve(chs_handle* H, double* rhs) {
   if (!H || !rhs) return CHS_ERR_ARG;
   return guard(H, [&] {
-    CK(cudaMemcpyAsync(H->pcor, rhs, H->n_ccc * sizeof(double), cudaMemcpyHostToDevice, H->st));
-    poisson_device(H, H->pcor);
-    CK(cudaMemcpyAsync(rhs, H->pcor, H->n_ccc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    // FP64 buffer: the correction field itself, or the staging array in the mixed form
+    double* buf = H->mixed ? H->stage : H->pcor;
+    CK(cudaMemcpyAsync(buf, rhs, H->n_ccc * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    poisson_device(H, buf);
+    CK(cudaMemcpyAsync(rhs, buf, H->n_ccc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
     CK(cudaStreamSynchronize(H->st));
   });
 }
@@ -1016,18 +1073,30 @@ int chs_diagnostics(chs_handle* H, chs_diag* out) {
     const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
     const int s_pcc[3] = {H->np[0], nc1, nc2}, s_cpc[3] = {nc0, H->np[1], nc2}, s_ccp[3] = {nc0, nc1, H->np[2]};
     const Pair bx = P2(H->ibc[0][V_QX]), by = P2(H->ibc[1][V_QY]), bz = P2(H->ibc[2][V_QZ]);
+    // The checks run in FP64.  In the mixed form the FP32 velocities are first widened into
+    // the (FP64-sized) RHS work arrays, and FP64 wall planes are built in the spare planes.
+    double *qx = H->qx, *qy = H->qy, *qz = H->qz, *fmaxp = H->fb_maxp, *fqy = H->fb_qy;
+    if (H->mixed) {
+      launch_convert(H->mx, reinterpret_cast<const float*>(H->qx), (int64_t)H->n_pcc, H->st);
+      launch_convert(H->my, reinterpret_cast<const float*>(H->qy), (int64_t)H->n_cpc, H->st);
+      launch_convert(H->mz, reinterpret_cast<const float*>(H->qz), (int64_t)H->n_ccp, H->st);
+      launch_fbcy_const(H->fb_comb, nc0, nc2, kMaxp, kMaxp, H->st);
+      launch_fbcy_const(H->fb_visc2, nc0, nc2, H->fbcy[V_QY][0], H->fbcy[V_QY][1], H->st);
+      qx = H->mx; qy = H->my; qz = H->mz; fmaxp = H->fb_comb; fqy = H->fb_visc2;
+      H->launches += 5;
+    }
     // divergence (Get_divergence_flow, src/eq_continuity.f90:91-161) into `div`
-    run_op(H, 0, D1P2C, bx, H->fb_maxp, src(H->qx), s_pcc, H->div, false, 1.0);
-    run_op(H, 1, D1P2C, by, nullptr, src(H->qy), s_cpc, H->div, true, 1.0);
-    run_op(H, 2, D1P2C, bz, nullptr, src(H->qz), s_ccp, H->div, true, 1.0);
+    run_op(H, 0, D1P2C, bx, fmaxp, src(qx), s_pcc, H->div, false, 1.0);
+    run_op(H, 1, D1P2C, by, nullptr, src(qy), s_cpc, H->div, true, 1.0);
+    run_op(H, 2, D1P2C, bz, nullptr, src(qz), s_ccp, H->div, true, 1.0);
     launch_absmax(H->div, (int64_t)H->n_ccc, H->partial, H->npart, H->scal + 2, H->st);
     // kinetic energy of the P2C-interpolated velocities (src/io_monitor.f90:209-241)
-    run_op(H, 0, M1P2C, bx, H->fb_maxp, src(H->qx), s_pcc, H->qxix, false, 1.0);
-    run_op(H, 1, M1P2C, by, H->periodic_y ? nullptr : H->fb_qy, src(H->qy), s_cpc, H->qyiy, false, 1.0);
-    run_op(H, 2, M1P2C, bz, H->fb_maxp, src(H->qz), s_ccp, H->qziz, false, 1.0);
+    run_op(H, 0, M1P2C, bx, fmaxp, src(qx), s_pcc, H->qxix, false, 1.0);
+    run_op(H, 1, M1P2C, by, H->periodic_y ? nullptr : fqy, src(qy), s_cpc, H->qyiy, false, 1.0);
+    run_op(H, 2, M1P2C, bz, fmaxp, src(qz), s_ccp, H->qziz, false, 1.0);
     launch_ke_density(H->qxdx, H->qxix, H->qyiy, H->qziz, (int64_t)H->n_ccc, H->st);
     launch_weighted_mean(H->qxdx, H->wy, nc0, nc1, nc2, H->partial, H->npart, H->scal + 4, H->vol, H->st);
-    launch_weighted_mean(H->qx, H->wy, H->np[0], nc1, nc2, H->partial, H->npart, H->scal + 5, H->vol, H->st);
+    launch_weighted_mean(qx, H->wy, H->np[0], nc1, nc2, H->partial, H->npart, H->scal + 5, H->vol, H->st);
     H->launches += 7;
     double s[8];
     CK(cudaMemcpyAsync(s, H->scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, H->st));
