@@ -101,6 +101,76 @@ def channel(nc=(128, 96, 128), rstret=0.075, ren=2800.0, iacc=IACCU_CP6, dt=None
 
 
 # ---------------------------------------------------------------------------
+# variable-property (thermal) runs
+# ---------------------------------------------------------------------------
+T_PC = 0.5  # pseudo-critical temperature of the synthetic fluid
+
+
+def _h_of_t(t):
+    """h(T) = integral of cp from T_PC (closed form for cp = 1 + 4/(1+((T-0.5)/0.02)^2))."""
+    x = np.asarray(t, np.float64) - T_PC
+    return x + 0.08 * np.arctan(x / 0.02)
+
+
+def synthetic_table(n=4096):
+    """Nondimensional property table of the heated-channel case, sorted by T.
+
+    cp(T) = 1 + 4/(1+((T-0.5)/0.02)^2), h = integral of cp dT, rho = 1 - 0.6 (1+tanh((T-0.5)/0.03))/2,
+    mu = rho^0.7, kappa = cp^0.5, beta = -(1/rho) drho/dT.  h is measured from the pseudo-critical
+    point and the T range is symmetric about it with h spanning a unit interval, h in [-1/2, 1/2];
+    with h = 0 at T = 0.5 the table's rho*h is monotonic in T, which the reference's rho*h lookup
+    requires (src/input_thermo.f90:560-598).  Columns are (T, h, rho, mu, kappa, cp, beta), the
+    nondimensional form of the reference's table file (P H T D M K CP B, src/input_thermo.f90:640-657).
+    """
+    lo, hi = 0.0, 0.5
+    for _ in range(200):  # x + 0.08 atan(x/0.02) = 1/2
+        mid = 0.5 * (lo + hi)
+        if _h_of_t(T_PC + mid) < 0.5:
+            lo = mid
+        else:
+            hi = mid
+    x = 0.5 * (lo + hi)
+    t = np.linspace(T_PC - x, T_PC + x, n)
+    h = _h_of_t(t)
+    cp = 1.0 + 4.0 / (1.0 + ((t - T_PC) / 0.02) ** 2)
+    th = np.tanh((t - T_PC) / 0.03)
+    d = 1.0 - 0.6 * (1.0 + th) / 2.0
+    m = d ** 0.7
+    k = cp ** 0.5
+    b = (0.3 / 0.03) * (1.0 - th * th) / d
+    return dict(t=t, h=h, d=d, m=m, k=k, cp=cp, b=b)
+
+
+def constant_table(n=256):
+    """Constant-property table (rho = mu = kappa = cp = 1, h = T): the variable-property path then
+    reproduces the constant-property momentum solution."""
+    t = np.linspace(-1.0, 2.0, n)
+    one = np.ones(n)
+    return dict(t=t, h=t.copy(), d=one, m=one.copy(), k=one.copy(), cp=one.copy(), b=np.zeros(n))
+
+
+@dataclass
+class ThermoConfig:
+    """Thermal set-up of a variable-property run (input_thermo / [thermo] section)."""
+    table: dict
+    t_ini: float = 0.47
+    prandtl: float = 1.0  # rPrRen = 1/(Re Pr) with unit reference properties (src/tools_solver.f90:63)
+    qw: tuple = (-1.0, 1.0)  # dT/dy at the y walls: heat flux q_w = 1 into the fluid at both walls
+
+
+def heated_channel(nc=(128, 96, 128), iacc=IACCU_CD2, dt=None, rstret=0.075, ren=2800.0, table=None, t_ini=0.47):
+    """Heated channel with variable properties (same grid and flow as the channel) and isoflux
+    y walls: T is Neumann at the walls, so the property BC is Dirichlet there
+    (src/bc_general.f90:182-186).  Returns (DomainConfig, ThermoConfig)."""
+    cfg = channel(nc=nc, rstret=rstret, ren=ren, iacc=iacc, dt=dt)
+    cfg.nominal_bc[1, V_TM] = IBC_NEUMANN
+    cfg.name = f"heated{nc[0]}x{nc[1]}x{nc[2]}"
+    tc = ThermoConfig(table=table if table is not None else synthetic_table(), t_ini=t_ini)
+    cfg.fbcy_const[V_TM] = tc.qw
+    return cfg, tc
+
+
+# ---------------------------------------------------------------------------
 # geometry (src/geometry.f90)
 # ---------------------------------------------------------------------------
 def _tanh_mapping(cfg, node, n):

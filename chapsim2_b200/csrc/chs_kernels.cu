@@ -714,13 +714,14 @@ void launch_ysolve_factor(double* Zr, double* D, int nxh, int ny, int nz, const 
   ysolve_factor_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(Zr, D, nxh, ny, nz, pa, pb, pc, lamx, lamz);
 }
 
-// One CTA per `lt` consecutive (kx, kz) columns: the columns are staged in shared memory with
-// coalesced row loads by all threads, swept by `lt` threads (one column each) with the
-// precomputed factors, and written back.
+// One CTA per `lt` consecutive (kx, kz) columns: the columns and their precomputed factors are
+// staged in shared memory with coalesced row loads by all threads (eight loads in flight per
+// thread), swept by `lt` threads (one column each), and written back.
 __global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data, int nxh, int ny, int nz,
                                                      const double* __restrict__ Zr, const double* __restrict__ D,
                                                      const double* __restrict__ pa, int lt) {
   extern __shared__ __align__(16) double2 sT[];  // [ny][lt] right-hand sides / solution
+  double2* sF = sT + (size_t)ny * lt;            // [ny][lt] (Zr, D) pairs
   const int tid = threadIdx.x;
   const int l = tid % lt;
   const int64_t nl = (int64_t)nxh * nz;
@@ -732,39 +733,45 @@ __global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data,
   double2* col = data + base;
   const int jstep = blockDim.x / lt;
   if (ok) {
-    for (int j0 = tid / lt; j0 < ny; j0 += 8 * jstep) {
-      double2 v[8];
+    for (int j0 = tid / lt; j0 < ny; j0 += 4 * jstep) {
+      double2 v[4];
+      double z[4], d[4];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < 4; ++u) {
         const int j = j0 + u * jstep;
-        if (j < ny) v[u] = col[(int64_t)j * nxh];
+        if (j < ny) {
+          v[u] = col[(int64_t)j * nxh];
+          z[u] = Zr[base + (int64_t)j * nxh];
+          d[u] = D[base + (int64_t)j * nxh];
+        }
       }
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < 4; ++u) {
         const int j = j0 + u * jstep;
-        if (j < ny) sT[j * lt + l] = v[u];
+        if (j < ny) {
+          sT[j * lt + l] = v[u];
+          sF[j * lt + l] = make_double2(z[u], d[u]);
+        }
       }
     }
   }
   __syncthreads();
   if (tid < lt && ok) {
     double2* T = sT + l;
-    const double* zr = Zr + base;
-    const double* dd = D + base;
+    const double2* F = sF + l;
     double2 tp = T[0];
-    double Z = zr[0];
-    tp.x *= Z; tp.y *= Z;
+    const double Z0 = F[0].x;
+    tp.x *= Z0; tp.y *= Z0;
     T[0] = tp;
-#pragma unroll 4
     for (int j = 1; j < ny - 1; ++j) {
-      const double z = zr[(int64_t)j * nxh], a = pa[j];
+      const double z = F[j * lt].x, a = pa[j];
       double2 v = T[j * lt];
       v.x = (v.x - a * tp.x) * z;
       v.y = (v.y - a * tp.y) * z;
       T[j * lt] = v;
       tp = v;
     }
-    const double zl = zr[(int64_t)(ny - 1) * nxh];
+    const double zl = F[(ny - 1) * lt].x;
     double2 v = T[(ny - 1) * lt];
     // TRID0's singular-pivot pin: the last unknown is zero when the pivot vanishes
     if (zl != 0.0) {
@@ -775,9 +782,8 @@ __global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data,
       v.y = 0.0;
     }
     T[(ny - 1) * lt] = v;
-#pragma unroll 4
     for (int j = ny - 2; j >= 0; --j) {
-      const double d = dd[(int64_t)j * nxh];
+      const double d = F[j * lt].y;
       double2 u = T[j * lt];
       u.x = u.x - d * v.x;
       u.y = u.y - d * v.y;
@@ -794,8 +800,8 @@ void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* Zr, con
                    cudaStream_t st) {
   if (ny < 2) throw std::runtime_error("ysolve: ny must be at least 2");
   int lt = 32;
-  while (lt > 4 && (size_t)ny * lt * 16 > 110 * 1024) lt /= 2;
-  const size_t shm = (size_t)ny * lt * 16;
+  while (lt > 4 && (size_t)ny * lt * 32 > 110 * 1024) lt /= 2;
+  const size_t shm = (size_t)ny * lt * 32;
   if (shm > 200 * 1024) throw std::runtime_error("ysolve: ny too large for the shared-memory tile");
   static bool attr_set = false;
   if (!attr_set) {

@@ -47,10 +47,41 @@ struct Domain {
   std::vector<double> xrt, zrt, pa, pb, pc;  // FISHPACK roots and y coefficients
 };
 
+// One thermal state (t_fluidThermoProperty, src/modules.f90): nondimensional values.
+struct Ftp {
+  double rhoh, h, t, d, m, k, cp, b;
+};
+
+// Property table sorted by T (ftplist, src/input_thermo.f90:512-556), nondimensional, with the
+// rho*h range used for clamping (:683-688).
+struct ThermoTable {
+  std::vector<double> t, h, d, m, k, cp, b, rhoh;
+  double dhmin = 0.0, dhmax = 0.0;
+  int n() const { return (int)t.size(); }
+};
+
+// Thermal state of a variable-property run (t_thermo plus the flow's density, viscosity and
+// momentum, src/modules.f90:412-681).  Ordering of ccc arrays: x fastest.
+struct Thermo {
+  ThermoTable tab;
+  double rPrRen = 0.0;
+  double qw[2] = {0.0, 0.0};  // wall heat flux (Neumann T) at y walls, fbcy_qw
+  std::vector<double> rhoh, hEnth, tTemp, kCond, dDens, mVisc, ene_rhs0;  // ccc
+  std::vector<double> gx, gy, gz;                                          // pcc, cpc, ccp
+  std::vector<Ftp> fbcy_ftp;  // wall states, reference layout (nc0, 4, nc2)
+};
+
 struct Flow {
   std::vector<double> qx, qy, qz, pres, pcor;
   std::vector<double> mx_rhs0, my_rhs0, mz_rhs0;
+  bool thermo = false;
+  Thermo th;
 };
+
+// ftp_refresh_thermal_properties_from_H / _from_DH (src/input_thermo.f90:345-446)
+void ftp_from_h(const ThermoTable& tb, Ftp& f);
+void ftp_from_dh(const ThermoTable& tb, Ftp& f);
+void ftp_from_t(const ThermoTable& tb, Ftp& f);
 
 int op_out_len(const Domain& dm, int dir, int fam);
 int op_in_len(const Domain& dm, int dir, int fam);

@@ -1,9 +1,9 @@
 // ORACLE (test infrastructure only; never linked into the product library).
 //
-// CPU FP64 restatement of CHAPSim2's flow-only, Cartesian RK3 substep:
+// CPU FP64 restatement of CHAPSim2's Cartesian RK3 substep, flow-only and variable-property:
 //   geometry            src/geometry.f90:151-269, :410-530
 //   boundary conditions src/bc_general.f90:137-248, :455-760, src/bc_dirichlet.f90:206-231, :461-516
-//   momentum RHS        src/eq_momentum2.f90:101-1571 (Cartesian, non-thermal branches)
+//   momentum RHS        src/eq_momentum2.f90:101-1571 (Cartesian branches)
 //   fractional step     src/eq_momentum2.f90:35-71, RK3 constants src/input_general.f90:851-886
 //   mass-flux driving   src/eq_momentum2.f90:1547-1562, src/tools_general.f90:1202-1268
 //   Poisson RHS         src/eq_momentum2.f90:1663-1718, src/eq_continuity.f90:91-161
@@ -12,7 +12,13 @@
 //   3D-FFT Poisson      src/poisson_1stderivcomp.f90:1016-1195 (poisson_000), :2343-2714
 //   correction          src/eq_momentum2.f90:1577-1660, :1799-1932
 //   KE monitor          src/io_monitor.f90:209-241
+//   energy equation     src/eq_energy.f90:148-458 (Compute_energy_rhs, Solve_energy_eq)
+//   property update     src/eq_energy.f90:14-146, src/input_thermo.f90:272-446 (table lookups)
+//   q <-> g conversion  src/para_conversion.f90:5-227
+//   momentum, thermal   src/eq_momentum2.f90:576-703 (g and mu interpolations) and the
+//                       is_thermo branches of :796-1457, :1577-1660, :1799-1932
 // Restriction: x and z must be periodic (the channel and Taylor-Green configurations).
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -246,6 +252,56 @@ struct Rhs3 {
   Arr mx, my, mz, px, py, pz;
 };
 
+static Arr op(const Domain& dm, int dir, int fam, const int ibc[2], const std::vector<double>* fbc, const Arr& in);
+static std::vector<double> fbcy_const_plane(int n1, int n3, double v1, double v2);
+
+static std::vector<double> extract_fbcy(const Arr& a);
+// x and z are periodic for every configuration of this build: their property BCs are periodic
+static const int* PER2_FTPX(const Domain&) { static const int p[2] = {BC_PERIODIC, BC_PERIODIC}; return p; }
+static const int* PER2_FTPZ(const Domain&) { static const int p[2] = {BC_PERIODIC, BC_PERIODIC}; return p; }
+
+// Property-dependent inputs of the momentum RHS (src/eq_momentum2.f90:576-703): interpolated
+// momentum g and viscosity.  For constant-property flow every factor is 1 and g = q.
+struct ThermoMom {
+  Arr gxix_ccc, gxiy_ppc, gxiz_pcp, gyix_ppc, gyiy_ccc, gyiz_cpp, gzix_pcp, gziy_cpp, gziz_ccc;
+  Arr mu_ccc, muixy_ppc, muixz_pcp, muiyz_cpp;
+  std::vector<double> fbcy_mu;  // mu at the y walls (fbcy_mu_c4c)
+};
+
+static void thermo_mom_inputs(const Domain& dm, const Flow& fl, ThermoMom& t) {
+  const int nc0 = dm.nc[0], nc1 = dm.nc[1], nc2 = dm.nc[2];
+  const int np0 = dm.np[0], np1 = dm.np[1], np2 = dm.np[2];
+  const Thermo& th = fl.th;
+  Arr gx(np0, nc1, nc2), gy(nc0, np1, nc2), gz(nc0, nc1, np2), mu(nc0, nc1, nc2);
+  gx.v = th.gx; gy.v = th.gy; gz.v = th.gz; mu.v = th.mVisc;
+  std::vector<double> fbcx_any((size_t)4 * np1 * np2 + 4 * nc1 * np2 + 16, MAXP);
+  std::vector<double> fbcz_any((size_t)np0 * np1 * 4 + 16, MAXP);
+  // no-slip walls: g = rho * q = 0 there (convert_primary_conservative, src/para_conversion.f90:5-227)
+  const auto fg_x = fbcy_const_plane(np0, nc2, dm.fbcy_const[V_QX][0], dm.fbcy_const[V_QX][1]);
+  const auto fg_y = fbcy_const_plane(nc0, nc2, dm.fbcy_const[V_QY][0], dm.fbcy_const[V_QY][1]);
+  const auto fg_z = fbcy_const_plane(nc0, np2, dm.fbcy_const[V_QZ][0], dm.fbcy_const[V_QZ][1]);
+  t.gxix_ccc = op(dm, 0, FAM_M1P2C, dm.ibcx[V_QX], &fbcx_any, gx);
+  t.gxiy_ppc = op(dm, 1, FAM_M1C2P, dm.ibcy[V_QX], &fg_x, gx);
+  t.gxiz_pcp = op(dm, 2, FAM_M1C2P, dm.ibcz[V_QX], &fbcz_any, gx);
+  t.gyix_ppc = op(dm, 0, FAM_M1C2P, dm.ibcx[V_QY], &fbcx_any, gy);
+  t.gyiy_ccc = op(dm, 1, FAM_M1P2C, dm.ibcy[V_QY], &fg_y, gy);
+  t.gyiz_cpp = op(dm, 2, FAM_M1C2P, dm.ibcz[V_QY], &fbcz_any, gy);
+  t.gzix_pcp = op(dm, 0, FAM_M1C2P, dm.ibcx[V_QZ], &fbcx_any, gz);
+  t.gziy_cpp = op(dm, 1, FAM_M1C2P, dm.ibcy[V_QZ], &fg_z, gz);
+  t.gziz_ccc = op(dm, 2, FAM_M1P2C, dm.ibcz[V_QZ], &fbcz_any, gz);
+  // viscosity at the y walls from the wall states (fbcy_ftp%m)
+  std::vector<double> fmu((size_t)nc0 * 4 * nc2);
+  for (size_t n = 0; n < fmu.size(); ++n) fmu[n] = th.fbcy_ftp[n].m;
+  t.mu_ccc = mu;
+  Arr muiy_cpc = op(dm, 1, FAM_M1C2P, dm.ibcy_ftp, &fmu, mu);
+  t.muixy_ppc = op(dm, 0, FAM_M1C2P, PER2_FTPX(dm), &fbcx_any, muiy_cpc);
+  Arr mu_pcc = op(dm, 0, FAM_M1C2P, PER2_FTPX(dm), &fbcx_any, mu);
+  t.muixz_pcp = op(dm, 2, FAM_M1C2P, PER2_FTPZ(dm), nullptr, mu_pcc);
+  t.muiyz_cpp = op(dm, 2, FAM_M1C2P, PER2_FTPZ(dm), nullptr, muiy_cpc);
+  // fbcy_mu_c4c: rows j = 1 and j = np of mu_cpc; planes 3, 4 repeat planes 1, 2
+  t.fbcy_mu = extract_fbcy(muiy_cpc);
+}
+
 static void momentum_rhs(const Domain& dm, const Flow& fl, Rhs3& out) {
   const int nc0 = dm.nc[0], nc1 = dm.nc[1], nc2 = dm.nc[2];
   const int np0 = dm.np[0], np1 = dm.np[1], np2 = dm.np[2];
@@ -312,24 +368,39 @@ static void momentum_rhs(const Domain& dm, const Flow& fl, Rhs3& out) {
   }
   const double rre = dm.rre;
   const double THIRD = 1.0 / 3.0;
+  // first factors of the convection products (g for variable properties, q otherwise) and the
+  // viscosity factors of the stresses (1 for constant properties)
+  ThermoMom tmo;
+  if (fl.thermo) thermo_mom_inputs(dm, fl, tmo);
+  const bool TH = fl.thermo;
+  const Arr& c_xix = TH ? tmo.gxix_ccc : qxix_ccc;
+  const Arr& c_yix = TH ? tmo.gyix_ppc : qyix_ppc;
+  const Arr& c_zix = TH ? tmo.gzix_pcp : qzix_pcp;
+  const Arr& c_xiy = TH ? tmo.gxiy_ppc : qxiy_ppc;
+  const Arr& c_yiy = TH ? tmo.gyiy_ccc : qyiy_ccc;
+  const Arr& c_ziy = TH ? tmo.gziy_cpp : qziy_cpp;
+  const Arr& c_xiz = TH ? tmo.gxiz_pcp : qxiz_pcp;
+  const Arr& c_yiz = TH ? tmo.gyiz_cpp : qyiz_cpp;
+  const Arr& c_ziz = TH ? tmo.gziz_ccc : qziz_ccc;
+  auto MU = [&](const Arr& m, size_t n) { return TH ? m.v[n] : 1.0; };
 
   // ---- x-momentum (eq_momentum2.f90:796-966)
   Arr mx(np0, nc1, nc2), mxy(np0, nc1, nc2), mxz(np0, nc1, nc2), px(np0, nc1, nc2);
   {
     Arr a(nc0, nc1, nc2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -qxix_ccc.v[n] * qxix_ccc.v[n];
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -c_xix.v[n] * qxix_ccc.v[n];
     Arr r = op(dm, 0, FAM_D1C2P, dm.mbcx_cov1, &fbcx_any, a);
     for (size_t n = 0; n < mx.size(); ++n) mx.v[n] = mx.v[n] + r.v[n];
   }
   {
     Arr a(np0, np1, nc2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -qyix_ppc.v[n] * qxiy_ppc.v[n];
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -c_yix.v[n] * qxiy_ppc.v[n];
     Arr r = op(dm, 1, FAM_D1P2C, dm.mbcy_cov1, nullptr, a);
     for (size_t n = 0; n < mxy.size(); ++n) mxy.v[n] = mxy.v[n] + r.v[n];
   }
   {
     Arr a(np0, nc1, np2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -qzix_pcp.v[n] * qxiz_pcp.v[n];
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -c_zix.v[n] * qxiz_pcp.v[n];
     Arr r = op(dm, 2, FAM_D1P2C, dm.mbcz_cov1, nullptr, a);
     for (size_t n = 0; n < mxz.size(); ++n) mxz.v[n] = mxz.v[n] + r.v[n];
   }
@@ -341,19 +412,19 @@ static void momentum_rhs(const Domain& dm, const Flow& fl, Rhs3& out) {
   }
   {
     Arr a(nc0, nc1, nc2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = 2.0 * 1.0 * (qxdx_ccc.v[n] - THIRD * div.v[n]);
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = 2.0 * MU(tmo.mu_ccc, n) * (qxdx_ccc.v[n] - THIRD * div.v[n]);
     Arr r = op(dm, 0, FAM_D1C2P, dm.mbcx_tau1, &fbcx_any, a);
     for (size_t n = 0; n < mx.size(); ++n) mx.v[n] = mx.v[n] + r.v[n] * rre;
   }
   {
     Arr a(np0, np1, nc2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qxdy_ppc.v[n] + qydx_ppc.v[n]) * 1.0;
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qxdy_ppc.v[n] + qydx_ppc.v[n]) * MU(tmo.muixy_ppc, n);
     Arr r = op(dm, 1, FAM_D1P2C, dm.mbcy_tau1, nullptr, a);
     for (size_t n = 0; n < mxy.size(); ++n) mxy.v[n] = mxy.v[n] + r.v[n] * rre;
   }
   {
     Arr a(np0, nc1, np2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qxdz_pcp.v[n] + qzdx_pcp.v[n]) * 1.0;
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qxdz_pcp.v[n] + qzdx_pcp.v[n]) * MU(tmo.muixz_pcp, n);
     Arr r = op(dm, 2, FAM_D1P2C, dm.mbcz_tau1, nullptr, a);
     for (size_t n = 0; n < mxz.size(); ++n) mxz.v[n] = mxz.v[n] + r.v[n] * rre;
   }
@@ -364,24 +435,29 @@ static void momentum_rhs(const Domain& dm, const Flow& fl, Rhs3& out) {
   Arr my(nc0, np1, nc2), myy(nc0, np1, nc2), myz(nc0, np1, nc2), py(nc0, np1, nc2);
   {
     Arr a(np0, np1, nc2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -qxiy_ppc.v[n] * qyix_ppc.v[n];
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -c_xiy.v[n] * qyix_ppc.v[n];
     Arr r = op(dm, 0, FAM_D1P2C, dm.mbcx_cov2, nullptr, a);
     for (size_t n = 0; n < my.size(); ++n) my.v[n] = my.v[n] + r.v[n];
   }
   {
     std::vector<double> fb;
     if (dm.fbcy_velo_required) {
+      // -fbcy_qy * fbcy_gy (thermo) or -fbcy_qy * fbcy_qy; the walls are at rest or moving with
+      // a constant velocity, and fbcy_gy = fbcy_qy * rho there (src/para_conversion.f90:157-169)
       fb = fbcy_qy;
-      for (auto& v : fb) v = -v * v;
+      for (size_t n = 0; n < fb.size(); ++n) {
+        const double g = TH ? fb[n] * fl.th.fbcy_ftp[n].d : fb[n];
+        fb[n] = -fb[n] * g;
+      }
     } else fb.assign(fbcy_qy.size(), MAXP);
     Arr a(nc0, nc1, nc2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -qyiy_ccc.v[n] * qyiy_ccc.v[n];
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -qyiy_ccc.v[n] * c_yiy.v[n];
     Arr r = op(dm, 1, FAM_D1C2P, dm.mbcy_cov2, &fb, a);
     for (size_t n = 0; n < myy.size(); ++n) myy.v[n] = myy.v[n] + r.v[n];
   }
   {
     Arr a(nc0, np1, np2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -qyiz_cpp.v[n] * qziy_cpp.v[n];
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -qyiz_cpp.v[n] * c_ziy.v[n];
     Arr r = op(dm, 2, FAM_D1P2C, dm.mbcz_cov2, nullptr, a);
     for (size_t n = 0; n < myz.size(); ++n) myz.v[n] = myz.v[n] + r.v[n];
   }
@@ -395,7 +471,7 @@ static void momentum_rhs(const Domain& dm, const Flow& fl, Rhs3& out) {
   }
   {
     Arr a(np0, np1, nc2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qxdy_ppc.v[n] + qydx_ppc.v[n]) * 1.0;
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qxdy_ppc.v[n] + qydx_ppc.v[n]) * MU(tmo.muixy_ppc, n);
     Arr r = op(dm, 0, FAM_D1P2C, dm.mbcx_tau2, nullptr, a);
     for (size_t n = 0; n < my.size(); ++n) my.v[n] = my.v[n] + r.v[n] * rre;
   }
@@ -403,16 +479,16 @@ static void momentum_rhs(const Domain& dm, const Flow& fl, Rhs3& out) {
     std::vector<double> fb;
     if (dm.fbcy_velo_required) {
       fb = extract_fbcy(qydy_cpc);
-      for (size_t n = 0; n < fb.size(); ++n) fb[n] = (fb[n] - THIRD * fbcy_div[n]) * 2.0 * 1.0;
+      for (size_t n = 0; n < fb.size(); ++n) fb[n] = (fb[n] - THIRD * fbcy_div[n]) * 2.0 * (TH ? tmo.fbcy_mu[n] : 1.0);
     } else fb.assign(fbcy_qy.size(), MAXP);
     Arr a(nc0, nc1, nc2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qydy_ccc.v[n] - THIRD * div.v[n]) * 2.0 * 1.0;
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qydy_ccc.v[n] - THIRD * div.v[n]) * 2.0 * MU(tmo.mu_ccc, n);
     Arr r = op(dm, 1, FAM_D1C2P, dm.mbcy_tau2, &fb, a);
     for (size_t n = 0; n < myy.size(); ++n) myy.v[n] = myy.v[n] + r.v[n] * rre;
   }
   {
     Arr a(nc0, np1, np2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qzdy_cpp.v[n] + qydz_cpp.v[n] - 0.0) * 1.0;
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qzdy_cpp.v[n] + qydz_cpp.v[n] - 0.0) * MU(tmo.muiyz_cpp, n);
     Arr r = op(dm, 2, FAM_D1P2C, dm.mbcz_tau2, nullptr, a);
     for (size_t n = 0; n < myz.size(); ++n) myz.v[n] = myz.v[n] + r.v[n] * rre;
   }
@@ -423,19 +499,19 @@ static void momentum_rhs(const Domain& dm, const Flow& fl, Rhs3& out) {
   Arr mz(nc0, nc1, np2), mzy(nc0, nc1, np2), mzz(nc0, nc1, np2), pz(nc0, nc1, np2);
   {
     Arr a(np0, nc1, np2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -qxiz_pcp.v[n] * qzix_pcp.v[n];
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -c_xiz.v[n] * qzix_pcp.v[n];
     Arr r = op(dm, 0, FAM_D1P2C, dm.mbcx_cov3, nullptr, a);
     for (size_t n = 0; n < mz.size(); ++n) mz.v[n] = mz.v[n] + r.v[n];
   }
   {
     Arr a(nc0, np1, np2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -qyiz_cpp.v[n] * qziy_cpp.v[n];
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -c_yiz.v[n] * qziy_cpp.v[n];
     Arr r = op(dm, 1, FAM_D1P2C, dm.mbcy_cov3, nullptr, a);
     for (size_t n = 0; n < mzy.size(); ++n) mzy.v[n] = mzy.v[n] + r.v[n];
   }
   {
     Arr a(nc0, nc1, nc2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -qziz_ccc.v[n] * qziz_ccc.v[n];
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = -c_ziz.v[n] * qziz_ccc.v[n];
     Arr r = op(dm, 2, FAM_D1C2P, dm.mbcz_cov3, &fbcz_any, a);
     for (size_t n = 0; n < mzz.size(); ++n) mzz.v[n] = mzz.v[n] + r.v[n];
   }
@@ -447,19 +523,19 @@ static void momentum_rhs(const Domain& dm, const Flow& fl, Rhs3& out) {
   }
   {
     Arr a(np0, nc1, np2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qxdz_pcp.v[n] + qzdx_pcp.v[n]) * 1.0;
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qxdz_pcp.v[n] + qzdx_pcp.v[n]) * MU(tmo.muixz_pcp, n);
     Arr r = op(dm, 0, FAM_D1P2C, dm.mbcx_tau3, nullptr, a);
     for (size_t n = 0; n < mz.size(); ++n) mz.v[n] = mz.v[n] + r.v[n] * rre;
   }
   {
     Arr a(nc0, np1, np2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qzdy_cpp.v[n] + qydz_cpp.v[n]) * 1.0;
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qzdy_cpp.v[n] + qydz_cpp.v[n]) * MU(tmo.muiyz_cpp, n);
     Arr r = op(dm, 1, FAM_D1P2C, dm.mbcy_tau3, nullptr, a);
     for (size_t n = 0; n < mzy.size(); ++n) mzy.v[n] = mzy.v[n] + r.v[n] * rre;
   }
   {
     Arr a(nc0, nc1, nc2);
-    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qzdz_ccc.v[n] - THIRD * div.v[n] + 0.0) * 2.0 * 1.0;
+    for (size_t n = 0; n < a.size(); ++n) a.v[n] = (qzdz_ccc.v[n] - THIRD * div.v[n] + 0.0) * 2.0 * MU(tmo.mu_ccc, n);
     Arr r = op(dm, 2, FAM_D1C2P, dm.mbcz_tau3, &fbcz_any, a);
     for (size_t n = 0; n < mzz.size(); ++n) mzz.v[n] = mzz.v[n] + r.v[n] * rre;
   }
@@ -707,10 +783,11 @@ static void poisson_3dfft(const Domain& dm, std::vector<double>& rhs) {
 }
 
 // Get_divergence_flow (eq_continuity.f90:91-161)
-static Arr divergence(const Domain& dm, const Flow& fl) {
+static Arr divergence(const Domain& dm, const std::vector<double>& ux, const std::vector<double>& uy,
+                      const std::vector<double>& uz) {
   const int nc0 = dm.nc[0], nc1 = dm.nc[1], nc2 = dm.nc[2];
   Arr qx(dm.np[0], nc1, nc2), qy(nc0, dm.np[1], nc2), qz(nc0, nc1, dm.np[2]);
-  qx.v = fl.qx; qy.v = fl.qy; qz.v = fl.qz;
+  qx.v = ux; qy.v = uy; qz.v = uz;
   std::vector<double> fbcx_any((size_t)4 * nc1 * nc2, MAXP);
   Arr a = op(dm, 0, FAM_D1P2C, dm.ibcx[V_QX], &fbcx_any, qx);
   Arr b = op(dm, 1, FAM_D1P2C, dm.ibcy[V_QY], nullptr, qy);
@@ -718,6 +795,9 @@ static Arr divergence(const Domain& dm, const Flow& fl) {
   Arr div(nc0, nc1, nc2);
   for (size_t n = 0; n < div.size(); ++n) div.v[n] = ((0.0 + a.v[n]) + b.v[n]) + c.v[n];
   return div;
+}
+static Arr divergence(const Domain& dm, const Flow& fl) {
+  return fl.thermo ? divergence(dm, fl.th.gx, fl.th.gy, fl.th.gz) : divergence(dm, fl.qx, fl.qy, fl.qz);
 }
 
 static void enforce_velo(const Domain& dm, Flow& fl) {
@@ -727,9 +807,15 @@ static void enforce_velo(const Domain& dm, Flow& fl) {
     if (dm.ibcy[V_QY][side] != BC_DIRICHLET) continue;
     int j = side == 0 ? 0 : np1 - 1;
     for (int k = 0; k < nc2; ++k)
-      for (int i = 0; i < nc0; ++i) fl.qy[((size_t)k * np1 + j) * nc0 + i] = dm.fbcy_const[V_QY][side];
+      for (int i = 0; i < nc0; ++i) {
+        const size_t c = ((size_t)k * np1 + j) * nc0 + i;
+        if (fl.thermo) fl.th.gy[c] = dm.fbcy_const[V_QY][side] * fl.th.fbcy_ftp[((size_t)k * 4 + side) * nc0 + i].d;
+        else fl.qy[c] = dm.fbcy_const[V_QY][side];
+      }
   }
 }
+
+void convert_q_g(const Domain& dm, Flow& fl, bool to_q);
 
 // Solve_momentum_eq (eq_momentum2.f90:1799-1932), flow-only Cartesian
 void momentum_substep(Domain& dm, Flow& fl, int isub, double* bulk_out) {
@@ -744,9 +830,13 @@ void momentum_substep(Domain& dm, Flow& fl, int isub, double* bulk_out) {
     for (auto& v : r.mx.v) v = v - bulk;
   }
   if (bulk_out) *bulk_out = bulk;
-  for (size_t n = 0; n < fl.qx.size(); ++n) fl.qx[n] = fl.qx[n] + r.mx.v[n];
-  for (size_t n = 0; n < fl.qy.size(); ++n) fl.qy[n] = fl.qy[n] + r.my.v[n];
-  for (size_t n = 0; n < fl.qz.size(); ++n) fl.qz[n] = fl.qz[n] + r.mz.v[n];
+  // the advanced variable: momentum g for variable properties, velocity q otherwise
+  std::vector<double>& ux = fl.thermo ? fl.th.gx : fl.qx;
+  std::vector<double>& uy = fl.thermo ? fl.th.gy : fl.qy;
+  std::vector<double>& uz = fl.thermo ? fl.th.gz : fl.qz;
+  for (size_t n = 0; n < ux.size(); ++n) ux[n] = ux[n] + r.mx.v[n];
+  for (size_t n = 0; n < uy.size(); ++n) uy[n] = uy[n] + r.my.v[n];
+  for (size_t n = 0; n < uz.size(); ++n) uz[n] = uz[n] + r.mz.v[n];
   enforce_velo(dm, fl);
   // solve_poisson (eq_momentum2.f90:1663-1718)
   Arr div = divergence(dm, fl);
@@ -768,10 +858,236 @@ void momentum_substep(Domain& dm, Flow& fl, int isub, double* bulk_out) {
   Arr dpy = op(dm, 1, FAM_D1C2P, dm.ibcy[V_PR], &fbcy_pr, phi);
   Arr dpz = op(dm, 2, FAM_D1C2P, dm.ibcz[V_PR], &fbcz_any, phi);
   const double f = dm.dt * dm.tAlpha[isub] * dm.sigma2p;
-  for (size_t n = 0; n < fl.qx.size(); ++n) fl.qx[n] = fl.qx[n] - f * dpx.v[n];
-  for (size_t n = 0; n < fl.qy.size(); ++n) fl.qy[n] = fl.qy[n] - f * dpy.v[n];
-  for (size_t n = 0; n < fl.qz.size(); ++n) fl.qz[n] = fl.qz[n] - f * dpz.v[n];
+  for (size_t n = 0; n < ux.size(); ++n) ux[n] = ux[n] - f * dpx.v[n];
+  for (size_t n = 0; n < uy.size(); ++n) uy[n] = uy[n] - f * dpy.v[n];
+  for (size_t n = 0; n < uz.size(); ++n) uz[n] = uz[n] - f * dpz.v[n];
   enforce_velo(dm, fl);
+  // Calculate_drhodt (src/eq_continuity.f90:26-78) adds (rho - rho_m1)/dt to the Poisson RHS,
+  // but Update_thermal_properties has already set rho_m1 = rho, so that term is zero and is
+  // left out here.
+  if (fl.thermo) convert_q_g(dm, fl, true);
+}
+
+// ---------------------------------------------------------------------------
+// Thermal property lookup (src/input_thermo.f90:345-446)
+// ---------------------------------------------------------------------------
+static const double MINP = 1.0e-20;  // src/modules.f90:141
+
+// bisection on a monotonic table column (the sign test of the reference: i1 moves while
+// (col[i1]-x)*(col[im]-x) > MINP), then linear weights
+static void bracket(const std::vector<double>& col, double x, int& i1, int& i2, double& w1) {
+  i1 = 0;
+  i2 = (int)col.size() - 1;
+  while (i2 - i1 > 1) {
+    const int im = i1 + (i2 - i1) / 2;
+    const double d1 = col[i1] - x, dmid = col[im] - x;
+    if (d1 * dmid > MINP) i1 = im;
+    else i2 = im;
+  }
+  w1 = (col[i2] - x) / (col[i2] - col[i1]);
+}
+
+void ftp_from_h(const ThermoTable& tb, Ftp& f) {
+  int i1, i2;
+  double w1;
+  bracket(tb.h, f.h, i1, i2, w1);
+  const double w2 = 1.0 - w1;
+  f.d = w1 * tb.d[i1] + w2 * tb.d[i2];
+  f.m = w1 * tb.m[i1] + w2 * tb.m[i2];
+  f.k = w1 * tb.k[i1] + w2 * tb.k[i2];
+  f.t = w1 * tb.t[i1] + w2 * tb.t[i2];
+  f.b = w1 * tb.b[i1] + w2 * tb.b[i2];
+  f.cp = w1 * tb.cp[i1] + w2 * tb.cp[i2];
+}
+
+void ftp_from_dh(const ThermoTable& tb, Ftp& f) {
+  if (f.rhoh < tb.dhmin) f.rhoh = tb.dhmin;
+  else if (f.rhoh > tb.dhmax) f.rhoh = tb.dhmax;
+  int i1, i2;
+  double w1;
+  bracket(tb.rhoh, f.rhoh, i1, i2, w1);
+  const double w2 = 1.0 - w1;
+  f.h = w1 * tb.h[i1] + w2 * tb.h[i2];
+  ftp_from_h(tb, f);
+  f.h = f.rhoh / f.d;
+  ftp_from_h(tb, f);
+}
+
+// ftp_refresh_thermal_properties_from_T_undim (src/input_thermo.f90:272-307): T -> all
+void ftp_from_t(const ThermoTable& tb, Ftp& f) {
+  int i1, i2;
+  double w1;
+  bracket(tb.t, f.t, i1, i2, w1);
+  const double w2 = 1.0 - w1;
+  f.d = w1 * tb.d[i1] + w2 * tb.d[i2];
+  f.m = w1 * tb.m[i1] + w2 * tb.m[i2];
+  f.k = w1 * tb.k[i1] + w2 * tb.k[i2];
+  f.h = w1 * tb.h[i1] + w2 * tb.h[i2];
+  f.b = w1 * tb.b[i1] + w2 * tb.b[i2];
+  f.cp = w1 * tb.cp[i1] + w2 * tb.cp[i2];
+  f.rhoh = f.d * f.h;
+}
+
+// Update_thermal_properties (src/eq_energy.f90:14-146), y walls only (x and z are periodic).
+// The top wall takes row np(2) of the interpolated rho*h (the reference indexes np(1) there).
+static void update_thermal_properties(const Domain& dm, Thermo& th) {
+  const int nc0 = dm.nc[0], nc1 = dm.nc[1], nc2 = dm.nc[2], np1 = dm.np[1];
+  const size_t n = (size_t)nc0 * nc1 * nc2;
+#pragma omp parallel for schedule(static)
+  for (long long c = 0; c < (long long)n; ++c) {
+    Ftp f{};
+    f.rhoh = th.rhoh[c];
+    ftp_from_dh(th.tab, f);
+    th.hEnth[c] = f.h;
+    th.tTemp[c] = f.t;
+    th.kCond[c] = f.k;
+    th.dDens[c] = f.d;
+    th.mVisc[c] = f.m;
+  }
+  if (dm.ibcy[V_TM][0] == BC_NEUMANN || dm.ibcy[V_TM][1] == BC_NEUMANN) {
+    Arr dh(nc0, nc1, nc2);
+    dh.v = th.rhoh;
+    Arr dh_cpc = op(dm, 1, FAM_M1C2P, dm.ibcy_ftp, nullptr, dh);
+    for (int side = 0; side < 2; ++side) {
+      if (dm.ibcy[V_TM][side] != BC_NEUMANN) continue;
+      const int j = side == 0 ? 0 : np1 - 1;
+      for (int k = 0; k < nc2; ++k)
+        for (int i = 0; i < nc0; ++i) {
+          Ftp f{};
+          f.rhoh = dh_cpc.at(i, j, k);
+          ftp_from_dh(th.tab, f);
+          th.fbcy_ftp[((size_t)k * 4 + side) * nc0 + i] = f;
+          th.fbcy_ftp[((size_t)k * 4 + side + 2) * nc0 + i] = f;
+        }
+    }
+  }
+}
+
+static std::vector<double> fbcy_prop(const Thermo& th, double Ftp::*field) {
+  std::vector<double> v(th.fbcy_ftp.size());
+  for (size_t n = 0; n < v.size(); ++n) v[n] = th.fbcy_ftp[n].*field;
+  return v;
+}
+
+// Compute_energy_rhs + Calculate_energy_fractional_step (src/eq_energy.f90:148-401).  The y
+// diffusion boundary value is taken from the wall rows of kappa*dT/dy (the reference tests the
+// x-velocity flag there and passes MAXP for an x-periodic channel).
+static void energy_rhs(const Domain& dm, Flow& fl, int isub, std::vector<double>& rhs) {
+  Thermo& th = fl.th;
+  const int nc0 = dm.nc[0], nc1 = dm.nc[1], nc2 = dm.nc[2];
+  const int np0 = dm.np[0], np1 = dm.np[1], np2 = dm.np[2];
+  int ftpx[2] = {BC_PERIODIC, BC_PERIODIC}, ftpz[2] = {BC_PERIODIC, BC_PERIODIC};
+  int ebcx_conv[2], ebcy_conv[2], ebcz_conv[2], ebcx_difu[2], ebcy_difu[2], ebcz_difu[2];
+  prod_of(dm.ibcx[V_QX], ftpx, ebcx_conv);
+  prod_of(dm.ibcy[V_QY], dm.ibcy_ftp, ebcy_conv);
+  prod_of(dm.ibcz[V_QZ], ftpz, ebcz_conv);
+  tau_of(dm.ibcx[V_TM], ftpx, ebcx_difu);
+  tau_of(dm.ibcy[V_TM], dm.ibcy_ftp, ebcy_difu);
+  tau_of(dm.ibcz[V_TM], ftpz, ebcz_difu);
+  Arr h(nc0, nc1, nc2), kc(nc0, nc1, nc2), T(nc0, nc1, nc2);
+  h.v = th.hEnth; kc.v = th.kCond; T.v = th.tTemp;
+  Arr gx(np0, nc1, nc2), gy(nc0, np1, nc2), gz(nc0, nc1, np2);
+  gx.v = th.gx; gy.v = th.gy; gz.v = th.gz;
+  std::vector<double> fbcx_any((size_t)4 * nc1 * nc2, MAXP), fbcz_any((size_t)nc0 * nc1 * 4, MAXP);
+  const auto fh = fbcy_prop(th, &Ftp::h), fk = fbcy_prop(th, &Ftp::k);
+  Arr h_pcc = op(dm, 0, FAM_M1C2P, ftpx, &fbcx_any, h);
+  Arr h_cpc = op(dm, 1, FAM_M1C2P, dm.ibcy_ftp, &fh, h);
+  Arr h_ccp = op(dm, 2, FAM_M1C2P, ftpz, &fbcz_any, h);
+  Arr k_pcc = op(dm, 0, FAM_M1C2P, ftpx, &fbcx_any, kc);
+  Arr k_cpc = op(dm, 1, FAM_M1C2P, dm.ibcy_ftp, &fk, kc);
+  Arr k_ccp = op(dm, 2, FAM_M1C2P, ftpz, &fbcz_any, kc);
+  const size_t n = (size_t)nc0 * nc1 * nc2;
+  std::vector<double> ex(n, 0.0), ey(n, 0.0), ez(n, 0.0);
+  {  // conv-x
+    Arr a(np0, nc1, nc2);
+    for (size_t m = 0; m < a.size(); ++m) a.v[m] = -gx.v[m] * h_pcc.v[m];
+    Arr r = op(dm, 0, FAM_D1P2C, ebcx_conv, nullptr, a);
+    for (size_t m = 0; m < n; ++m) ex[m] = ex[m] + r.v[m];
+  }
+  {  // conv-y
+    Arr a(nc0, np1, nc2);
+    for (size_t m = 0; m < a.size(); ++m) a.v[m] = -gy.v[m] * h_cpc.v[m];
+    Arr r = op(dm, 1, FAM_D1P2C, ebcy_conv, nullptr, a);
+    for (size_t m = 0; m < n; ++m) ey[m] = ey[m] + r.v[m];
+  }
+  {  // conv-z
+    Arr a(nc0, nc1, np2);
+    for (size_t m = 0; m < a.size(); ++m) a.v[m] = -gz.v[m] * h_ccp.v[m];
+    Arr r = op(dm, 2, FAM_D1P2C, ebcz_conv, nullptr, a);
+    for (size_t m = 0; m < n; ++m) ez[m] = ez[m] + r.v[m];
+  }
+  const double rpr = th.rPrRen;
+  {  // diff-x (get_fbcx_iTh gives zeros for periodic x; no velocity walls in x: MAXP)
+    std::vector<double> f0((size_t)4 * nc1 * nc2, 0.0);
+    Arr d = op(dm, 0, FAM_D1C2P, dm.ibcx[V_TM], &f0, T);
+    for (size_t m = 0; m < d.size(); ++m) d.v[m] = d.v[m] * k_pcc.v[m];
+    Arr r = op(dm, 0, FAM_D1P2C, ebcx_difu, &fbcx_any, d);
+    for (size_t m = 0; m < n; ++m) ex[m] = ex[m] + r.v[m] * rpr;
+  }
+  {  // diff-y: get_fbcy_iTh: planes 1, 2 = q_w for Neumann sides (T values for Dirichlet), 3, 4 = 0
+    std::vector<double> f((size_t)nc0 * 4 * nc2, 0.0);
+    for (int k = 0; k < nc2; ++k)
+      for (int side = 0; side < 2; ++side)
+        for (int i = 0; i < nc0; ++i) {
+          double v = 0.0;
+          if (dm.ibcy[V_TM][side] == BC_NEUMANN) v = th.qw[side];
+          else if (dm.ibcy[V_TM][side] == BC_DIRICHLET) v = th.fbcy_ftp[((size_t)k * 4 + side) * nc0 + i].t;
+          f[((size_t)k * 4 + side) * nc0 + i] = v;
+        }
+    Arr d = op(dm, 1, FAM_D1C2P, dm.ibcy[V_TM], &f, T);
+    for (size_t m = 0; m < d.size(); ++m) d.v[m] = d.v[m] * k_cpc.v[m];
+    const auto fw = extract_fbcy(d);
+    Arr r = op(dm, 1, FAM_D1P2C, ebcy_difu, &fw, d);
+    for (size_t m = 0; m < n; ++m) ey[m] = ey[m] + r.v[m] * rpr;
+  }
+  {  // diff-z
+    std::vector<double> f0((size_t)nc0 * nc1 * 4, 0.0);
+    Arr d = op(dm, 2, FAM_D1C2P, dm.ibcz[V_TM], &f0, T);
+    for (size_t m = 0; m < d.size(); ++m) d.v[m] = d.v[m] * k_ccp.v[m];
+    Arr r = op(dm, 2, FAM_D1P2C, ebcz_difu, nullptr, d);
+    for (size_t m = 0; m < n; ++m) ez[m] = ez[m] + r.v[m] * rpr;
+  }
+  rhs.assign(n, 0.0);
+  for (size_t m = 0; m < n; ++m) rhs[m] = ex[m] + (ey[m] + ez[m]);
+  // Calculate_energy_fractional_step (:148-177)
+  for (size_t m = 0; m < n; ++m) {
+    const double cur = rhs[m], last = th.ene_rhs0[m];
+    const double tot = dm.tGamma[isub] * cur + dm.tZeta[isub] * last;
+    th.ene_rhs0[m] = cur;
+    rhs[m] = dm.dt * tot;
+  }
+}
+
+// Solve_energy_eq (src/eq_energy.f90:405-458)
+void energy_substep(Domain& dm, Flow& fl, int isub) {
+  std::vector<double> rhs;
+  energy_rhs(dm, fl, isub, rhs);
+  for (size_t m = 0; m < rhs.size(); ++m) fl.th.rhoh[m] = fl.th.rhoh[m] + rhs[m];
+  update_thermal_properties(dm, fl.th);
+}
+
+// convert_primary_conservative (src/para_conversion.f90:5-227): q = g / rho_face (g2q) or
+// g = q * rho_face (q2g); the wall values of g and q are zero for the no-slip channel
+void convert_q_g(const Domain& dm, Flow& fl, bool to_q) {
+  Thermo& th = fl.th;
+  const int nc0 = dm.nc[0], nc1 = dm.nc[1], nc2 = dm.nc[2];
+  Arr d(nc0, nc1, nc2);
+  d.v = th.dDens;
+  std::vector<double> fbcx_any((size_t)4 * nc1 * nc2, MAXP), fbcz_any((size_t)nc0 * nc1 * 4, MAXP);
+  const int per[2] = {BC_PERIODIC, BC_PERIODIC};
+  const auto fd = fbcy_prop(th, &Ftp::d);
+  Arr dx = op(dm, 0, FAM_M1C2P, per, &fbcx_any, d);
+  Arr dy = op(dm, 1, FAM_M1C2P, dm.ibcy_ftp, &fd, d);
+  Arr dz = op(dm, 2, FAM_M1C2P, per, &fbcz_any, d);
+  if (to_q) {
+    for (size_t m = 0; m < fl.qx.size(); ++m) fl.qx[m] = th.gx[m] / dx.v[m];
+    for (size_t m = 0; m < fl.qy.size(); ++m) fl.qy[m] = th.gy[m] / dy.v[m];
+    for (size_t m = 0; m < fl.qz.size(); ++m) fl.qz[m] = th.gz[m] / dz.v[m];
+  } else {
+    for (size_t m = 0; m < fl.qx.size(); ++m) th.gx[m] = fl.qx[m] * dx.v[m];
+    for (size_t m = 0; m < fl.qy.size(); ++m) th.gy[m] = fl.qy[m] * dy.v[m];
+    for (size_t m = 0; m < fl.qz.size(); ++m) th.gz[m] = fl.qz[m] * dz.v[m];
+  }
 }
 
 // bulk kinetic energy (io_monitor.f90:209-241)
@@ -960,6 +1276,87 @@ int orc_momentum_substep(void* p, int isub, double* bulk) {
   } catch (const std::exception& e) {
     std::fprintf(stderr, "orc_momentum_substep: %s\n", e.what());
     return 1;
+  }
+}
+
+// Variable-property run: nondimensional table (sorted by T), 1/(Re Pr), wall heat fluxes and
+// the initial temperature (initialise_thermal_properties, src/input_thermo.f90:1070-1103; the
+// momentum g = rho q of the initial velocity, src/initialisation.f90:389).  Call after the
+// velocity has been set.
+int orc_thermo_init(void* p, int n, const double* t, const double* h, const double* d, const double* m,
+                    const double* k, const double* cp, const double* b, double rPrRen, const double* qw,
+                    double t_ini) {
+  try {
+    auto* H = static_cast<OrcHandle*>(p);
+    Domain& dm = H->dm;
+    Flow& fl = H->fl;
+    Thermo& th = fl.th;
+    ThermoTable& tb = th.tab;
+    tb.t.assign(t, t + n); tb.h.assign(h, h + n); tb.d.assign(d, d + n); tb.m.assign(m, m + n);
+    tb.k.assign(k, k + n); tb.cp.assign(cp, cp + n); tb.b.assign(b, b + n);
+    tb.rhoh.resize(n);
+    for (int i = 0; i < n; ++i) tb.rhoh[i] = tb.d[i] * tb.h[i];
+    tb.dhmin = *std::min_element(tb.rhoh.begin(), tb.rhoh.end());
+    tb.dhmax = *std::max_element(tb.rhoh.begin(), tb.rhoh.end());
+    th.rPrRen = rPrRen;
+    th.qw[0] = qw[0]; th.qw[1] = qw[1];
+    Ftp f0{};
+    f0.t = t_ini;
+    ftp_from_t(tb, f0);
+    const size_t nccc = (size_t)dm.nc[0] * dm.nc[1] * dm.nc[2];
+    th.rhoh.assign(nccc, f0.rhoh); th.hEnth.assign(nccc, f0.h); th.tTemp.assign(nccc, f0.t);
+    th.kCond.assign(nccc, f0.k); th.dDens.assign(nccc, f0.d); th.mVisc.assign(nccc, f0.m);
+    th.ene_rhs0.assign(nccc, 0.0);
+    th.fbcy_ftp.assign((size_t)dm.nc[0] * 4 * dm.nc[2], f0);
+    th.gx.assign(fl.qx.size(), 0.0); th.gy.assign(fl.qy.size(), 0.0); th.gz.assign(fl.qz.size(), 0.0);
+    fl.thermo = true;
+    convert_q_g(dm, fl, false);
+    return 0;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "orc_thermo_init: %s\n", e.what());
+    return 1;
+  }
+}
+
+// One substep of the time loop (src/chapsim.f90:292-309): energy (variable-property runs, isub
+// >= 1) then momentum.  isub = 0 is the initial momentum-only step (src/chapsim.f90:135).
+int orc_substep(void* p, int isub, double* bulk) {
+  try {
+    auto* H = static_cast<OrcHandle*>(p);
+    if (H->fl.thermo && isub >= 1) energy_substep(H->dm, H->fl, isub);
+    momentum_substep(H->dm, H->fl, isub, bulk);
+    return 0;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "orc_substep: %s\n", e.what());
+    return 1;
+  }
+}
+
+// thermal fields out (ccc): rho*h, h, T, kappa, rho, mu; momentum gx, gy, gz
+void orc_get_thermo(void* p, double* rhoh, double* h, double* T, double* k, double* d, double* m, double* gx,
+                    double* gy, double* gz) {
+  auto* H = static_cast<OrcHandle*>(p);
+  const Thermo& th = H->fl.th;
+  std::memcpy(rhoh, th.rhoh.data(), th.rhoh.size() * sizeof(double));
+  std::memcpy(h, th.hEnth.data(), th.hEnth.size() * sizeof(double));
+  std::memcpy(T, th.tTemp.data(), th.tTemp.size() * sizeof(double));
+  std::memcpy(k, th.kCond.data(), th.kCond.size() * sizeof(double));
+  std::memcpy(d, th.dDens.data(), th.dDens.size() * sizeof(double));
+  std::memcpy(m, th.mVisc.data(), th.mVisc.size() * sizeof(double));
+  std::memcpy(gx, th.gx.data(), th.gx.size() * sizeof(double));
+  std::memcpy(gy, th.gy.data(), th.gy.size() * sizeof(double));
+  std::memcpy(gz, th.gz.data(), th.gz.size() * sizeof(double));
+}
+
+// per-value property lookup from rho*h with the handle's table: out[6][n] = h, T, rho, mu, kappa, cp
+void orc_ftp_from_dh(void* p, int n, const double* rhoh, double* out) {
+  auto* H = static_cast<OrcHandle*>(p);
+  for (int i = 0; i < n; ++i) {
+    Ftp f{};
+    f.rhoh = rhoh[i];
+    ftp_from_dh(H->fl.th.tab, f);
+    out[i] = f.h; out[n + i] = f.t; out[2 * n + i] = f.d; out[3 * n + i] = f.m; out[4 * n + i] = f.k;
+    out[5 * n + i] = f.cp;
   }
 }
 

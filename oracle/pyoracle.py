@@ -50,6 +50,11 @@ def lib():
         L.orc_bulk_ke.argtypes = [ctypes.c_void_p]
         L.orc_vol_average_pcc.restype = ctypes.c_double
         L.orc_vol_average_pcc.argtypes = [ctypes.c_void_p, D]
+        L.orc_thermo_init.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D, D, D, D, D, D, ctypes.c_double, D,
+                                      ctypes.c_double]
+        L.orc_substep.argtypes = [ctypes.c_void_p, ctypes.c_int, D]
+        L.orc_get_thermo.argtypes = [ctypes.c_void_p, D, D, D, D, D, D, D, D, D]
+        L.orc_ftp_from_dh.argtypes = [ctypes.c_void_p, ctypes.c_int, D, D]
         _lib = L
     return _lib
 
@@ -161,10 +166,37 @@ class Oracle:
             raise RuntimeError("orc_momentum_rhs failed")
         return out
 
+    def thermo_init(self, tc):
+        """Start a variable-property run (call after set_fields): table, 1/(Re Pr), wall fluxes, T_ini."""
+        tb = tc.table
+        cols = [np.ascontiguousarray(tb[k], np.float64) for k in ("t", "h", "d", "m", "k", "cp", "b")]
+        qw = np.ascontiguousarray(tc.qw, np.float64)
+        rpr = 1.0 / (self.cfg.ren * tc.prandtl)
+        if lib().orc_thermo_init(self.h, len(cols[0]), *[_p(c) for c in cols], rpr, _p(qw), float(tc.t_ini)) != 0:
+            raise RuntimeError("orc_thermo_init failed")
+        self._keep_table = cols
+
+    def get_thermo(self):
+        """dict of rhoh, h, T, k, d, m (ccc) and gx, gy, gz."""
+        out = {k: np.zeros(self.shape_ccc) for k in ("rhoh", "h", "T", "k", "d", "m")}
+        out["gx"] = np.zeros(self.shape_pcc)
+        out["gy"] = np.zeros(self.shape_cpc)
+        out["gz"] = np.zeros(self.shape_ccp)
+        lib().orc_get_thermo(self.h, *[_p(out[k]) for k in ("rhoh", "h", "T", "k", "d", "m", "gx", "gy", "gz")])
+        return out
+
+    def ftp_from_dh(self, rhoh):
+        """Property lookup from rho*h: (h, T, rho, mu, kappa, cp) arrays."""
+        r = np.ascontiguousarray(rhoh, np.float64).ravel()
+        out = np.zeros((6, r.size))
+        lib().orc_ftp_from_dh(self.h, r.size, _p(r), _p(out))
+        return out
+
     def substep(self, isub):
+        """One substep of the time loop: energy (variable-property runs) then momentum."""
         bulk = np.zeros(1)
-        if lib().orc_momentum_substep(self.h, int(isub), _p(bulk)) != 0:
-            raise RuntimeError("orc_momentum_substep failed")
+        if lib().orc_substep(self.h, int(isub), _p(bulk)) != 0:
+            raise RuntimeError("orc_substep failed")
         return float(bulk[0])
 
     def step(self):
