@@ -48,8 +48,17 @@ __device__ __forceinline__ T eval_term(const TermT<T>& t, int64_t a) {
     case T_X: return T(t.s) * t.X[a];
     case T_XY: return T(t.s) * (t.X[a] * t.Y[a]);
     case T_XpY: return T(t.s) * (t.X[a] + T(t.c) * t.Y[a]);
+    case T_XpYZ: return T(t.s) * (t.X[a] + T(t.c) * t.Y[a]) * t.Z[a];
     default: return T(0);
   }
+}
+
+// store one operator output: out = g*v, out += g*v, out = num / (g*v) or out = num * (g*v)
+template <typename T>
+__device__ __forceinline__ void store_out(const LineIOT<T>& io, int64_t a, T g, T v) {
+  if (io.omode == O_DIV) io.out[a] = io.onum[a] / (g * v);
+  else if (io.omode == O_MUL) io.out[a] = io.onum[a] * (g * v);
+  else io.out[a] = io.accumulate ? io.out[a] + g * v : g * v;
 }
 
 template <typename T>
@@ -234,7 +243,7 @@ __global__ void __launch_bounds__(256) line_op_kernel(const __grid_constant__ Op
       if (L >= nlines) break;
       const T v = finish(l, p, L);
       const int64_t a = g0 + e;
-      io.out[a] = io.accumulate ? io.out[a] + g * v : g * v;
+      store_out(io, a, g, v);
     }
   } else {
     const int l = tid % LT;
@@ -244,7 +253,7 @@ __global__ void __launch_bounds__(256) line_op_kernel(const __grid_constant__ Op
       for (int p = tid / LT; p < nout; p += nt / LT) {
         const T v = finish(l, p, L);
         const int64_t a = base + p * ps;
-        io.out[a] = io.accumulate ? io.out[a] + g * v : g * v;
+        store_out(io, a, g, v);
       }
     }
   }
@@ -326,7 +335,7 @@ __global__ void __launch_bounds__(256) stencil_op_kernel(const __grid_constant__
   if (P.lmap >= 0) v *= T(table[P.lmap + p]);
   if (P.neu1 && p == 0) v = io.fbc[L];
   if (P.neu2 && p == nout - 1) v = io.fbc[nlines + L];
-  io.out[o] = io.accumulate ? io.out[o] + g * v : g * v;
+  store_out(io, o, g, v);
 }
 
 template <typename T, int DIR>
@@ -1049,5 +1058,140 @@ __global__ void ke_density_kernel(double* __restrict__ out, const double* __rest
 void launch_ke_density(double* out, const double* u, const double* v, const double* w, int64_t n, cudaStream_t st) {
   ke_density_kernel<<<148 * 8, 256, 0, st>>>(out, u, v, w, n);
 }
+
+}  // namespace chs
+
+// ===========================================================================
+// Variable-property kernels: table lookups of src/input_thermo.f90:345-446 and the energy
+// update of src/eq_energy.f90:148-177, :430-440.  Lookups run in FP64 whatever T is.
+// ===========================================================================
+namespace chs {
+
+// bisection with the reference's sign test ((col[i1]-x)*(col[im]-x) > MINP moves i1); at most
+// log2(n) iterations
+__device__ __forceinline__ void tab_bracket(const double* __restrict__ col, int n, double x, int& i1, int& i2,
+                                            double& w1) {
+  int a = 0, b = n - 1;
+  while (b - a > 1) {
+    const int m = a + (b - a) / 2;
+    const double d1 = __ldg(col + a) - x, dm = __ldg(col + m) - x;
+    if (d1 * dm > 1.0e-20) a = m;
+    else b = m;
+  }
+  const double ca = __ldg(col + a), cb = __ldg(col + b);
+  i1 = a;
+  i2 = b;
+  w1 = (cb - x) / (cb - ca);
+}
+
+struct CellProps {
+  double h, t, k, d, m;
+};
+
+__device__ __forceinline__ CellProps props_from_dh(const ThermoTab& tb, double rhoh) {
+  if (rhoh < tb.dhmin) rhoh = tb.dhmin;
+  else if (rhoh > tb.dhmax) rhoh = tb.dhmax;
+  int i1, i2;
+  double w1;
+  tab_bracket(tb.rhoh, tb.n, rhoh, i1, i2, w1);
+  double w2 = 1.0 - w1;
+  const double h0 = w1 * __ldg(tb.h + i1) + w2 * __ldg(tb.h + i2);
+  tab_bracket(tb.h, tb.n, h0, i1, i2, w1);
+  w2 = 1.0 - w1;
+  const double d0 = w1 * __ldg(tb.d + i1) + w2 * __ldg(tb.d + i2);
+  CellProps p;
+  p.h = rhoh / d0;
+  tab_bracket(tb.h, tb.n, p.h, i1, i2, w1);
+  w2 = 1.0 - w1;
+  p.d = w1 * __ldg(tb.d + i1) + w2 * __ldg(tb.d + i2);
+  p.m = w1 * __ldg(tb.m + i1) + w2 * __ldg(tb.m + i2);
+  p.k = w1 * __ldg(tb.k + i1) + w2 * __ldg(tb.k + i2);
+  p.t = w1 * __ldg(tb.t + i1) + w2 * __ldg(tb.t + i2);
+  return p;
+}
+
+template <typename T>
+__global__ void property_update_kernel(const __grid_constant__ ThermoTab tb, const T* __restrict__ rhoh,
+                                       T* __restrict__ h, T* __restrict__ t, T* __restrict__ k, T* __restrict__ d,
+                                       T* __restrict__ m, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const CellProps p = props_from_dh(tb, (double)rhoh[i]);
+    h[i] = T(p.h);
+    t[i] = T(p.t);
+    k[i] = T(p.k);
+    d[i] = T(p.d);
+    m[i] = T(p.m);
+  }
+}
+template <typename T>
+void launch_property_update(const ThermoTab& tb, const T* rhoh, T* h, T* t, T* k, T* d, T* m, int64_t n,
+                            cudaStream_t st) {
+  property_update_kernel<T><<<148 * 8, 256, 0, st>>>(tb, rhoh, h, t, k, d, m, n);
+}
+
+template <typename T>
+__global__ void wall_props_kernel(const __grid_constant__ ThermoTab tb, const T* __restrict__ dh, int n1, int n2,
+                                  int n3, int s0, int s1, T* __restrict__ fh, T* __restrict__ fk,
+                                  T* __restrict__ fm, T* __restrict__ fd) {
+  const int64_t nl = (int64_t)n1 * n3;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < 2 * nl; g += (int64_t)gridDim.x * blockDim.x) {
+    const int side = g < nl ? 0 : 1;
+    if ((side == 0 && !s0) || (side == 1 && !s1)) continue;
+    const int64_t L = g - side * nl;
+    const int64_t k = L / n1, i = L - k * n1;
+    const int j = side == 0 ? 0 : n2 - 1;
+    const CellProps p = props_from_dh(tb, (double)dh[(k * n2 + j) * n1 + i]);
+    for (int u = side; u < 4; u += 2) {
+      fh[u * nl + L] = T(p.h);
+      fk[u * nl + L] = T(p.k);
+      fm[u * nl + L] = T(p.m);
+      fd[u * nl + L] = T(p.d);
+    }
+  }
+}
+template <typename T>
+void launch_wall_props(const ThermoTab& tb, const T* dh_cpc, int n1, int n2, int n3, int s0, int s1, T* fh, T* fk,
+                       T* fm, T* fd, cudaStream_t st) {
+  wall_props_kernel<T><<<148, 256, 0, st>>>(tb, dh_cpc, n1, n2, n3, s0, s1, fh, fk, fm, fd);
+}
+
+template <typename T>
+__global__ void energy_advance_kernel(T* __restrict__ rhs, T* __restrict__ rhs0, T* __restrict__ rhoh, int64_t n,
+                                      double dt, double gam, double zeta) {
+  const T tdt = T(dt), tg = T(gam), tz = T(zeta);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T cur = rhs[i], last = rhs0[i];
+    const T tot = tg * cur + tz * last;
+    rhs0[i] = cur;
+    const T r1 = tdt * tot;
+    rhs[i] = r1;
+    rhoh[i] = rhoh[i] + r1;
+  }
+}
+template <typename T>
+void launch_energy_advance(T* rhs, T* rhs0, T* rhoh, int64_t n, double dt, double gam, double zeta,
+                           cudaStream_t st) {
+  energy_advance_kernel<T><<<148 * 8, 256, 0, st>>>(rhs, rhs0, rhoh, n, dt, gam, zeta);
+}
+
+template <typename T>
+__global__ void fill_kernel(T* __restrict__ a, double v, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = T(v);
+}
+template <typename T>
+void launch_fill(T* a, double v, int64_t n, cudaStream_t st) {
+  fill_kernel<T><<<148 * 4, 256, 0, st>>>(a, v, n);
+}
+
+#define CHS_INST_THERMO(T)                                                                                      \
+  template void launch_property_update<T>(const ThermoTab&, const T*, T*, T*, T*, T*, T*, int64_t, cudaStream_t); \
+  template void launch_wall_props<T>(const ThermoTab&, const T*, int, int, int, int, int, T*, T*, T*, T*,        \
+                                     cudaStream_t);                                                             \
+  template void launch_energy_advance<T>(T*, T*, T*, int64_t, double, double, double, cudaStream_t); \
+  template void launch_fill<T>(T*, double, int64_t, cudaStream_t);
+CHS_INST_THERMO(double)
+CHS_INST_THERMO(float)
+#undef CHS_INST_THERMO
 
 }  // namespace chs

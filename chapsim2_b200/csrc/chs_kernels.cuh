@@ -13,7 +13,11 @@ namespace chs {
 //   T_X     s * X
 //   T_XY    s * (X * Y)
 //   T_XpY   s * (X + c * Y)
-enum TermMode { T_NONE = 0, T_X = 1, T_XY = 2, T_XpY = 3 };
+//   T_XpYZ  s * (X + c * Y) * Z
+enum TermMode { T_NONE = 0, T_X = 1, T_XY = 2, T_XpY = 3, T_XpYZ = 4 };
+// Output of a line operator with result v: O_STORE out = g*v (or out += g*v when accumulating),
+// O_DIV out = num / (g*v), O_MUL out = num * (g*v)
+enum OutMode { O_STORE = 0, O_DIV = 1, O_MUL = 2 };
 
 template <typename T>
 struct TermT {
@@ -21,6 +25,7 @@ struct TermT {
   const T* Y;
   int mode;
   double s, c;
+  const T* Z;
 };
 using Term = TermT<double>;
 
@@ -32,6 +37,8 @@ struct LineIOT {
   int accumulate;     // 0: out = g * r ; 1: out += g * r
   double g;
   int n1, n2, n3;     // extents of the INPUT array (x fastest)
+  int omode;          // OutMode
+  const T* onum;      // numerator / factor of O_DIV / O_MUL (output layout)
 };
 using LineIO = LineIOT<double>;
 
@@ -101,6 +108,31 @@ void launch_axpby(T* out, const T* a, double sa, const T* b, double sb, int64_t 
 // float <-> double field conversion
 void launch_convert(float* out, const double* in, int64_t n, cudaStream_t st);
 void launch_convert(double* out, const float* in, int64_t n, cudaStream_t st);
+// ---- variable-property (thermal) kernels ----
+// nondimensional property table on the device, sorted by T (FP64 columns)
+struct ThermoTab {
+  const double *t, *h, *d, *m, *k, *rhoh;
+  int n;
+  double dhmin, dhmax;
+};
+// per-cell update from rho*h: h, T, kappa, rho, mu (ftp_refresh_thermal_properties_from_DH)
+template <typename T>
+void launch_property_update(const ThermoTab& tb, const T* rhoh, T* h, T* t, T* k, T* d, T* m, int64_t n,
+                            cudaStream_t st);
+// wall states from the wall rows (j = 0 and n2-1) of rho*h interpolated to the y faces:
+// planes [4][n1*n3] of h, kappa, mu, rho; side s fills planes s and s+2; flags select sides
+template <typename T>
+void launch_wall_props(const ThermoTab& tb, const T* dh_cpc, int n1, int n2, int n3, int s0, int s1, T* fh, T* fk,
+                       T* fm, T* fd, cudaStream_t st);
+// energy fractional step and update: r1 = dt*(gam*r + zeta*r0); r0 = r; rhoh += r1
+template <typename T>
+void launch_energy_advance(T* rhs, T* rhs0, T* rhoh, int64_t n, double dt, double gam, double zeta,
+                           cudaStream_t st);
+
+// a[i] = v
+template <typename T>
+void launch_fill(T* a, double v, int64_t n, cudaStream_t st);
+
 // max |a| and NaN flag into out[0], out[1] (two-pass with partials)
 void launch_absmax(const double* a, int64_t n, double* partial, int npart, double* out, cudaStream_t st);
 // 0.5*(u^2+v^2+w^2) over ccc

@@ -130,6 +130,21 @@ struct chs_handle {
   double *fb_qx, *fb_qy, *fb_qz, *fb_pr, *fb_mpr, *fb_conv2, *fb_visc2, *fb_comb, *fb_maxp;
   double *wy, *partial, *scal;
   double* stage = nullptr;  // mixed precision: FP64 staging for host transfers
+  // variable-property (thermal) state: src/modules.f90:412-681
+  bool thermo = false;
+  ThermoTab tab{};
+  double rPrRen = 0.0;
+  double *gx = nullptr, *gy = nullptr, *gz = nullptr;
+  double *rhoh = nullptr, *hEnth = nullptr, *tTemp = nullptr, *kCond = nullptr, *dDens = nullptr, *mVisc = nullptr;
+  double *erhs = nullptr, *erhs0 = nullptr;
+  double *gxix = nullptr, *gxiy = nullptr, *gxiz = nullptr, *gyix = nullptr, *gyiy = nullptr, *gyiz = nullptr;
+  double *gzix = nullptr, *gziy = nullptr, *gziz = nullptr;
+  double *muiy_cpc = nullptr, *muixy_ppc = nullptr, *mu_pcc = nullptr, *muixz_pcp = nullptr, *muiyz_cpp = nullptr;
+  double *h_pcc = nullptr, *h_cpc = nullptr, *h_ccp = nullptr, *k_pcc = nullptr, *k_cpc = nullptr, *k_ccp = nullptr;
+  double *dTx = nullptr, *dTy = nullptr, *dTz = nullptr, *dh_cpc = nullptr;
+  double *fb_h = nullptr, *fb_k = nullptr, *fb_m = nullptr, *fb_d = nullptr, *fb_qw = nullptr, *fb_zero = nullptr;
+  double *fb_dtk = nullptr;
+  Pair ebcx_conv, ebcy_conv, ebcz_conv, ebcx_difu, ebcy_difu, ebcz_difu, ftpy;
   double vol = 0.0;
   int npart = 0;
   // Poisson
@@ -185,13 +200,17 @@ void upload_table(chs_handle* H);
 template <class T>
 struct Id { using type = T; };
 
+// parts of a substep: the energy equation (variable-property runs) and the momentum equation
+enum { PART_ENERGY = 1, PART_MOMENTUM = 2, PART_ALL = 3 };
+const int kPer2[2] = {BC_PERIODIC, BC_PERIODIC};
+
 // input expression: up to two terms (see LineIOT)
 template <typename T>
 struct SrcT {
   TermT<T> t[2] = {{nullptr, nullptr, T_NONE, 0.0, 0.0}, {nullptr, nullptr, T_NONE, 0.0, 0.0}};
   int narrays() const {
     int n = 0;
-    for (const auto& x : t) n += (x.X ? 1 : 0) + (x.Y ? 1 : 0);
+    for (const auto& x : t) n += (x.X ? 1 : 0) + (x.Y ? 1 : 0) + (x.Z ? 1 : 0);
     return n;
   }
 };
@@ -202,6 +221,13 @@ SrcT<T> prod(const T* a, const T* b, double s) { SrcT<T> x; x.t[0] = TermT<T>{a,
 template <typename T>
 SrcT<T> lin(const T* a, const T* b, double c1, double s) {
   SrcT<T> x; x.t[0] = TermT<T>{a, b, T_XpY, s, c1}; return x;
+}
+// s * (a + c1*b) * m, or lin(a, b, c1, s) when m is null (constant properties: mu = 1)
+template <typename T>
+SrcT<T> linm(const T* a, const T* b, double c1, double s, const T* m) {
+  SrcT<T> x;
+  x.t[0] = m ? TermT<T>{a, b, T_XpYZ, s, c1, m} : TermT<T>{a, b, T_XpY, s, c1};
+  return x;
 }
 // a + w * b, for two single-term expressions
 template <typename T>
@@ -215,7 +241,8 @@ SrcT<T> plus(const SrcT<T>& a, const SrcT<T>& b, double w) {
 // run one operator: direction d, family fam, operation bc, boundary planes fbc (null = absent)
 template <typename T>
 void run_op(chs_handle* H, int d, int fam, Pair bc, const typename Id<T>::type* fbc, const SrcT<T>& in,
-            const int n_in[3], T* out, bool accumulate, double g) {
+            const int n_in[3], T* out, bool accumulate, double g, int omode = O_STORE,
+            const typename Id<T>::type* onum = nullptr) {
   const size_t tsz = H->book.table.size();
   const OpPlan& P = H->plan(d, fam, bc, fbc != nullptr);
   if (H->book.table.size() != tsz) upload_table(H);
@@ -227,10 +254,13 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const typename Id<T>::type* 
   io.accumulate = accumulate ? 1 : 0;
   io.g = g;
   io.n1 = n_in[0]; io.n2 = n_in[1]; io.n3 = n_in[2];
+  io.omode = omode;
+  io.onum = onum;
   const double nin_tot = (double)n_in[0] * n_in[1] * n_in[2];
   const double nout_tot = nin_tot / P.nin * P.nout;
   const int narr = in.narrays();
-  const double bytes = (double)sizeof(T) * (narr * nin_tot + (accumulate ? 2.0 : 1.0) * nout_tot);
+  const double bytes =
+      (double)sizeof(T) * (narr * nin_tot + ((accumulate || omode != O_STORE) ? 2.0 : 1.0) * nout_tot);
   cudaEvent_t e0 = H->prof_begin();
   launch_line_op(d, P, io, H->table, H->st);
   H->prof_end(e0, 0, d, bytes);
@@ -283,6 +313,14 @@ void build_bcs(chs_handle* H, const chs_config* c) {
     for (int n = 0; n < 2; ++n)
       ftp[d][n] = H->ibc[d][V_TM][n] == BC_NEUMANN ? BC_DIRICHLET : H->ibc[d][V_TM][n];
   auto& B = H->ibc;
+  // energy-equation operations (config_calc_eqs_ibc, src/bc_general.f90:660-685)
+  H->ftpy = Pair{{ftp[1][0], ftp[1][1]}};
+  H->ebcx_conv = prod_of(B[0][V_QX], ftp[0]);
+  H->ebcy_conv = prod_of(B[1][V_QY], ftp[1]);
+  H->ebcz_conv = prod_of(B[2][V_QZ], ftp[2]);
+  H->ebcx_difu = tau_of(B[0][V_TM], ftp[0]);
+  H->ebcy_difu = tau_of(B[1][V_TM], ftp[1]);
+  H->ebcz_difu = tau_of(B[2][V_TM], ftp[2]);
   // config_calc_eqs_ibc (src/bc_general.f90:512-677)
   H->mbcx_cov1 = prod_of(B[0][V_QX], B[0][V_QX]);
   H->mbcy_cov1 = prod_of(B[1][V_QY], B[1][V_QX]);
@@ -588,8 +626,12 @@ void poisson_device(chs_handle* H, T* rhs) {
 
 // the substep body (enqueued on H->st; capturable); T is the field type
 template <typename T>
-void substep_body_t(chs_handle* H, int isub) {
+void energy_body_t(chs_handle* H, int isub);
+template <typename T>
+void substep_body_t(chs_handle* H, int isub, int parts) {
   auto A = [](double* p) { return reinterpret_cast<T*>(p); };
+  if ((parts & PART_ENERGY) && H->thermo && isub >= 1) energy_body_t<T>(H, isub);
+  if (!(parts & PART_MOMENTUM)) return;
   cudaStream_t st = H->st;
   const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
   const int np0 = H->np[0], np1 = H->np[1], np2 = H->np[2];
@@ -608,6 +650,11 @@ void substep_body_t(chs_handle* H, int isub) {
   const T* fypr = H->periodic_y ? nullptr : A(H->fb_pr);
   const T* fympr = H->periodic_y ? nullptr : A(H->fb_mpr);
   const double rre = H->rre, third = 1.0 / 3.0;
+  const bool TH = H->thermo;
+  // the advanced variable: momentum g for variable properties, velocity q otherwise
+  double* ux = TH ? H->gx : H->qx;
+  double* uy = TH ? H->gy : H->qy;
+  double* uz = TH ? H->gz : H->qz;
 
   // ---- 1. derived quantities (src/eq_momentum2.f90:347-508)
   run_op(H, 0, M1P2C, bx_qx, any, src(A(H->qx)), s_pcc, A(H->qxix), false, 1.0);
@@ -628,6 +675,40 @@ void substep_body_t(chs_handle* H, int isub) {
   run_op(H, 1, D1C2P, by_qz, fyqz, src(A(H->qz)), s_ccp, A(H->qzdy), false, 1.0);
   run_op(H, 2, M1P2C, bz_qz, any, src(A(H->qz)), s_ccp, A(H->qziz), false, 1.0);
   run_op(H, 2, D1P2C, bz_qz, nullptr, src(A(H->qz)), s_ccp, A(H->qzdz), false, 1.0);
+  // ---- 1b. variable properties: interpolated g and mu (src/eq_momentum2.f90:576-703)
+  if (TH) {
+    const T* fz = A(H->fb_zero);  // no-slip walls: g = 0 there
+    const Pair per = P2(kPer2);
+    run_op(H, 0, M1P2C, bx_qx, any, src(A(H->gx)), s_pcc, A(H->gxix), false, 1.0);
+    run_op(H, 1, M1C2P, by_qx, fz, src(A(H->gx)), s_pcc, A(H->gxiy), false, 1.0);
+    run_op(H, 2, M1C2P, bz_qx, any, src(A(H->gx)), s_pcc, A(H->gxiz), false, 1.0);
+    run_op(H, 0, M1C2P, bx_qy, any, src(A(H->gy)), s_cpc, A(H->gyix), false, 1.0);
+    run_op(H, 1, M1P2C, by_qy, fz, src(A(H->gy)), s_cpc, A(H->gyiy), false, 1.0);
+    run_op(H, 2, M1C2P, bz_qy, any, src(A(H->gy)), s_cpc, A(H->gyiz), false, 1.0);
+    run_op(H, 0, M1C2P, bx_qz, any, src(A(H->gz)), s_ccp, A(H->gzix), false, 1.0);
+    run_op(H, 1, M1C2P, by_qz, fz, src(A(H->gz)), s_ccp, A(H->gziy), false, 1.0);
+    run_op(H, 2, M1P2C, bz_qz, any, src(A(H->gz)), s_ccp, A(H->gziz), false, 1.0);
+    run_op(H, 1, M1C2P, H->ftpy, A(H->fb_m), src(A(H->mVisc)), s_ccc, A(H->muiy_cpc), false, 1.0);
+    run_op(H, 0, M1C2P, per, any, src(A(H->muiy_cpc)), s_cpc, A(H->muixy_ppc), false, 1.0);
+    run_op(H, 0, M1C2P, per, any, src(A(H->mVisc)), s_ccc, A(H->mu_pcc), false, 1.0);
+    run_op(H, 2, M1C2P, per, nullptr, src(A(H->mu_pcc)), s_pcc, A(H->muixz_pcp), false, 1.0);
+    run_op(H, 2, M1C2P, per, nullptr, src(A(H->muiy_cpc)), s_cpc, A(H->muiyz_cpp), false, 1.0);
+  }
+  // first factors of the convection products and viscosity factors of the stresses
+  const T* c_xix = A(TH ? H->gxix : H->qxix);
+  const T* c_yix = A(TH ? H->gyix : H->qyix);
+  const T* c_zix = A(TH ? H->gzix : H->qzix);
+  const T* c_xiy = A(TH ? H->gxiy : H->qxiy);
+  const T* c_yiy = A(TH ? H->gyiy : H->qyiy);
+  const T* c_ziy = A(TH ? H->gziy : H->qziy);
+  const T* c_xiz = A(TH ? H->gxiz : H->qxiz);
+  const T* c_yiz = A(TH ? H->gyiz : H->qyiz);
+  const T* c_ziz = A(TH ? H->gziz : H->qziz);
+  const T* mu_c = TH ? A(H->mVisc) : nullptr;
+  const T* mu_xy = TH ? A(H->muixy_ppc) : nullptr;
+  const T* mu_xz = TH ? A(H->muixz_pcp) : nullptr;
+  const T* mu_yz = TH ? A(H->muiyz_cpp) : nullptr;
+
   // div = qxdx + qydy + qzdz (:512-534)
   PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, launch_axpby(A(H->div), A(H->qxdx), 1.0, A(H->qydy), 1.0, (int64_t)H->n_ccc, st));
   PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, launch_axpby(A(H->div), A(H->div), 1.0, A(H->qzdz), 1.0, (int64_t)H->n_ccc, st));
@@ -643,7 +724,8 @@ void substep_body_t(chs_handle* H, int isub) {
     PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc,
          launch_axpby(A(H->qxdx_cpc), A(H->qxdx_cpc), 1.0, A(H->qzdz_cpc), 1.0, (int64_t)H->n_cpc, st));
     PROF(H, 3, 48.0 / 8.0 * sizeof(T) * nc0 * nc2,
-         launch_fbcy_extract<T>(A(H->fb_visc2), A(H->qydy_cpc), A(H->qxdx_cpc), nullptr, -third, 1.0, 2.0, nc0, np1, nc2, st));
+         launch_fbcy_extract<T>(A(H->fb_visc2), A(H->qydy_cpc), A(H->qxdx_cpc), TH ? A(H->muiy_cpc) : nullptr,
+                                -third, TH ? 2.0 : 1.0, 2.0, nc0, np1, nc2, st));
     H->launches += 3;
   }
 
@@ -651,34 +733,34 @@ void substep_body_t(chs_handle* H, int isub) {
   // operator (same family and boundary pair), and the operator is linear in its input and
   // boundary values, so op(conv) + rre*op(diff) runs as op(conv + rre*diff) in one launch.
   // x-momentum (:796-966)
-  run_pair(H, 0, D1C2P, H->mbcx_cov1, any, prod(A(H->qxix), A(H->qxix), -1.0), H->mbcx_tau1, any,
-           lin(A(H->qxdx), A(H->div), -third, 2.0), rre, s_ccc, A(H->mx), false, nullptr);
-  run_pair(H, 1, D1P2C, H->mbcy_cov1, nullptr, prod(A(H->qyix), A(H->qxiy), -1.0), H->mbcy_tau1, nullptr,
-           lin(A(H->qxdy), A(H->qydx), 1.0, 1.0), rre, s_ppc, A(H->mx), true, nullptr);
-  run_pair(H, 2, D1P2C, H->mbcz_cov1, nullptr, prod(A(H->qzix), A(H->qxiz), -1.0), H->mbcz_tau1, nullptr,
-           lin(A(H->qxdz), A(H->qzdx), 1.0, 1.0), rre, s_pcp, A(H->mx), true, nullptr);
+  run_pair(H, 0, D1C2P, H->mbcx_cov1, any, prod(c_xix, A(H->qxix), -1.0), H->mbcx_tau1, any,
+           linm(A(H->qxdx), A(H->div), -third, 2.0, mu_c), rre, s_ccc, A(H->mx), false, nullptr);
+  run_pair(H, 1, D1P2C, H->mbcy_cov1, nullptr, prod(c_yix, A(H->qxiy), -1.0), H->mbcy_tau1, nullptr,
+           linm(A(H->qxdy), A(H->qydx), 1.0, 1.0, mu_xy), rre, s_ppc, A(H->mx), true, nullptr);
+  run_pair(H, 2, D1P2C, H->mbcz_cov1, nullptr, prod(c_zix, A(H->qxiz), -1.0), H->mbcz_tau1, nullptr,
+           linm(A(H->qxdz), A(H->qzdx), 1.0, 1.0, mu_xz), rre, s_pcp, A(H->mx), true, nullptr);
   run_op(H, 0, D1C2P, bx_pr, any, src(A(H->pres), -1.0), s_ccc, A(H->px), false, 1.0);
   // y-momentum (:978-1242)
-  run_pair(H, 0, D1P2C, H->mbcx_cov2, nullptr, prod(A(H->qxiy), A(H->qyix), -1.0), H->mbcx_tau2, nullptr,
-           lin(A(H->qxdy), A(H->qydx), 1.0, 1.0), rre, s_ppc, A(H->my), false, nullptr);
+  run_pair(H, 0, D1P2C, H->mbcx_cov2, nullptr, prod(c_xiy, A(H->qyix), -1.0), H->mbcx_tau2, nullptr,
+           linm(A(H->qxdy), A(H->qydx), 1.0, 1.0, mu_xy), rre, s_ppc, A(H->my), false, nullptr);
   if (H->fbcy_velo) {
     PROF(H, 3, 24.0 / 8.0 * sizeof(T) * 4 * nc0 * nc2,
          launch_axpby(A(H->fb_comb), A(H->fb_conv2), 1.0, A(H->fb_visc2), rre, (int64_t)4 * nc0 * nc2, st));
     H->launches++;
   }
-  run_pair(H, 1, D1C2P, H->mbcy_cov2, H->fbcy_velo ? A(H->fb_conv2) : A(H->fb_maxp), prod(A(H->qyiy), A(H->qyiy), -1.0),
-           H->mbcy_tau2, H->fbcy_velo ? A(H->fb_visc2) : A(H->fb_maxp), lin(A(H->qydy), A(H->div), -third, 2.0), rre, s_ccc,
+  run_pair(H, 1, D1C2P, H->mbcy_cov2, H->fbcy_velo ? A(H->fb_conv2) : A(H->fb_maxp), prod(A(H->qyiy), c_yiy, -1.0),
+           H->mbcy_tau2, H->fbcy_velo ? A(H->fb_visc2) : A(H->fb_maxp), linm(A(H->qydy), A(H->div), -third, 2.0, mu_c), rre, s_ccc,
            A(H->my), true, A(H->fb_comb));
-  run_pair(H, 2, D1P2C, H->mbcz_cov2, nullptr, prod(A(H->qyiz), A(H->qziy), -1.0), H->mbcz_tau2, nullptr,
-           lin(A(H->qzdy), A(H->qydz), 1.0, 1.0), rre, s_cpp, A(H->my), true, nullptr);
+  run_pair(H, 2, D1P2C, H->mbcz_cov2, nullptr, prod(A(H->qyiz), c_ziy, -1.0), H->mbcz_tau2, nullptr,
+           linm(A(H->qzdy), A(H->qydz), 1.0, 1.0, mu_yz), rre, s_cpp, A(H->my), true, nullptr);
   run_op(H, 1, D1C2P, by_pr, fympr, src(A(H->pres), -1.0), s_ccc, A(H->py), false, 1.0);
   // z-momentum (:1262-1457)
-  run_pair(H, 0, D1P2C, H->mbcx_cov3, nullptr, prod(A(H->qxiz), A(H->qzix), -1.0), H->mbcx_tau3, nullptr,
-           lin(A(H->qxdz), A(H->qzdx), 1.0, 1.0), rre, s_pcp, A(H->mz), false, nullptr);
-  run_pair(H, 1, D1P2C, H->mbcy_cov3, nullptr, prod(A(H->qyiz), A(H->qziy), -1.0), H->mbcy_tau3, nullptr,
-           lin(A(H->qzdy), A(H->qydz), 1.0, 1.0), rre, s_cpp, A(H->mz), true, nullptr);
-  run_pair(H, 2, D1C2P, H->mbcz_cov3, any, prod(A(H->qziz), A(H->qziz), -1.0), H->mbcz_tau3, any,
-           lin(A(H->qzdz), A(H->div), -third, 2.0), rre, s_ccc, A(H->mz), true, nullptr);
+  run_pair(H, 0, D1P2C, H->mbcx_cov3, nullptr, prod(c_xiz, A(H->qzix), -1.0), H->mbcx_tau3, nullptr,
+           linm(A(H->qxdz), A(H->qzdx), 1.0, 1.0, mu_xz), rre, s_pcp, A(H->mz), false, nullptr);
+  run_pair(H, 1, D1P2C, H->mbcy_cov3, nullptr, prod(c_yiz, A(H->qziy), -1.0), H->mbcy_tau3, nullptr,
+           linm(A(H->qzdy), A(H->qydz), 1.0, 1.0, mu_yz), rre, s_cpp, A(H->mz), true, nullptr);
+  run_pair(H, 2, D1C2P, H->mbcz_cov3, any, prod(c_ziz, A(H->qziz), -1.0), H->mbcz_tau3, any,
+           linm(A(H->qzdz), A(H->div), -third, 2.0, mu_c), rre, s_ccc, A(H->mz), true, nullptr);
   run_op(H, 2, D1C2P, bz_pr, any, src(A(H->pres), -1.0), s_ccc, A(H->pz), false, 1.0);
 
   // ---- 3. fractional step, mass flux
@@ -700,38 +782,103 @@ void substep_body_t(chs_handle* H, int isub) {
     H->launches += 2;
   }
   // ---- 4. q += rhs, walls
-  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_pcc, launch_update_q(A(H->qx), A(H->mx), bulk, (int64_t)H->n_pcc, st));
-  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc, launch_update_q(A(H->qy), A(H->my), nullptr, (int64_t)H->n_cpc, st));
-  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccp, launch_update_q(A(H->qz), A(H->mz), nullptr, (int64_t)H->n_ccp, st));
+  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_pcc, launch_update_q(A(ux), A(H->mx), bulk, (int64_t)H->n_pcc, st));
+  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc, launch_update_q(A(uy), A(H->my), nullptr, (int64_t)H->n_cpc, st));
+  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccp, launch_update_q(A(uz), A(H->mz), nullptr, (int64_t)H->n_ccp, st));
   H->launches += 3;
   const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
   if (w0 || w1) {
     PROF(H, 3, 16.0 / 8.0 * sizeof(T) * nc0 * nc2,
-         launch_set_yrows(A(H->qy), nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+         launch_set_yrows(A(uy), nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
     H->launches++;
   }
-  // ---- 5. Poisson RHS, solve, pressure and projection
+  // ---- 5. Poisson RHS, solve, pressure and projection.  For variable properties the reference
+  // adds (rho - rho_m1)/dt (Calculate_drhodt, src/eq_continuity.f90:26-78), but
+  // Update_thermal_properties has already set rho_m1 = rho, so the term is zero and left out.
   const double coeff = 1.0 / (H->tAlpha[isub] * H->sigma2p * H->dt);
-  run_op(H, 0, D1P2C, bx_qx, any, src(A(H->qx)), s_pcc, A(H->pcor), false, coeff);
-  run_op(H, 1, D1P2C, by_qy, nullptr, src(A(H->qy)), s_cpc, A(H->pcor), true, coeff);
-  run_op(H, 2, D1P2C, bz_qz, nullptr, src(A(H->qz)), s_ccp, A(H->pcor), true, coeff);
+  run_op(H, 0, D1P2C, bx_qx, any, src(A(ux)), s_pcc, A(H->pcor), false, coeff);
+  run_op(H, 1, D1P2C, by_qy, nullptr, src(A(uy)), s_cpc, A(H->pcor), true, coeff);
+  run_op(H, 2, D1P2C, bz_qz, nullptr, src(A(uz)), s_ccp, A(H->pcor), true, coeff);
   poisson_device<T>(H, A(H->pcor));
   PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, launch_axpby(A(H->pres), A(H->pres), 1.0, A(H->pcor), 1.0, (int64_t)H->n_ccc, st));
   H->launches++;
   const double f = H->dt * H->tAlpha[isub] * H->sigma2p;
-  run_op(H, 0, D1C2P, bx_pr, any, src(A(H->pcor)), s_ccc, A(H->qx), true, -f);
-  run_op(H, 1, D1C2P, by_pr, fypr, src(A(H->pcor)), s_ccc, A(H->qy), true, -f);
-  run_op(H, 2, D1C2P, bz_pr, any, src(A(H->pcor)), s_ccc, A(H->qz), true, -f);
+  run_op(H, 0, D1C2P, bx_pr, any, src(A(H->pcor)), s_ccc, A(ux), true, -f);
+  run_op(H, 1, D1C2P, by_pr, fypr, src(A(H->pcor)), s_ccc, A(uy), true, -f);
+  run_op(H, 2, D1C2P, bz_pr, any, src(A(H->pcor)), s_ccc, A(uz), true, -f);
   if (w0 || w1) {
     PROF(H, 3, 16.0 / 8.0 * sizeof(T) * nc0 * nc2,
-         launch_set_yrows(A(H->qy), nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+         launch_set_yrows(A(uy), nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+    H->launches++;
+  }
+  // ---- 6. variable properties: q = g / rho_face (convert_primary_conservative IG2Q,
+  // src/para_conversion.f90:5-227), the interpolation and the division in one pass per direction
+  if (TH) {
+    const Pair per = P2(kPer2);
+    run_op(H, 0, M1C2P, per, any, src(A(H->dDens)), s_ccc, A(H->qx), false, 1.0, O_DIV, A(H->gx));
+    run_op(H, 1, M1C2P, H->ftpy, A(H->fb_d), src(A(H->dDens)), s_ccc, A(H->qy), false, 1.0, O_DIV, A(H->gy));
+    run_op(H, 2, M1C2P, per, any, src(A(H->dDens)), s_ccc, A(H->qz), false, 1.0, O_DIV, A(H->gz));
+  }
+}
+
+// Solve_energy_eq (src/eq_energy.f90:405-458): energy RHS (Compute_energy_rhs, :179-401), the
+// fractional step (:148-177), rho*h update and property update (:14-146).  The y diffusion
+// boundary value is the wall row of kappa*dT/dy (the reference tests the x-velocity flag there and
+// passes MAXP for an x-periodic channel); the top wall state uses row np(2) of the interpolated
+// rho*h (the reference indexes np(1)).
+template <typename T>
+void energy_body_t(chs_handle* H, int isub) {
+  auto A = [](double* p) { return reinterpret_cast<T*>(p); };
+  cudaStream_t st = H->st;
+  const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
+  const int np0 = H->np[0], np1 = H->np[1], np2 = H->np[2];
+  const int s_pcc[3] = {np0, nc1, nc2}, s_cpc[3] = {nc0, np1, nc2}, s_ccp[3] = {nc0, nc1, np2};
+  const int s_ccc[3] = {nc0, nc1, nc2};
+  const auto& B = H->ibc;
+  const T* any = A(H->fb_maxp);
+  const T* fz = A(H->fb_zero);
+  const Pair per = P2(kPer2);
+  const double rpr = H->rPrRen;
+  // faces of h and kappa; temperature gradients
+  run_op(H, 0, M1C2P, per, any, src(A(H->hEnth)), s_ccc, A(H->h_pcc), false, 1.0);
+  run_op(H, 1, M1C2P, H->ftpy, A(H->fb_h), src(A(H->hEnth)), s_ccc, A(H->h_cpc), false, 1.0);
+  run_op(H, 2, M1C2P, per, any, src(A(H->hEnth)), s_ccc, A(H->h_ccp), false, 1.0);
+  run_op(H, 0, M1C2P, per, any, src(A(H->kCond)), s_ccc, A(H->k_pcc), false, 1.0);
+  run_op(H, 1, M1C2P, H->ftpy, A(H->fb_k), src(A(H->kCond)), s_ccc, A(H->k_cpc), false, 1.0);
+  run_op(H, 2, M1C2P, per, any, src(A(H->kCond)), s_ccc, A(H->k_ccp), false, 1.0);
+  run_op(H, 0, D1C2P, P2(B[0][V_TM]), fz, src(A(H->tTemp)), s_ccc, A(H->dTx), false, 1.0);
+  run_op(H, 1, D1C2P, P2(B[1][V_TM]), A(H->fb_qw), src(A(H->tTemp)), s_ccc, A(H->dTy), false, 1.0);
+  run_op(H, 2, D1C2P, P2(B[2][V_TM]), fz, src(A(H->tTemp)), s_ccc, A(H->dTz), false, 1.0);
+  PROF(H, 3, 3.0 * sizeof(T) * nc0 * nc2,
+       launch_fbcy_extract<T>(A(H->fb_dtk), A(H->dTy), nullptr, A(H->k_cpc), 0.0, 1.0, 1.0, nc0, np1, nc2, st));
+  H->launches++;
+  // conv + diffusion per direction (one launch where the two operators share a plan)
+  run_pair(H, 0, D1P2C, H->ebcx_conv, any, prod(A(H->gx), A(H->h_pcc), -1.0), H->ebcx_difu, any,
+           prod(A(H->dTx), A(H->k_pcc), 1.0), rpr, s_pcc, A(H->erhs), false, nullptr);
+  run_op(H, 1, D1P2C, H->ebcy_conv, nullptr, prod(A(H->gy), A(H->h_cpc), -1.0), s_cpc, A(H->erhs), true, 1.0);
+  run_op(H, 1, D1P2C, H->ebcy_difu, A(H->fb_dtk), prod(A(H->dTy), A(H->k_cpc), 1.0), s_cpc, A(H->erhs), true, rpr);
+  run_pair(H, 2, D1P2C, H->ebcz_conv, nullptr, prod(A(H->gz), A(H->h_ccp), -1.0), H->ebcz_difu, nullptr,
+           prod(A(H->dTz), A(H->k_ccp), 1.0), rpr, s_ccp, A(H->erhs), true, nullptr);
+  PROF(H, 3, 5.0 * sizeof(T) * H->n_ccc,
+       launch_energy_advance<T>(A(H->erhs), A(H->erhs0), A(H->rhoh), (int64_t)H->n_ccc, H->dt, H->tGamma[isub],
+                                H->tZeta[isub], st));
+  PROF(H, 3, 6.0 * sizeof(T) * H->n_ccc,
+       launch_property_update<T>(H->tab, A(H->rhoh), A(H->hEnth), A(H->tTemp), A(H->kCond), A(H->dDens),
+                                 A(H->mVisc), (int64_t)H->n_ccc, st));
+  H->launches += 2;
+  const int s0 = B[1][V_TM][0] == BC_NEUMANN, s1 = B[1][V_TM][1] == BC_NEUMANN;
+  if (s0 || s1) {
+    run_op(H, 1, M1C2P, H->ftpy, nullptr, src(A(H->rhoh)), s_ccc, A(H->dh_cpc), false, 1.0);
+    PROF(H, 3, 10.0 * sizeof(T) * nc0 * nc2,
+         launch_wall_props<T>(H->tab, A(H->dh_cpc), nc0, np1, nc2, s0, s1, A(H->fb_h), A(H->fb_k), A(H->fb_m),
+                              A(H->fb_d), st));
     H->launches++;
   }
 }
 
-void substep_body(chs_handle* H, int isub) {
-  if (H->mixed) substep_body_t<float>(H, isub);
-  else substep_body_t<double>(H, isub);
+void substep_body(chs_handle* H, int isub, int parts = PART_ALL) {
+  if (H->mixed) substep_body_t<float>(H, isub, parts);
+  else substep_body_t<double>(H, isub, parts);
 }
 
 // Prepare every plan the substep uses (plans are host objects; the table must be final
@@ -770,6 +917,125 @@ void prepare_plans(chs_handle* H) {
   upload_table(H);
 }
 
+// operator plans of the variable-property path (energy equation, g and mu interpolations,
+// q <-> g conversion), in the order energy_body_t and substep_body_t use them
+void prepare_thermo_plans(chs_handle* H) {
+  const auto& B = H->ibc;
+  const Pair per = P2(kPer2);
+  struct Rec { int d, fam; Pair bc; bool f; };
+  const std::vector<Rec> r = {
+      {0, M1C2P, per, true}, {1, M1C2P, H->ftpy, true}, {2, M1C2P, per, true},
+      {0, D1C2P, P2(B[0][V_TM]), true}, {1, D1C2P, P2(B[1][V_TM]), true}, {2, D1C2P, P2(B[2][V_TM]), true},
+      {0, D1P2C, H->ebcx_conv, true}, {0, D1P2C, H->ebcx_difu, true},
+      {1, D1P2C, H->ebcy_conv, false}, {1, D1P2C, H->ebcy_difu, true},
+      {2, D1P2C, H->ebcz_conv, false}, {2, D1P2C, H->ebcz_difu, false},
+      {1, M1C2P, H->ftpy, false},
+      {0, M1P2C, P2(B[0][V_QX]), true}, {1, M1C2P, P2(B[1][V_QX]), true}, {2, M1C2P, P2(B[2][V_QX]), true},
+      {0, M1C2P, P2(B[0][V_QY]), true}, {1, M1P2C, P2(B[1][V_QY]), true}, {2, M1C2P, P2(B[2][V_QY]), true},
+      {0, M1C2P, P2(B[0][V_QZ]), true}, {1, M1C2P, P2(B[1][V_QZ]), true}, {2, M1P2C, P2(B[2][V_QZ]), true},
+      {2, M1C2P, per, false},
+  };
+  for (const auto& x : r) H->plan(x.d, x.fam, x.bc, x.f);
+  upload_table(H);
+}
+
+// host-side lookup of the initial state from T (ftp_refresh_thermal_properties_from_T_undim,
+// src/input_thermo.f90:272-307): bisection on the T column with the reference's sign test
+struct HostFtp { double h, d, m, k, rhoh; };
+HostFtp host_ftp_from_t(const chs_thermo* c, double t) {
+  int a = 0, b = c->ntable - 1;
+  while (b - a > 1) {
+    const int m = a + (b - a) / 2;
+    if ((c->t[a] - t) * (c->t[m] - t) > 1.0e-20) a = m;
+    else b = m;
+  }
+  const double w1 = (c->t[b] - t) / (c->t[b] - c->t[a]), w2 = 1.0 - w1;
+  HostFtp f;
+  f.h = w1 * c->h[a] + w2 * c->h[b];
+  f.d = w1 * c->d[a] + w2 * c->d[b];
+  f.m = w1 * c->m[a] + w2 * c->m[b];
+  f.k = w1 * c->k[a] + w2 * c->k[b];
+  f.rhoh = f.d * f.h;
+  return f;
+}
+
+template <typename T>
+void thermo_fill_t(chs_handle* H, const HostFtp& f, double t_ini) {
+  auto A = [](double* p) { return reinterpret_cast<T*>(p); };
+  const int64_t n = (int64_t)H->n_ccc;
+  const int64_t nl = (int64_t)H->nc[0] * H->nc[2];
+  cudaStream_t st = H->st;
+  launch_fill(A(H->rhoh), f.rhoh, n, st);
+  launch_fill(A(H->hEnth), f.h, n, st);
+  launch_fill(A(H->tTemp), t_ini, n, st);
+  launch_fill(A(H->kCond), f.k, n, st);
+  launch_fill(A(H->dDens), f.d, n, st);
+  launch_fill(A(H->mVisc), f.m, n, st);
+  launch_fill(A(H->fb_h), f.h, 4 * nl, st);
+  launch_fill(A(H->fb_k), f.k, 4 * nl, st);
+  launch_fill(A(H->fb_m), f.m, 4 * nl, st);
+  launch_fill(A(H->fb_d), f.d, 4 * nl, st);
+  // get_fbcy_iTh (src/bc_general.f90:784-805): planes 1, 2 = dT/dy at the Neumann walls, 3, 4 = 0
+  launch_fill(A(H->fb_qw), H->fbcy[V_TM][0], nl, st);
+  launch_fill(A(H->fb_qw) + nl, H->fbcy[V_TM][1], nl, st);
+  H->launches += 12;
+  // g = q * rho_face (convert_primary_conservative IQ2G, src/initialisation.f90:389)
+  const int s_ccc[3] = {H->nc[0], H->nc[1], H->nc[2]};
+  const Pair per = P2(kPer2);
+  const T* any = A(H->fb_maxp);
+  run_op(H, 0, M1C2P, per, any, src(A(H->dDens)), s_ccc, A(H->gx), false, 1.0, O_MUL, A(H->qx));
+  run_op(H, 1, M1C2P, H->ftpy, A(H->fb_d), src(A(H->dDens)), s_ccc, A(H->gy), false, 1.0, O_MUL, A(H->qy));
+  run_op(H, 2, M1C2P, per, any, src(A(H->dDens)), s_ccc, A(H->gz), false, 1.0, O_MUL, A(H->qz));
+}
+
+void thermo_init(chs_handle* H, const chs_thermo* c) {
+  if (H->periodic_y) throw std::invalid_argument("variable properties need the channel (y walls)");
+  for (int v = V_QX; v <= V_QZ; ++v)
+    if (H->fbcy[v][0] != 0.0 || H->fbcy[v][1] != 0.0)
+      throw std::invalid_argument("variable properties need walls at rest");
+  for (int n = 0; n < 2; ++n) {
+    if (H->ibc[1][V_TM][n] != BC_NEUMANN) throw std::invalid_argument("variable properties need isoflux (Neumann T) y walls");
+    if (H->ibc[0][V_TM][n] != BC_PERIODIC || H->ibc[2][V_TM][n] != BC_PERIODIC)
+      throw std::invalid_argument("T must be periodic in x and z");
+  }
+  const int n = c->ntable;
+  if (n < 2 || !c->t || !c->h || !c->d || !c->m || !c->k) throw std::invalid_argument("property table missing");
+  std::vector<double> rhoh(n);
+  for (int i = 0; i < n; ++i) rhoh[i] = c->d[i] * c->h[i];
+  for (int i = 1; i < n; ++i) {
+    if (!(c->t[i] > c->t[i - 1])) throw std::invalid_argument("property table must be sorted by increasing T");
+    if (!(rhoh[i] > rhoh[i - 1]) || !(c->h[i] > c->h[i - 1]))
+      throw std::invalid_argument("rho*h and h must increase with T for the rho*h lookup");
+  }
+  if (!(c->t_ini >= c->t[0] && c->t_ini <= c->t[n - 1])) throw std::invalid_argument("t_ini outside the table");
+  double* cols = H->dalloc<double>((size_t)6 * n);
+  const double* srcs[6] = {c->t, c->h, c->d, c->m, c->k, rhoh.data()};
+  for (int j = 0; j < 6; ++j)
+    CK(cudaMemcpyAsync(cols + (size_t)j * n, srcs[j], n * sizeof(double), cudaMemcpyHostToDevice, H->st));
+  H->tab = ThermoTab{cols, cols + n, cols + 2 * n, cols + 3 * n, cols + 4 * n, cols + 5 * n, n,
+                     *std::min_element(rhoh.begin(), rhoh.end()), *std::max_element(rhoh.begin(), rhoh.end())};
+  H->rPrRen = c->rPrRen;
+  const size_t nc = H->n_ccc;
+  for (double** p : {&H->rhoh, &H->hEnth, &H->tTemp, &H->kCond, &H->dDens, &H->mVisc, &H->erhs, &H->erhs0,
+                     &H->gxix, &H->gyiy, &H->gziz, &H->h_pcc, &H->h_ccp, &H->k_pcc, &H->k_ccp, &H->dTx, &H->dTz,
+                     &H->mu_pcc})
+    *p = H->dalloc<double>(nc + (size_t)H->nc[1] * H->nc[2] + (size_t)H->nc[0] * H->nc[1]);
+  H->gx = H->dalloc<double>(H->n_pcc); H->gy = H->dalloc<double>(H->n_cpc); H->gz = H->dalloc<double>(H->n_ccp);
+  for (double** p : {&H->gxiy, &H->gyix, &H->muixy_ppc}) *p = H->dalloc<double>(H->n_ppc);
+  for (double** p : {&H->gxiz, &H->gzix, &H->muixz_pcp}) *p = H->dalloc<double>(H->n_pcp);
+  for (double** p : {&H->gyiz, &H->gziy, &H->muiyz_cpp}) *p = H->dalloc<double>(H->n_cpp);
+  for (double** p : {&H->muiy_cpc, &H->h_cpc, &H->k_cpc, &H->dTy, &H->dh_cpc}) *p = H->dalloc<double>(H->n_cpc);
+  const size_t nl = (size_t)H->nc[0] * H->nc[2];
+  for (double** p : {&H->fb_h, &H->fb_k, &H->fb_m, &H->fb_d, &H->fb_qw, &H->fb_zero, &H->fb_dtk})
+    *p = H->dalloc<double>(4 * nl);
+  H->thermo = true;
+  prepare_thermo_plans(H);
+  const HostFtp f = host_ftp_from_t(c, c->t_ini);
+  if (H->mixed) thermo_fill_t<float>(H, f, c->t_ini);
+  else thermo_fill_t<double>(H, f, c->t_ini);
+  CK(cudaStreamSynchronize(H->st));
+}
+
 void set_err(chs_handle* H, const char* fmt, ...) {
   if (!H) return;
   char buf[1024];
@@ -806,6 +1072,20 @@ double* field_ptr(chs_handle* H, int field, size_t* n) {
     case CHS_MX_RHS0: *n = H->n_pcc; return H->mx0;
     case CHS_MY_RHS0: *n = H->n_cpc; return H->my0;
     case CHS_MZ_RHS0: *n = H->n_ccp; return H->mz0;
+    default: break;
+  }
+  if (!H->thermo) throw std::invalid_argument("unknown field id, or a thermal field without chs_thermo_init");
+  switch (field) {
+    case CHS_GX: *n = H->n_pcc; return H->gx;
+    case CHS_GY: *n = H->n_cpc; return H->gy;
+    case CHS_GZ: *n = H->n_ccp; return H->gz;
+    case CHS_RHOH: *n = H->n_ccc; return H->rhoh;
+    case CHS_HENTH: *n = H->n_ccc; return H->hEnth;
+    case CHS_TTEMP: *n = H->n_ccc; return H->tTemp;
+    case CHS_KCOND: *n = H->n_ccc; return H->kCond;
+    case CHS_DDENS: *n = H->n_ccc; return H->dDens;
+    case CHS_MVISC: *n = H->n_ccc; return H->mVisc;
+    case CHS_ENE_RHS0: *n = H->n_ccc; return H->erhs0;
     default: throw std::invalid_argument("unknown field id");
   }
 }
@@ -910,11 +1190,32 @@ int chs_download_field(chs_handle* H, int field, double* host, size_t n) {
   });
 }
 
+int chs_thermo_init(chs_handle* H, const chs_thermo* th) {
+  if (!H || !th) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    if (H->thermo) throw std::invalid_argument("chs_thermo_init was already called");
+    thermo_init(H, th);
+  });
+}
+
+int chs_energy_substep(chs_handle* H, int isub) {
+  if (!H) return CHS_ERR_ARG;
+  if (isub < 1 || isub > 3) { set_err(H, "isub must be 1..3"); return CHS_ERR_ARG; }
+  return guard(H, [&] {
+    if (!H->thermo) throw std::invalid_argument("chs_energy_substep needs chs_thermo_init");
+    substep_body(H, isub, PART_ENERGY);
+    CK(cudaGetLastError());
+  });
+}
+
 int chs_momentum_substep(chs_handle* H, int isub) {
   if (!H) return CHS_ERR_ARG;
   if (isub < 0 || isub > 3) { set_err(H, "isub must be 0..3"); return CHS_ERR_ARG; }
   return guard(H, [&] {
-    if (isub >= 1 && H->gexec[isub]) {
+    if (H->thermo) {
+      // the captured graphs hold the whole substep (energy + momentum)
+      substep_body(H, isub, PART_MOMENTUM);
+    } else if (isub >= 1 && H->gexec[isub]) {
       CK(cudaGraphLaunch(H->gexec[isub], H->st));
       H->launches += H->kernels_per_sub[isub];
     } else {
@@ -940,6 +1241,11 @@ int chs_step(chs_handle* H, int nsteps) {
 int chs_momentum_substep_host(chs_handle* H, int isub, double* qx, double* qy, double* qz, double* pres) {
   if (!H || !qx || !qy || !qz || !pres) return CHS_ERR_ARG;
   if (isub < 0 || isub > 3) { set_err(H, "isub must be 0..3"); return CHS_ERR_ARG; }
+  if (H->thermo) {
+    set_err(H, "variable-property runs keep g and the thermal fields on the device: use chs_upload_field/"
+               "chs_download_field around chs_energy_substep and chs_momentum_substep");
+    return CHS_ERR_STATE;
+  }
   return guard(H, [&] {
     h2d_field(H, H->qx, qx, H->n_pcc);
     h2d_field(H, H->qy, qy, H->n_cpc);
@@ -1075,20 +1381,31 @@ int chs_diagnostics(chs_handle* H, chs_diag* out) {
     const Pair bx = P2(H->ibc[0][V_QX]), by = P2(H->ibc[1][V_QY]), bz = P2(H->ibc[2][V_QZ]);
     // The checks run in FP64.  In the mixed form the FP32 velocities are first widened into
     // the (FP64-sized) RHS work arrays, and FP64 wall planes are built in the spare planes.
+    // the divergence is that of the advanced variable (g for variable properties)
     double *qx = H->qx, *qy = H->qy, *qz = H->qz, *fmaxp = H->fb_maxp, *fqy = H->fb_qy;
+    double *ux = H->thermo ? H->gx : H->qx, *uy = H->thermo ? H->gy : H->qy, *uz = H->thermo ? H->gz : H->qz;
     if (H->mixed) {
       launch_convert(H->mx, reinterpret_cast<const float*>(H->qx), (int64_t)H->n_pcc, H->st);
       launch_convert(H->my, reinterpret_cast<const float*>(H->qy), (int64_t)H->n_cpc, H->st);
       launch_convert(H->mz, reinterpret_cast<const float*>(H->qz), (int64_t)H->n_ccp, H->st);
+      if (H->thermo) {
+        launch_convert(H->px, reinterpret_cast<const float*>(H->gx), (int64_t)H->n_pcc, H->st);
+        launch_convert(H->py, reinterpret_cast<const float*>(H->gy), (int64_t)H->n_cpc, H->st);
+        launch_convert(H->pz, reinterpret_cast<const float*>(H->gz), (int64_t)H->n_ccp, H->st);
+        ux = H->px; uy = H->py; uz = H->pz;
+        H->launches += 3;
+      } else {
+        ux = H->mx; uy = H->my; uz = H->mz;
+      }
       launch_fbcy_const(H->fb_comb, nc0, nc2, kMaxp, kMaxp, H->st);
       launch_fbcy_const(H->fb_visc2, nc0, nc2, H->fbcy[V_QY][0], H->fbcy[V_QY][1], H->st);
       qx = H->mx; qy = H->my; qz = H->mz; fmaxp = H->fb_comb; fqy = H->fb_visc2;
       H->launches += 5;
     }
     // divergence (Get_divergence_flow, src/eq_continuity.f90:91-161) into `div`
-    run_op(H, 0, D1P2C, bx, fmaxp, src(qx), s_pcc, H->div, false, 1.0);
-    run_op(H, 1, D1P2C, by, nullptr, src(qy), s_cpc, H->div, true, 1.0);
-    run_op(H, 2, D1P2C, bz, nullptr, src(qz), s_ccp, H->div, true, 1.0);
+    run_op(H, 0, D1P2C, bx, fmaxp, src(ux), s_pcc, H->div, false, 1.0);
+    run_op(H, 1, D1P2C, by, nullptr, src(uy), s_cpc, H->div, true, 1.0);
+    run_op(H, 2, D1P2C, bz, nullptr, src(uz), s_ccp, H->div, true, 1.0);
     launch_absmax(H->div, (int64_t)H->n_ccc, H->partial, H->npart, H->scal + 2, H->st);
     // kinetic energy of the P2C-interpolated velocities (src/io_monitor.f90:209-241)
     run_op(H, 0, M1P2C, bx, fmaxp, src(qx), s_pcc, H->qxix, false, 1.0);

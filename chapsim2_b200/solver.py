@@ -16,6 +16,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libchapsim_gpu.so")
 
 CHS_QX, CHS_QY, CHS_QZ, CHS_PRES, CHS_PCOR, CHS_MX_RHS0, CHS_MY_RHS0, CHS_MZ_RHS0 = range(8)
+(CHS_GX, CHS_GY, CHS_GZ, CHS_RHOH, CHS_HENTH, CHS_TTEMP, CHS_KCOND, CHS_DDENS, CHS_MVISC,
+ CHS_ENE_RHS0) = range(8, 18)
 CHS_FP64, CHS_MIXED = 0, 1
 CHS_OK, CHS_ERR_ARG, CHS_ERR_CUDA, CHS_ERR_STATE, CHS_ERR_NUMERIC = range(5)
 _D = ctypes.POINTER(ctypes.c_double)
@@ -37,6 +39,11 @@ class ChsConfig(ctypes.Structure):
     ]
 
 
+class ChsThermo(ctypes.Structure):
+    _fields_ = [("ntable", ctypes.c_int), ("t", _D), ("h", _D), ("d", _D), ("m", _D), ("k", _D), ("cp", _D),
+                ("b", _D), ("rPrRen", ctypes.c_double), ("t_ini", ctypes.c_double)]
+
+
 class ChsDiag(ctypes.Structure):
     _fields_ = [("max_div", ctypes.c_double), ("bulk_ke", ctypes.c_double), ("bulk_u", ctypes.c_double),
                 ("last_bulk_rhs", ctypes.c_double), ("nan_flag", ctypes.c_int)]
@@ -46,7 +53,7 @@ EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field
             "chs_step", "chs_poisson_solve", "chs_poisson_solve_device", "chs_diagnostics", "chs_op3d",
             "chs_plan_inspect", "chs_sync", "chs_kernel_launches", "chs_last_error", "chs_momentum_substep_host",
             "chs_time_steps", "chs_time_steps_host", "chs_host_alloc", "chs_host_free", "chs_profile_substep",
-            "chs_poisson_periodic_static"]
+            "chs_poisson_periodic_static", "chs_thermo_init", "chs_energy_substep"]
 
 
 class ChsKprof(ctypes.Structure):
@@ -88,6 +95,8 @@ def load():
     L.chs_host_free.argtypes = [ctypes.c_void_p]
     L.chs_profile_substep.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ChsKprof), ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int)]
+    L.chs_thermo_init.argtypes = [ctypes.c_void_p, ctypes.POINTER(ChsThermo)]
+    L.chs_energy_substep.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.chs_poisson_periodic_static.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_void_p,
                                               ctypes.c_char_p, ctypes.c_size_t]
@@ -199,10 +208,37 @@ class Solver:
 
     def download(self, field):
         shp = {CHS_QX: 0, CHS_MX_RHS0: 0, CHS_QY: 1, CHS_MY_RHS0: 1, CHS_QZ: 2, CHS_MZ_RHS0: 2,
-               CHS_PRES: 3, CHS_PCOR: 3}[field]
+               CHS_PRES: 3, CHS_PCOR: 3, CHS_GX: 0, CHS_GY: 1, CHS_GZ: 2}.get(field, 3)
         a = np.zeros(self.shapes[shp])
         self._check(self.L.chs_download_field(self.h, field, _ptr(a), a.size), "chs_download_field")
         return a
+
+    def thermo_init(self, tc):
+        """Start a variable-property run (after set_fields): table, 1/(Re Pr) and T_ini."""
+        tb = tc.table
+        self._tcols = [np.ascontiguousarray(tb[k], np.float64) for k in ("t", "h", "d", "m", "k", "cp", "b")]
+        th = ChsThermo()
+        th.ntable = len(self._tcols[0])
+        th.t, th.h, th.d, th.m, th.k, th.cp, th.b = [_ptr(c) for c in self._tcols]
+        th.rPrRen = 1.0 / (self.cfg.ren * tc.prandtl)
+        th.t_ini = float(tc.t_ini)
+        self._check(self.L.chs_thermo_init(self.h, ctypes.byref(th)), "chs_thermo_init")
+
+    def Solve_energy_eq(self, isub):
+        """Energy equation and property update of one RK3 substep (isub 1..3)."""
+        self._check(self.L.chs_energy_substep(self.h, int(isub)), "chs_energy_substep")
+
+    def substep(self, isub):
+        """One substep of the time loop: energy (variable-property runs) then momentum."""
+        if getattr(self, "_tcols", None) is not None and isub >= 1:
+            self.Solve_energy_eq(isub)
+        self.Solve_momentum_eq(isub)
+
+    def get_thermo(self):
+        """dict of rhoh, h, T, k, d, m (ccc) and gx, gy, gz."""
+        ids = dict(rhoh=CHS_RHOH, h=CHS_HENTH, T=CHS_TTEMP, k=CHS_KCOND, d=CHS_DDENS, m=CHS_MVISC, gx=CHS_GX,
+                   gy=CHS_GY, gz=CHS_GZ)
+        return {k: self.download(v) for k, v in ids.items()}
 
     def set_fields(self, qx, qy, qz, p):
         for f, a in ((CHS_QX, qx), (CHS_QY, qy), (CHS_QZ, qz), (CHS_PRES, p)):

@@ -33,7 +33,11 @@ enum chs_status {
 /* field identifiers for upload/download */
 enum chs_field {
   CHS_QX = 0, CHS_QY = 1, CHS_QZ = 2, CHS_PRES = 3, CHS_PCOR = 4,
-  CHS_MX_RHS0 = 5, CHS_MY_RHS0 = 6, CHS_MZ_RHS0 = 7
+  CHS_MX_RHS0 = 5, CHS_MY_RHS0 = 6, CHS_MZ_RHS0 = 7,
+  /* variable-property runs (after chs_thermo_init): fl%gx..gz, tm%rhoh, tm%hEnth, tm%tTemp,
+   * tm%kCond, fl%dDens, fl%mVisc, tm%ene_rhs0 */
+  CHS_GX = 8, CHS_GY = 9, CHS_GZ = 10, CHS_RHOH = 11, CHS_HENTH = 12, CHS_TTEMP = 13,
+  CHS_KCOND = 14, CHS_DDENS = 15, CHS_MVISC = 16, CHS_ENE_RHS0 = 17
 };
 
 /* precision of the path */
@@ -61,6 +65,19 @@ typedef struct chs_config {
   const double* ymap_pt;    /* yMappingpt(:,1), nc[1]+1 */
   const double* ymap_cc;    /* yMappingcc(:,1), nc[1] */
 } chs_config;
+
+/*
+ * Variable-property set-up: the nondimensional property table (ftplist after
+ * Buildup_thermo_mapping_relations, src/input_thermo.f90:600-693), sorted by
+ * increasing T with rho*h increasing, 1/(Re Pr) (Update_PrGr,
+ * src/tools_solver.f90:49-87) and the initial uniform temperature.
+ */
+typedef struct chs_thermo {
+  int ntable;
+  const double *t, *h, *d, *m, *k, *cp, *b;  /* T, h, rho, mu, kappa, cp, beta columns */
+  double rPrRen;
+  double t_ini;
+} chs_thermo;
 
 typedef struct chs_diag {
   double max_div;      /* max |div u| over the domain (Check_element_mass_conservation, src/eq_continuity.f90:337-397) */
@@ -124,6 +141,21 @@ typedef struct chs_kprof {
   float ms;
 } chs_kprof;
 int chs_profile_substep(chs_handle* h, int isub, chs_kprof* out, int max, int* n);
+
+/* Replaces Buildup_thermo_mapping_relations + initialise_thermal_properties
+ * (src/chapsim.f90:103-108, src/input_thermo.f90:1070-1103) and the q -> g
+ * conversion of the initial field (src/initialisation.f90:389).  Call once,
+ * after the velocity has been uploaded.  Needs the channel (y walls at rest,
+ * Neumann T there, x and z periodic); the wall dT/dy values are the config's
+ * fbcy_const[4][side]. */
+int chs_thermo_init(chs_handle* h, const chs_thermo* th);
+
+/* Replaces Solve_energy_eq(fl, tm, dm, isub) (src/eq_energy.f90:405-458):
+ * energy RHS, RK3 fractional step, rho*h update and the property update of
+ * Update_thermal_properties (src/eq_energy.f90:14-146).  isub 1..3.  In a
+ * variable-property run chs_momentum_substep then advances g and converts it to
+ * q, and chs_step runs both equations per substep. */
+int chs_energy_substep(chs_handle* h, int isub);
 
 /* Same as chs_poisson_solve on a device buffer (no host copies). */
 int chs_poisson_solve_device(chs_handle* h, double* d_rhs_inout);

@@ -1,0 +1,87 @@
+"""Variable-property (heated channel) path on the GPU against the FP64 oracle."""
+import numpy as np
+import pytest
+
+from chapsim2_b200 import config as C
+from chapsim2_b200 import initial as I
+from chapsim2_b200 import solver as S
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def _pair(cfg, tc, precision=S.CHS_FP64):
+    f = I.channel_fields(cfg)
+    o = po.Oracle(cfg)
+    o.set_fields(*f)
+    o.thermo_init(tc)
+    g = S.Solver(cfg, precision=precision)
+    g.set_fields(*f)
+    g.thermo_init(tc)
+    return o, g
+
+
+@pytest.mark.parametrize("acc", [1, 3])
+def test_heated_channel_substeps_vs_oracle(acc):
+    cfg, tc = C.heated_channel(nc=(24, 18, 16), iacc=acc, dt=0.004, t_ini=0.49)
+    o, g = _pair(cfg, tc)
+    th_o, th_g = o.get_thermo(), g.get_thermo()
+    for k in ("gx", "gy", "gz", "rhoh", "d"):
+        assert rel(th_g[k], th_o[k]) < 1e-13, k
+    o.substep(0)
+    g.substep(0)
+    for isub in (1, 2, 3, 1, 2, 3):
+        o.substep(isub)
+        g.substep(isub)
+    ref, got = o.get_fields(), g.get_fields()
+    for name, a, b in zip(("qx", "qy", "qz", "p"), got[:4], ref[:4]):
+        assert rel(a, b) < 1e-10, (name, rel(a, b))
+    th_o, th_g = o.get_thermo(), g.get_thermo()
+    for k in ("rhoh", "h", "T", "k", "d", "m", "gx", "gy", "gz"):
+        assert rel(th_g[k], th_o[k]) < 1e-10, (k, rel(th_g[k], th_o[k]))
+    g.close()
+
+
+def test_heated_channel_mixed_profiles():
+    cfg, tc = C.heated_channel(nc=(32, 24, 16), iacc=1, dt=0.004, t_ini=0.49)
+    o, g = _pair(cfg, tc, precision=S.CHS_MIXED)
+    o.substep(0)
+    g.substep(0)
+    for _ in range(4):
+        for isub in (1, 2, 3):
+            o.substep(isub)
+            g.substep(isub)
+    sh = cfg.shapes()
+    got, ref = g.get_fields(), o.get_fields()
+    pu = lambda a: a.reshape(sh[0]).mean(axis=(0, 2))
+    assert rel(pu(got[0]), pu(ref[0])) < 1e-5
+    tg, to = g.get_thermo(), o.get_thermo()
+    pt = lambda a: a.reshape(sh[3]).mean(axis=(0, 2))
+    assert rel(pt(tg["T"]), pt(to["T"])) < 1e-5
+    g.close()
+
+
+def test_energy_and_momentum_entry_points_match_step():
+    cfg, tc = C.heated_channel(nc=(24, 18, 16), iacc=1, dt=0.004)
+    f = I.channel_fields(cfg)
+    a = S.Solver(cfg)
+    b = S.Solver(cfg)
+    for g in (a, b):
+        g.set_fields(*f)
+        g.thermo_init(tc)
+        g.Solve_momentum_eq(0)
+    for isub in (1, 2, 3):
+        a.Solve_energy_eq(isub)
+        a.Solve_momentum_eq(isub)
+    b.step(1)
+    for x, y in zip(a.get_fields(), b.get_fields()):
+        assert np.array_equal(x, y)
+    ta, tb = a.get_thermo(), b.get_thermo()
+    for k in ta:
+        assert np.array_equal(ta[k], tb[k]), k
+    a.close()
+    b.close()
