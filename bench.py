@@ -1,15 +1,23 @@
 """Benchmark of the CHAPSim2 per-timestep hot path on B200.
 
 Metric: Mcell-RK3-substeps/s (cells x substeps / s / 1e6), whole job.
-Workload: the periodic turbulent channel, 128 x 96 x 128 cells, tanh
-stretching beta = 1.5, Re_b = 2800, constant mass flux, FP64, CD2 operators
-(the only accuracy whose operators are consistent with the FISHPACK 2nd-order
-Poisson solver), synthetic Poiseuille + seeded noise initial
-field, dt from CFL 0.8 frozen.
+Default workload (--workload heated): the heated channel with variable
+properties, 128 x 96 x 128 cells, tanh stretching beta = 1.5, Re_b = 2800,
+constant mass flux, isoflux y walls (dT/dy = -/+1), the synthetic 4096-row
+property table (cp peak at T = 0.5), CD2 operators (the accuracy whose operators
+are consistent with the 2nd-order FISHPACK Poisson solver), synthetic
+Poiseuille + seeded noise initial velocity, T_ini = 0.47, dt from CFL 0.8
+frozen.  --workload channel runs the flow-only channel instead.
 
-One "step" is one RK3 time step (3 substeps) replayed from captured CUDA
-graphs with all state resident in HBM.  The per-step working set (~40 FP64
-fields of 12.6 MB) exceeds the 126 MB L2, so no L2 flush is inserted.
+`value` is the plain FP64 path (the drop-in).  `forms` adds the mixed form
+(FP32 fields, operators and RHS; FP64 Poisson, mass-flux mean and checks) on
+the same workload and step count, with its speed-up and the relative L2 error
+of its x-z-mean u and T profiles against the FP64 path.
+
+One "step" is one RK3 time step (3 substeps, energy then momentum each) replayed
+from captured CUDA graphs with all state resident in HBM.  The per-step working
+set (~70 FP64 fields of 12.6 MB) exceeds the 126 MB L2, so no L2 flush is
+inserted.
 
 --impl reference times the CPU restatement of the reference's path (the
 oracle; the Fortran/MPI reference cannot be built in this image) on all host
@@ -38,15 +46,28 @@ from chapsim2_b200 import initial as I  # noqa: E402
 
 METRIC = "Mcell-RK3-substeps/s on 1 B200: mixed+MLP vs plain FP64 at ≤1e-5 L2; HBM frac"
 UNIT = "Mcell-substeps/s"
-# compulsory traffic per cell per RK3 substep, flow-only FP64 (30 words)
-BYTES_PER_CELL_SUBSTEP_FP64 = 240.0
+# compulsory traffic per cell per RK3 substep: flow-only FP64 (30 words), variable-property FP64
+# (57 words: + energy 10, property update 7, momentum with g and mu 4, drho/dt 2, g->q 4)
+BYTES_PER_CELL_SUBSTEP = {"channel": 240.0, "heated": 456.0}
 
 
-def workload(nc=(128, 96, 128), iacc=C.IACCU_CD2):
-    cfg = C.channel(nc=nc, iacc=iacc)
+def workload(kind="heated", nc=(128, 96, 128), iacc=C.IACCU_CD2):
+    """(cfg, fields, thermo config or None)."""
+    if kind == "heated":
+        cfg, tc = C.heated_channel(nc=nc, iacc=iacc)
+    else:
+        cfg, tc = C.channel(nc=nc, iacc=iacc), None
     fields = I.channel_fields(cfg)
     cfg.dt = I.cfl_dt(cfg, *fields[:3], cfl=0.8)
-    return cfg, fields
+    return cfg, fields, tc
+
+
+def describe(cfg, tc):
+    n = f"{cfg.nc[0]}x{cfg.nc[1]}x{cfg.nc[2]}"
+    if tc is None:
+        return f"channel {n} flow-only, beta=1.5, Re_b=2800, CD2"
+    return (f"heated channel {n}, variable properties (synthetic 4096-row table), isoflux walls, beta=1.5, "
+            f"Re_b=2800, CD2")
 
 
 def measured_peaks():
@@ -137,11 +158,13 @@ def barrier(dist):
         dist.barrier()
 
 
-def cpu_time_oracle(cfg, fields, nsub):
+def cpu_time_oracle(cfg, fields, tc, nsub):
     """Oracle (CPU restatement) on all host threads: seconds for nsub substeps after the initial step."""
     from oracle import pyoracle as po
     o = po.Oracle(cfg)
     o.set_fields(*fields)
+    if tc is not None:
+        o.thermo_init(tc)
     o.substep(0)
     t0 = time.perf_counter()
     for i in range(nsub):
@@ -149,21 +172,20 @@ def cpu_time_oracle(cfg, fields, nsub):
     return time.perf_counter() - t0
 
 
-def run_reference(args, cfg, fields, world, rank, dist):
+def run_reference(args, cfg, fields, tc, world, rank, dist):
     if rank != 0:
         return None
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    cpu_time_oracle(cfg, fields, args.warmup)
-    t = cpu_time_oracle(cfg, fields, args.steps)
+    cpu_time_oracle(cfg, fields, tc, args.warmup)
+    t = cpu_time_oracle(cfg, fields, tc, args.steps)
     value = cfg.ncell * args.steps / t / 1e6
-    sample = f"{args.steps} substeps of the {cfg.nc[0]}x{cfg.nc[1]}x{cfg.nc[2]} channel (CD2, FP64)"
+    sample = f"{args.steps} substeps of the {describe(cfg, tc)} (FP64)"
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"channel {cfg.nc[0]}x{cfg.nc[1]}x{cfg.nc[2]} flow-only, beta=1.5, Re_b=2800, CD2",
-                   "step": "one RK3 substep", "cells": cfg.ncell},
+        "config": {"workload": describe(cfg, tc), "step": "one RK3 substep", "cells": cfg.ncell},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -192,11 +214,28 @@ def roofline(prof, peak, peak_kind):
             "classes": {k: {"ms": v["ms"], "launches": v["n"]} for k, v in by.items()}}
 
 
-def run_ours(args, cfg, fields, world, rank, local, dist):
-    from chapsim2_b200 import solver as S
-    g = S.Solver(cfg, device=local)
+def make_solver(S, cfg, fields, tc, local, precision):
+    g = S.Solver(cfg, device=local, precision=precision)
     g.set_fields(*fields)
+    if tc is not None:
+        g.thermo_init(tc)
     g.Solve_momentum_eq(0)
+    return g
+
+
+def xz_profiles(g, cfg, tc):
+    """x-z-mean profiles of u and (variable properties) T."""
+    sh = cfg.shapes()
+    out = {"u": g.download(0).reshape(sh[0]).mean(axis=(0, 2))}
+    if tc is not None:
+        from chapsim2_b200 import solver as S
+        out["T"] = g.download(S.CHS_TTEMP).reshape(sh[3]).mean(axis=(0, 2))
+    return out
+
+
+def run_ours(args, cfg, fields, tc, world, rank, local, dist):
+    from chapsim2_b200 import solver as S
+    g = make_solver(S, cfg, fields, tc, local, S.CHS_FP64)
     g.step(args.warmup)
     g.sync()
     clocks = ClockSampler(local)
@@ -212,71 +251,72 @@ def run_ours(args, cfg, fields, world, rank, local, dist):
     value = world * cfg.ncell * sub / (ms_max * 1e-3) / 1e6
     diag = g.diagnostics()
 
-    # end to end through the host-array drop-in: pinned host fields in/out every substep
+    # end to end through the host-array drop-in: the primary state lives in pinned host arrays and
+    # is copied in and out around every substep (Solve_energy_eq + Solve_momentum_eq on host data)
     shp = cfg.shapes()
-    host = [g.pinned(s) for s in shp]
-    cur = g.get_fields()[:4]
-    for h, a in zip(host, cur):
+    ids = [S.CHS_QX, S.CHS_QY, S.CHS_QZ, S.CHS_PRES]
+    if tc is not None:
+        ids += [S.CHS_GX, S.CHS_GY, S.CHS_GZ, S.CHS_RHOH]
+    host = {}
+    for f in ids:
+        a = g.download(f)
+        h = g.pinned(a.shape)
         h[...] = a
+        host[f] = h
     barrier(dist)
-    ms_e2e = g.time_steps_host(args.steps, *host)
+    ms_e2e = g.time_steps_host_fields(args.steps, host)
     barrier(dist)
     ms_e2e = max_over_ranks(dist, ms_e2e)
-    field_bytes = sum(int(np.prod(s)) for s in shp) * 8
+    field_bytes = sum(h.size for h in host.values()) * 8
     e2e = {"value": world * cfg.ncell * sub / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": 3 * field_bytes, "d2h_bytes_per_step": 3 * field_bytes,
-           "path": "chs_momentum_substep_host semantics: fields H2D, graph substep, fields D2H, x3 per step"}
+           "path": "chs_time_steps_host_fields: pinned host state copied in and out around every substep "
+                   f"({len(ids)} fields), substep graph in between"}
 
     peak, peak_kind = measured_peaks()
     prof = g.profile_substep(1)
     rl = roofline(prof, peak, peak_kind)
-    step_model = {"bytes_per_cell_substep": BYTES_PER_CELL_SUBSTEP_FP64,
-                  "achieved_gbs": BYTES_PER_CELL_SUBSTEP_FP64 * cfg.ncell * sub / (ms * 1e-3) / 1e9}
+    bpc = BYTES_PER_CELL_SUBSTEP[args.workload]
+    step_model = {"bytes_per_cell_substep": bpc, "achieved_gbs": bpc * cfg.ncell * sub / (ms * 1e-3) / 1e9}
     step_model["frac"] = step_model["achieved_gbs"] / peak
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"channel {cfg.nc[0]}x{cfg.nc[1]}x{cfg.nc[2]} flow-only, beta=1.5, Re_b=2800, CD2",
+        "config": {"workload": describe(cfg, tc),
                    "step": "one RK3 step (3 substeps), CUDA-graph replay",
                    "cells": cfg.ncell, "dt": cfg.dt, "precision": "fp64",
-                   "l2": "working set ~40 FP64 fields x 12.6 MB per step > 126 MB L2; no flush",
+                   "l2": "working set of ~70 FP64 fields x 12.6 MB per step > 126 MB L2; no flush",
                    "parallelism": f"replicas x{world}"},
         "roofline": rl, "step_model": step_model, "e2e": e2e,
         "gpu_launches": l1 - l0, "clocks": clk,
         "diagnostics": {"max_div": diag["max_div"], "bulk_u": diag["bulk_u"], "bulk_ke": diag["bulk_ke"],
                         "nan": diag["nan_flag"]},
     }
-    # the mixed-precision form on the same workload and step count (FP32 fields/operators,
-    # FP64 Poisson, mass-flux mean and checks)
-    m = S.Solver(cfg, device=local, precision=S.CHS_MIXED)
-    m.set_fields(*fields)
-    m.Solve_momentum_eq(0)
+
+    # the mixed-precision form on the same workload and step count
+    m = make_solver(S, cfg, fields, tc, local, S.CHS_MIXED)
     m.step(args.warmup)
     m.sync()
     barrier(dist)
     ms_m = m.time_steps(args.steps)
     barrier(dist)
     ms_m = max_over_ranks(dist, ms_m)
-    m.step(args.steps)  # matches the FP64 handle's e2e steps
-    sh = cfg.shapes()[0]
-    pm = m.get_fields()[0].reshape(sh).mean(axis=(0, 2))
-    pd = g.get_fields()[0].reshape(sh).mean(axis=(0, 2))
-    out["forms"] = {
-        "fp64": {"value": value, "ms_per_step": ms_max / args.steps},
-        "mixed": {"value": world * cfg.ncell * sub / (ms_m * 1e-3) / 1e6, "ms_per_step": ms_m / args.steps,
-                  "speedup_vs_fp64": ms_max / ms_m,
-                  "u_mean_profile_rel_l2_vs_fp64": float(np.linalg.norm(pm - pd) / np.linalg.norm(pd)),
-                  "steps_compared": 1 + args.warmup + 2 * args.steps},
-    }
+    m.step(args.steps)  # the FP64 handle also ran args.steps e2e steps
+    pm, pd = xz_profiles(m, cfg, tc), xz_profiles(g, cfg, tc)
+    mixed = {"value": world * cfg.ncell * sub / (ms_m * 1e-3) / 1e6, "ms_per_step": ms_m / args.steps,
+             "speedup_vs_fp64": ms_max / ms_m, "steps_compared": 1 + args.warmup + 2 * args.steps}
+    for k in pd:
+        mixed[f"{k}_mean_profile_rel_l2_vs_fp64"] = float(np.linalg.norm(pm[k] - pd[k]) / np.linalg.norm(pd[k]))
+    out["forms"] = {"fp64": {"value": value, "ms_per_step": ms_max / args.steps}, "mixed": mixed}
     m.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
         nsub = 6
-        t = cpu_time_oracle(cfg, fields, nsub)
+        t = cpu_time_oracle(cfg, fields, tc, nsub)
         out["cpu_baseline"] = {"value": cfg.ncell * nsub / t / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
-                               "sample": f"{nsub} substeps of the same channel (oracle, OpenMP)"}
+                               "sample": f"{nsub} substeps of the same workload (oracle, OpenMP, FP64)"}
     g.close()
     return out
 
@@ -287,22 +327,23 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="heated", choices=["heated", "channel"])
     ap.add_argument("--nc", type=int, nargs=3, default=[128, 96, 128])
     ap.add_argument("--iacc", type=int, default=C.IACCU_CD2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    cfg, fields = workload(tuple(args.nc), args.iacc)
+    cfg, fields, tc = workload(args.workload, tuple(args.nc), args.iacc)
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))
-        out = run_reference(args, cfg, fields, world, rank, None)
+        out = run_reference(args, cfg, fields, tc, world, rank, None)
         if out is not None:
             print(json.dumps(out))
         return
     world, rank, local, dist = dist_setup(args.gpus)
-    out = run_ours(args, cfg, fields, world, rank, local, dist)
+    out = run_ours(args, cfg, fields, tc, world, rank, local, dist)
     if rank == 0:
         print(json.dumps(out))
     if dist is not None:

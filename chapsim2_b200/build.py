@@ -6,7 +6,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libchapsim_gpu.so")
-SOURCES = ["chs_plan.cpp", "chs_kernels.cu", "chs_solver.cu", "chs_static.cu"]
+SOURCES = ["chs_plan.cpp", "chs_kernels.cu", "chs_solver.cu", "chs_static.cu", "chs_mlp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

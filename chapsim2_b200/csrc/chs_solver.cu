@@ -1316,6 +1316,36 @@ int chs_time_steps_host(chs_handle* H, int nsteps, double* qx, double* qy, doubl
   });
 }
 
+int chs_time_steps_host_fields(chs_handle* H, int nsteps, int nfields, const int* ids, double* const* bufs,
+                               float* ms) {
+  if (!H || !ms || nsteps < 0 || nfields < 0 || (nfields > 0 && (!ids || !bufs))) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    std::vector<double*> dev(nfields);
+    std::vector<size_t> cnt(nfields);
+    for (int f = 0; f < nfields; ++f) {
+      if (!bufs[f]) throw std::invalid_argument("null host buffer");
+      dev[f] = field_ptr(H, ids[f], &cnt[f]);
+    }
+    if (!H->gexec[1]) capture_graphs(H);
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, H->st));
+    for (int s = 0; s < nsteps; ++s)
+      for (int isub = 1; isub <= 3; ++isub) {
+        for (int f = 0; f < nfields; ++f) h2d_field(H, dev[f], bufs[f], cnt[f]);
+        CK(cudaGraphLaunch(H->gexec[isub], H->st));
+        H->launches += H->kernels_per_sub[isub];
+        for (int f = 0; f < nfields; ++f) d2h_field(H, bufs[f], dev[f], cnt[f]);
+      }
+    CK(cudaEventRecord(b, H->st));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  });
+}
+
 void* chs_host_alloc(size_t bytes) {
   void* p = nullptr;
   if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) return nullptr;

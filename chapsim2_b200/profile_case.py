@@ -1,4 +1,4 @@
-"""Run a few substeps of the channel (or Taylor-Green) case for profilers.
+"""Run a few substeps of the channel, heated channel or Taylor-Green case for profilers.
 
 Launches every kernel individually (no graph replay), so a profiler sees one
 launch per operator.  Example:
@@ -17,23 +17,31 @@ from chapsim2_b200 import solver as S  # noqa: E402
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--case", default="channel", choices=["channel", "tgv"])
+    ap.add_argument("--case", default="channel", choices=["channel", "heated", "tgv"])
     ap.add_argument("--nc", type=int, nargs=3, default=[128, 96, 128])
     ap.add_argument("--iacc", type=int, default=C.IACCU_CD2)
     ap.add_argument("--substeps", type=int, default=3)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     a = ap.parse_args()
+    tc = None
     if a.case == "channel":
         cfg = C.channel(nc=tuple(a.nc), iacc=a.iacc)
+        f = I.channel_fields(cfg)
+        cfg.dt = I.cfl_dt(cfg, *f[:3], cfl=0.8)
+    elif a.case == "heated":
+        cfg, tc = C.heated_channel(nc=tuple(a.nc), iacc=a.iacc)
         f = I.channel_fields(cfg)
         cfg.dt = I.cfl_dt(cfg, *f[:3], cfl=0.8)
     else:
         cfg = C.taylor_green(a.nc[0], iacc=a.iacc)
         f = I.taylor_green_fields(cfg)
-    g = S.Solver(cfg)
+    g = S.Solver(cfg, precision=S.CHS_MIXED if a.precision == "mixed" else S.CHS_FP64)
     g.set_fields(*f)
+    if tc is not None:
+        g.thermo_init(tc)
     g.Solve_momentum_eq(0)
     for i in range(a.substeps):
-        g.Solve_momentum_eq(1 + i % 3)
+        g.substep(1 + i % 3)
     d = g.diagnostics()
     print(f"{a.case} {cfg.nc} iacc={a.iacc}: {a.substeps} substeps, launches={g.kernel_launches()}, "
           f"max_div={d['max_div']:.3e}, nan={d['nan_flag']}")

@@ -53,7 +53,7 @@ EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field
             "chs_step", "chs_poisson_solve", "chs_poisson_solve_device", "chs_diagnostics", "chs_op3d",
             "chs_plan_inspect", "chs_sync", "chs_kernel_launches", "chs_last_error", "chs_momentum_substep_host",
             "chs_time_steps", "chs_time_steps_host", "chs_host_alloc", "chs_host_free", "chs_profile_substep",
-            "chs_poisson_periodic_static", "chs_thermo_init", "chs_energy_substep"]
+            "chs_poisson_periodic_static", "chs_thermo_init", "chs_energy_substep", "chs_time_steps_host_fields"]
 
 
 class ChsKprof(ctypes.Structure):
@@ -96,6 +96,9 @@ def load():
     L.chs_profile_substep.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ChsKprof), ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int)]
     L.chs_thermo_init.argtypes = [ctypes.c_void_p, ctypes.POINTER(ChsThermo)]
+    L.chs_time_steps_host_fields.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D),
+                                             ctypes.POINTER(ctypes.c_float)]
     L.chs_energy_substep.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.chs_poisson_periodic_static.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_void_p,
@@ -305,6 +308,16 @@ class Solver:
         ms = ctypes.c_float()
         self._check(self.L.chs_time_steps_host(self.h, int(nsteps), _ptr(qx), _ptr(qy), _ptr(qz), _ptr(p),
                                                ctypes.byref(ms)), "chs_time_steps_host")
+        return float(ms.value)
+
+    def time_steps_host_fields(self, nsteps, fields):
+        """fields: dict {chs_field id: pinned host array}; returns ms of nsteps steps with the arrays
+        copied in and out every substep."""
+        ids = (ctypes.c_int * len(fields))(*[int(k) for k in fields])
+        bufs = (_D * len(fields))(*[_ptr(a) for a in fields.values()])
+        ms = ctypes.c_float()
+        self._check(self.L.chs_time_steps_host_fields(self.h, int(nsteps), len(fields), ids, bufs, ctypes.byref(ms)),
+                    "chs_time_steps_host_fields")
         return float(ms.value)
 
     def profile_substep(self, isub=1, maxk=512):

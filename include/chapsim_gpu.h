@@ -127,6 +127,14 @@ int chs_time_steps(chs_handle* h, int nsteps, float* ms);
  * handle's stream; *ms = elapsed device time including the copies. */
 int chs_time_steps_host(chs_handle* h, int nsteps, double* qx, double* qy, double* qz, double* pres, float* ms);
 
+/* Like chs_time_steps_host for any set of fields (chs_field ids): every substep
+ * copies the listed host arrays in, replays the substep graph (energy and
+ * momentum for variable-property runs) and copies them back.  This is the
+ * host-array drop-in of one time-loop substep (src/chapsim.f90:292-309) for a
+ * caller that keeps those arrays on the host. */
+int chs_time_steps_host_fields(chs_handle* h, int nsteps, int nfields, const int* ids, double* const* bufs,
+                               float* ms);
+
 /* Page-locked host buffers for the host-array entry points. */
 void* chs_host_alloc(size_t bytes);
 void chs_host_free(void* p);
