@@ -191,7 +191,7 @@ def run_reference(args, cfg, fields, tc, world, rank, dist):
     }
 
 
-def roofline(prof, peak, peak_kind):
+def roofline(prof, peak, peak_kind, workload):
     by = {}
     for r in prof:
         k = ("line_op", "fft", "ysolve", "elementwise")[r["kind"]]
@@ -206,7 +206,7 @@ def roofline(prof, peak, peak_kind):
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            traffic = json.load(f).get(dom)
+            traffic = json.load(f).get(workload, {}).get(dom)
     return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
             "bytes_per_launch": a["bytes"] / a["n"], "ms_per_launch": a["ms"] / a["n"], "launches": a["n"],
@@ -275,7 +275,7 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
 
     peak, peak_kind = measured_peaks()
     prof = g.profile_substep(1)
-    rl = roofline(prof, peak, peak_kind)
+    rl = roofline(prof, peak, peak_kind, args.workload)
     bpc = BYTES_PER_CELL_SUBSTEP[args.workload]
     step_model = {"bytes_per_cell_substep": bpc, "achieved_gbs": bpc * cfg.ncell * sub / (ms * 1e-3) / 1e9}
     step_model["frac"] = step_model["achieved_gbs"] / peak

@@ -25,6 +25,7 @@
 
 #include "../../include/chapsim_gpu.h"
 #include "chs_kernels.cuh"
+#include "chs_mlp.cuh"
 #include "chs_plan.h"
 
 using namespace chs;
@@ -145,6 +146,16 @@ struct chs_handle {
   double *fb_h = nullptr, *fb_k = nullptr, *fb_m = nullptr, *fb_d = nullptr, *fb_qw = nullptr, *fb_zero = nullptr;
   double *fb_dtk = nullptr;
   Pair ebcx_conv, ebcy_conv, ebcz_conv, ebcx_difu, ebcy_difu, ebcz_difu, ftpy;
+  // MLP surrogate of the property update
+  bool mlp_ready = false;
+  int mlp_mode = 0;  // 0: table lookups (the reference's method), 1: network with table fallback
+  float* mlp_params = nullptr;
+  uint16_t* mlp_wpack = nullptr;
+  unsigned long long* mlp_nfb = nullptr;
+  MlpNorm mlp_norm{};
+  MlpSmall mlp_small{};
+  MlpCheck mlp_check{};
+  std::vector<double> tab_host_t, tab_host_rhoh;
   double vol = 0.0;
   int npart = 0;
   // Poisson
@@ -862,9 +873,16 @@ void energy_body_t(chs_handle* H, int isub) {
   PROF(H, 3, 5.0 * sizeof(T) * H->n_ccc,
        launch_energy_advance<T>(A(H->erhs), A(H->erhs0), A(H->rhoh), (int64_t)H->n_ccc, H->dt, H->tGamma[isub],
                                 H->tZeta[isub], st));
-  PROF(H, 3, 6.0 * sizeof(T) * H->n_ccc,
-       launch_property_update<T>(H->tab, A(H->rhoh), A(H->hEnth), A(H->tTemp), A(H->kCond), A(H->dDens),
-                                 A(H->mVisc), (int64_t)H->n_ccc, st));
+  if (H->mlp_mode == 1) {
+    PROF(H, 3, 6.0 * sizeof(T) * H->n_ccc,
+         launch_mlp_props<T>(H->tab, H->mlp_norm, H->mlp_small, H->mlp_check, H->mlp_wpack, A(H->rhoh),
+                             A(H->hEnth), A(H->tTemp), A(H->kCond), A(H->dDens), A(H->mVisc), (int64_t)H->n_ccc,
+                             H->mlp_nfb, st));
+  } else {
+    PROF(H, 3, 6.0 * sizeof(T) * H->n_ccc,
+         launch_property_update<T>(H->tab, A(H->rhoh), A(H->hEnth), A(H->tTemp), A(H->kCond), A(H->dDens),
+                                   A(H->mVisc), (int64_t)H->n_ccc, st));
+  }
   H->launches += 2;
   const int s0 = B[1][V_TM][0] == BC_NEUMANN, s1 = B[1][V_TM][1] == BC_NEUMANN;
   if (s0 || s1) {
@@ -1015,6 +1033,27 @@ void thermo_init(chs_handle* H, const chs_thermo* c) {
   H->tab = ThermoTab{cols, cols + n, cols + 2 * n, cols + 3 * n, cols + 4 * n, cols + 5 * n, n,
                      *std::min_element(rhoh.begin(), rhoh.end()), *std::max_element(rhoh.begin(), rhoh.end())};
   H->rPrRen = c->rPrRen;
+  H->tab_host_t.assign(c->t, c->t + n);
+  H->tab_host_rhoh = rhoh;
+  {
+    // normalisation of the surrogate: rho*h over the table range, outputs over their column ranges
+    MlpNorm& nm = H->mlp_norm;
+    nm.xa = 2.0 / (H->tab.dhmax - H->tab.dhmin);
+    nm.xb = -1.0 - nm.xa * H->tab.dhmin;
+    const double* cols[4] = {c->t, c->d, c->m, c->k};
+    for (int j = 0; j < 4; ++j) {
+      const double lo = *std::min_element(cols[j], cols[j] + n), hi = *std::max_element(cols[j], cols[j] + n);
+      nm.ya[j] = hi > lo ? 0.5 * (hi - lo) : 1.0;
+      nm.yb[j] = 0.5 * (hi + lo);
+    }
+    MlpCheck& ck = H->mlp_check;
+    ck.t0 = c->t[0];
+    ck.dt_tab = (c->t[n - 1] - c->t[0]) / (n - 1);
+    double dev = 0.0;
+    for (int i = 0; i < n; ++i) dev = std::max(dev, std::fabs(c->t[i] - (ck.t0 + i * ck.dt_tab)));
+    ck.uniform_t = dev <= 1e-9 * (c->t[n - 1] - c->t[0]) ? 1 : 0;
+    ck.tol = 1.0e-4;
+  }
   const size_t nc = H->n_ccc;
   for (double** p : {&H->rhoh, &H->hEnth, &H->tTemp, &H->kCond, &H->dDens, &H->mVisc, &H->erhs, &H->erhs0,
                      &H->gxix, &H->gyiy, &H->gziz, &H->h_pcc, &H->h_ccp, &H->k_pcc, &H->k_ccp, &H->dTx, &H->dTz,
@@ -1034,6 +1073,142 @@ void thermo_init(chs_handle* H, const chs_thermo* c) {
   if (H->mixed) thermo_fill_t<float>(H, f, c->t_ini);
   else thermo_fill_t<double>(H, f, c->t_ini);
   CK(cudaStreamSynchronize(H->st));
+}
+
+// ---- MLP surrogate: training and evaluation -------------------------------------------------
+struct MlpBuffers {
+  float *grads = nullptr, *m = nullptr, *v = nullptr, *work = nullptr, *xs = nullptr, *ys = nullptr;
+  float *bx = nullptr, *bt = nullptr, *loss = nullptr;
+  int B = 0, N = 0;
+};
+
+void mlp_alloc_core(chs_handle* H) {
+  if (H->mlp_params) return;
+  H->mlp_params = H->dalloc<float>(MLP_NPARAM);
+  H->mlp_wpack = H->dalloc<uint16_t>(2 * 4096);
+  H->mlp_nfb = H->dalloc<unsigned long long>(1);
+}
+
+// Xavier-uniform weights from a seeded splitmix64 stream, zero biases
+void mlp_init_host(std::vector<float>& p, uint64_t seed) {
+  p.assign(MLP_NPARAM, 0.0f);
+  uint64_t st = seed;
+  auto next = [&]() {
+    st += 0x9E3779B97F4A7C15ull;
+    uint64_t z = st;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  };
+  auto fill = [&](int off, int fan_out, int fan_in) {
+    const double lim = std::sqrt(6.0 / (fan_in + fan_out));
+    for (int i = 0; i < fan_out * fan_in; ++i) p[off + i] = (float)((2.0 * next() - 1.0) * lim);
+  };
+  fill(MLP_P_W1, MLP_H, 1);
+  fill(MLP_P_W2, MLP_H, MLP_H);
+  fill(MLP_P_W3, MLP_H, MLP_H);
+  fill(MLP_P_W4, MLP_NOUT, MLP_H);
+}
+
+// host copy of the small layers and the BF16 packing of the 64x64 layers
+void mlp_finalize(chs_handle* H) {
+  std::vector<float> p(MLP_NPARAM);
+  CK(cudaMemcpyAsync(p.data(), H->mlp_params, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, H->st));
+  CK(cudaStreamSynchronize(H->st));
+  MlpSmall& sm = H->mlp_small;
+  for (int i = 0; i < MLP_H; ++i) {
+    sm.w1[i] = p[MLP_P_W1 + i];
+    sm.b1[i] = p[MLP_P_B1 + i];
+    sm.b2[i] = p[MLP_P_B2 + i];
+    sm.b3[i] = p[MLP_P_B3 + i];
+  }
+  for (int i = 0; i < MLP_NOUT * MLP_H; ++i) sm.w4[i] = p[MLP_P_W4 + i];
+  for (int i = 0; i < MLP_NOUT; ++i) sm.b4[i] = p[MLP_P_B4 + i];
+  mlp_pack(H->mlp_params, H->mlp_wpack, H->st);
+  H->launches++;
+  H->mlp_ready = true;
+}
+
+void mlp_train(chs_handle* H, const chs_mlp_train_cfg* c, chs_mlp_report* rep) {
+  if (!H->thermo) throw std::invalid_argument("the MLP surrogate needs chs_thermo_init");
+  if (c->nsamples < 1024 || c->batch < 64 || c->batch > 65536 || c->epochs < 1 || !(c->lr > 0.0))
+    throw std::invalid_argument("bad MLP training configuration");
+  mlp_alloc_core(H);
+  cudaStream_t st = H->st;
+  const int N = c->nsamples, B = c->batch;
+  MlpBuffers b;
+  auto ta = [&](size_t n) {
+    float* p = nullptr;
+    CK(cudaMallocAsync(&p, n * sizeof(float), st));
+    CK(cudaMemsetAsync(p, 0, n * sizeof(float), st));
+    return p;
+  };
+  b.grads = ta(MLP_NPARAM); b.m = ta(MLP_NPARAM); b.v = ta(MLP_NPARAM);
+  b.work = ta((size_t)8 * B * MLP_H); b.xs = ta(N); b.ys = ta((size_t)4 * N);
+  b.bx = ta(B); b.bt = ta((size_t)4 * B); b.loss = ta(1);
+  std::vector<float> p0;
+  mlp_init_host(p0, c->seed);
+  CK(cudaMemcpyAsync(H->mlp_params, p0.data(), MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, st));
+  mlp_make_samples(H->tab, H->mlp_norm, c->seed ^ 0x5A5A5A5Aull, N, b.xs, b.ys, st);
+  const long long steps = (long long)c->epochs * ((N + B - 1) / B);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, st));
+  const double pi = 3.141592653589793238462643383279502884;
+  for (long long s = 1; s <= steps; ++s) {
+    mlp_gather(b.xs, b.ys, N, c->seed, s, B, b.bx, b.bt, st);
+    mlp_grad(H->mlp_params, b.bx, b.bt, B, b.grads, b.loss, b.work, st);
+    // cosine decay to 1% of the initial rate
+    const double lr = c->lr * (0.01 + 0.99 * 0.5 * (1.0 + std::cos(pi * (double)s / (double)steps)));
+    mlp_adam(H->mlp_params, b.grads, b.m, b.v, MLP_NPARAM, (float)lr, s, st);
+  }
+  CK(cudaEventRecord(e1, st));
+  CK(cudaGetLastError());
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.0f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  float loss = 0.0f;
+  CK(cudaMemcpyAsync(&loss, b.loss, sizeof(float), cudaMemcpyDeviceToHost, st));
+  for (float* q : {b.grads, b.m, b.v, b.work, b.xs, b.ys, b.bx, b.bt, b.loss}) CK(cudaFreeAsync(q, st));
+  CK(cudaStreamSynchronize(st));
+  H->launches += steps * 15 + 2;
+  mlp_finalize(H);
+  rep->final_loss = loss;
+  rep->train_ms = ms;
+  rep->steps = (int)steps;
+}
+
+// network (with the per-cell check at tol; tol < 0 accepts every network value) on n host values
+void mlp_eval(chs_handle* H, int n, const double* rhoh, double tol, double* out, unsigned long long* nfb) {
+  if (!H->mlp_ready) throw std::invalid_argument("the MLP surrogate is not trained");
+  cudaStream_t st = H->st;
+  double* d = nullptr;
+  unsigned long long* cnt = nullptr;
+  CK(cudaMallocAsync(&d, (size_t)6 * n * sizeof(double), st));
+  CK(cudaMallocAsync(&cnt, sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
+  CK(cudaMemcpyAsync(d, rhoh, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st));
+  MlpCheck ck = H->mlp_check;
+  ck.tol = tol < 0.0 ? 1.0e300 : tol;
+  double *t = d + n, *rho = d + 2 * (size_t)n, *mu = d + 3 * (size_t)n, *ka = d + 4 * (size_t)n, *h = d + 5 * (size_t)n;
+  launch_mlp_props<double>(H->tab, H->mlp_norm, H->mlp_small, ck, H->mlp_wpack, d, h, t, ka, rho, mu, n, cnt, st);
+  H->launches++;
+  CK(cudaGetLastError());
+  // out[5][n] = T, rho, mu, kappa, h
+  CK(cudaMemcpyAsync(out, t, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(out + n, rho, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(out + 2 * (size_t)n, mu, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(out + 3 * (size_t)n, ka, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(out + 4 * (size_t)n, h, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(nfb, cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CK(cudaFreeAsync(d, st));
+  CK(cudaFreeAsync(cnt, st));
+  CK(cudaStreamSynchronize(st));
+  if (*nfb >> 62) throw std::runtime_error("MLP inference: tensor-core wait timed out");
 }
 
 void set_err(chs_handle* H, const char* fmt, ...) {
@@ -1196,6 +1371,88 @@ int chs_thermo_init(chs_handle* H, const chs_thermo* th) {
     if (H->thermo) throw std::invalid_argument("chs_thermo_init was already called");
     thermo_init(H, th);
   });
+}
+
+int chs_mlp_train(chs_handle* H, const chs_mlp_train_cfg* cfg, chs_mlp_report* rep) {
+  if (!H || !cfg || !rep) return CHS_ERR_ARG;
+  return guard(H, [&] { mlp_train(H, cfg, rep); });
+}
+
+int chs_mlp_set_mode(chs_handle* H, int mode, double tol) {
+  if (!H || mode < 0 || mode > 1) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    if (mode == 1 && !H->mlp_ready) throw std::invalid_argument("the MLP surrogate is not trained");
+    if (tol > 0.0) H->mlp_check.tol = tol;
+    if (mode != H->mlp_mode) drop_graphs(H);
+    H->mlp_mode = mode;
+    if (H->mlp_nfb) CK(cudaMemsetAsync(H->mlp_nfb, 0, sizeof(unsigned long long), H->st));
+  });
+}
+
+int chs_mlp_fallbacks(chs_handle* H, unsigned long long* count) {
+  if (!H || !count) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    *count = 0;
+    if (H->mlp_nfb) {
+      CK(cudaMemcpyAsync(count, H->mlp_nfb, sizeof(unsigned long long), cudaMemcpyDeviceToHost, H->st));
+      CK(cudaStreamSynchronize(H->st));
+    }
+  });
+}
+
+int chs_mlp_params(chs_handle* H, float* buf, int n, int set) {
+  if (!H || !buf || n != MLP_NPARAM) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    if (set) {
+      mlp_alloc_core(H);
+      CK(cudaMemcpyAsync(H->mlp_params, buf, n * sizeof(float), cudaMemcpyHostToDevice, H->st));
+      mlp_finalize(H);
+      drop_graphs(H);
+    } else {
+      if (!H->mlp_params) throw std::invalid_argument("no MLP parameters");
+      CK(cudaMemcpyAsync(buf, H->mlp_params, n * sizeof(float), cudaMemcpyDeviceToHost, H->st));
+      CK(cudaStreamSynchronize(H->st));
+    }
+  });
+}
+
+int chs_mlp_grad(chs_handle* H, const float* params, int B, const float* x, const float* t, float* grad,
+                 float* loss) {
+  if (!H || !params || !x || !t || !grad || !loss || B < 1 || B > 65536) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    cudaStream_t st = H->st;
+    float* d = nullptr;
+    const size_t need = (size_t)2 * MLP_NPARAM + B + (size_t)4 * B + (size_t)8 * B * MLP_H + 1;
+    CK(cudaMallocAsync(&d, need * sizeof(float), st));
+    float *P = d, *G = d + MLP_NPARAM, *X = G + MLP_NPARAM, *Tt = X + B, *W = Tt + (size_t)4 * B;
+    float* L = W + (size_t)8 * B * MLP_H;
+    CK(cudaMemcpyAsync(P, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(X, x, (size_t)B * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(Tt, t, (size_t)4 * B * sizeof(float), cudaMemcpyHostToDevice, st));
+    mlp_grad(P, X, Tt, B, G, L, W, st);
+    H->launches += 13;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(grad, G, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(loss, L, sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaFreeAsync(d, st));
+    CK(cudaStreamSynchronize(st));
+  });
+}
+
+int chs_mlp_eval(chs_handle* H, int n, const double* rhoh, double tol, double* out, unsigned long long* nfallback) {
+  if (!H || n < 1 || !rhoh || !out || !nfallback) return CHS_ERR_ARG;
+  return guard(H, [&] { mlp_eval(H, n, rhoh, tol, out, nfallback); });
+}
+
+int chs_mlp_norm(const chs_handle* H, double* out) {
+  if (!H || !out || !H->thermo) return CHS_ERR_ARG;
+  out[0] = H->mlp_norm.xa;
+  out[1] = H->mlp_norm.xb;
+  for (int j = 0; j < MLP_NOUT; ++j) {
+    out[2 + j] = H->mlp_norm.ya[j];
+    out[6 + j] = H->mlp_norm.yb[j];
+  }
+  return CHS_OK;
 }
 
 int chs_energy_substep(chs_handle* H, int isub) {

@@ -44,6 +44,18 @@ class ChsThermo(ctypes.Structure):
                 ("b", _D), ("rPrRen", ctypes.c_double), ("t_ini", ctypes.c_double)]
 
 
+class ChsMlpTrainCfg(ctypes.Structure):
+    _fields_ = [("nsamples", ctypes.c_int), ("batch", ctypes.c_int), ("epochs", ctypes.c_int),
+                ("lr", ctypes.c_double), ("seed", ctypes.c_ulonglong)]
+
+
+class ChsMlpReport(ctypes.Structure):
+    _fields_ = [("final_loss", ctypes.c_double), ("train_ms", ctypes.c_double), ("steps", ctypes.c_int)]
+
+
+MLP_NPARAM = 8708
+
+
 class ChsDiag(ctypes.Structure):
     _fields_ = [("max_div", ctypes.c_double), ("bulk_ke", ctypes.c_double), ("bulk_u", ctypes.c_double),
                 ("last_bulk_rhs", ctypes.c_double), ("nan_flag", ctypes.c_int)]
@@ -53,7 +65,9 @@ EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field
             "chs_step", "chs_poisson_solve", "chs_poisson_solve_device", "chs_diagnostics", "chs_op3d",
             "chs_plan_inspect", "chs_sync", "chs_kernel_launches", "chs_last_error", "chs_momentum_substep_host",
             "chs_time_steps", "chs_time_steps_host", "chs_host_alloc", "chs_host_free", "chs_profile_substep",
-            "chs_poisson_periodic_static", "chs_thermo_init", "chs_energy_substep", "chs_time_steps_host_fields"]
+            "chs_poisson_periodic_static", "chs_thermo_init", "chs_energy_substep", "chs_time_steps_host_fields",
+            "chs_mlp_train", "chs_mlp_set_mode", "chs_mlp_fallbacks", "chs_mlp_params", "chs_mlp_grad",
+            "chs_mlp_eval", "chs_mlp_norm"]
 
 
 class ChsKprof(ctypes.Structure):
@@ -96,6 +110,15 @@ def load():
     L.chs_profile_substep.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ChsKprof), ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int)]
     L.chs_thermo_init.argtypes = [ctypes.c_void_p, ctypes.POINTER(ChsThermo)]
+    _F = ctypes.POINTER(ctypes.c_float)
+    L.chs_mlp_train.argtypes = [ctypes.c_void_p, ctypes.POINTER(ChsMlpTrainCfg), ctypes.POINTER(ChsMlpReport)]
+    L.chs_mlp_set_mode.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+    L.chs_mlp_fallbacks.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong)]
+    L.chs_mlp_params.argtypes = [ctypes.c_void_p, _F, ctypes.c_int, ctypes.c_int]
+    L.chs_mlp_grad.argtypes = [ctypes.c_void_p, _F, ctypes.c_int, _F, _F, _F, _F]
+    L.chs_mlp_eval.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_double, _D,
+                               ctypes.POINTER(ctypes.c_ulonglong)]
+    L.chs_mlp_norm.argtypes = [ctypes.c_void_p, _D]
     L.chs_time_steps_host_fields.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D),
                                              ctypes.POINTER(ctypes.c_float)]
@@ -236,6 +259,56 @@ class Solver:
         if getattr(self, "_tcols", None) is not None and isub >= 1:
             self.Solve_energy_eq(isub)
         self.Solve_momentum_eq(isub)
+
+    # ---- MLP surrogate of the property update
+    def mlp_train(self, nsamples=1000000, batch=4096, epochs=20, lr=2e-3, seed=20250101):
+        cfg = ChsMlpTrainCfg(int(nsamples), int(batch), int(epochs), float(lr), int(seed))
+        rep = ChsMlpReport()
+        self._check(self.L.chs_mlp_train(self.h, ctypes.byref(cfg), ctypes.byref(rep)), "chs_mlp_train")
+        return dict(final_loss=rep.final_loss, train_ms=rep.train_ms, steps=rep.steps)
+
+    def mlp_set_mode(self, mode, tol=-1.0):
+        self._check(self.L.chs_mlp_set_mode(self.h, int(mode), float(tol)), "chs_mlp_set_mode")
+
+    def mlp_fallbacks(self):
+        c = ctypes.c_ulonglong()
+        self._check(self.L.chs_mlp_fallbacks(self.h, ctypes.byref(c)), "chs_mlp_fallbacks")
+        return int(c.value)
+
+    def mlp_params(self, values=None):
+        _F = ctypes.POINTER(ctypes.c_float)
+        if values is None:
+            out = np.zeros(MLP_NPARAM, np.float32)
+            self._check(self.L.chs_mlp_params(self.h, out.ctypes.data_as(_F), MLP_NPARAM, 0), "chs_mlp_params")
+            return out
+        v = np.ascontiguousarray(values, np.float32)
+        self._check(self.L.chs_mlp_params(self.h, v.ctypes.data_as(_F), MLP_NPARAM, 1), "chs_mlp_params")
+
+    def mlp_grad(self, params, x, t):
+        _F = ctypes.POINTER(ctypes.c_float)
+        p = np.ascontiguousarray(params, np.float32)
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.zeros(MLP_NPARAM, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check(self.L.chs_mlp_grad(self.h, p.ctypes.data_as(_F), len(x), x.ctypes.data_as(_F),
+                                        t.ctypes.data_as(_F), g.ctypes.data_as(_F), loss.ctypes.data_as(_F)),
+                    "chs_mlp_grad")
+        return float(loss[0]), g
+
+    def mlp_eval(self, rhoh, tol=-1.0):
+        """(out[5][n] = T, rho, mu, kappa, h; number of table fallbacks)."""
+        r = np.ascontiguousarray(rhoh, np.float64).ravel()
+        out = np.zeros((5, r.size))
+        c = ctypes.c_ulonglong()
+        self._check(self.L.chs_mlp_eval(self.h, r.size, _ptr(r), float(tol), _ptr(out), ctypes.byref(c)),
+                    "chs_mlp_eval")
+        return out, int(c.value)
+
+    def mlp_norm(self):
+        o = np.zeros(10)
+        self._check(self.L.chs_mlp_norm(self.h, _ptr(o)), "chs_mlp_norm")
+        return dict(xa=o[0], xb=o[1], ya=o[2:6].copy(), yb=o[6:10].copy())
 
     def get_thermo(self):
         """dict of rhoh, h, T, k, d, m (ccc) and gx, gy, gz."""
