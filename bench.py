@@ -321,19 +321,76 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
     return out
 
 
+def run_ensemble(args, world, rank, local, dist):
+    """Batched ensemble (48 periodic channels of seeded uneven grids and Re_b in [2000, 5000]),
+    mixed precision, autotuned launch shapes, one graph launch per substep for all members."""
+    from chapsim2_b200 import solver as S
+    cfgs = C.ensemble_members(n=args.members)
+    members, tuned = [], {}
+    for cfg in cfgs:
+        f = I.channel_fields(cfg)
+        cfg.dt = I.cfl_dt(cfg, *f[:3], cfl=0.8)
+        g = S.Solver(cfg, device=local, precision=S.CHS_MIXED)
+        g.set_fields(*f)
+        g.Solve_momentum_eq(0)
+        tuned[cfg.nc] = g.autotune(nsteps=2)[:2]
+        members.append(g)
+    e = S.Ensemble(members)
+    e.step(args.warmup)
+    cells = sum(c.ncell for c in cfgs)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(dist)
+    l0 = e.kernel_launches()
+    ms = e.time_steps(args.steps)
+    l1 = e.kernel_launches()
+    barrier(dist)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(dist, ms)
+    sub = 3 * args.steps
+    value = world * cells * sub / (ms_max * 1e-3) / 1e6
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+           "config": {"workload": f"ensemble of {len(cfgs)} channels, grids Nx in 64/96/128, Ny in 64/96, "
+                                  f"Nz in 64/96/128, Re_b in [2000, 5000], mixed precision, CD2",
+                      "cells": cells, "step": "one RK3 step = 3 graph launches for all members",
+                      "autotuned": {f"{k[0]}x{k[1]}x{k[2]}": list(v) for k, v in tuned.items()},
+                      "parallelism": f"replicas x{world}"},
+           "e2e": None, "gpu_launches": l1 - l0, "clocks": clk}
+    e.close()
+    for g in members:
+        g.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="heated", choices=["heated", "channel"])
+    ap.add_argument("--workload", default="heated", choices=["heated", "channel", "ensemble"])
+    ap.add_argument("--members", type=int, default=48)
     ap.add_argument("--nc", type=int, nargs=3, default=[128, 96, 128])
     ap.add_argument("--iacc", type=int, default=C.IACCU_CD2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "ensemble":
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the ensemble workload has no CPU arm; "
+                                  "run --workload heated or channel"}))
+            return
+        world, rank, local, dist = dist_setup(args.gpus)
+        out = run_ensemble(args, world, rank, local, dist)
+        if rank == 0:
+            print(json.dumps(out))
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     cfg, fields, tc = workload(args.workload, tuple(args.nc), args.iacc)
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))

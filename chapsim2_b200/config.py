@@ -170,6 +170,29 @@ def heated_channel(nc=(128, 96, 128), iacc=IACCU_CD2, dt=None, rstret=0.075, ren
     return cfg, tc
 
 
+def ensemble_members(n=48, seed=4242, nx=(64, 96, 128), ny=(64, 96), nz=(64, 96, 128), re=(2000.0, 5000.0),
+                     iacc=IACCU_CD2):
+    """Members of the batched ensemble: periodic channels 4pi x 2 x 4pi/3 with tanh stretching
+    beta = 1.5 whose grids (Nx, Ny, Nz) and bulk Reynolds numbers are drawn by a seeded splitmix64
+    stream."""
+    state = [seed & 0xFFFFFFFFFFFFFFFF]
+
+    def u():
+        state[0] = (state[0] + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+        z = state[0]
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+        z ^= z >> 31
+        return (z >> 11) / float(1 << 53)
+
+    out = []
+    for _ in range(n):
+        g = (nx[int(u() * len(nx))], ny[int(u() * len(ny))], nz[int(u() * len(nz))])
+        r = re[0] + (re[1] - re[0]) * u()
+        out.append(channel(nc=g, ren=r, iacc=iacc))
+    return out
+
+
 # ---------------------------------------------------------------------------
 # geometry (src/geometry.f90)
 # ---------------------------------------------------------------------------

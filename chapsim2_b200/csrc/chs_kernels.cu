@@ -284,7 +284,7 @@ __device__ __forceinline__ T bulk_fn(const F& f, int i, T r1, T r2) {
 }
 
 template <typename T, int DIR, int FAM>
-__global__ void __launch_bounds__(256) stencil_op_kernel(const __grid_constant__ OpPlan P,
+__global__ void __launch_bounds__(512) stencil_op_kernel(const __grid_constant__ OpPlan P,
                                                          const __grid_constant__ LineIOT<T> io,
                                                          const double* __restrict__ table, int nlines, int m1,
                                                          int m2) {
@@ -347,11 +347,12 @@ static void launch_stencil_dir(const OpPlan& P, const LineIOT<T>& io, const doub
   if ((int64_t)m[0] * m[1] > 0x7fffffff || m[2] > 65535)
     throw std::runtime_error("explicit operator: array extents out of range");
   const int plane = m[0] * m[1];
-  dim3 grid((unsigned)((plane + 255) / 256), (unsigned)m[2]);
+  const int bs = (io.block == 128 || io.block == 512) ? io.block : 256;  // tunable CTA size
+  dim3 grid((unsigned)((plane + bs - 1) / bs), (unsigned)m[2]);
   switch (P.fam) {
 #define CHS_CASE(F)                                                                                 \
   case F:                                                                                           \
-    stencil_op_kernel<T, DIR, F><<<grid, 256, 0, st>>>(P, io, table, nlines, m[0], m[1]);           \
+    stencil_op_kernel<T, DIR, F><<<grid, bs, 0, st>>>(P, io, table, nlines, m[0], m[1]);            \
     break;
     CHS_CASE(D1C2C)
     CHS_CASE(D1P2P)
@@ -411,7 +412,7 @@ void launch_line_op_t(int d, const OpPlan& P, const LineIOT<T>& io, const double
   const int nmax = P.nin > P.nout ? P.nin : P.nout;
   // up to 64 lines per CTA, fewer while the tile exceeds ~45 KB so that four or more CTAs
   // (32+ warps) stay resident per SM
-  int LT = 64;
+  int LT = (io.lt_max == 16 || io.lt_max == 32) ? io.lt_max : 64;  // tunable lines per CTA
   while (LT > 16 && ((size_t)nmax * (LT + 1) + 5 * (size_t)nmax) * sizeof(T) > 45 * 1024) LT /= 2;
   const size_t shm = ((size_t)nmax * (LT + 1) + 5 * (size_t)nmax) * sizeof(T);
   if (shm > (size_t)kLineSmemMax) throw std::runtime_error("line operator: line too long for the shared-memory tile");

@@ -39,6 +39,8 @@ struct LineIOT {
   int n1, n2, n3;     // extents of the INPUT array (x fastest)
   int omode;          // OutMode
   const T* onum;      // numerator / factor of O_DIV / O_MUL (output layout)
+  int block;          // launch shape chosen by the autotuner: explicit-operator CTA size (0 = 256)
+  int lt_max;         // and lines per CTA of the compact-scheme tile kernel (0 = 64)
 };
 using LineIO = LineIOT<double>;
 

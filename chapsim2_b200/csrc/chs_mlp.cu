@@ -309,6 +309,9 @@ __global__ void __launch_bounds__(128) mlp_props_kernel(
       if (tid == 0) issue_layer(tmem, sa, sw + layer * 8192, bar);
       if (!mbar_wait(bar, phase)) failed = 1;
       phase ^= 1;
+      // a wait that gave up leaves the accumulators unread: every thread sees the flag here
+      __syncthreads();
+      if (failed) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       uint32_t r[64];
       tmem_ld64(tl, r);

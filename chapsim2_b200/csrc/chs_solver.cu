@@ -117,7 +117,8 @@ struct chs_handle {
   PlanBook book;
   std::map<std::tuple<int, int, int, int, int>, OpPlan> plans;
   double* table = nullptr;
-  std::vector<void*> allocs;
+  std::vector<std::pair<void*, size_t>> allocs;
+  int tune_block = 0, tune_lt = 0;  // launch shapes picked by chs_autotune (0 = defaults)
   long long launches = 0;
   std::string err;
 
@@ -190,7 +191,7 @@ struct chs_handle {
     void* p = nullptr;
     CK(cudaMalloc(&p, n * sizeof(T) + 64));
     CK(cudaMemsetAsync(p, 0, n * sizeof(T) + 64, st));
-    allocs.push_back(p);
+    allocs.push_back({p, n * sizeof(T) + 64});
     return static_cast<T*>(p);
   }
   const OpPlan& plan(int d, int fam, Pair bc, bool has_fbc) {
@@ -267,6 +268,8 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const typename Id<T>::type* 
   io.n1 = n_in[0]; io.n2 = n_in[1]; io.n3 = n_in[2];
   io.omode = omode;
   io.onum = onum;
+  io.block = H->tune_block;
+  io.lt_max = H->tune_lt;
   const double nin_tot = (double)n_in[0] * n_in[1] * n_in[2];
   const double nout_tot = nin_tot / P.nin * P.nout;
   const int narr = in.narrays();
@@ -1309,7 +1312,228 @@ void capture_graphs(chs_handle* H) {
 
 }  // namespace
 
+// Batched ensemble of independent handles: one captured graph per RK3 substep whose branches
+// (one per member, on the member's stream) run concurrently, so one graph launch advances every
+// member.  The members stay owned by the caller.
+struct chs_ensemble {
+  std::vector<chs_handle*> m;
+  cudaStream_t st = nullptr;
+  cudaEvent_t fork = nullptr, done = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t g[4] = {nullptr, nullptr, nullptr, nullptr};
+  long long kps[4] = {0, 0, 0, 0};
+  long long launches = 0;
+  std::string err;
+};
+
+namespace {
+
+void ensemble_capture(chs_ensemble* E) {
+  for (int isub = 1; isub <= 3; ++isub) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(E->st, cudaStreamCaptureModeThreadLocal));
+    long long kernels = 0;
+    try {
+      CK(cudaEventRecord(E->fork, E->st));
+      for (size_t i = 0; i < E->m.size(); ++i) {
+        chs_handle* H = E->m[i];
+        CK(cudaStreamWaitEvent(H->st, E->fork, 0));
+        const long long before = H->launches;
+        H->capturing = true;
+        substep_body(H, isub);
+        H->capturing = false;
+        kernels += H->launches - before;
+        H->launches = before;
+        CK(cudaEventRecord(E->join[i], H->st));
+        CK(cudaStreamWaitEvent(E->st, E->join[i], 0));
+      }
+    } catch (...) {
+      for (chs_handle* H : E->m) H->capturing = false;
+      cudaStreamEndCapture(E->st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CK(cudaStreamEndCapture(E->st, &g));
+    CK(cudaGraphInstantiate(&E->g[isub], g, 0));
+    CK(cudaGraphDestroy(g));
+    E->kps[isub] = kernels;
+  }
+}
+
+// order the ensemble stream after each member's pending work, run, then order the members after it
+void ensemble_run(chs_ensemble* E, int nsteps) {
+  for (size_t i = 0; i < E->m.size(); ++i) {
+    CK(cudaEventRecord(E->join[i], E->m[i]->st));
+    CK(cudaStreamWaitEvent(E->st, E->join[i], 0));
+  }
+  for (int s = 0; s < nsteps; ++s)
+    for (int isub = 1; isub <= 3; ++isub) {
+      CK(cudaGraphLaunch(E->g[isub], E->st));
+      E->launches += E->kps[isub];
+    }
+  CK(cudaEventRecord(E->done, E->st));
+  for (chs_handle* H : E->m) CK(cudaStreamWaitEvent(H->st, E->done, 0));
+}
+
+int eguard(chs_ensemble* E, const std::function<void()>& f) {
+  try {
+    f();
+    return CHS_OK;
+  } catch (const CudaError& e) {
+    E->err = e.what();
+    return CHS_ERR_CUDA;
+  } catch (const std::exception& e) {
+    E->err = e.what();
+    return CHS_ERR_ARG;
+  }
+}
+
+// copy every device allocation of the handle into one buffer (or back), for trial runs
+void snapshot(chs_handle* H, char* buf, bool save) {
+  size_t off = 0;
+  for (auto& a : H->allocs) {
+    if (save) CK(cudaMemcpyAsync(buf + off, a.first, a.second, cudaMemcpyDeviceToDevice, H->st));
+    else CK(cudaMemcpyAsync(a.first, buf + off, a.second, cudaMemcpyDeviceToDevice, H->st));
+    off += a.second;
+  }
+}
+
+float time_steps_ms(chs_handle* H, int nsteps) {
+  if (!H->gexec[1]) capture_graphs(H);
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, H->st));
+  for (int s = 0; s < nsteps; ++s)
+    for (int isub = 1; isub <= 3; ++isub) CK(cudaGraphLaunch(H->gexec[isub], H->st));
+  CK(cudaEventRecord(b, H->st));
+  CK(cudaEventSynchronize(b));
+  float ms = 0.0f;
+  CK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms;
+}
+
+}  // namespace
+
 extern "C" {
+
+int chs_autotune(chs_handle* H, int nsteps, int* block, int* lt_max, float* best_ms) {
+  if (!H || !block || !lt_max || !best_ms || nsteps < 1) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    size_t total = 0;
+    for (auto& a : H->allocs) total += a.second;
+    char* snap = nullptr;
+    CK(cudaMalloc(&snap, total));
+    snapshot(H, snap, true);
+    const int blocks[3] = {128, 256, 512};
+    const bool compact = H->iacc >= 3;
+    const int lts[3] = {16, 32, 64};
+    int bb = 256, bl = 64;
+    float best = 1e30f;
+    try {
+      for (int b : blocks)
+        for (int l : lts) {
+          if (!compact && l != 64) continue;
+          H->tune_block = b;
+          H->tune_lt = l;
+          drop_graphs(H);
+          time_steps_ms(H, 1);  // capture and warm up
+          const float ms = time_steps_ms(H, nsteps);
+          snapshot(H, snap, false);
+          if (ms < best) { best = ms; bb = b; bl = l; }
+        }
+    } catch (...) {
+      snapshot(H, snap, false);
+      cudaStreamSynchronize(H->st);
+      cudaFree(snap);
+      throw;
+    }
+    CK(cudaStreamSynchronize(H->st));
+    cudaFree(snap);
+    H->tune_block = bb;
+    H->tune_lt = bl;
+    drop_graphs(H);
+    *block = bb;
+    *lt_max = bl;
+    *best_ms = best;
+  });
+}
+
+int chs_ensemble_create(chs_handle* const* members, int n, chs_ensemble** out) {
+  if (!members || n < 1 || !out) return CHS_ERR_ARG;
+  auto* E = new chs_ensemble();
+  const int rc = eguard(E, [&] {
+    int dev0 = -1;
+    for (int i = 0; i < n; ++i) {
+      if (!members[i]) throw std::invalid_argument("null member");
+      if (dev0 < 0) dev0 = members[i]->device;
+      if (members[i]->device != dev0) throw std::invalid_argument("ensemble members must share one device");
+      E->m.push_back(members[i]);
+    }
+    CK(cudaSetDevice(dev0));
+    CK(cudaStreamCreateWithFlags(&E->st, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&E->fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&E->done, cudaEventDisableTiming));
+    E->join.resize(n);
+    for (auto& e : E->join) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (chs_handle* H : E->m) CK(cudaStreamSynchronize(H->st));
+    ensemble_capture(E);
+  });
+  if (rc != CHS_OK) {
+    std::fprintf(stderr, "chs_ensemble_create: %s\n", E->err.c_str());
+    chs_ensemble_destroy(E);
+    *out = nullptr;
+    return rc;
+  }
+  *out = E;
+  return CHS_OK;
+}
+
+int chs_ensemble_step(chs_ensemble* E, int nsteps) {
+  if (!E || nsteps < 0) return CHS_ERR_ARG;
+  return eguard(E, [&] {
+    ensemble_run(E, nsteps);
+    CK(cudaGetLastError());
+  });
+}
+
+int chs_ensemble_time_steps(chs_ensemble* E, int nsteps, float* ms) {
+  if (!E || !ms || nsteps < 0) return CHS_ERR_ARG;
+  return eguard(E, [&] {
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    for (size_t i = 0; i < E->m.size(); ++i) {
+      CK(cudaEventRecord(E->join[i], E->m[i]->st));
+      CK(cudaStreamWaitEvent(E->st, E->join[i], 0));
+    }
+    CK(cudaEventRecord(a, E->st));
+    ensemble_run(E, nsteps);
+    CK(cudaEventRecord(b, E->st));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  });
+}
+
+long long chs_ensemble_kernel_launches(const chs_ensemble* E) { return E ? E->launches : 0; }
+
+int chs_ensemble_destroy(chs_ensemble* E) {
+  if (!E) return CHS_OK;
+  if (E->st) cudaStreamSynchronize(E->st);
+  for (auto& g : E->g)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto& e : E->join)
+    if (e) cudaEventDestroy(e);
+  if (E->fork) cudaEventDestroy(E->fork);
+  if (E->done) cudaEventDestroy(E->done);
+  if (E->st) cudaStreamDestroy(E->st);
+  delete E;
+  return CHS_OK;
+}
 
 int chs_create(const chs_config* cfg, int device, chs_handle** out) {
   if (!cfg || !out) return CHS_ERR_ARG;
@@ -1337,7 +1561,7 @@ int chs_destroy(chs_handle* H) {
   if (H->st) cudaStreamSynchronize(H->st);
   drop_graphs(H);
   if (H->table) cudaFree(H->table);
-  for (void* p : H->allocs) cudaFree(p);
+  for (auto& a : H->allocs) cudaFree(a.first);
   if (H->st) cudaStreamDestroy(H->st);
   delete H;
   return CHS_OK;

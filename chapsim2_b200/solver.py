@@ -67,7 +67,8 @@ EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field
             "chs_time_steps", "chs_time_steps_host", "chs_host_alloc", "chs_host_free", "chs_profile_substep",
             "chs_poisson_periodic_static", "chs_thermo_init", "chs_energy_substep", "chs_time_steps_host_fields",
             "chs_mlp_train", "chs_mlp_set_mode", "chs_mlp_fallbacks", "chs_mlp_params", "chs_mlp_grad",
-            "chs_mlp_eval", "chs_mlp_norm"]
+            "chs_mlp_eval", "chs_mlp_norm", "chs_ensemble_create", "chs_ensemble_step", "chs_ensemble_time_steps",
+            "chs_ensemble_kernel_launches", "chs_ensemble_destroy", "chs_autotune"]
 
 
 class ChsKprof(ctypes.Structure):
@@ -119,6 +120,14 @@ def load():
     L.chs_mlp_eval.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_double, _D,
                                ctypes.POINTER(ctypes.c_ulonglong)]
     L.chs_mlp_norm.argtypes = [ctypes.c_void_p, _D]
+    L.chs_ensemble_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.chs_ensemble_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.chs_ensemble_time_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.chs_ensemble_kernel_launches.restype = ctypes.c_longlong
+    L.chs_ensemble_kernel_launches.argtypes = [ctypes.c_void_p]
+    L.chs_ensemble_destroy.argtypes = [ctypes.c_void_p]
+    L.chs_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]
     L.chs_time_steps_host_fields.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D),
                                              ctypes.POINTER(ctypes.c_float)]
@@ -259,6 +268,13 @@ class Solver:
         if getattr(self, "_tcols", None) is not None and isub >= 1:
             self.Solve_energy_eq(isub)
         self.Solve_momentum_eq(isub)
+
+    def autotune(self, nsteps=2):
+        """Pick the fastest launch shapes for this handle; returns (block, lt_max, ms per nsteps)."""
+        b, l, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        self._check(self.L.chs_autotune(self.h, int(nsteps), ctypes.byref(b), ctypes.byref(l), ctypes.byref(ms)),
+                    "chs_autotune")
+        return b.value, l.value, ms.value
 
     # ---- MLP surrogate of the property update
     def mlp_train(self, nsamples=1000000, batch=4096, epochs=20, lr=2e-3, seed=20250101):
@@ -404,3 +420,43 @@ class Solver:
 
     def kernel_launches(self):
         return int(self.L.chs_kernel_launches(self.h))
+
+
+class Ensemble:
+    """Independent Solvers advanced together: one CUDA-graph launch per RK3 substep for all members."""
+
+    def __init__(self, solvers):
+        self.L = load()
+        self.members = list(solvers)
+        arr = (ctypes.c_void_p * len(self.members))(*[m.h.value for m in self.members])
+        e = ctypes.c_void_p()
+        rc = self.L.chs_ensemble_create(arr, len(self.members), ctypes.byref(e))
+        if rc != 0 or not e.value:
+            raise RuntimeError(f"chs_ensemble_create failed with status {rc}")
+        self.e = e
+
+    def step(self, nsteps=1):
+        rc = self.L.chs_ensemble_step(self.e, int(nsteps))
+        if rc != 0:
+            raise RuntimeError(f"chs_ensemble_step failed with status {rc}")
+
+    def time_steps(self, nsteps):
+        ms = ctypes.c_float()
+        rc = self.L.chs_ensemble_time_steps(self.e, int(nsteps), ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"chs_ensemble_time_steps failed with status {rc}")
+        return float(ms.value)
+
+    def kernel_launches(self):
+        return int(self.L.chs_ensemble_kernel_launches(self.e))
+
+    def close(self):
+        if getattr(self, "e", None) and self.e.value:
+            self.L.chs_ensemble_destroy(self.e)
+            self.e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -205,6 +205,28 @@ int chs_mlp_eval(chs_handle* h, int n, const double* rhoh, double tol, double* o
 /* normalisation: out[10] = xa, xb (x = xa*rhoh + xb), ya[4], yb[4] (value = ya*y + yb) */
 int chs_mlp_norm(const chs_handle* h, double* out);
 
+/*
+ * Batched ensembles (no counterpart in the reference, which runs one domain per
+ * MPI job): independent handles, of any grids, Reynolds numbers and precisions,
+ * on one device advance together.  Each RK3 substep is one captured CUDA graph
+ * whose branches are the members' substeps on their own streams, so one graph
+ * launch advances every member and the members' kernels overlap on the GPU.
+ * The members stay owned by the caller and must have taken their initial step
+ * (chs_momentum_substep(h, 0)); their own entry points stay usable and are
+ * ordered after the ensemble's work.
+ */
+typedef struct chs_ensemble chs_ensemble;
+int chs_ensemble_create(chs_handle* const* members, int n, chs_ensemble** out);
+int chs_ensemble_step(chs_ensemble* e, int nsteps);
+int chs_ensemble_time_steps(chs_ensemble* e, int nsteps, float* ms);
+long long chs_ensemble_kernel_launches(const chs_ensemble* e);
+int chs_ensemble_destroy(chs_ensemble* e);
+
+/* Autotuner: times nsteps RK3 steps for each candidate launch shape (CTA size
+ * of the explicit line operators; lines per CTA of the compact-scheme tile) on
+ * this handle, restoring the state after each trial, and keeps the fastest. */
+int chs_autotune(chs_handle* h, int nsteps, int* block, int* lt_max, float* best_ms);
+
 /* Same as chs_poisson_solve on a device buffer (no host copies). */
 int chs_poisson_solve_device(chs_handle* h, double* d_rhs_inout);
 
