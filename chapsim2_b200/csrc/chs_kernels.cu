@@ -283,60 +283,99 @@ __device__ __forceinline__ T bulk_fn(const F& f, int i, T r1, T r2) {
   return v;
 }
 
+// int32-offset evaluation of the input expression (arrays below 2^31 values)
+template <typename T>
+__device__ __forceinline__ T eval_term32(const TermT<T>& t, int a) {
+  switch (t.mode) {
+    case T_X: return T(t.s) * t.X[a];
+    case T_XY: return T(t.s) * (t.X[a] * t.Y[a]);
+    case T_XpY: return T(t.s) * (t.X[a] + T(t.c) * t.Y[a]);
+    case T_XpYZ: return T(t.s) * (t.X[a] + T(t.c) * t.Y[a]) * t.Z[a];
+    default: return T(0);
+  }
+}
+template <typename T>
+__device__ __forceinline__ T eval_expr32(const LineIOT<T>& io, int a) {
+  T v = eval_term32(io.t[0], a);
+  if (io.t[1].mode != T_NONE) v += eval_term32(io.t[1], a);
+  return v;
+}
+
+// Each thread owns one (i, j) position of the output plane and kStencilPlanes consecutive k
+// planes, so the index decomposition and the per-launch constants are paid once per
+// kStencilPlanes outputs and the loads of the planes are independent.
+constexpr int kStencilPlanes = 1;
+
 template <typename T, int DIR, int FAM>
 __global__ void __launch_bounds__(512) stencil_op_kernel(const __grid_constant__ OpPlan P,
                                                          const __grid_constant__ LineIOT<T> io,
                                                          const double* __restrict__ table, int nlines, int m1,
-                                                         int m2) {
-  // output array (m1, m2, m3), x fastest: blockIdx.y is the outermost index k, the x grid
-  // covers the (i, j) plane
+                                                         int m2, int m3) {
+  // output array (m1, m2, m3), x fastest: blockIdx.y covers groups of k planes, the x grid the
+  // (i, j) plane
   const int nin = P.nin, nout = P.nout;
   const int plane = m1 * m2;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= plane) return;
-  const int k = blockIdx.y;
   const int j = q / m1;
   const int i = q - j * m1;
-  int p, L;
-  int64_t ibase, istride;
-  if (DIR == 0) {
-    p = i;
-    L = j + m2 * k;
-    ibase = (int64_t)L * nin;
-    istride = 1;
-  } else if (DIR == 1) {
-    p = j;
-    L = i + m1 * k;
-    ibase = (int64_t)k * nin * m1 + i;
-    istride = m1;
-  } else {
-    p = k;
-    L = q;
-    ibase = q;
-    istride = plane;
-  }
-  const int64_t o = (int64_t)plane * k + q;
   const T dd = T(P.dd), r1 = T(P.r1), r2 = T(P.r2), g = T(io.g);
-  auto f = [&](int qq) -> T { return eval_expr(io, ibase + (int64_t)qq * istride); };
-  T v;
-  if (p >= P.b_lo && p <= P.b_hi) {
-    v = bulk_fn<FAM>(f, p, r1, r2) * dd;
-  } else {
-    v = T(0);
-    for (int s = 0; s < P.nspec; ++s) {
-      if (P.sp[s].row != p) continue;
-      const SpecialRow& R = P.sp[s];
-      T acc = T(0);
-      for (int t = 0; t < R.nt; ++t) acc += T(R.w[t]) * f(R.idx[t]);
-      for (int u = 0; u < 4; ++u)
-        if (R.wb[u] != 0.0) acc += T(R.wb[u]) * io.fbc[u * nlines + L];
-      v = acc * dd;
+  const int k0 = blockIdx.y * kStencilPlanes;
+  // all planes' values first, then the stores: the inputs never alias the output, so the loads of
+  // the kStencilPlanes planes are all in flight together
+  T vals[kStencilPlanes];
+  int Ls[kStencilPlanes], ps[kStencilPlanes];
+#pragma unroll
+  for (int kk = 0; kk < kStencilPlanes; ++kk) {
+    const int k = k0 + kk < m3 ? k0 + kk : m3 - 1;
+    int p, L, ibase, istride;
+    if (DIR == 0) {
+      p = i;
+      L = j + m2 * k;
+      ibase = L * nin;
+      istride = 1;
+    } else if (DIR == 1) {
+      p = j;
+      L = i + m1 * k;
+      ibase = k * nin * m1 + i;
+      istride = m1;
+    } else {
+      p = k;
+      L = q;
+      ibase = q;
+      istride = plane;
     }
+    auto f = [&](int qq) -> T { return eval_expr32(io, ibase + qq * istride); };
+    T v;
+    if (p >= P.b_lo && p <= P.b_hi) {
+      v = bulk_fn<FAM>(f, p, r1, r2) * dd;
+    } else {
+      v = T(0);
+      for (int s = 0; s < P.nspec; ++s) {
+        if (P.sp[s].row != p) continue;
+        const SpecialRow& R = P.sp[s];
+        T acc = T(0);
+        for (int t = 0; t < R.nt; ++t) acc += T(R.w[t]) * f(R.idx[t]);
+        for (int u = 0; u < 4; ++u)
+          if (R.wb[u] != 0.0) acc += T(R.wb[u]) * io.fbc[u * nlines + L];
+        v = acc * dd;
+      }
+    }
+    vals[kk] = v;
+    Ls[kk] = L;
+    ps[kk] = p;
   }
-  if (P.lmap >= 0) v *= T(table[P.lmap + p]);
-  if (P.neu1 && p == 0) v = io.fbc[L];
-  if (P.neu2 && p == nout - 1) v = io.fbc[nlines + L];
-  store_out(io, o, g, v);
+#pragma unroll
+  for (int kk = 0; kk < kStencilPlanes; ++kk) {
+    const int k = k0 + kk;
+    if (k >= m3) break;
+    const int p = ps[kk], L = Ls[kk];
+    T v = vals[kk];
+    if (P.lmap >= 0) v *= T(table[P.lmap + p]);
+    if (P.neu1 && p == 0) v = io.fbc[L];
+    if (P.neu2 && p == nout - 1) v = io.fbc[nlines + L];
+    store_out(io, (int64_t)(plane * k + q), g, v);
+  }
 }
 
 template <typename T, int DIR>
@@ -344,15 +383,16 @@ static void launch_stencil_dir(const OpPlan& P, const LineIOT<T>& io, const doub
                                int nlines) {
   int m[3] = {io.n1, io.n2, io.n3};
   m[DIR] = P.nout;
-  if ((int64_t)m[0] * m[1] > 0x7fffffff || m[2] > 65535)
-    throw std::runtime_error("explicit operator: array extents out of range");
+  const int64_t nin_tot = (int64_t)io.n1 * io.n2 * io.n3, nout_tot = (int64_t)m[0] * m[1] * m[2];
+  if (nin_tot >= 0x7fffffff || nout_tot >= 0x7fffffff)
+    throw std::runtime_error("explicit operator: arrays of 2^31 or more values are not supported");
   const int plane = m[0] * m[1];
   const int bs = (io.block == 128 || io.block == 512) ? io.block : 256;  // tunable CTA size
-  dim3 grid((unsigned)((plane + bs - 1) / bs), (unsigned)m[2]);
+  dim3 grid((unsigned)((plane + bs - 1) / bs), (unsigned)((m[2] + kStencilPlanes - 1) / kStencilPlanes));
   switch (P.fam) {
 #define CHS_CASE(F)                                                                                 \
   case F:                                                                                           \
-    stencil_op_kernel<T, DIR, F><<<grid, bs, 0, st>>>(P, io, table, nlines, m[0], m[1]);            \
+    stencil_op_kernel<T, DIR, F><<<grid, bs, 0, st>>>(P, io, table, nlines, m[0], m[1], m[2]);      \
     break;
     CHS_CASE(D1C2C)
     CHS_CASE(D1P2P)
