@@ -405,6 +405,134 @@ static void launch_stencil_dir(const OpPlan& P, const LineIOT<T>& io, const doub
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fused explicit operators: one pass computes sum_m g_m op_m(in_m) at every output value and
+// applies the epilogue (store, RK3 fractional step, or the energy update with the property
+// lookup).  Each term is evaluated like stencil_op_kernel evaluates one output value.
+// ---------------------------------------------------------------------------
+template <typename T, int DIR, int FAM>
+__device__ __forceinline__ T fused_term_at(const FusedTerm<T>& ft, const double* __restrict__ table, int i, int j,
+                                           int k) {
+  const OpPlan& P = ft.P;
+  const int nin = P.nin, nout = P.nout;
+  int p, L, ibase, istride;
+  if (DIR == 0) {
+    p = i;
+    L = j + ft.n2 * k;
+    ibase = L * nin;
+    istride = 1;
+  } else if (DIR == 1) {
+    p = j;
+    L = i + ft.n1 * k;
+    ibase = k * nin * ft.n1 + i;
+    istride = ft.n1;
+  } else {
+    p = k;
+    L = i + ft.n1 * j;
+    ibase = L;
+    istride = ft.n1 * ft.n2;
+  }
+  auto f = [&](int qq) -> T {
+    const int a = ibase + qq * istride;
+    T v = eval_term32(ft.t[0], a);
+    if (ft.t[1].mode != T_NONE) v += eval_term32(ft.t[1], a);
+    return v;
+  };
+  const T dd = T(P.dd);
+  T v;
+  if (p >= P.b_lo && p <= P.b_hi) {
+    v = bulk_fn<FAM>(f, p, T(P.r1), T(P.r2)) * dd;
+  } else {
+    v = T(0);
+    for (int s = 0; s < P.nspec; ++s) {
+      if (P.sp[s].row != p) continue;
+      const SpecialRow& R = P.sp[s];
+      T acc = T(0);
+      for (int t = 0; t < R.nt; ++t) acc += T(R.w[t]) * f(R.idx[t]);
+      for (int u = 0; u < 4; ++u)
+        if (R.wb[u] != 0.0) acc += T(R.wb[u]) * ft.fbc[u * ft.nlines + L];
+      v = acc * dd;
+    }
+  }
+  if (P.lmap >= 0) v *= T(table[P.lmap + p]);
+  if (P.neu1 && p == 0) v = ft.fbc[L];
+  if (P.neu2 && p == nout - 1) v = ft.fbc[ft.nlines + L];
+  return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fused_kernel(const __grid_constant__ FusedIO<T> F,
+                                                    const double* __restrict__ table) {
+  const int plane = F.m1 * F.m2;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= plane) return;
+  const int k = blockIdx.y;
+  const int j = q / F.m1;
+  const int i = q - j * F.m1;
+  T sum0 = T(0), sum1 = T(0);
+  for (int mt = 0; mt < F.nterm; ++mt) {
+    const FusedTerm<T>& ft = F.term[mt];
+    T v;
+    switch (ft.dir * 8 + ft.P.fam) {
+      case 0 * 8 + D1C2P: v = fused_term_at<T, 0, D1C2P>(ft, table, i, j, k); break;
+      case 1 * 8 + D1C2P: v = fused_term_at<T, 1, D1C2P>(ft, table, i, j, k); break;
+      case 2 * 8 + D1C2P: v = fused_term_at<T, 2, D1C2P>(ft, table, i, j, k); break;
+      case 0 * 8 + D1P2C: v = fused_term_at<T, 0, D1P2C>(ft, table, i, j, k); break;
+      case 1 * 8 + D1P2C: v = fused_term_at<T, 1, D1P2C>(ft, table, i, j, k); break;
+      case 2 * 8 + D1P2C: v = fused_term_at<T, 2, D1P2C>(ft, table, i, j, k); break;
+      default: v = T(0);
+    }
+    const T gv = T(ft.g) * v;
+    if (ft.group == 0) sum0 = sum0 + gv;
+    else sum1 = sum1 + gv;
+  }
+  const int64_t o = (int64_t)plane * k + q;
+  if (F.epilogue == EP_STORE) {
+    F.out[o] = sum0;
+  } else if (F.epilogue == EP_ACCUM) {
+    F.out[o] = F.out[o] + sum0;
+  } else if (F.epilogue == EP_FRAC) {
+    const T last = F.rhs0[o];
+    T tot = T(F.gam) * sum0 + T(F.zeta) * last;
+    F.rhs0[o] = sum0;
+    tot = tot + T(F.alpha) * sum1;
+    F.out[o] = T(F.dt) * tot;
+  } else {  // EP_ENERGY
+    const T last = F.rhs0[o];
+    const T tot = T(F.gam) * sum0 + T(F.zeta) * last;
+    F.rhs0[o] = sum0;
+    const T r1 = T(F.dt) * tot;
+    const T rh = F.rhoh[o] + r1;
+    F.rhoh[o] = rh;
+    if (F.props) {
+      const CellProps pr = props_from_dh(F.tab, (double)rh);
+      F.h[o] = T(pr.h);
+      F.t[o] = T(pr.t);
+      F.k[o] = T(pr.k);
+      F.d[o] = T(pr.d);
+      F.m[o] = T(pr.m);
+    }
+  }
+}
+
+template <typename T>
+void launch_fused(const FusedIO<T>& f, const double* table, cudaStream_t st) {
+  if (f.nterm < 1 || f.nterm > kMaxFusedTerms) throw std::runtime_error("fused operator: bad term count");
+  if ((int64_t)f.m1 * f.m2 * f.m3 >= 0x7fffffff || f.m3 > 65535)
+    throw std::runtime_error("fused operator: array extents out of range");
+  for (int t = 0; t < f.nterm; ++t) {
+    const FusedTerm<T>& ft = f.term[t];
+    if (ft.P.tdma) throw std::runtime_error("fused operator: compact (line-solve) plans cannot be fused");
+    if (ft.P.fam != D1C2P && ft.P.fam != D1P2C) throw std::runtime_error("fused operator: unsupported family");
+    if ((int64_t)ft.n1 * ft.n2 * ft.n3 >= 0x7fffffff) throw std::runtime_error("fused operator: input too large");
+  }
+  const int plane = f.m1 * f.m2;
+  dim3 grid((unsigned)((plane + 255) / 256), (unsigned)f.m3);
+  fused_kernel<T><<<grid, 256, 0, st>>>(f, table);
+}
+template void launch_fused<double>(const FusedIO<double>&, const double*, cudaStream_t);
+template void launch_fused<float>(const FusedIO<float>&, const double*, cudaStream_t);
+
 constexpr int kLineSmemMax = 200 * 1024;
 
 template <typename T, int DIR>

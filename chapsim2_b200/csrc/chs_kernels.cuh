@@ -48,6 +48,51 @@ using LineIO = LineIOT<double>;
 void launch_line_op(int d, const OpPlan& plan, const LineIO& io, const double* table, cudaStream_t st);
 void launch_line_op(int d, const OpPlan& plan, const LineIOT<float>& io, const double* table, cudaStream_t st);
 
+// nondimensional property table on the device, sorted by T (FP64 columns)
+struct ThermoTab {
+  const double *t, *h, *d, *m, *k, *rhoh;
+  int n;
+  double dhmin, dhmax;
+};
+
+// ---- fused explicit operators: out(i,j,k) = sum over terms of g_m * op_m(in_m)(i,j,k) ----
+// Every term is an explicit (no line solve) D1C2P or D1P2C plan of any direction whose output
+// array has the shape of `out`; the sum is formed per output value, so the partial results never
+// go through HBM.  Epilogues fold the RK3 fractional step (and, for the energy equation, the
+// rho*h update and the table property update) into the same pass.
+constexpr int kMaxFusedTerms = 6;
+template <typename T>
+struct FusedTerm {
+  OpPlan P;
+  int dir;
+  TermT<T> t[2];      // input expression
+  const T* fbc;       // boundary planes [4][nlines] or null
+  int n1, n2, n3;     // input extents
+  int nlines;
+  double g;           // weight
+  int group;          // 0: the flux sum F, 1: the pressure-gradient sum (EP_FRAC)
+};
+enum FusedEpilogue { EP_STORE = 0, EP_ACCUM = 1, EP_FRAC = 2, EP_ENERGY = 3 };
+template <typename T>
+struct FusedIO {
+  FusedTerm<T> term[kMaxFusedTerms];
+  int nterm;
+  T* out;
+  int m1, m2, m3;     // output extents
+  int epilogue;
+  // EP_FRAC: out = dt*(gam*F + zeta*rhs0 + alpha*pfc), rhs0 = F.
+  // EP_ENERGY: r1 = dt*(gam*F + zeta*rhs0), rhs0 = F, rhoh += r1, then (props) h, T, kappa, rho,
+  // mu from the table; out is unused
+  T* rhs0;
+  double dt, gam, zeta, alpha;
+  T* rhoh;
+  int props;
+  T *h, *t, *k, *d, *m;
+  ThermoTab tab;
+};
+template <typename T>
+void launch_fused(const FusedIO<T>& f, const double* table, cudaStream_t st);
+
 // number of lines of a direction for an input array of extents n1 x n2 x n3
 inline int64_t num_lines(int d, int n1, int n2, int n3) {
   return d == 0 ? (int64_t)n2 * n3 : (d == 1 ? (int64_t)n1 * n3 : (int64_t)n1 * n2);
@@ -111,12 +156,6 @@ void launch_axpby(T* out, const T* a, double sa, const T* b, double sb, int64_t 
 void launch_convert(float* out, const double* in, int64_t n, cudaStream_t st);
 void launch_convert(double* out, const float* in, int64_t n, cudaStream_t st);
 // ---- variable-property (thermal) kernels ----
-// nondimensional property table on the device, sorted by T (FP64 columns)
-struct ThermoTab {
-  const double *t, *h, *d, *m, *k, *rhoh;
-  int n;
-  double dhmin, dhmax;
-};
 // per-cell update from rho*h: h, T, kappa, rho, mu (ftp_refresh_thermal_properties_from_DH)
 template <typename T>
 void launch_property_update(const ThermoTab& tb, const T* rhoh, T* h, T* t, T* k, T* d, T* m, int64_t n,

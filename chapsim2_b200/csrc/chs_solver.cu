@@ -307,6 +307,128 @@ void run_pair(chs_handle* H, int d, int fam, Pair bc1, const typename Id<T>::typ
   }
 }
 
+// One term of a fused sum: operator (direction, family, boundary pair, planes), input
+// expression, input extents, weight and group (0 flux, 1 pressure gradient)
+template <typename T>
+struct OpTerm {
+  int d, fam;
+  Pair bc;
+  const T* fbc;
+  SrcT<T> in;
+  int n_in[3];
+  double g;
+  int group;
+};
+
+template <typename T>
+OpTerm<T> term(int d, int fam, Pair bc, const T* fbc, const SrcT<T>& in, const int n_in[3], double g, int group) {
+  return OpTerm<T>{d, fam, bc, fbc, in, {n_in[0], n_in[1], n_in[2]}, g, group};
+}
+
+// the terms of op(a; f1) + w*op(b; f2), merged into one when they share a plan (as run_pair)
+template <typename T>
+void pair_terms(std::vector<OpTerm<T>>& v, int d, int fam, Pair bc1, const typename Id<T>::type* f1,
+                const SrcT<T>& a, Pair bc2, const typename Id<T>::type* f2, const SrcT<T>& b, double w,
+                const int n_in[3], const typename Id<T>::type* fcomb, int group) {
+  const bool same = bc1.v[0] == bc2.v[0] && bc1.v[1] == bc2.v[1] && ((f1 == nullptr) == (f2 == nullptr)) &&
+                    (f1 == f2 || fcomb != nullptr);
+  if (same) {
+    v.push_back(term<T>(d, fam, bc1, (f1 == f2) ? f1 : fcomb, plus(a, b, w), n_in, 1.0, group));
+  } else {
+    v.push_back(term<T>(d, fam, bc1, f1, a, n_in, 1.0, group));
+    v.push_back(term<T>(d, fam, bc2, f2, b, n_in, w, group));
+  }
+}
+
+// Sum of explicit operators with an epilogue, as one fused launch when every plan is explicit
+// (no line solve) and the terms fit, else as the equivalent sequence of line operators followed by
+// the elementwise epilogue.  out has extents m; for EP_FRAC the fallback puts the pressure
+// gradient in pfc_scratch.
+template <typename T>
+void run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const int m[3], int epilogue, T* rhs0,
+               int isub, T* pfc_scratch, T* rhoh = nullptr, bool props = false) {
+  cudaStream_t st = H->st;
+  const size_t tsz = H->book.table.size();
+  bool fuse = !terms.empty() && (int)terms.size() <= kMaxFusedTerms;
+  for (const auto& t : terms) {
+    const OpPlan& P = H->plan(t.d, t.fam, t.bc, t.fbc != nullptr);
+    if (P.tdma || (t.fam != D1C2P && t.fam != D1P2C)) fuse = false;
+  }
+  if (H->book.table.size() != tsz) upload_table(H);
+  const double nout = (double)m[0] * m[1] * m[2];
+  if (fuse) {
+    FusedIO<T> F{};
+    F.nterm = (int)terms.size();
+    double bytes = 0.0;
+    for (int i = 0; i < F.nterm; ++i) {
+      const OpTerm<T>& t = terms[i];
+      FusedTerm<T>& ft = F.term[i];
+      ft.P = H->plan(t.d, t.fam, t.bc, t.fbc != nullptr);
+      ft.dir = t.d;
+      ft.t[0] = t.in.t[0];
+      ft.t[1] = t.in.t[1];
+      ft.fbc = t.fbc;
+      ft.n1 = t.n_in[0]; ft.n2 = t.n_in[1]; ft.n3 = t.n_in[2];
+      ft.nlines = (int)num_lines(t.d, t.n_in[0], t.n_in[1], t.n_in[2]);
+      ft.g = t.g;
+      ft.group = t.group;
+      bytes += (double)sizeof(T) * t.in.narrays() * t.n_in[0] * t.n_in[1] * t.n_in[2];
+    }
+    F.out = out;
+    F.m1 = m[0]; F.m2 = m[1]; F.m3 = m[2];
+    F.epilogue = epilogue;
+    F.rhs0 = rhs0;
+    F.dt = H->dt; F.gam = H->tGamma[isub]; F.zeta = H->tZeta[isub]; F.alpha = H->tAlpha[isub];
+    F.rhoh = rhoh;
+    F.props = props ? 1 : 0;
+    if (props) {
+      const int n = (int)H->n_ccc;
+      (void)n;
+      F.h = reinterpret_cast<T*>(H->hEnth); F.t = reinterpret_cast<T*>(H->tTemp);
+      F.k = reinterpret_cast<T*>(H->kCond); F.d = reinterpret_cast<T*>(H->dDens);
+      F.m = reinterpret_cast<T*>(H->mVisc);
+      F.tab = H->tab;
+    }
+    const double ob = epilogue == EP_STORE ? 1.0 : epilogue == EP_ACCUM ? 2.0 : epilogue == EP_FRAC ? 3.0
+                                                                          : (props ? 9.0 : 4.0);
+    bytes += (double)sizeof(T) * ob * nout;
+    cudaEvent_t e0 = H->prof_begin();
+    launch_fused(F, H->table, st);
+    H->prof_end(e0, 0, -1, bytes);
+    H->launches++;
+    return;
+  }
+  // fallback: one line operator per term, then the elementwise epilogue
+  T* tgt0 = out;
+  bool first0 = epilogue != EP_ACCUM, first1 = true;
+  for (const auto& t : terms) {
+    if (t.group == 0) {
+      run_op<T>(H, t.d, t.fam, t.bc, t.fbc, t.in, t.n_in, tgt0, !first0, t.g);
+      first0 = false;
+    } else {
+      run_op<T>(H, t.d, t.fam, t.bc, t.fbc, t.in, t.n_in, pfc_scratch, !first1, t.g);
+      first1 = false;
+    }
+  }
+  if (epilogue == EP_FRAC) {
+    PROF(H, 3, 5.0 * sizeof(T) * nout,
+         launch_fractional_step(out, rhs0, pfc_scratch, (int64_t)nout, H->dt, H->tGamma[isub], H->tZeta[isub],
+                                H->tAlpha[isub], st));
+    H->launches++;
+  } else if (epilogue == EP_ENERGY) {
+    PROF(H, 3, 5.0 * sizeof(T) * nout,
+         launch_energy_advance<T>(out, rhs0, rhoh, (int64_t)nout, H->dt, H->tGamma[isub], H->tZeta[isub], st));
+    H->launches++;
+    if (props) {
+      PROF(H, 3, 6.0 * sizeof(T) * nout,
+           launch_property_update<T>(H->tab, rhoh, reinterpret_cast<T*>(H->hEnth), reinterpret_cast<T*>(H->tTemp),
+                                     reinterpret_cast<T*>(H->kCond), reinterpret_cast<T*>(H->dDens),
+                                     reinterpret_cast<T*>(H->mVisc), (int64_t)nout, st));
+      H->launches++;
+    }
+  }
+}
+
 void build_bcs(chs_handle* H, const chs_config* c) {
   std::memcpy(H->ibc, c->nominal_bc, sizeof(H->ibc));
   std::memcpy(H->fbcy, c->fbcy_const, sizeof(H->fbcy));
@@ -743,51 +865,56 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
     H->launches += 3;
   }
 
-  // ---- 2. momentum RHS.  The convection and diffusion terms of one direction share the
-  // operator (same family and boundary pair), and the operator is linear in its input and
-  // boundary values, so op(conv) + rre*op(diff) runs as op(conv + rre*diff) in one launch.
+  // ---- 2-3. momentum RHS and fractional step, one fused pass per component.  The convection and
+  // diffusion terms of one direction share the operator (same family and boundary pair), and the
+  // operator is linear in its input and boundary values, so op(conv) + rre*op(diff) is
+  // op(conv + rre*diff); the three directions, the pressure gradient and the fractional step
+  // (:35-71) are summed per output value.
+  const int m_pcc[3] = {np0, nc1, nc2}, m_cpc[3] = {nc0, np1, nc2}, m_ccp[3] = {nc0, nc1, np2};
   // x-momentum (:796-966)
-  run_pair(H, 0, D1C2P, H->mbcx_cov1, any, prod(c_xix, A(H->qxix), -1.0), H->mbcx_tau1, any,
-           linm(A(H->qxdx), A(H->div), -third, 2.0, mu_c), rre, s_ccc, A(H->mx), false, nullptr);
-  run_pair(H, 1, D1P2C, H->mbcy_cov1, nullptr, prod(c_yix, A(H->qxiy), -1.0), H->mbcy_tau1, nullptr,
-           linm(A(H->qxdy), A(H->qydx), 1.0, 1.0, mu_xy), rre, s_ppc, A(H->mx), true, nullptr);
-  run_pair(H, 2, D1P2C, H->mbcz_cov1, nullptr, prod(c_zix, A(H->qxiz), -1.0), H->mbcz_tau1, nullptr,
-           linm(A(H->qxdz), A(H->qzdx), 1.0, 1.0, mu_xz), rre, s_pcp, A(H->mx), true, nullptr);
-  run_op(H, 0, D1C2P, bx_pr, any, src(A(H->pres), -1.0), s_ccc, A(H->px), false, 1.0);
+  {
+    std::vector<OpTerm<T>> t;
+    pair_terms(t, 0, D1C2P, H->mbcx_cov1, any, prod(c_xix, A(H->qxix), -1.0), H->mbcx_tau1, any,
+               linm(A(H->qxdx), A(H->div), -third, 2.0, mu_c), rre, s_ccc, nullptr, 0);
+    pair_terms(t, 1, D1P2C, H->mbcy_cov1, nullptr, prod(c_yix, A(H->qxiy), -1.0), H->mbcy_tau1, nullptr,
+               linm(A(H->qxdy), A(H->qydx), 1.0, 1.0, mu_xy), rre, s_ppc, nullptr, 0);
+    pair_terms(t, 2, D1P2C, H->mbcz_cov1, nullptr, prod(c_zix, A(H->qxiz), -1.0), H->mbcz_tau1, nullptr,
+               linm(A(H->qxdz), A(H->qzdx), 1.0, 1.0, mu_xz), rre, s_pcp, nullptr, 0);
+    t.push_back(term<T>(0, D1C2P, bx_pr, any, src(A(H->pres), -1.0), s_ccc, 1.0, 1));
+    run_fused<T>(H, t, A(H->mx), m_pcc, EP_FRAC, A(H->mx0), isub, A(H->px));
+  }
   // y-momentum (:978-1242)
-  run_pair(H, 0, D1P2C, H->mbcx_cov2, nullptr, prod(c_xiy, A(H->qyix), -1.0), H->mbcx_tau2, nullptr,
-           linm(A(H->qxdy), A(H->qydx), 1.0, 1.0, mu_xy), rre, s_ppc, A(H->my), false, nullptr);
   if (H->fbcy_velo) {
     PROF(H, 3, 24.0 / 8.0 * sizeof(T) * 4 * nc0 * nc2,
          launch_axpby(A(H->fb_comb), A(H->fb_conv2), 1.0, A(H->fb_visc2), rre, (int64_t)4 * nc0 * nc2, st));
     H->launches++;
   }
-  run_pair(H, 1, D1C2P, H->mbcy_cov2, H->fbcy_velo ? A(H->fb_conv2) : A(H->fb_maxp), prod(A(H->qyiy), c_yiy, -1.0),
-           H->mbcy_tau2, H->fbcy_velo ? A(H->fb_visc2) : A(H->fb_maxp), linm(A(H->qydy), A(H->div), -third, 2.0, mu_c), rre, s_ccc,
-           A(H->my), true, A(H->fb_comb));
-  run_pair(H, 2, D1P2C, H->mbcz_cov2, nullptr, prod(A(H->qyiz), c_ziy, -1.0), H->mbcz_tau2, nullptr,
-           linm(A(H->qzdy), A(H->qydz), 1.0, 1.0, mu_yz), rre, s_cpp, A(H->my), true, nullptr);
-  run_op(H, 1, D1C2P, by_pr, fympr, src(A(H->pres), -1.0), s_ccc, A(H->py), false, 1.0);
+  {
+    std::vector<OpTerm<T>> t;
+    pair_terms(t, 0, D1P2C, H->mbcx_cov2, nullptr, prod(c_xiy, A(H->qyix), -1.0), H->mbcx_tau2, nullptr,
+               linm(A(H->qxdy), A(H->qydx), 1.0, 1.0, mu_xy), rre, s_ppc, nullptr, 0);
+    pair_terms(t, 1, D1C2P, H->mbcy_cov2, H->fbcy_velo ? A(H->fb_conv2) : A(H->fb_maxp),
+               prod(A(H->qyiy), c_yiy, -1.0), H->mbcy_tau2, H->fbcy_velo ? A(H->fb_visc2) : A(H->fb_maxp),
+               linm(A(H->qydy), A(H->div), -third, 2.0, mu_c), rre, s_ccc, A(H->fb_comb), 0);
+    pair_terms(t, 2, D1P2C, H->mbcz_cov2, nullptr, prod(A(H->qyiz), c_ziy, -1.0), H->mbcz_tau2, nullptr,
+               linm(A(H->qzdy), A(H->qydz), 1.0, 1.0, mu_yz), rre, s_cpp, nullptr, 0);
+    t.push_back(term<T>(1, D1C2P, by_pr, fympr, src(A(H->pres), -1.0), s_ccc, 1.0, 1));
+    run_fused<T>(H, t, A(H->my), m_cpc, EP_FRAC, A(H->my0), isub, A(H->py));
+  }
   // z-momentum (:1262-1457)
-  run_pair(H, 0, D1P2C, H->mbcx_cov3, nullptr, prod(c_xiz, A(H->qzix), -1.0), H->mbcx_tau3, nullptr,
-           linm(A(H->qxdz), A(H->qzdx), 1.0, 1.0, mu_xz), rre, s_pcp, A(H->mz), false, nullptr);
-  run_pair(H, 1, D1P2C, H->mbcy_cov3, nullptr, prod(c_yiz, A(H->qziy), -1.0), H->mbcy_tau3, nullptr,
-           linm(A(H->qzdy), A(H->qydz), 1.0, 1.0, mu_yz), rre, s_cpp, A(H->mz), true, nullptr);
-  run_pair(H, 2, D1C2P, H->mbcz_cov3, any, prod(c_ziz, A(H->qziz), -1.0), H->mbcz_tau3, any,
-           linm(A(H->qzdz), A(H->div), -third, 2.0, mu_c), rre, s_ccc, A(H->mz), true, nullptr);
-  run_op(H, 2, D1C2P, bz_pr, any, src(A(H->pres), -1.0), s_ccc, A(H->pz), false, 1.0);
+  {
+    std::vector<OpTerm<T>> t;
+    pair_terms(t, 0, D1P2C, H->mbcx_cov3, nullptr, prod(c_xiz, A(H->qzix), -1.0), H->mbcx_tau3, nullptr,
+               linm(A(H->qxdz), A(H->qzdx), 1.0, 1.0, mu_xz), rre, s_pcp, nullptr, 0);
+    pair_terms(t, 1, D1P2C, H->mbcy_cov3, nullptr, prod(c_yiz, A(H->qziy), -1.0), H->mbcy_tau3, nullptr,
+               linm(A(H->qzdy), A(H->qydz), 1.0, 1.0, mu_yz), rre, s_cpp, nullptr, 0);
+    pair_terms(t, 2, D1C2P, H->mbcz_cov3, any, prod(c_ziz, A(H->qziz), -1.0), H->mbcz_tau3, any,
+               linm(A(H->qzdz), A(H->div), -third, 2.0, mu_c), rre, s_ccc, nullptr, 0);
+    t.push_back(term<T>(2, D1C2P, bz_pr, any, src(A(H->pres), -1.0), s_ccc, 1.0, 1));
+    run_fused<T>(H, t, A(H->mz), m_ccp, EP_FRAC, A(H->mz0), isub, A(H->pz));
+  }
 
-  // ---- 3. fractional step, mass flux
-  PROF(H, 3, 40.0 / 8.0 * sizeof(T) * H->n_pcc,
-       launch_fractional_step(A(H->mx), A(H->mx0), A(H->px), (int64_t)H->n_pcc, H->dt, H->tGamma[isub], H->tZeta[isub],
-                              H->tAlpha[isub], st));
-  PROF(H, 3, 40.0 / 8.0 * sizeof(T) * H->n_cpc,
-       launch_fractional_step(A(H->my), A(H->my0), A(H->py), (int64_t)H->n_cpc, H->dt, H->tGamma[isub], H->tZeta[isub],
-                              H->tAlpha[isub], st));
-  PROF(H, 3, 40.0 / 8.0 * sizeof(T) * H->n_ccp,
-       launch_fractional_step(A(H->mz), A(H->mz0), A(H->pz), (int64_t)H->n_ccp, H->dt, H->tGamma[isub], H->tZeta[isub],
-                              H->tAlpha[isub], st));
-  H->launches += 3;
+  // ---- 3b. mass flux
   const double* bulk = nullptr;
   if (H->idriven == 1) {
     PROF(H, 3, 8.0 / 8.0 * sizeof(T) * H->n_pcc,
@@ -810,9 +937,12 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
   // adds (rho - rho_m1)/dt (Calculate_drhodt, src/eq_continuity.f90:26-78), but
   // Update_thermal_properties has already set rho_m1 = rho, so the term is zero and left out.
   const double coeff = 1.0 / (H->tAlpha[isub] * H->sigma2p * H->dt);
-  run_op(H, 0, D1P2C, bx_qx, any, src(A(ux)), s_pcc, A(H->pcor), false, coeff);
-  run_op(H, 1, D1P2C, by_qy, nullptr, src(A(uy)), s_cpc, A(H->pcor), true, coeff);
-  run_op(H, 2, D1P2C, bz_qz, nullptr, src(A(uz)), s_ccp, A(H->pcor), true, coeff);
+  {
+    std::vector<OpTerm<T>> t = {term<T>(0, D1P2C, bx_qx, any, src(A(ux)), s_pcc, coeff, 0),
+                                term<T>(1, D1P2C, by_qy, nullptr, src(A(uy)), s_cpc, coeff, 0),
+                                term<T>(2, D1P2C, bz_qz, nullptr, src(A(uz)), s_ccp, coeff, 0)};
+    run_fused<T>(H, t, A(H->pcor), s_ccc, EP_STORE, nullptr, isub, nullptr);
+  }
   poisson_device<T>(H, A(H->pcor));
   PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, launch_axpby(A(H->pres), A(H->pres), 1.0, A(H->pcor), 1.0, (int64_t)H->n_ccc, st));
   H->launches++;
@@ -866,27 +996,26 @@ void energy_body_t(chs_handle* H, int isub) {
   PROF(H, 3, 3.0 * sizeof(T) * nc0 * nc2,
        launch_fbcy_extract<T>(A(H->fb_dtk), A(H->dTy), nullptr, A(H->k_cpc), 0.0, 1.0, 1.0, nc0, np1, nc2, st));
   H->launches++;
-  // conv + diffusion per direction (one launch where the two operators share a plan)
-  run_pair(H, 0, D1P2C, H->ebcx_conv, any, prod(A(H->gx), A(H->h_pcc), -1.0), H->ebcx_difu, any,
-           prod(A(H->dTx), A(H->k_pcc), 1.0), rpr, s_pcc, A(H->erhs), false, nullptr);
-  run_op(H, 1, D1P2C, H->ebcy_conv, nullptr, prod(A(H->gy), A(H->h_cpc), -1.0), s_cpc, A(H->erhs), true, 1.0);
-  run_op(H, 1, D1P2C, H->ebcy_difu, A(H->fb_dtk), prod(A(H->dTy), A(H->k_cpc), 1.0), s_cpc, A(H->erhs), true, rpr);
-  run_pair(H, 2, D1P2C, H->ebcz_conv, nullptr, prod(A(H->gz), A(H->h_ccp), -1.0), H->ebcz_difu, nullptr,
-           prod(A(H->dTz), A(H->k_ccp), 1.0), rpr, s_ccp, A(H->erhs), true, nullptr);
-  PROF(H, 3, 5.0 * sizeof(T) * H->n_ccc,
-       launch_energy_advance<T>(A(H->erhs), A(H->erhs0), A(H->rhoh), (int64_t)H->n_ccc, H->dt, H->tGamma[isub],
-                                H->tZeta[isub], st));
-  if (H->mlp_mode == 1) {
+  // conv + diffusion per direction, the fractional step, the rho*h update and (table mode) the
+  // property update in one fused pass
+  const bool table_props = H->mlp_mode != 1;
+  {
+    std::vector<OpTerm<T>> t;
+    pair_terms(t, 0, D1P2C, H->ebcx_conv, any, prod(A(H->gx), A(H->h_pcc), -1.0), H->ebcx_difu, any,
+               prod(A(H->dTx), A(H->k_pcc), 1.0), rpr, s_pcc, nullptr, 0);
+    t.push_back(term<T>(1, D1P2C, H->ebcy_conv, nullptr, prod(A(H->gy), A(H->h_cpc), -1.0), s_cpc, 1.0, 0));
+    t.push_back(term<T>(1, D1P2C, H->ebcy_difu, A(H->fb_dtk), prod(A(H->dTy), A(H->k_cpc), 1.0), s_cpc, rpr, 0));
+    pair_terms(t, 2, D1P2C, H->ebcz_conv, nullptr, prod(A(H->gz), A(H->h_ccp), -1.0), H->ebcz_difu, nullptr,
+               prod(A(H->dTz), A(H->k_ccp), 1.0), rpr, s_ccp, nullptr, 0);
+    run_fused<T>(H, t, A(H->erhs), s_ccc, EP_ENERGY, A(H->erhs0), isub, nullptr, A(H->rhoh), table_props);
+  }
+  if (!table_props) {
     PROF(H, 3, 6.0 * sizeof(T) * H->n_ccc,
          launch_mlp_props<T>(H->tab, H->mlp_norm, H->mlp_small, H->mlp_check, H->mlp_wpack, A(H->rhoh),
                              A(H->hEnth), A(H->tTemp), A(H->kCond), A(H->dDens), A(H->mVisc), (int64_t)H->n_ccc,
                              H->mlp_nfb, st));
-  } else {
-    PROF(H, 3, 6.0 * sizeof(T) * H->n_ccc,
-         launch_property_update<T>(H->tab, A(H->rhoh), A(H->hEnth), A(H->tTemp), A(H->kCond), A(H->dDens),
-                                   A(H->mVisc), (int64_t)H->n_ccc, st));
+    H->launches++;
   }
-  H->launches += 2;
   const int s0 = B[1][V_TM][0] == BC_NEUMANN, s1 = B[1][V_TM][1] == BC_NEUMANN;
   if (s0 || s1) {
     run_op(H, 1, M1C2P, H->ftpy, nullptr, src(A(H->rhoh)), s_ccc, A(H->dh_cpc), false, 1.0);
