@@ -515,6 +515,79 @@ __global__ void __launch_bounds__(256) fused_kernel(const __grid_constant__ Fuse
   }
 }
 
+// epilogue shared by the generic and the specialised fused kernels
+template <typename T>
+__device__ __forceinline__ void fused_epilogue(const FusedIO<T>& F, int64_t o, T sum0, T sum1) {
+  if (F.epilogue == EP_STORE) {
+    F.out[o] = sum0;
+  } else if (F.epilogue == EP_ACCUM) {
+    F.out[o] = F.out[o] + sum0;
+  } else if (F.epilogue == EP_FRAC) {
+    const T last = F.rhs0[o];
+    T tot = T(F.gam) * sum0 + T(F.zeta) * last;
+    F.rhs0[o] = sum0;
+    tot = tot + T(F.alpha) * sum1;
+    F.out[o] = T(F.dt) * tot;
+  } else {
+    const T last = F.rhs0[o];
+    const T tot = T(F.gam) * sum0 + T(F.zeta) * last;
+    F.rhs0[o] = sum0;
+    const T r1 = T(F.dt) * tot;
+    const T rh = F.rhoh[o] + r1;
+    F.rhoh[o] = rh;
+    if (F.props) {
+      const CellProps pr = props_from_dh(F.tab, (double)rh);
+      F.h[o] = T(pr.h);
+      F.t[o] = T(pr.t);
+      F.k[o] = T(pr.k);
+      F.d[o] = T(pr.d);
+      F.m[o] = T(pr.m);
+    }
+  }
+}
+
+// Specialisation for a term list known at compile time (the signatures the substep uses): every
+// term is evaluated inline, so the loads of all terms can be in flight together.
+template <int D, int FM>
+struct TermSig {
+  static constexpr int dir = D, fam = FM;
+};
+
+template <typename T, typename... S>
+__global__ void __launch_bounds__(256) fused_kernel_sig(const __grid_constant__ FusedIO<T> F,
+                                                        const double* __restrict__ table) {
+  const int plane = F.m1 * F.m2;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= plane) return;
+  const int k = blockIdx.y;
+  const int j = q / F.m1;
+  const int i = q - j * F.m1;
+  constexpr int N = sizeof...(S);
+  T v[N];
+  int idx = 0;
+  ((v[idx] = fused_term_at<T, S::dir, S::fam>(F.term[idx], table, i, j, k), ++idx), ...);
+  T sum0 = T(0), sum1 = T(0);
+#pragma unroll
+  for (int t = 0; t < N; ++t) {
+    const T gv = T(F.term[t].g) * v[t];
+    if (F.term[t].group == 0) sum0 = sum0 + gv;
+    else sum1 = sum1 + gv;
+  }
+  fused_epilogue(F, (int64_t)plane * k + q, sum0, sum1);
+}
+
+template <typename T, typename... S>
+static bool try_sig(const FusedIO<T>& f, const double* table, cudaStream_t st, dim3 grid) {
+  constexpr int N = sizeof...(S);
+  if (f.nterm != N) return false;
+  const int dirs[N] = {S::dir...};
+  const int fams[N] = {S::fam...};
+  for (int t = 0; t < N; ++t)
+    if (f.term[t].dir != dirs[t] || f.term[t].P.fam != fams[t]) return false;
+  fused_kernel_sig<T, S...><<<grid, 256, 0, st>>>(f, table);
+  return true;
+}
+
 template <typename T>
 void launch_fused(const FusedIO<T>& f, const double* table, cudaStream_t st) {
   if (f.nterm < 1 || f.nterm > kMaxFusedTerms) throw std::runtime_error("fused operator: bad term count");
@@ -528,6 +601,18 @@ void launch_fused(const FusedIO<T>& f, const double* table, cudaStream_t st) {
   }
   const int plane = f.m1 * f.m2;
   dim3 grid((unsigned)((plane + 255) / 256), (unsigned)f.m3);
+  using C0 = TermSig<0, D1C2P>;
+  using C1 = TermSig<1, D1C2P>;
+  using C2 = TermSig<2, D1C2P>;
+  using P0 = TermSig<0, D1P2C>;
+  using P1 = TermSig<1, D1P2C>;
+  using P2 = TermSig<2, D1P2C>;
+  // the momentum components, the Poisson right-hand side and the energy equation
+  if (try_sig<T, C0, P1, P2, C0>(f, table, st, grid)) return;
+  if (try_sig<T, P0, C1, P2, C1>(f, table, st, grid)) return;
+  if (try_sig<T, P0, P1, C2, C2>(f, table, st, grid)) return;
+  if (try_sig<T, P0, P1, P2>(f, table, st, grid)) return;
+  if (try_sig<T, P0, P1, P1, P2>(f, table, st, grid)) return;
   fused_kernel<T><<<grid, 256, 0, st>>>(f, table);
 }
 template void launch_fused<double>(const FusedIO<double>&, const double*, cudaStream_t);
