@@ -515,6 +515,62 @@ __global__ void __launch_bounds__(256) fused_kernel(const __grid_constant__ Fuse
   }
 }
 
+// input-expression term with its mode known at compile time
+template <int M, typename T>
+__device__ __forceinline__ T eval_term_ct(const TermT<T>& t, int a) {
+  if (M == T_X) return T(t.s) * t.X[a];
+  if (M == T_XY) return T(t.s) * (t.X[a] * t.Y[a]);
+  if (M == T_XpY) return T(t.s) * (t.X[a] + T(t.c) * t.Y[a]);
+  if (M == T_XpYZ) return T(t.s) * (t.X[a] + T(t.c) * t.Y[a]) * t.Z[a];
+  return T(0);
+}
+
+// bulk row of one term (the caller has checked that p is a bulk row): straight-line code with
+// unconditional loads, the second stencil pair only when R2
+template <typename T, int DIR, int FAM, bool R2, int M0, int M1>
+__device__ __forceinline__ T bulk_term(const FusedTerm<T>& ft, const double* __restrict__ table, int i, int j,
+                                       int k) {
+  const OpPlan& P = ft.P;
+  const int nin = P.nin;
+  int p, ibase, istride;
+  if (DIR == 0) {
+    p = i;
+    ibase = (j + ft.n2 * k) * nin;
+    istride = 1;
+  } else if (DIR == 1) {
+    p = j;
+    ibase = k * nin * ft.n1 + i;
+    istride = ft.n1;
+  } else {
+    p = k;
+    ibase = i + ft.n1 * j;
+    istride = ft.n1 * ft.n2;
+  }
+  auto f = [&](int qq) -> T {
+    const int a = ibase + qq * istride;
+    T v = eval_term_ct<M0>(ft.t[0], a);
+    if (M1 != T_NONE) v += eval_term_ct<M1>(ft.t[1], a);
+    return v;
+  };
+  const T r1 = T(P.r1), r2 = T(P.r2);
+  T v;
+  if (FAM == D1C2P) {
+    v = r1 * (f(p) - f(p - 1));
+    if (R2) v += r2 * (f(p + 1) - f(p - 2));
+  } else {  // D1P2C
+    v = r1 * (f(p + 1) - f(p));
+    if (R2) v += r2 * (f(p + 2) - f(p - 1));
+  }
+  v = v * T(P.dd);
+  if (P.lmap >= 0) v *= T(table[P.lmap + p]);
+  return v;
+}
+
+template <int DIR>
+__device__ __forceinline__ int term_pos(int i, int j, int k) {
+  return DIR == 0 ? i : (DIR == 1 ? j : k);
+}
+
 // epilogue shared by the generic and the specialised fused kernels
 template <typename T>
 __device__ __forceinline__ void fused_epilogue(const FusedIO<T>& F, int64_t o, T sum0, T sum1) {
@@ -548,12 +604,12 @@ __device__ __forceinline__ void fused_epilogue(const FusedIO<T>& F, int64_t o, T
 
 // Specialisation for a term list known at compile time (the signatures the substep uses): every
 // term is evaluated inline, so the loads of all terms can be in flight together.
-template <int D, int FM>
+template <int D, int FM, int M0, int M1 = T_NONE>
 struct TermSig {
-  static constexpr int dir = D, fam = FM;
+  static constexpr int dir = D, fam = FM, m0 = M0, m1 = M1;
 };
 
-template <typename T, typename... S>
+template <typename T, bool R2, typename... S>
 __global__ void __launch_bounds__(256) fused_kernel_sig(const __grid_constant__ FusedIO<T> F,
                                                         const double* __restrict__ table) {
   const int plane = F.m1 * F.m2;
@@ -564,8 +620,23 @@ __global__ void __launch_bounds__(256) fused_kernel_sig(const __grid_constant__ 
   const int i = q - j * F.m1;
   constexpr int N = sizeof...(S);
   T v[N];
-  int idx = 0;
-  ((v[idx] = fused_term_at<T, S::dir, S::fam>(F.term[idx], table, i, j, k), ++idx), ...);
+  // bulk rows of every term (nearly all outputs): branch-free evaluation so the loads of all
+  // terms can be issued together; boundary rows take the general path
+  bool bulk = true;
+  {
+    int idx = 0;
+    ((bulk = bulk && term_pos<S::dir>(i, j, k) >= F.term[idx].P.b_lo &&
+             term_pos<S::dir>(i, j, k) <= F.term[idx].P.b_hi && !F.term[idx].P.neu1 && !F.term[idx].P.neu2,
+      ++idx),
+     ...);
+  }
+  if (bulk) {
+    int idx = 0;
+    ((v[idx] = bulk_term<T, S::dir, S::fam, R2, S::m0, S::m1>(F.term[idx], table, i, j, k), ++idx), ...);
+  } else {
+    int idx = 0;
+    ((v[idx] = fused_term_at<T, S::dir, S::fam>(F.term[idx], table, i, j, k), ++idx), ...);
+  }
   T sum0 = T(0), sum1 = T(0);
 #pragma unroll
   for (int t = 0; t < N; ++t) {
@@ -582,9 +653,16 @@ static bool try_sig(const FusedIO<T>& f, const double* table, cudaStream_t st, d
   if (f.nterm != N) return false;
   const int dirs[N] = {S::dir...};
   const int fams[N] = {S::fam...};
-  for (int t = 0; t < N; ++t)
+  const int m0s[N] = {S::m0...};
+  const int m1s[N] = {S::m1...};
+  bool r2 = false;
+  for (int t = 0; t < N; ++t) {
     if (f.term[t].dir != dirs[t] || f.term[t].P.fam != fams[t]) return false;
-  fused_kernel_sig<T, S...><<<grid, 256, 0, st>>>(f, table);
+    if (f.term[t].t[0].mode != m0s[t] || f.term[t].t[1].mode != m1s[t]) return false;
+    if (f.term[t].P.r2 != 0.0) r2 = true;
+  }
+  if (r2) fused_kernel_sig<T, true, S...><<<grid, 256, 0, st>>>(f, table);
+  else fused_kernel_sig<T, false, S...><<<grid, 256, 0, st>>>(f, table);
   return true;
 }
 
@@ -601,18 +679,37 @@ void launch_fused(const FusedIO<T>& f, const double* table, cudaStream_t st) {
   }
   const int plane = f.m1 * f.m2;
   dim3 grid((unsigned)((plane + 255) / 256), (unsigned)f.m3);
-  using C0 = TermSig<0, D1C2P>;
-  using C1 = TermSig<1, D1C2P>;
-  using C2 = TermSig<2, D1C2P>;
-  using P0 = TermSig<0, D1P2C>;
-  using P1 = TermSig<1, D1P2C>;
-  using P2 = TermSig<2, D1P2C>;
-  // the momentum components, the Poisson right-hand side and the energy equation
-  if (try_sig<T, C0, P1, P2, C0>(f, table, st, grid)) return;
-  if (try_sig<T, P0, C1, P2, C1>(f, table, st, grid)) return;
-  if (try_sig<T, P0, P1, C2, C2>(f, table, st, grid)) return;
-  if (try_sig<T, P0, P1, P2>(f, table, st, grid)) return;
-  if (try_sig<T, P0, P1, P1, P2>(f, table, st, grid)) return;
+  // momentum terms: conv (X*Y) + diffusion (X + cY, times mu for variable properties); pressure
+  // gradient (X); divergence (X); energy conv and diffusion (X*Y)
+  using XC0 = TermSig<0, D1C2P, T_XY, T_XpY>;
+  using XC1 = TermSig<1, D1C2P, T_XY, T_XpY>;
+  using XC2 = TermSig<2, D1C2P, T_XY, T_XpY>;
+  using XP0 = TermSig<0, D1P2C, T_XY, T_XpY>;
+  using XP1 = TermSig<1, D1P2C, T_XY, T_XpY>;
+  using XP2 = TermSig<2, D1P2C, T_XY, T_XpY>;
+  using ZC0 = TermSig<0, D1C2P, T_XY, T_XpYZ>;
+  using ZC1 = TermSig<1, D1C2P, T_XY, T_XpYZ>;
+  using ZC2 = TermSig<2, D1C2P, T_XY, T_XpYZ>;
+  using ZP0 = TermSig<0, D1P2C, T_XY, T_XpYZ>;
+  using ZP1 = TermSig<1, D1P2C, T_XY, T_XpYZ>;
+  using ZP2 = TermSig<2, D1P2C, T_XY, T_XpYZ>;
+  using GC0 = TermSig<0, D1C2P, T_X>;
+  using GC1 = TermSig<1, D1C2P, T_X>;
+  using GC2 = TermSig<2, D1C2P, T_X>;
+  using DP0 = TermSig<0, D1P2C, T_X>;
+  using DP1 = TermSig<1, D1P2C, T_X>;
+  using DP2 = TermSig<2, D1P2C, T_X>;
+  using EP0 = TermSig<0, D1P2C, T_XY, T_XY>;
+  using EP1 = TermSig<1, D1P2C, T_XY>;
+  using EP2 = TermSig<2, D1P2C, T_XY, T_XY>;
+  if (try_sig<T, XC0, XP1, XP2, GC0>(f, table, st, grid)) return;
+  if (try_sig<T, XP0, XC1, XP2, GC1>(f, table, st, grid)) return;
+  if (try_sig<T, XP0, XP1, XC2, GC2>(f, table, st, grid)) return;
+  if (try_sig<T, ZC0, ZP1, ZP2, GC0>(f, table, st, grid)) return;
+  if (try_sig<T, ZP0, ZC1, ZP2, GC1>(f, table, st, grid)) return;
+  if (try_sig<T, ZP0, ZP1, ZC2, GC2>(f, table, st, grid)) return;
+  if (try_sig<T, DP0, DP1, DP2>(f, table, st, grid)) return;
+  if (try_sig<T, EP0, EP1, EP1, EP2>(f, table, st, grid)) return;
   fused_kernel<T><<<grid, 256, 0, st>>>(f, table);
 }
 template void launch_fused<double>(const FusedIO<double>&, const double*, cudaStream_t);
