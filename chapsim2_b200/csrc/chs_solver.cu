@@ -119,6 +119,7 @@ struct chs_handle {
   double* table = nullptr;
   std::vector<std::pair<void*, size_t>> allocs;
   int tune_block = 0, tune_lt = 0;  // launch shapes picked by chs_autotune (0 = defaults)
+  int tune_fuse = 0;                // 1: fused operator sums (chs_autotune decides; off by default)
   long long launches = 0;
   std::string err;
 
@@ -349,7 +350,7 @@ void run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const
                int isub, T* pfc_scratch, T* rhoh = nullptr, bool props = false) {
   cudaStream_t st = H->st;
   const size_t tsz = H->book.table.size();
-  bool fuse = !terms.empty() && (int)terms.size() <= kMaxFusedTerms;
+  bool fuse = H->tune_fuse && !terms.empty() && (int)terms.size() <= kMaxFusedTerms;
   for (const auto& t : terms) {
     const OpPlan& P = H->plan(t.d, t.fam, t.bc, t.fbc != nullptr);
     if (P.tdma || (t.fam != D1C2P && t.fam != D1P2C)) fuse = false;
@@ -1548,8 +1549,8 @@ float time_steps_ms(chs_handle* H, int nsteps) {
 
 extern "C" {
 
-int chs_autotune(chs_handle* H, int nsteps, int* block, int* lt_max, float* best_ms) {
-  if (!H || !block || !lt_max || !best_ms || nsteps < 1) return CHS_ERR_ARG;
+int chs_autotune(chs_handle* H, int nsteps, int* block, int* lt_max, int* fused, float* best_ms) {
+  if (!H || !block || !lt_max || !fused || !best_ms || nsteps < 1) return CHS_ERR_ARG;
   return guard(H, [&] {
     size_t total = 0;
     for (auto& a : H->allocs) total += a.second;
@@ -1559,20 +1560,22 @@ int chs_autotune(chs_handle* H, int nsteps, int* block, int* lt_max, float* best
     const int blocks[3] = {128, 256, 512};
     const bool compact = H->iacc >= 3;
     const int lts[3] = {16, 32, 64};
-    int bb = 256, bl = 64;
+    int bb = 256, bl = 64, bf = 0;
     float best = 1e30f;
     try {
-      for (int b : blocks)
-        for (int l : lts) {
-          if (!compact && l != 64) continue;
-          H->tune_block = b;
-          H->tune_lt = l;
-          drop_graphs(H);
-          time_steps_ms(H, 1);  // capture and warm up
-          const float ms = time_steps_ms(H, nsteps);
-          snapshot(H, snap, false);
-          if (ms < best) { best = ms; bb = b; bl = l; }
-        }
+      for (int fu = 0; fu <= 1; ++fu)
+        for (int b : blocks)
+          for (int l : lts) {
+            if (!compact && l != 64) continue;
+            H->tune_block = b;
+            H->tune_lt = l;
+            H->tune_fuse = fu;
+            drop_graphs(H);
+            time_steps_ms(H, 1);  // capture and warm up
+            const float ms = time_steps_ms(H, nsteps);
+            snapshot(H, snap, false);
+            if (ms < best) { best = ms; bb = b; bl = l; bf = fu; }
+          }
     } catch (...) {
       snapshot(H, snap, false);
       cudaStreamSynchronize(H->st);
@@ -1583,10 +1586,24 @@ int chs_autotune(chs_handle* H, int nsteps, int* block, int* lt_max, float* best
     cudaFree(snap);
     H->tune_block = bb;
     H->tune_lt = bl;
+    H->tune_fuse = bf;
     drop_graphs(H);
     *block = bb;
     *lt_max = bl;
+    *fused = bf;
     *best_ms = best;
+  });
+}
+
+int chs_set_launch_shape(chs_handle* H, int block, int lt_max, int fused) {
+  if (!H || (block != 0 && block != 128 && block != 256 && block != 512) ||
+      (lt_max != 0 && lt_max != 16 && lt_max != 32 && lt_max != 64) || (fused != 0 && fused != 1))
+    return CHS_ERR_ARG;
+  return guard(H, [&] {
+    H->tune_block = block;
+    H->tune_lt = lt_max;
+    H->tune_fuse = fused;
+    drop_graphs(H);
   });
 }
 

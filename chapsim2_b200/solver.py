@@ -68,7 +68,7 @@ EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field
             "chs_poisson_periodic_static", "chs_thermo_init", "chs_energy_substep", "chs_time_steps_host_fields",
             "chs_mlp_train", "chs_mlp_set_mode", "chs_mlp_fallbacks", "chs_mlp_params", "chs_mlp_grad",
             "chs_mlp_eval", "chs_mlp_norm", "chs_ensemble_create", "chs_ensemble_step", "chs_ensemble_time_steps",
-            "chs_ensemble_kernel_launches", "chs_ensemble_destroy", "chs_autotune"]
+            "chs_ensemble_kernel_launches", "chs_ensemble_destroy", "chs_autotune", "chs_set_launch_shape"]
 
 
 class ChsKprof(ctypes.Structure):
@@ -120,6 +120,7 @@ def load():
     L.chs_mlp_eval.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_double, _D,
                                ctypes.POINTER(ctypes.c_ulonglong)]
     L.chs_mlp_norm.argtypes = [ctypes.c_void_p, _D]
+    L.chs_set_launch_shape.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.chs_ensemble_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
     L.chs_ensemble_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.chs_ensemble_time_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
@@ -127,7 +128,8 @@ def load():
     L.chs_ensemble_kernel_launches.argtypes = [ctypes.c_void_p]
     L.chs_ensemble_destroy.argtypes = [ctypes.c_void_p]
     L.chs_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
-                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]
+                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                               ctypes.POINTER(ctypes.c_float)]
     L.chs_time_steps_host_fields.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D),
                                              ctypes.POINTER(ctypes.c_float)]
@@ -270,11 +272,14 @@ class Solver:
         self.Solve_momentum_eq(isub)
 
     def autotune(self, nsteps=2):
-        """Pick the fastest launch shapes for this handle; returns (block, lt_max, ms per nsteps)."""
-        b, l, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
-        self._check(self.L.chs_autotune(self.h, int(nsteps), ctypes.byref(b), ctypes.byref(l), ctypes.byref(ms)),
-                    "chs_autotune")
-        return b.value, l.value, ms.value
+        """Pick the fastest launch shapes for this handle; returns (block, lt_max, fused, ms per nsteps)."""
+        b, l, fu, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        self._check(self.L.chs_autotune(self.h, int(nsteps), ctypes.byref(b), ctypes.byref(l), ctypes.byref(fu),
+                                        ctypes.byref(ms)), "chs_autotune")
+        return b.value, l.value, fu.value, ms.value
+
+    def set_launch_shape(self, block=0, lt_max=0, fused=0):
+        self._check(self.L.chs_set_launch_shape(self.h, int(block), int(lt_max), int(fused)), "chs_set_launch_shape")
 
     # ---- MLP surrogate of the property update
     def mlp_train(self, nsamples=1000000, batch=4096, epochs=20, lr=2e-3, seed=20250101):

@@ -223,9 +223,14 @@ long long chs_ensemble_kernel_launches(const chs_ensemble* e);
 int chs_ensemble_destroy(chs_ensemble* e);
 
 /* Autotuner: times nsteps RK3 steps for each candidate launch shape (CTA size
- * of the explicit line operators; lines per CTA of the compact-scheme tile) on
- * this handle, restoring the state after each trial, and keeps the fastest. */
-int chs_autotune(chs_handle* h, int nsteps, int* block, int* lt_max, float* best_ms);
+ * of the explicit line operators; lines per CTA of the compact-scheme tile;
+ * separate operators or fused per-component sums) on this handle, restoring
+ * the state after each trial, and keeps the fastest. */
+int chs_autotune(chs_handle* h, int nsteps, int* block, int* lt_max, int* fused, float* best_ms);
+/* Set the launch shape directly (e.g. the one chs_autotune found for another
+ * handle of the same grid): block 0/128/256/512, lt_max 0/16/32/64, fused 0/1;
+ * 0 selects the defaults. */
+int chs_set_launch_shape(chs_handle* h, int block, int lt_max, int fused);
 
 /* Same as chs_poisson_solve on a device buffer (no host copies). */
 int chs_poisson_solve_device(chs_handle* h, double* d_rhs_inout);

@@ -49,8 +49,8 @@ def test_autotune_keeps_the_state():
     for g in (a, b):
         g.set_fields(*f)
         g.Solve_momentum_eq(0)
-    blk, lt, ms = a.autotune(nsteps=2)
-    assert blk in (128, 256, 512) and lt in (16, 32, 64) and ms > 0
+    blk, lt, fu, ms = a.autotune(nsteps=2)
+    assert blk in (128, 256, 512) and lt in (16, 32, 64) and fu in (0, 1) and ms > 0
     for p, q in zip(a.get_fields(), b.get_fields()):
         assert np.array_equal(p, q)
     a.step(2)
@@ -59,3 +59,28 @@ def test_autotune_keeps_the_state():
         assert np.max(np.abs(p - q)) <= 1e-12 * max(1.0, np.max(np.abs(q)))
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("heated", [False, True])
+@pytest.mark.parametrize("precision", [S.CHS_FP64, S.CHS_MIXED])
+def test_fused_sums_match_separate_operators(heated, precision):
+    """The fused per-component passes (an autotuner choice) give the separate operators' result."""
+    if heated:
+        cfg, tc = C.heated_channel(nc=(24, 18, 16), iacc=1, dt=0.004)
+    else:
+        cfg, tc = C.channel(nc=(24, 18, 16), iacc=1, dt=0.004), None
+    f = I.channel_fields(cfg)
+    out = []
+    for fused in (0, 1):
+        g = S.Solver(cfg, precision=precision)
+        g.set_fields(*f)
+        if tc is not None:
+            g.thermo_init(tc)
+        g.set_launch_shape(0, 0, fused)
+        g.Solve_momentum_eq(0)
+        g.step(2)
+        out.append([*g.get_fields()[:4]] + ([g.get_thermo()["T"]] if tc is not None else []))
+        g.close()
+    tol = 1e-12 if precision == S.CHS_FP64 else 1e-5
+    for a, b in zip(*out):
+        assert np.linalg.norm(a - b) <= tol * max(np.linalg.norm(b), 1e-30)
