@@ -347,7 +347,10 @@ __global__ void __launch_bounds__(512) stencil_op_kernel(const __grid_constant__
     }
     auto f = [&](int qq) -> T { return eval_expr32(io, ibase + qq * istride); };
     T v;
-    if (p >= P.b_lo && p <= P.b_hi) {
+    if (P.wrap) {
+      auto fw = [&](int qq) -> T { return f(qq < 0 ? qq + nin : (qq >= nin ? qq - nin : qq)); };
+      v = bulk_fn<FAM>(fw, p, r1, r2) * dd;
+    } else if (p >= P.b_lo && p <= P.b_hi) {
       v = bulk_fn<FAM>(f, p, r1, r2) * dd;
     } else {
       v = T(0);
@@ -546,7 +549,9 @@ __device__ __forceinline__ T bulk_term(const FusedTerm<T>& ft, const double* __r
     ibase = i + ft.n1 * j;
     istride = ft.n1 * ft.n2;
   }
+  const bool wrap = P.wrap;
   auto f = [&](int qq) -> T {
+    if (wrap) qq = qq < 0 ? qq + nin : (qq >= nin ? qq - nin : qq);
     const int a = ibase + qq * istride;
     T v = eval_term_ct<M0>(ft.t[0], a);
     if (M1 != T_NONE) v += eval_term_ct<M1>(ft.t[1], a);
@@ -625,8 +630,9 @@ __global__ void __launch_bounds__(256) fused_kernel_sig(const __grid_constant__ 
   bool bulk = true;
   {
     int idx = 0;
-    ((bulk = bulk && term_pos<S::dir>(i, j, k) >= F.term[idx].P.b_lo &&
-             term_pos<S::dir>(i, j, k) <= F.term[idx].P.b_hi && !F.term[idx].P.neu1 && !F.term[idx].P.neu2,
+    ((bulk = bulk && (F.term[idx].P.wrap || (term_pos<S::dir>(i, j, k) >= F.term[idx].P.b_lo &&
+                                              term_pos<S::dir>(i, j, k) <= F.term[idx].P.b_hi &&
+                                              !F.term[idx].P.neu1 && !F.term[idx].P.neu2)),
       ++idx),
      ...);
   }

@@ -694,6 +694,40 @@ OpPlan PlanBook::make(int d, int fam, const int ibc0[2], bool has_fbc) {
       if (p.neu1 || p.neu2) p.needs_fbc = 1;
     }
   }
+  // A periodic explicit line whose boundary rows equal the bulk stencil with wrapped indices runs
+  // every row through the bulk formula (no per-row branches in the kernels).  The check compares
+  // the assembled boundary rows with the kernels' bulk formula term by term.
+  p.wrap = 0;
+  if (p.tdma == 0 && ibc[0] == BC_PERIODIC && ibc[1] == BC_PERIODIC && p.nin == p.nout && p.lmap < 0 && !p.neu1 &&
+      !p.neu2) {
+    int o[4];
+    double cf[4];
+    const double r1 = p.r1, r2 = p.r2;
+    switch (fam) {
+      case M1P2C: o[0] = 0; o[1] = 1; o[2] = -1; o[3] = 2; cf[0] = r1; cf[1] = r1; cf[2] = r2; cf[3] = r2; break;
+      case M1C2P: o[0] = 0; o[1] = -1; o[2] = 1; o[3] = -2; cf[0] = r1; cf[1] = r1; cf[2] = r2; cf[3] = r2; break;
+      case D1C2C:
+      case D1P2P: o[0] = 1; o[1] = -1; o[2] = 2; o[3] = -2; cf[0] = r1; cf[1] = -r1; cf[2] = r2; cf[3] = -r2; break;
+      case D1C2P: o[0] = 0; o[1] = -1; o[2] = 1; o[3] = -2; cf[0] = r1; cf[1] = -r1; cf[2] = r2; cf[3] = -r2; break;
+      default: o[0] = 1; o[1] = 0; o[2] = 2; o[3] = -1; cf[0] = r1; cf[1] = -r1; cf[2] = r2; cf[3] = -r2; break;
+    }
+    const int n = p.nin;
+    const double tol = 1e-13 * (std::fabs(r1) + std::fabs(r2));
+    bool ok = true;
+    int covered = 0;
+    for (int s = 0; s < p.nspec && ok; ++s) {
+      const SpecialRow& S = p.sp[s];
+      for (int u = 0; u < 4; ++u)
+        if (S.wb[u] != 0.0) ok = false;
+      std::vector<double> want(n, 0.0), have(n, 0.0);
+      for (int k = 0; k < 4; ++k) want[((S.row + o[k]) % n + n) % n] += cf[k];
+      for (int t = 0; t < S.nt; ++t) have[S.idx[t]] += S.w[t];
+      for (int i = 0; i < n && ok; ++i)
+        if (std::fabs(want[i] - have[i]) > tol) ok = false;
+      if (S.row < p.b_lo || S.row > p.b_hi) ++covered;
+    }
+    if (ok && covered == p.b_lo + (p.nout - 1 - p.b_hi)) p.wrap = 1;
+  }
   return p;
 }
 

@@ -62,6 +62,8 @@ struct OpPlan {
   int64_t lmap;          // y-mapping multiplier (nout) or -1
   int neu1, neu2;        // overwrite first/last row with fbc(1)/fbc(2)
   int needs_fbc;         // 1 if any boundary value is read
+  int wrap;              // periodic explicit line whose boundary rows are the bulk stencil with
+                         // wrapped indices: every row may use the bulk formula
 };
 
 // Builds plans and the LHS/mapping table they reference.

@@ -2145,7 +2145,7 @@ int chs_plan_inspect(const chs_config* cfg, int dir, int fam, int ibc1, int ibc2
     double hd[20] = {(double)P.fam, (double)P.nin, (double)P.nout, (double)P.b_lo, (double)P.b_hi,
                      (double)P.off[0], (double)P.off[1], (double)P.off[2], (double)P.off[3], P.sgn, P.r1, P.r2,
                      P.dd, (double)P.nspec, (double)P.tdma, P.b1, P.an, P.cn, P.inv_den,
-                     (double)(P.neu1 * 2 + P.neu2)};
+                     (double)(P.neu1 * 2 + P.neu2 + 4 * P.wrap)};
     for (int i = 0; i < 20; ++i) buf[i] = hd[i];
     for (int k = 0; k < P.nspec; ++k) {
       double* o = buf + 20 + 26 * k;

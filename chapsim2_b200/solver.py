@@ -192,8 +192,8 @@ def plan_inspect(cfg, d, fam, ibc, has_fbc):
     h = buf[:20]
     p = dict(fam=int(h[0]), nin=int(h[1]), nout=int(h[2]), b_lo=int(h[3]), b_hi=int(h[4]),
              off=[int(x) for x in h[5:9]], sgn=h[9], r1=h[10], r2=h[11], dd=h[12], nspec=int(h[13]),
-             tdma=int(h[14]), b1=h[15], an=h[16], cn=h[17], inv_den=h[18], neu1=int(h[19]) // 2,
-             neu2=int(h[19]) % 2)
+             tdma=int(h[14]), b1=h[15], an=h[16], cn=h[17], inv_den=h[18], neu1=(int(h[19]) // 2) % 2,
+             neu2=int(h[19]) % 2, wrap=int(h[19]) // 4)
     rows = []
     for k in range(p["nspec"]):
         o = buf[20 + 26 * k: 46 + 26 * k]

@@ -34,7 +34,10 @@ def run_plan(p, fi3d, d, fbc_lines=None):
         nsw = nout - 1 if p["tdma"] == 2 else nout
         prev = 0.0
         for i in range(nout):
-            if p["b_lo"] <= i <= p["b_hi"]:
+            if p.get("wrap", 0):
+                g = lambda o: f[(i + o) % nin]
+                rr = (p["r1"] * (g(off[0]) + p["sgn"] * g(off[1])) + p["r2"] * (g(off[2]) + p["sgn"] * g(off[3]))) * p["dd"]
+            elif p["b_lo"] <= i <= p["b_hi"]:
                 g = lambda o: f[i + o]
                 rr = (p["r1"] * (g(off[0]) + p["sgn"] * g(off[1])) + p["r2"] * (g(off[2]) + p["sgn"] * g(off[3]))) * p["dd"]
             else:

@@ -54,3 +54,16 @@ def test_plan_boundary_rows_small():
     for r in p["rows"]:
         assert len(r["idx"]) <= 6
         assert all((i < 6) or (i >= p["nin"] - 6) for i in r["idx"])
+
+
+@pytest.mark.parametrize("acc", [1, 2, 3, 4])
+@pytest.mark.parametrize("fam", range(6))
+def test_periodic_explicit_plans_wrap(acc, fam):
+    """Periodic explicit lines carry the wrap flag (every row through the bulk formula with
+    wrapped indices); compact and wall-bounded lines never do."""
+    cfg = C.channel(nc=(12, 10, 8), iacc=acc)
+    for d in (0, 2):
+        p = S.plan_inspect(cfg, d, fam, (1, 1), False)
+        assert p["wrap"] == (1 if p["tdma"] == 0 else 0), (d, p["tdma"])
+    for ibc in WALL_BCS:
+        assert S.plan_inspect(cfg, 1, fam, ibc, True)["wrap"] == 0
