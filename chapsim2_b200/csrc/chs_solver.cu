@@ -12,7 +12,9 @@
 // All state stays in HBM; the substep is captured once into a CUDA graph.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -170,6 +172,185 @@ struct chs_handle {
   cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
   long long kernels_per_sub[4] = {0, 0, 0, 0};
   bool capturing = false;
+  // Dataflow scheduling of a captured substep.  Each launch names the buffers it reads and
+  // writes; it goes to one of up to kLanes streams and waits (by event) only for the launches it
+  // depends on: the last writer of every buffer it touches and, for the buffers it writes, the
+  // readers since that write.  The captured graph then holds the true dependency edges, so
+  // independent operators (the derived velocity gradients, the three momentum components, the
+  // energy fluxes) run concurrently and fill each other's ramp-up and tail.  Every node keeps a
+  // vector clock (per lane, the latest node of that lane it already follows); a launch goes to a
+  // lane whose last node it already follows, so stream order adds no false edge when one exists.
+  // Launches that name no buffers act as barriers.  Only active while a substep graph is
+  // captured; eager runs stay on `st` in program order.
+  static constexpr int kLanes = 8;
+  // lanes used by the next capture (1: one stream, program order).  Three measured fastest on the
+  // 128x96x128 channel and heated-channel substeps (8-10% over one lane; more lanes lose again).
+  int dag_lanes = 3;
+  cudaStream_t lane[kLanes] = {};
+  bool dag_on = false;
+  struct BufSpan { uintptr_t lo, hi; int id; };
+  struct BufState { int writer = -1; std::vector<int> readers; };
+  struct Clock { int v[kLanes]; };
+  std::vector<BufSpan> spans;
+  std::vector<BufState> bstate;
+  std::vector<int> node_lane;
+  std::vector<Clock> node_vc;
+  std::vector<cudaEvent_t> evpool;
+  int lane_last[kLanes];
+  int fence = -1, cur_node = -1;
+  struct Bufs { const void* p[12]; int n = 0; };
+  std::vector<int> pend_r, pend_w, deps;
+  int buf_id(const void* q) const {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(q);
+    size_t lo = 0, hi = spans.size();
+    while (lo < hi) {
+      const size_t m = (lo + hi) / 2;
+      if (spans[m].hi <= a) lo = m + 1;
+      else hi = m;
+    }
+    if (lo < spans.size() && spans[lo].lo <= a && a < spans[lo].hi) return spans[lo].id;
+    return (int)spans.size();  // not a handle buffer: one shared id, ordered conservatively
+  }
+  cudaEvent_t node_event(int n) {
+    while ((int)evpool.size() <= n) {
+      cudaEvent_t e;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      evpool.push_back(e);
+    }
+    return evpool[n];
+  }
+  // vector clock of a node that follows the nodes in `ds`
+  Clock clock_after(const std::vector<int>& ds) const {
+    Clock c;
+    for (int l = 0; l < kLanes; ++l) c.v[l] = -1;
+    for (int d : ds) {
+      for (int l = 0; l < kLanes; ++l) c.v[l] = std::max(c.v[l], node_vc[d].v[l]);
+      c.v[node_lane[d]] = std::max(c.v[node_lane[d]], d);
+    }
+    return c;
+  }
+  void dag_start() {
+    if (dag_lanes <= 1) return;
+    for (int l = 1; l < dag_lanes; ++l)
+      if (!lane[l]) CK(cudaStreamCreateWithFlags(&lane[l], cudaStreamNonBlocking));
+    lane[0] = st;
+    spans.clear();
+    for (size_t i = 0; i < allocs.size(); ++i) {
+      const uintptr_t a = reinterpret_cast<uintptr_t>(allocs[i].first);
+      spans.push_back(BufSpan{a, a + allocs[i].second, (int)i});
+    }
+    std::sort(spans.begin(), spans.end(), [](const BufSpan& x, const BufSpan& y) { return x.lo < y.lo; });
+    bstate.assign(spans.size() + 1, BufState{});
+    // node 0: the fork on the capturing stream; every lane starts after it
+    node_lane.assign(1, 0);
+    node_vc.assign(1, Clock{});
+    for (int l = 0; l < kLanes; ++l) node_vc[0].v[l] = -1;
+    CK(cudaEventRecord(node_event(0), st));
+    for (int l = 1; l < dag_lanes; ++l) CK(cudaStreamWaitEvent(lane[l], node_event(0), 0));
+    for (int l = 0; l < kLanes; ++l) lane_last[l] = l == 0 ? 0 : -1;
+    fence = 0;
+    cur_node = -1;
+    dag_on = true;
+  }
+  // join every lane back into the capturing stream (also on error paths, before the capture ends)
+  void dag_stop() {
+    if (!dag_on) return;
+    dag_on = false;
+    const Clock& c0 = node_vc[lane_last[0]];
+    for (int l = 1; l < dag_lanes; ++l)
+      if (lane_last[l] > c0.v[l]) cudaStreamWaitEvent(st, node_event(lane_last[l]), 0);
+  }
+  // make lane `ln` wait for the nodes in ds; returns the new node's clock
+  Clock join_into(int ln, std::vector<int>& ds) {
+    std::sort(ds.begin(), ds.end(), std::greater<int>());
+    ds.erase(std::unique(ds.begin(), ds.end()), ds.end());
+    Clock have;
+    for (int l = 0; l < kLanes; ++l) have.v[l] = -1;
+    if (lane_last[ln] >= 0) {
+      have = node_vc[lane_last[ln]];
+      have.v[ln] = lane_last[ln];
+    }
+    for (int d : ds) {
+      const int L = node_lane[d];
+      if (have.v[L] >= d) continue;  // already follows d (stream order or an earlier wait)
+      CK(cudaStreamWaitEvent(lane[ln], node_event(d), 0));
+      for (int l = 0; l < kLanes; ++l) have.v[l] = std::max(have.v[l], node_vc[d].v[l]);
+      have.v[L] = std::max(have.v[L], d);
+    }
+    return have;
+  }
+  cudaStream_t dag_begin(const Bufs& R, const Bufs& W) {
+    if (!dag_on) return st;
+    pend_r.clear();
+    pend_w.clear();
+    for (int i = 0; i < R.n; ++i)
+      if (R.p[i]) pend_r.push_back(buf_id(R.p[i]));
+    for (int i = 0; i < W.n; ++i)
+      if (W.p[i]) pend_w.push_back(buf_id(W.p[i]));
+    deps.assign(1, fence);
+    for (int b : pend_r)
+      if (bstate[b].writer >= 0) deps.push_back(bstate[b].writer);
+    for (int b : pend_w) {
+      if (bstate[b].writer >= 0) deps.push_back(bstate[b].writer);
+      for (int r : bstate[b].readers) deps.push_back(r);
+    }
+    const Clock need = clock_after(deps);
+    // a lane whose last node the launch already follows adds no false edge; prefer the lane of the
+    // latest dependency (no wait needed for it), else the lane idle longest
+    int latest = *std::max_element(deps.begin(), deps.end());
+    int ln = -1;
+    if (lane_last[node_lane[latest]] == latest) ln = node_lane[latest];
+    for (int l = 0; l < dag_lanes && ln < 0; ++l)
+      if (lane_last[l] <= need.v[l]) ln = l;
+    if (ln < 0) {
+      ln = 0;
+      for (int l = 1; l < dag_lanes; ++l)
+        if (lane_last[l] < lane_last[ln]) ln = l;
+    }
+    const Clock c = join_into(ln, deps);
+    cur_node = (int)node_lane.size();
+    node_lane.push_back(ln);
+    node_vc.push_back(c);
+    return lane[ln];
+  }
+  void dag_end() {
+    if (!dag_on) return;
+    const int n = cur_node, ln = node_lane[n];
+    CK(cudaEventRecord(node_event(n), lane[ln]));
+    lane_last[ln] = n;
+    for (int b : pend_r) bstate[b].readers.push_back(n);
+    for (int b : pend_w) {
+      bstate[b].writer = n;
+      bstate[b].readers.clear();
+    }
+    cur_node = -1;
+  }
+  // a launch that names no buffers: runs on `st` after everything before it, and everything after
+  // it waits for it
+  cudaStream_t dag_barrier_begin() {
+    if (!dag_on) return st;
+    deps.clear();
+    for (int l = 0; l < dag_lanes; ++l)
+      if (lane_last[l] >= 0) deps.push_back(lane_last[l]);
+    const Clock c = join_into(0, deps);
+    cur_node = (int)node_lane.size();
+    node_lane.push_back(0);
+    node_vc.push_back(c);
+    return st;
+  }
+  void dag_barrier_end() {
+    if (!dag_on) return;
+    const int n = cur_node;
+    CK(cudaEventRecord(node_event(n), st));
+    lane_last[0] = n;
+    for (auto& b : bstate) {
+      b.writer = -1;
+      b.readers.clear();
+    }
+    fence = n;
+    cur_node = -1;
+  }
+
   // per-kernel profiling (chs_profile_substep)
   bool profiling = false;
   struct Rec { int kind, dir; double bytes; cudaEvent_t e0, e1; };
@@ -204,6 +385,15 @@ struct chs_handle {
     return plans.emplace(key, p).first->second;
   }
 };
+
+// buffers a launch reads or writes (null entries are ignored)
+template <class... Ps>
+chs_handle::Bufs bufs(Ps... ps) {
+  static_assert(sizeof...(Ps) <= 12, "too many buffers");
+  chs_handle::Bufs b;
+  ((b.p[b.n++] = static_cast<const void*>(ps)), ...);
+  return b;
+}
 
 namespace {
 
@@ -276,18 +466,35 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const typename Id<T>::type* 
   const int narr = in.narrays();
   const double bytes =
       (double)sizeof(T) * (narr * nin_tot + ((accumulate || omode != O_STORE) ? 2.0 : 1.0) * nout_tot);
+  cudaStream_t s = H->dag_begin(bufs(io.t[0].X, io.t[0].Y, io.t[0].Z, io.t[1].X, io.t[1].Y, io.t[1].Z, io.fbc, io.onum,
+                                     accumulate ? out : nullptr),
+                                bufs(out));
   cudaEvent_t e0 = H->prof_begin();
-  launch_line_op(d, P, io, H->table, H->st);
+  launch_line_op(d, P, io, H->table, s);
   H->prof_end(e0, 0, d, bytes);
+  H->dag_end();
   H->launches++;
 }
 
-// profile wrapper for the other kernel classes
+// profile wrapper for the other kernel classes; without a buffer list the launch is a barrier of
+// the dataflow schedule
 #define PROF(H, kind, bytes, ...)                       \
   do {                                                   \
+    (H)->dag_barrier_begin();                            \
     cudaEvent_t e0_ = (H)->prof_begin();                 \
     __VA_ARGS__;                                         \
     (H)->prof_end(e0_, kind, -1, (bytes));               \
+    (H)->dag_barrier_end();                              \
+  } while (0)
+// the same with the buffers read (R) and written (W); the launch expression uses `st`, which here
+// names the lane the schedule picked
+#define PROFD(H, kind, bytes, R, W, ...)                 \
+  do {                                                   \
+    cudaStream_t st = (H)->dag_begin(R, W);              \
+    cudaEvent_t e0_ = (H)->prof_begin();                 \
+    __VA_ARGS__;                                         \
+    (H)->prof_end(e0_, kind, -1, (bytes));               \
+    (H)->dag_end();                                      \
   } while (0)
 
 // op(a; fbc1) + w*op(b; fbc2).  When both terms use the same plan the sum runs as one launch
@@ -393,9 +600,11 @@ void run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const
     const double ob = epilogue == EP_STORE ? 1.0 : epilogue == EP_ACCUM ? 2.0 : epilogue == EP_FRAC ? 3.0
                                                                           : (props ? 9.0 : 4.0);
     bytes += (double)sizeof(T) * ob * nout;
+    H->dag_barrier_begin();
     cudaEvent_t e0 = H->prof_begin();
     launch_fused(F, H->table, st);
     H->prof_end(e0, 0, -1, bytes);
+    H->dag_barrier_end();
     H->launches++;
     return;
   }
@@ -412,16 +621,16 @@ void run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const
     }
   }
   if (epilogue == EP_FRAC) {
-    PROF(H, 3, 5.0 * sizeof(T) * nout,
+    PROFD(H, 3, 5.0 * sizeof(T) * nout, bufs(pfc_scratch), bufs(out, rhs0),
          launch_fractional_step(out, rhs0, pfc_scratch, (int64_t)nout, H->dt, H->tGamma[isub], H->tZeta[isub],
                                 H->tAlpha[isub], st));
     H->launches++;
   } else if (epilogue == EP_ENERGY) {
-    PROF(H, 3, 5.0 * sizeof(T) * nout,
+    PROFD(H, 3, 5.0 * sizeof(T) * nout, bufs(), bufs(out, rhs0, rhoh),
          launch_energy_advance<T>(out, rhs0, rhoh, (int64_t)nout, H->dt, H->tGamma[isub], H->tZeta[isub], st));
     H->launches++;
     if (props) {
-      PROF(H, 3, 6.0 * sizeof(T) * nout,
+      PROFD(H, 3, 6.0 * sizeof(T) * nout, bufs(rhoh), bufs(H->hEnth, H->tTemp, H->kCond, H->dDens, H->mVisc),
            launch_property_update<T>(H->tab, rhoh, reinterpret_cast<T*>(H->hEnth), reinterpret_cast<T*>(H->tTemp),
                                      reinterpret_cast<T*>(H->kCond), reinterpret_cast<T*>(H->dDens),
                                      reinterpret_cast<T*>(H->mVisc), (int64_t)nout, st));
@@ -769,7 +978,6 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
   auto A = [](double* p) { return reinterpret_cast<T*>(p); };
   if ((parts & PART_ENERGY) && H->thermo && isub >= 1) energy_body_t<T>(H, isub);
   if (!(parts & PART_MOMENTUM)) return;
-  cudaStream_t st = H->st;
   const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
   const int np0 = H->np[0], np1 = H->np[1], np2 = H->np[2];
   const int s_pcc[3] = {np0, nc1, nc2}, s_cpc[3] = {nc0, np1, nc2}, s_ccp[3] = {nc0, nc1, np2};
@@ -847,8 +1055,10 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
   const T* mu_yz = TH ? A(H->muiyz_cpp) : nullptr;
 
   // div = qxdx + qydy + qzdz (:512-534)
-  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, launch_axpby(A(H->div), A(H->qxdx), 1.0, A(H->qydy), 1.0, (int64_t)H->n_ccc, st));
-  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, launch_axpby(A(H->div), A(H->div), 1.0, A(H->qzdz), 1.0, (int64_t)H->n_ccc, st));
+  PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, bufs(H->qxdx, H->qydy), bufs(H->div),
+        launch_axpby(A(H->div), A(H->qxdx), 1.0, A(H->qydy), 1.0, (int64_t)H->n_ccc, st));
+  PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, bufs(H->qzdz), bufs(H->div),
+        launch_axpby(A(H->div), A(H->div), 1.0, A(H->qzdz), 1.0, (int64_t)H->n_ccc, st));
   H->launches += 2;
   if (H->fbcy_velo) {
     // wall divergence for the y-viscous boundary value (:374-442, :537-546)
@@ -856,11 +1066,12 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
     run_op(H, 1, D1C2P, by_qy, fyqy, src(A(H->qyiy)), s_ccc, A(H->qydy_cpc), false, 1.0);
     run_op(H, 2, D1P2C, bz_qz, nullptr, src(A(H->qziy)), s_cpp, A(H->qzdz_cpc), false, 1.0);
     // fbcy_div = walls of (qxdx + qydy + qzdz)_cpc; visc2 bc = (qydy_cpc - div/3) * 2 (:1156-1171)
-    PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc,
-         launch_axpby(A(H->qxdx_cpc), A(H->qxdx_cpc), 1.0, A(H->qydy_cpc), 1.0, (int64_t)H->n_cpc, st));
-    PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc,
-         launch_axpby(A(H->qxdx_cpc), A(H->qxdx_cpc), 1.0, A(H->qzdz_cpc), 1.0, (int64_t)H->n_cpc, st));
-    PROF(H, 3, 48.0 / 8.0 * sizeof(T) * nc0 * nc2,
+    PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc, bufs(H->qydy_cpc), bufs(H->qxdx_cpc),
+          launch_axpby(A(H->qxdx_cpc), A(H->qxdx_cpc), 1.0, A(H->qydy_cpc), 1.0, (int64_t)H->n_cpc, st));
+    PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc, bufs(H->qzdz_cpc), bufs(H->qxdx_cpc),
+          launch_axpby(A(H->qxdx_cpc), A(H->qxdx_cpc), 1.0, A(H->qzdz_cpc), 1.0, (int64_t)H->n_cpc, st));
+    PROFD(H, 3, 48.0 / 8.0 * sizeof(T) * nc0 * nc2, bufs(H->qydy_cpc, H->qxdx_cpc, TH ? H->muiy_cpc : nullptr),
+          bufs(H->fb_visc2),
          launch_fbcy_extract<T>(A(H->fb_visc2), A(H->qydy_cpc), A(H->qxdx_cpc), TH ? A(H->muiy_cpc) : nullptr,
                                 -third, TH ? 2.0 : 1.0, 2.0, nc0, np1, nc2, st));
     H->launches += 3;
@@ -886,8 +1097,8 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
   }
   // y-momentum (:978-1242)
   if (H->fbcy_velo) {
-    PROF(H, 3, 24.0 / 8.0 * sizeof(T) * 4 * nc0 * nc2,
-         launch_axpby(A(H->fb_comb), A(H->fb_conv2), 1.0, A(H->fb_visc2), rre, (int64_t)4 * nc0 * nc2, st));
+    PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * 4 * nc0 * nc2, bufs(H->fb_conv2, H->fb_visc2), bufs(H->fb_comb),
+          launch_axpby(A(H->fb_comb), A(H->fb_conv2), 1.0, A(H->fb_visc2), rre, (int64_t)4 * nc0 * nc2, st));
     H->launches++;
   }
   {
@@ -918,20 +1129,23 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
   // ---- 3b. mass flux
   const double* bulk = nullptr;
   if (H->idriven == 1) {
-    PROF(H, 3, 8.0 / 8.0 * sizeof(T) * H->n_pcc,
+    PROFD(H, 3, 8.0 / 8.0 * sizeof(T) * H->n_pcc, bufs(H->mx, H->wy), bufs(H->partial, H->scal),
          launch_weighted_mean(A(H->mx), H->wy, np0, nc1, nc2, H->partial, H->npart, H->scal + 0, H->vol, st));
     bulk = H->scal + 0;
     H->launches += 2;
   }
   // ---- 4. q += rhs, walls
-  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_pcc, launch_update_q(A(ux), A(H->mx), bulk, (int64_t)H->n_pcc, st));
-  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc, launch_update_q(A(uy), A(H->my), nullptr, (int64_t)H->n_cpc, st));
-  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccp, launch_update_q(A(uz), A(H->mz), nullptr, (int64_t)H->n_ccp, st));
+  PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_pcc, bufs(H->mx, bulk), bufs(ux),
+        launch_update_q(A(ux), A(H->mx), bulk, (int64_t)H->n_pcc, st));
+  PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc, bufs(H->my), bufs(uy),
+        launch_update_q(A(uy), A(H->my), nullptr, (int64_t)H->n_cpc, st));
+  PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccp, bufs(H->mz), bufs(uz),
+        launch_update_q(A(uz), A(H->mz), nullptr, (int64_t)H->n_ccp, st));
   H->launches += 3;
   const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
   if (w0 || w1) {
-    PROF(H, 3, 16.0 / 8.0 * sizeof(T) * nc0 * nc2,
-         launch_set_yrows(A(uy), nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+    PROFD(H, 3, 16.0 / 8.0 * sizeof(T) * nc0 * nc2, bufs(), bufs(uy),
+          launch_set_yrows(A(uy), nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
     H->launches++;
   }
   // ---- 5. Poisson RHS, solve, pressure and projection.  For variable properties the reference
@@ -945,15 +1159,16 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
     run_fused<T>(H, t, A(H->pcor), s_ccc, EP_STORE, nullptr, isub, nullptr);
   }
   poisson_device<T>(H, A(H->pcor));
-  PROF(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, launch_axpby(A(H->pres), A(H->pres), 1.0, A(H->pcor), 1.0, (int64_t)H->n_ccc, st));
+  PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, bufs(H->pcor), bufs(H->pres),
+        launch_axpby(A(H->pres), A(H->pres), 1.0, A(H->pcor), 1.0, (int64_t)H->n_ccc, st));
   H->launches++;
   const double f = H->dt * H->tAlpha[isub] * H->sigma2p;
   run_op(H, 0, D1C2P, bx_pr, any, src(A(H->pcor)), s_ccc, A(ux), true, -f);
   run_op(H, 1, D1C2P, by_pr, fypr, src(A(H->pcor)), s_ccc, A(uy), true, -f);
   run_op(H, 2, D1C2P, bz_pr, any, src(A(H->pcor)), s_ccc, A(uz), true, -f);
   if (w0 || w1) {
-    PROF(H, 3, 16.0 / 8.0 * sizeof(T) * nc0 * nc2,
-         launch_set_yrows(A(uy), nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+    PROFD(H, 3, 16.0 / 8.0 * sizeof(T) * nc0 * nc2, bufs(), bufs(uy),
+          launch_set_yrows(A(uy), nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
     H->launches++;
   }
   // ---- 6. variable properties: q = g / rho_face (convert_primary_conservative IG2Q,
@@ -974,7 +1189,6 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
 template <typename T>
 void energy_body_t(chs_handle* H, int isub) {
   auto A = [](double* p) { return reinterpret_cast<T*>(p); };
-  cudaStream_t st = H->st;
   const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
   const int np0 = H->np[0], np1 = H->np[1], np2 = H->np[2];
   const int s_pcc[3] = {np0, nc1, nc2}, s_cpc[3] = {nc0, np1, nc2}, s_ccp[3] = {nc0, nc1, np2};
@@ -994,8 +1208,8 @@ void energy_body_t(chs_handle* H, int isub) {
   run_op(H, 0, D1C2P, P2(B[0][V_TM]), fz, src(A(H->tTemp)), s_ccc, A(H->dTx), false, 1.0);
   run_op(H, 1, D1C2P, P2(B[1][V_TM]), A(H->fb_qw), src(A(H->tTemp)), s_ccc, A(H->dTy), false, 1.0);
   run_op(H, 2, D1C2P, P2(B[2][V_TM]), fz, src(A(H->tTemp)), s_ccc, A(H->dTz), false, 1.0);
-  PROF(H, 3, 3.0 * sizeof(T) * nc0 * nc2,
-       launch_fbcy_extract<T>(A(H->fb_dtk), A(H->dTy), nullptr, A(H->k_cpc), 0.0, 1.0, 1.0, nc0, np1, nc2, st));
+  PROFD(H, 3, 3.0 * sizeof(T) * nc0 * nc2, bufs(H->dTy, H->k_cpc), bufs(H->fb_dtk),
+        launch_fbcy_extract<T>(A(H->fb_dtk), A(H->dTy), nullptr, A(H->k_cpc), 0.0, 1.0, 1.0, nc0, np1, nc2, st));
   H->launches++;
   // conv + diffusion per direction, the fractional step, the rho*h update and (table mode) the
   // property update in one fused pass
@@ -1011,7 +1225,8 @@ void energy_body_t(chs_handle* H, int isub) {
     run_fused<T>(H, t, A(H->erhs), s_ccc, EP_ENERGY, A(H->erhs0), isub, nullptr, A(H->rhoh), table_props);
   }
   if (!table_props) {
-    PROF(H, 3, 6.0 * sizeof(T) * H->n_ccc,
+    PROFD(H, 3, 6.0 * sizeof(T) * H->n_ccc, bufs(H->rhoh, H->mlp_wpack),
+          bufs(H->hEnth, H->tTemp, H->kCond, H->dDens, H->mVisc, H->mlp_nfb),
          launch_mlp_props<T>(H->tab, H->mlp_norm, H->mlp_small, H->mlp_check, H->mlp_wpack, A(H->rhoh),
                              A(H->hEnth), A(H->tTemp), A(H->kCond), A(H->dDens), A(H->mVisc), (int64_t)H->n_ccc,
                              H->mlp_nfb, st));
@@ -1020,7 +1235,7 @@ void energy_body_t(chs_handle* H, int isub) {
   const int s0 = B[1][V_TM][0] == BC_NEUMANN, s1 = B[1][V_TM][1] == BC_NEUMANN;
   if (s0 || s1) {
     run_op(H, 1, M1C2P, H->ftpy, nullptr, src(A(H->rhoh)), s_ccc, A(H->dh_cpc), false, 1.0);
-    PROF(H, 3, 10.0 * sizeof(T) * nc0 * nc2,
+    PROFD(H, 3, 10.0 * sizeof(T) * nc0 * nc2, bufs(H->dh_cpc), bufs(H->fb_h, H->fb_k, H->fb_m, H->fb_d),
          launch_wall_props<T>(H->tab, A(H->dh_cpc), nc0, np1, nc2, s0, s1, A(H->fb_h), A(H->fb_k), A(H->fb_m),
                               A(H->fb_d), st));
     H->launches++;
@@ -1425,8 +1640,11 @@ void capture_graphs(chs_handle* H) {
     CK(cudaStreamBeginCapture(H->st, cudaStreamCaptureModeThreadLocal));
     H->capturing = true;
     try {
+      H->dag_start();
       substep_body(H, isub);
+      H->dag_stop();
     } catch (...) {
+      H->dag_stop();
       H->capturing = false;
       cudaStreamEndCapture(H->st, &g);
       throw;
@@ -1607,6 +1825,14 @@ int chs_set_launch_shape(chs_handle* H, int block, int lt_max, int fused) {
   });
 }
 
+int chs_set_lanes(chs_handle* H, int lanes) {
+  if (!H || lanes < 1 || lanes > chs_handle::kLanes) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    H->dag_lanes = lanes;
+    drop_graphs(H);
+  });
+}
+
 int chs_ensemble_create(chs_handle* const* members, int n, chs_ensemble** out) {
   if (!members || n < 1 || !out) return CHS_ERR_ARG;
   auto* E = new chs_ensemble();
@@ -1708,6 +1934,9 @@ int chs_destroy(chs_handle* H) {
   drop_graphs(H);
   if (H->table) cudaFree(H->table);
   for (auto& a : H->allocs) cudaFree(a.first);
+  for (int l = 1; l < chs_handle::kLanes; ++l)
+    if (H->lane[l]) cudaStreamDestroy(H->lane[l]);
+  for (cudaEvent_t e : H->evpool) cudaEventDestroy(e);
   if (H->st) cudaStreamDestroy(H->st);
   delete H;
   return CHS_OK;

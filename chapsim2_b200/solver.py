@@ -68,7 +68,8 @@ EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field
             "chs_poisson_periodic_static", "chs_thermo_init", "chs_energy_substep", "chs_time_steps_host_fields",
             "chs_mlp_train", "chs_mlp_set_mode", "chs_mlp_fallbacks", "chs_mlp_params", "chs_mlp_grad",
             "chs_mlp_eval", "chs_mlp_norm", "chs_ensemble_create", "chs_ensemble_step", "chs_ensemble_time_steps",
-            "chs_ensemble_kernel_launches", "chs_ensemble_destroy", "chs_autotune", "chs_set_launch_shape"]
+            "chs_ensemble_kernel_launches", "chs_ensemble_destroy", "chs_autotune", "chs_set_launch_shape",
+            "chs_set_lanes"]
 
 
 class ChsKprof(ctypes.Structure):
@@ -121,6 +122,7 @@ def load():
                                ctypes.POINTER(ctypes.c_ulonglong)]
     L.chs_mlp_norm.argtypes = [ctypes.c_void_p, _D]
     L.chs_set_launch_shape.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.chs_set_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.chs_ensemble_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
     L.chs_ensemble_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.chs_ensemble_time_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
@@ -280,6 +282,10 @@ class Solver:
 
     def set_launch_shape(self, block=0, lt_max=0, fused=0):
         self._check(self.L.chs_set_launch_shape(self.h, int(block), int(lt_max), int(fused)), "chs_set_launch_shape")
+
+    def set_lanes(self, lanes):
+        """Streams a captured substep spreads its independent launches over (1..8)."""
+        self._check(self.L.chs_set_lanes(self.h, int(lanes)), "chs_set_lanes")
 
     # ---- MLP surrogate of the property update
     def mlp_train(self, nsamples=1000000, batch=4096, epochs=20, lr=2e-3, seed=20250101):
