@@ -53,6 +53,12 @@ struct ThermoTab {
   const double *t, *h, *d, *m, *k, *rhoh;
   int n;
   double dhmin, dhmax;
+  // bracket index of the rho*h (0) and h (1) columns: for each of ix_nb uniform bins over
+  // [ix_lo, ix_hi], the bisection state (a, b) that every value of the bin reaches, so the search
+  // starts there and takes the same path as from (0, n-1); null: full bisection
+  const int2* ix[2];
+  double ix_lo[2], ix_hi[2], ix_iw[2];
+  int ix_nb;
 };
 
 // ---- fused explicit operators: out(i,j,k) = sum over terms of g_m * op_m(in_m)(i,j,k) ----

@@ -1380,6 +1380,44 @@ void thermo_init(chs_handle* H, const chs_thermo* c) {
     CK(cudaMemcpyAsync(cols + (size_t)j * n, srcs[j], n * sizeof(double), cudaMemcpyHostToDevice, H->st));
   H->tab = ThermoTab{cols, cols + n, cols + 2 * n, cols + 3 * n, cols + 4 * n, cols + 5 * n, n,
                      *std::min_element(rhoh.begin(), rhoh.end()), *std::max_element(rhoh.begin(), rhoh.end())};
+  {
+    // bracket index of the strictly increasing rho*h and h columns (2n bins each).  For x fixed,
+    // the sign test (col[a]-x)*(col[m]-x) > MINP holds on two rays (below col[a], above col[m])
+    // and fails on the interval between them, so when both ends of a bin (widened by 1e-6 of a bin
+    // against rounding of the bin index) take the same branch, and for the 'a = m' branch lie on
+    // the same ray, every value of the bin takes that branch.  The index stores the state where
+    // the ends first part; the device search continues from it along the same path.
+    const int nb = 2 * n;
+    std::vector<int> ixh(4 * (size_t)nb);
+    const double* icol[2] = {rhoh.data(), c->h};
+    for (int q = 0; q < 2; ++q) {
+      const double* col = icol[q];
+      const double lo = col[0], hi = col[n - 1], w = (hi - lo) / nb;
+      const double del = std::max(1e-6 * w, 1e-13 * std::max(std::fabs(lo), std::fabs(hi)));
+      for (int bi = 0; bi < nb; ++bi) {
+        const double xl = lo + bi * w - del, xh = lo + (bi + 1) * w + del;
+        int a = 0, b = n - 1;
+        while (b - a > 1) {
+          const int m = a + (b - a) / 2;
+          const double ca = col[a], cm = col[m];
+          const bool dl = (ca - xl) * (cm - xl) > 1.0e-20, dh = (ca - xh) * (cm - xh) > 1.0e-20;
+          if (dl != dh || (dl && ((xl < ca) != (xh < ca)))) break;
+          if (dl) a = m;
+          else b = m;
+        }
+        ixh[(size_t)q * 2 * nb + 2 * bi] = a;
+        ixh[(size_t)q * 2 * nb + 2 * bi + 1] = b;
+      }
+      H->tab.ix_lo[q] = lo;
+      H->tab.ix_hi[q] = hi;
+      H->tab.ix_iw[q] = 1.0 / w;
+    }
+    int2* ixd = H->dalloc<int2>(2 * (size_t)nb);
+    CK(cudaMemcpyAsync(ixd, ixh.data(), ixh.size() * sizeof(int), cudaMemcpyHostToDevice, H->st));
+    H->tab.ix[0] = ixd;
+    H->tab.ix[1] = ixd + nb;
+    H->tab.ix_nb = nb;
+  }
   H->rPrRen = c->rPrRen;
   H->tab_host_t.assign(c->t, c->t + n);
   H->tab_host_rhoh = rhoh;

@@ -85,3 +85,38 @@ def test_energy_and_momentum_entry_points_match_step():
         assert np.array_equal(ta[k], tb[k]), k
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("nonuniform", [False, True])
+def test_indexed_table_lookup_matches_oracle(nonuniform):
+    """The device lookup starts its bisection from a per-bin bracket index; at the table nodes,
+    their midpoints, the index's bin edges and one ulp either side, and random values, it gives the
+    oracle's full-bisection lookup (tolerance 1e-13 of each column's range: the interpolation may
+    use fused multiply-adds on the device)."""
+    cfg, tc = C.heated_channel(nc=(16, 16, 16), iacc=1, dt=0.004)
+    if nonuniform:
+        # cluster the table rows towards the hot end so the index bins hold very different counts
+        tb = tc.table
+        s = np.linspace(0.0, 1.0, tb["t"].size) ** 3
+        t_new = tb["t"][0] + (tb["t"][-1] - tb["t"][0]) * s
+        for key in ("h", "d", "m", "k"):
+            tb[key] = np.interp(t_new, tb["t"], tb[key])
+        tb["t"] = t_new
+    o, g = _pair(cfg, tc)
+    g.mlp_params(np.random.default_rng(3).normal(0.0, 0.1, S.MLP_NPARAM).astype(np.float32))
+    tb = tc.table
+    rh_tab = tb["d"] * tb["h"]
+    lo, hi = rh_tab[0], rh_tab[-1]
+    nb = 2 * rh_tab.size
+    edges = lo + np.arange(nb + 1) * ((hi - lo) / nb)
+    rng = np.random.default_rng(11)
+    x = np.concatenate([rh_tab, 0.5 * (rh_tab[1:] + rh_tab[:-1]), edges, np.nextafter(edges, -np.inf),
+                        np.nextafter(edges, np.inf), rng.uniform(lo, hi, 20000)])
+    x = np.clip(x, lo, hi)
+    out, nfb = g.mlp_eval(x, tol=0.0)  # tolerance 0: every value takes the table lookup
+    assert nfb == x.size
+    h, T, d, m, k, cp = o.ftp_from_dh(x)
+    for name, got, ref in zip(("T", "rho", "mu", "kappa", "h"), out, (T, d, m, k, h)):
+        err = np.max(np.abs(got - ref))
+        assert err <= 1e-13 * (ref.max() - ref.min()), (name, err)
+    g.close()
