@@ -274,8 +274,13 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
                    f"({len(ids)} fields), substep graph in between"}
 
     peak, peak_kind = measured_peaks()
-    prof = g.profile_substep(1)
+    # per-launch CUDA events inside a one-stream graph replay of substep 1 (the timed path, without
+    # the concurrency of the dataflow lanes), and the same after eager launches for comparison
+    prof = g.profile_substep_graph(1)
     rl = roofline(prof, peak, peak_kind, args.workload)
+    rl["timing"] = "CUDA events around each launch in a one-stream graph replay of one substep"
+    eager = roofline(g.profile_substep(1), peak, peak_kind, args.workload)
+    rl["eager"] = {"achieved": eager["achieved"], "frac": eager["frac"], "ms_per_launch": eager["ms_per_launch"]}
     bpc = BYTES_PER_CELL_SUBSTEP[args.workload]
     step_model = {"bytes_per_cell_substep": bpc, "achieved_gbs": bpc * cfg.ncell * sub / (ms * 1e-3) / 1e9}
     step_model["frac"] = step_model["achieved_gbs"] / peak

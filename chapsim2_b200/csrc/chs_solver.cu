@@ -355,16 +355,21 @@ struct chs_handle {
   bool profiling = false;
   struct Rec { int kind, dir; double bytes; cudaEvent_t e0, e1; };
   std::vector<Rec> recs;
+  // while a profiled substep is captured, the events become event-record nodes of the graph
+  void prof_record(cudaEvent_t e) {
+    if (capturing) CK(cudaEventRecordWithFlags(e, st, cudaEventRecordExternal));
+    else CK(cudaEventRecord(e, st));
+  }
   cudaEvent_t prof_begin() {
     cudaEvent_t e = nullptr;
-    if (profiling) { CK(cudaEventCreate(&e)); CK(cudaEventRecord(e, st)); }
+    if (profiling) { CK(cudaEventCreate(&e)); prof_record(e); }
     return e;
   }
   void prof_end(cudaEvent_t e0, int kind, int dir, double bytes) {
     if (!profiling) return;
     cudaEvent_t e1;
     CK(cudaEventCreate(&e1));
-    CK(cudaEventRecord(e1, st));
+    prof_record(e1);
     recs.push_back(Rec{kind, dir, bytes, e0, e1});
   }
 
@@ -2263,6 +2268,55 @@ int chs_profile_substep(chs_handle* H, int isub, chs_kprof* out, int max, int* n
     }
     H->profiling = false;
     CK(cudaStreamSynchronize(H->st));
+    int k = 0;
+    for (auto& r : H->recs) {
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, r.e0, r.e1));
+      if (k < max) out[k] = chs_kprof{r.kind, r.dir, r.bytes, ms};
+      ++k;
+      cudaEventDestroy(r.e0);
+      cudaEventDestroy(r.e1);
+    }
+    H->recs.clear();
+    *n = k;
+  });
+}
+
+int chs_profile_substep_graph(chs_handle* H, int isub, chs_kprof* out, int max, int* n) {
+  if (!H || !out || !n || isub < 1 || isub > 3) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    for (auto& r : H->recs) { cudaEventDestroy(r.e0); cudaEventDestroy(r.e1); }
+    H->recs.clear();
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    CK(cudaStreamSynchronize(H->st));
+    CK(cudaStreamBeginCapture(H->st, cudaStreamCaptureModeThreadLocal));
+    H->capturing = true;
+    H->profiling = true;
+    const long long before = H->launches;
+    try {
+      substep_body(H, isub);
+    } catch (...) {
+      H->profiling = false;
+      H->capturing = false;
+      cudaStreamEndCapture(H->st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    H->profiling = false;
+    H->capturing = false;
+    CK(cudaStreamEndCapture(H->st, &g));
+    const long long nk = H->launches - before;
+    H->launches = before;
+    const cudaError_t ei = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    CK(ei);
+    CK(cudaGraphUpload(ge, H->st));
+    CK(cudaStreamSynchronize(H->st));
+    CK(cudaGraphLaunch(ge, H->st));
+    H->launches += nk;
+    CK(cudaStreamSynchronize(H->st));
+    cudaGraphExecDestroy(ge);
     int k = 0;
     for (auto& r : H->recs) {
       float ms = 0.0f;

@@ -69,7 +69,7 @@ EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field
             "chs_mlp_train", "chs_mlp_set_mode", "chs_mlp_fallbacks", "chs_mlp_params", "chs_mlp_grad",
             "chs_mlp_eval", "chs_mlp_norm", "chs_ensemble_create", "chs_ensemble_step", "chs_ensemble_time_steps",
             "chs_ensemble_kernel_launches", "chs_ensemble_destroy", "chs_autotune", "chs_set_launch_shape",
-            "chs_set_lanes"]
+            "chs_set_lanes", "chs_profile_substep_graph"]
 
 
 class ChsKprof(ctypes.Structure):
@@ -111,6 +111,8 @@ def load():
     L.chs_host_free.argtypes = [ctypes.c_void_p]
     L.chs_profile_substep.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ChsKprof), ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int)]
+    L.chs_profile_substep_graph.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ChsKprof), ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_int)]
     L.chs_thermo_init.argtypes = [ctypes.c_void_p, ctypes.POINTER(ChsThermo)]
     _F = ctypes.POINTER(ctypes.c_float)
     L.chs_mlp_train.argtypes = [ctypes.c_void_p, ctypes.POINTER(ChsMlpTrainCfg), ctypes.POINTER(ChsMlpReport)]
@@ -424,6 +426,14 @@ class Solver:
         arr = (ChsKprof * maxk)()
         n = ctypes.c_int()
         self._check(self.L.chs_profile_substep(self.h, int(isub), arr, maxk, ctypes.byref(n)), "chs_profile_substep")
+        return [dict(kind=arr[i].kind, dir=arr[i].dir, bytes=arr[i].bytes, ms=arr[i].ms) for i in range(n.value)]
+
+    def profile_substep_graph(self, isub=1, maxk=512):
+        """Per-launch profile of one substep replayed as a CUDA graph (advances the state)."""
+        arr = (ChsKprof * maxk)()
+        n = ctypes.c_int()
+        self._check(self.L.chs_profile_substep_graph(self.h, int(isub), arr, maxk, ctypes.byref(n)),
+                    "chs_profile_substep_graph")
         return [dict(kind=arr[i].kind, dir=arr[i].dir, bytes=arr[i].bytes, ms=arr[i].ms) for i in range(n.value)]
 
     def sync(self):

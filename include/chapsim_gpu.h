@@ -149,6 +149,12 @@ typedef struct chs_kprof {
   float ms;
 } chs_kprof;
 int chs_profile_substep(chs_handle* h, int isub, chs_kprof* out, int max, int* n);
+/* The same profile taken inside a CUDA graph of the substep (isub 1..3): the
+ * substep is captured on one stream with an event-record node around every
+ * launch and replayed once, so each duration is the launch's time in graph
+ * replay (the timed path) rather than after an eager launch.  Advances the
+ * state by that substep, like chs_momentum_substep. */
+int chs_profile_substep_graph(chs_handle* h, int isub, chs_kprof* out, int max, int* n);
 
 /* Replaces Buildup_thermo_mapping_relations + initialise_thermal_properties
  * (src/chapsim.f90:103-108, src/input_thermo.f90:1070-1103) and the q -> g
