@@ -7,7 +7,9 @@ constant mass flux, isoflux y walls (dT/dy = -/+1), the synthetic 4096-row
 property table (cp peak at T = 0.5), CD2 operators (the accuracy whose operators
 are consistent with the 2nd-order FISHPACK Poisson solver), synthetic
 Poiseuille + seeded noise initial velocity, T_ini = 0.47, dt from CFL 0.8
-frozen.  --workload channel runs the flow-only channel instead.
+frozen.  --workload channel runs the flow-only channel instead; --workload
+large the Re_tau ~ 395 heated channel, 384 x 256 x 384 cells (37.7M), beta =
+1.8, Re_b = 6875 (its CPU sample is one substep per step).
 
 `value` is the plain FP64 path (the drop-in).  `forms` adds the mixed form
 (FP32 fields, operators and RHS; FP64 Poisson, mass-flux mean and checks) on
@@ -48,13 +50,15 @@ METRIC = "Mcell-RK3-substeps/s on 1 B200: mixed+MLP vs plain FP64 at ≤1e-5 L2;
 UNIT = "Mcell-substeps/s"
 # compulsory traffic per cell per RK3 substep: flow-only FP64 (30 words), variable-property FP64
 # (57 words: + energy 10, property update 7, momentum with g and mu 4, drho/dt 2, g->q 4)
-BYTES_PER_CELL_SUBSTEP = {"channel": 240.0, "heated": 456.0}
+BYTES_PER_CELL_SUBSTEP = {"channel": 240.0, "heated": 456.0, "large": 456.0}
 
 
 def workload(kind="heated", nc=(128, 96, 128), iacc=C.IACCU_CD2):
     """(cfg, fields, thermo config or None)."""
     if kind == "heated":
         cfg, tc = C.heated_channel(nc=nc, iacc=iacc)
+    elif kind == "large":
+        cfg, tc = C.heated_channel(nc=(384, 256, 384), iacc=iacc, rstret=0.09, ren=6875.0)
     else:
         cfg, tc = C.channel(nc=nc, iacc=iacc), None
     fields = I.channel_fields(cfg)
@@ -65,9 +69,10 @@ def workload(kind="heated", nc=(128, 96, 128), iacc=C.IACCU_CD2):
 def describe(cfg, tc):
     n = f"{cfg.nc[0]}x{cfg.nc[1]}x{cfg.nc[2]}"
     if tc is None:
-        return f"channel {n} flow-only, beta=1.5, Re_b=2800, CD2"
-    return (f"heated channel {n}, variable properties (synthetic 4096-row table), isoflux walls, beta=1.5, "
-            f"Re_b=2800, CD2")
+        return f"channel {n} flow-only, beta={20.0 * cfg.rstret:g}, Re_b={cfg.ren:g}, CD2"
+    beta, reb = 20.0 * cfg.rstret, cfg.ren
+    return (f"heated channel {n}, variable properties (synthetic 4096-row table), isoflux walls, beta={beta:g}, "
+            f"Re_b={reb:g}, CD2")
 
 
 def measured_peaks():
@@ -177,13 +182,17 @@ def run_reference(args, cfg, fields, tc, world, rank, dist):
         return None
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    cpu_time_oracle(cfg, fields, tc, args.warmup)
-    t = cpu_time_oracle(cfg, fields, tc, args.steps)
-    value = cfg.ncell * args.steps / t / 1e6
-    sample = f"{args.steps} substeps of the {describe(cfg, tc)} (FP64)"
+    nsteps, nwarm = args.steps, args.warmup
+    if args.workload == "large":  # about 20 s of CPU work per substep: a bounded sample
+        nsteps, nwarm = min(nsteps, 2), 0
+    if nwarm:
+        cpu_time_oracle(cfg, fields, tc, nwarm)
+    t = cpu_time_oracle(cfg, fields, tc, nsteps)
+    value = cfg.ncell * nsteps / t / 1e6
+    sample = f"{nsteps} substeps of the {describe(cfg, tc)} (FP64)"
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps,
+        "steps": nsteps, "warmup": nwarm, "ms_per_step": 1000.0 * t / nsteps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": describe(cfg, tc), "step": "one RK3 substep", "cells": cfg.ncell},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
@@ -273,6 +282,10 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
            "path": "chs_time_steps_host_fields: pinned host state copied in and out around every substep "
                    f"({len(ids)} fields), substep graph in between"}
 
+    # x-z-mean profiles after the same number of steps the other forms take (1 + warmup + 2 steps);
+    # the profiling below advances this handle by two more substeps
+    pd = xz_profiles(g, cfg, tc)
+    steps_done = args.warmup + 2 * args.steps  # RK3 steps after the initial projection
     peak, peak_kind = measured_peaks()
     # per-launch CUDA events inside a one-stream graph replay of substep 1 (the timed path, without
     # the concurrency of the dataflow lanes), and the same after eager launches for comparison
@@ -292,7 +305,8 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
         "config": {"workload": describe(cfg, tc),
                    "step": "one RK3 step (3 substeps), CUDA-graph replay",
                    "cells": cfg.ncell, "dt": cfg.dt, "precision": "fp64",
-                   "l2": "working set of ~70 FP64 fields x 12.6 MB per step > 126 MB L2; no flush",
+                   "l2": f"working set of ~70 FP64 fields x {8e-6 * cfg.ncell:.1f} MB per step > 126 MB L2; "
+                         "no flush",
                    "parallelism": f"replicas x{world}"},
         "roofline": rl, "step_model": step_model, "e2e": e2e,
         "gpu_launches": l1 - l0, "clocks": clk,
@@ -309,9 +323,9 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
     barrier(dist)
     ms_m = max_over_ranks(dist, ms_m)
     m.step(args.steps)  # the FP64 handle also ran args.steps e2e steps
-    pm, pd = xz_profiles(m, cfg, tc), xz_profiles(g, cfg, tc)
+    pm = xz_profiles(m, cfg, tc)
     mixed = {"value": world * cfg.ncell * sub / (ms_m * 1e-3) / 1e6, "ms_per_step": ms_m / args.steps,
-             "speedup_vs_fp64": ms_max / ms_m, "steps_compared": 1 + args.warmup + 2 * args.steps}
+             "speedup_vs_fp64": ms_max / ms_m, "steps_compared": steps_done}
     for k in pd:
         mixed[f"{k}_mean_profile_rel_l2_vs_fp64"] = float(np.linalg.norm(pm[k] - pd[k]) / np.linalg.norm(pd[k]))
     out["forms"] = {"fp64": {"value": value, "ms_per_step": ms_max / args.steps}, "mixed": mixed}
@@ -332,7 +346,7 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
         fb = n.mlp_fallbacks()
         pn = xz_profiles(n, cfg, tc)
         ml = {"value": world * cfg.ncell * sub / (ms_n * 1e-3) / 1e6, "ms_per_step": ms_n / args.steps,
-              "speedup_vs_fp64": ms_max / ms_n, "steps_compared": 1 + args.warmup + 2 * args.steps,
+              "speedup_vs_fp64": ms_max / ms_n, "steps_compared": steps_done,
               "check_tol": args.mlp_tol, "table_fallback_fraction": fb / float(cfg.ncell * 3 * (2 * args.steps + args.warmup)),
               "training": rep}
         for k in pd:
@@ -341,7 +355,7 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
         n.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        nsub = 6
+        nsub = 1 if args.workload == "large" else 6
         t = cpu_time_oracle(cfg, fields, tc, nsub)
         out["cpu_baseline"] = {"value": cfg.ncell * nsub / t / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
                                "sample": f"{nsub} substeps of the same workload (oracle, OpenMP, FP64)"}
@@ -401,7 +415,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="heated", choices=["heated", "channel", "ensemble"])
+    ap.add_argument("--workload", default="heated", choices=["heated", "channel", "large", "ensemble"])
     ap.add_argument("--members", type=int, default=48)
     ap.add_argument("--nc", type=int, nargs=3, default=[128, 96, 128])
     ap.add_argument("--iacc", type=int, default=C.IACCU_CD2)

@@ -1818,10 +1818,11 @@ int chs_autotune(chs_handle* H, int nsteps, int* block, int* lt_max, int* fused,
     char* snap = nullptr;
     CK(cudaMalloc(&snap, total));
     snapshot(H, snap, true);
-    const int blocks[3] = {128, 256, 512};
+    // 0: the specialised explicit-operator kernels; 128/256/512: the generic kernel's CTA size
+    const int blocks[4] = {0, 128, 256, 512};
     const bool compact = H->iacc >= 3;
     const int lts[3] = {16, 32, 64};
-    int bb = 256, bl = 64, bf = 0;
+    int bb = 0, bl = 64, bf = 0;
     float best = 1e30f;
     try {
       for (int fu = 0; fu <= 1; ++fu)

@@ -3,6 +3,7 @@
 Launches every kernel individually (no graph replay), so a profiler sees one
 launch per operator.  Example:
     python chapsim2_b200/profile_case.py --nc 128 96 128 --substeps 3
+    python chapsim2_b200/profile_case.py --case heated --precision mixed --mlp-epochs 4
 """
 import argparse
 import os
@@ -22,6 +23,8 @@ def main():
     ap.add_argument("--iacc", type=int, default=C.IACCU_CD2)
     ap.add_argument("--substeps", type=int, default=3)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--mlp-epochs", type=int, default=0,
+                    help="heated case: train the property surrogate for this many epochs and use it")
     a = ap.parse_args()
     tc = None
     if a.case == "channel":
@@ -39,6 +42,9 @@ def main():
     g.set_fields(*f)
     if tc is not None:
         g.thermo_init(tc)
+        if a.mlp_epochs > 0:
+            g.mlp_train(nsamples=200000, batch=4096, epochs=a.mlp_epochs, lr=3e-3, seed=7)
+            g.mlp_set_mode(1, tol=1e-4)
     g.Solve_momentum_eq(0)
     for i in range(a.substeps):
         g.substep(1 + i % 3)

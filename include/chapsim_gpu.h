@@ -228,8 +228,9 @@ int chs_ensemble_time_steps(chs_ensemble* e, int nsteps, float* ms);
 long long chs_ensemble_kernel_launches(const chs_ensemble* e);
 int chs_ensemble_destroy(chs_ensemble* e);
 
-/* Autotuner: times nsteps RK3 steps for each candidate launch shape (CTA size
- * of the explicit line operators; lines per CTA of the compact-scheme tile;
+/* Autotuner: times nsteps RK3 steps for each candidate launch shape (explicit
+ * line operators: the specialised kernels, block 0, or the generic kernel with
+ * a CTA size of 128/256/512; lines per CTA of the compact-scheme tile;
  * separate operators or fused per-component sums) on this handle, restoring
  * the state after each trial, and keeps the fastest. */
 int chs_autotune(chs_handle* h, int nsteps, int* block, int* lt_max, int* fused, float* best_ms);
