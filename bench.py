@@ -331,8 +331,8 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
     out["forms"] = {"fp64": {"value": value, "ms_per_step": ms_max / args.steps}, "mixed": mixed}
     m.close()
     if tc is not None and not args.no_mlp:
-        # mixed precision + the MLP property update (network trained here on the GPU, per-cell
-        # check against the table at tol, table fallback)
+        # mixed precision + the MLP property update (network trained here on the GPU; its T picks the
+        # table row where each cell's search starts, verified by the table, else a full search)
         n = make_solver(S, cfg, fields, tc, local, S.CHS_MIXED)
         rep = n.mlp_train(nsamples=1000000, batch=8192, epochs=args.mlp_epochs, lr=2e-3, seed=20250101)
         n.mlp_set_mode(1, tol=args.mlp_tol)
@@ -347,7 +347,7 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
         pn = xz_profiles(n, cfg, tc)
         ml = {"value": world * cfg.ncell * sub / (ms_n * 1e-3) / 1e6, "ms_per_step": ms_n / args.steps,
               "speedup_vs_fp64": ms_max / ms_n, "steps_compared": steps_done,
-              "check_tol": args.mlp_tol, "table_fallback_fraction": fb / float(cfg.ncell * 3 * (2 * args.steps + args.warmup)),
+              "t_error_bound": args.mlp_tol, "table_fallback_fraction": fb / float(cfg.ncell * 3 * (2 * args.steps + args.warmup)),
               "training": rep}
         for k in pd:
             ml[f"{k}_mean_profile_rel_l2_vs_fp64"] = float(np.linalg.norm(pn[k] - pd[k]) / np.linalg.norm(pd[k]))
@@ -422,7 +422,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mlp", action="store_true")
     ap.add_argument("--mlp-epochs", type=int, default=200)
-    ap.add_argument("--mlp-tol", type=float, default=1e-4)
+    ap.add_argument("--mlp-tol", type=float, default=2e-3)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

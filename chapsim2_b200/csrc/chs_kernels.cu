@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(256) stencil_win_kernel(const __grid_constant_
   int L, ibase, istride, p0;
   int64_t obase, ostride;
   if (DIR == 1) {
-    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     p0 = (blockIdx.y * blockDim.y + threadIdx.y) * kWin;
     const int k = blockIdx.z;
     if (i >= n1 || p0 >= nout) return;
@@ -521,30 +521,41 @@ __global__ void __launch_bounds__(256) stencil_win_kernel(const __grid_constant_
   }
 }
 
-// x lines (DIR 0): blockDim.y lines per CTA, the expression of each line staged in shared memory
+// x lines (DIR 0): each warp forms a segment of kSeg consecutive outputs of one line from a
+// warp-private shared-memory copy of the input expression over the segment and two values either
+// side (wrapped for periodic lines); boundary rows of non-periodic lines read the input directly
+constexpr int kSeg = 128, kSegHalo = 2, kSegLen = kSeg + 2 * kSegHalo;
 template <typename T, int FAM, int M0, int M1>
-__global__ void __launch_bounds__(256) stencil_xrow_kernel(const __grid_constant__ OpPlan P,
+__global__ void __launch_bounds__(256) stencil_xseg_kernel(const __grid_constant__ OpPlan P,
                                                            const __grid_constant__ LineIOT<T> io,
-                                                           const double* __restrict__ table, int nlines) {
-  extern __shared__ __align__(16) unsigned char xrow_smem[];
-  T* row = reinterpret_cast<T*>(xrow_smem) + threadIdx.y * P.nin;
+                                                           const double* __restrict__ table, int nlines, int nseg) {
+  __shared__ T tile[8][kSegLen];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * 8 + warp;  // global warp = line * nseg + segment
+  if (gw >= nlines * nseg) return;
+  const int L = gw / nseg, i0 = (gw - L * nseg) * kSeg;
   const int nin = P.nin, nout = P.nout;
-  const int L = blockIdx.x * blockDim.y + threadIdx.y;
-  const bool live = L < nlines;
   const int ibase = L * nin;
-  if (live)
-    for (int x = threadIdx.x; x < nin; x += blockDim.x) row[x] = expr_ro<M0, M1>(io, ibase + x);
-  __syncthreads();
-  if (!live) return;
-  const T r1 = T(P.r1), r2 = T(P.r2), dd = T(P.dd);
   const bool wrap = P.wrap != 0;
-  auto f = [&](int qq) -> T { return row[qq]; };
-  auto fw = [&](int qq) -> T { return row[qq < 0 ? qq + nin : (qq >= nin ? qq - nin : qq)]; };
+  T* s = tile[warp];
+  for (int t = lane; t < kSegLen; t += 32) {
+    int q = i0 - kSegHalo + t;
+    // lines shorter than the segment wrap more than once
+    if (wrap) q = ((q % nin) + nin) % nin;
+    else q = q < 0 ? 0 : (q >= nin ? nin - 1 : q);  // clamped slots are read by boundary rows only
+    s[t] = expr_ro<M0, M1>(io, ibase + q);
+  }
+  __syncwarp();
+  const T r1 = T(P.r1), r2 = T(P.r2), dd = T(P.dd);
+  auto fs = [&](int qq) -> T { return s[qq - i0 + kSegHalo]; };
+  auto f = [&](int qq) -> T { return expr_ro<M0, M1>(io, ibase + qq); };
   const int64_t obase = (int64_t)L * nout;
-  for (int p = threadIdx.x; p < nout; p += blockDim.x) {
+#pragma unroll
+  for (int m = 0; m < kSeg / 32; ++m) {
+    const int p = i0 + lane + 32 * m;
+    if (p >= nout) break;
     T v;
-    if (wrap) v = bulk_fn<FAM>(fw, p, r1, r2) * dd;
-    else if (p >= P.b_lo && p <= P.b_hi) v = bulk_fn<FAM>(f, p, r1, r2) * dd;
+    if (wrap || (p >= P.b_lo && p <= P.b_hi)) v = bulk_fn<FAM>(fs, p, r1, r2) * dd;
     else v = boundary_row(P, io, f, p, L, nlines);
     finish_row(P, io, table, p, L, nlines, obase + p, v);
   }
@@ -553,15 +564,16 @@ __global__ void __launch_bounds__(256) stencil_xrow_kernel(const __grid_constant
 template <typename T, int DIR, int FAM, int M0, int M1>
 static void launch_win(const OpPlan& P, const LineIOT<T>& io, const double* table, cudaStream_t st, int nlines) {
   if (DIR == 0) {
-    const int rows = 2;
-    const size_t shm = (size_t)rows * P.nin * sizeof(T);
-    dim3 grid((unsigned)((nlines + rows - 1) / rows));
-    stencil_xrow_kernel<T, FAM, M0, M1><<<grid, dim3(128, rows), shm, st>>>(P, io, table, nlines);
+    const int nseg = (P.nout + kSeg - 1) / kSeg;
+    const int64_t warps = (int64_t)nlines * nseg;
+    if (warps >= 0x7fffffff) throw std::runtime_error("explicit operator: too many line segments");
+    stencil_xseg_kernel<T, FAM, M0, M1><<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(P, io, table, nlines, nseg);
   } else if (DIR == 1) {
-    const int by = 8;
+    // wide rows of x per warp group (contiguous DRAM segments), the rest of the CTA along y
+    const int bx = io.n1 >= 128 ? 128 : (io.n1 >= 64 ? 64 : 32), by = 256 / bx;
     const int chunks = (P.nout + kWin - 1) / kWin;
-    dim3 grid((unsigned)((io.n1 + 31) / 32), (unsigned)((chunks + by - 1) / by), (unsigned)io.n3);
-    stencil_win_kernel<T, 1, FAM, M0, M1><<<grid, dim3(32, by), 0, st>>>(P, io, table, nlines);
+    dim3 grid((unsigned)((io.n1 + bx - 1) / bx), (unsigned)((chunks + by - 1) / by), (unsigned)io.n3);
+    stencil_win_kernel<T, 1, FAM, M0, M1><<<grid, dim3(bx, by), 0, st>>>(P, io, table, nlines);
   } else {
     const int plane = io.n1 * io.n2;
     dim3 grid((unsigned)((plane + 255) / 256), (unsigned)((P.nout + kWin - 1) / kWin));
@@ -574,7 +586,6 @@ static void launch_win(const OpPlan& P, const LineIOT<T>& io, const double* tabl
 template <typename T, int DIR>
 static bool try_launch_win(const OpPlan& P, const LineIOT<T>& io, const double* table, cudaStream_t st,
                            int nlines) {
-  if (DIR == 0 && (size_t)2 * P.nin * sizeof(T) > 48 * 1024) return false;
   const int m0 = io.t[0].mode, m1 = io.t[1].mode;
   const int sig = m0 * 8 + m1;
 #define CHS_WIN(F, A, B)                                        \
@@ -1448,11 +1459,15 @@ template <typename T>
 __global__ void weighted_partial_kernel(const T* __restrict__ a, const double* __restrict__ wy, int n1, int n2,
                                         int n3, double* __restrict__ partial) {
   __shared__ double red[256];
-  const int64_t n = (int64_t)n1 * n2 * n3;
+  // rows (j, k) in turn, two per CTA pass (threadIdx.x / 128), x strided by 128 within a row
+  const int nrow = n2 * n3, half = threadIdx.x >> 7, tx = threadIdx.x & 127;
   double acc = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int j = (int)((i / n1) % n2);
-    acc += (double)a[i] * wy[j];
+  for (int r = blockIdx.x * 2 + half; r < nrow; r += gridDim.x * 2) {
+    const double w = wy[r % n2];
+    const T* row = a + (int64_t)r * n1;
+    double s = 0.0;
+    for (int i = tx; i < n1; i += 128) s += (double)row[i];
+    acc += s * w;
   }
   red[threadIdx.x] = acc;
   __syncthreads();

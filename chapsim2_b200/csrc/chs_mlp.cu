@@ -340,47 +340,40 @@ __global__ void __launch_bounds__(128) mlp_props_kernel(
       for (int o = 0; o < 64; ++o) s = fmaf(sm.w4[j * 64 + o], acc[o], s);
       y[j] = nm.ya[j] * (double)s + nm.yb[j];
     }
-    bool use_net = valid && rh >= tb.dhmin && rh <= tb.dhmax;
-    if (use_net) {
-      double chk;
-      if (ck.uniform_t) {
+    // the network's T selects the table row where the rho*h search starts; the table judges it
+    // exactly (the search from that row is verified, else it runs from scratch), so the stored
+    // properties are always the table lookup's
+    bool fb = false;
+    if (valid && !ck.raw) {
+      int hint = -1;
+      if (ck.win < 0) {
+        // no hint: the full table search for every cell
+      } else if (ck.uniform_t) {
         const double f = (y[0] - ck.t0) / ck.dt_tab;
-        if (!(f >= 0.0 && f <= (double)(tb.n - 1))) {
-          use_net = false;
-          chk = 0.0;
-        } else {
-          int i = (int)f;
-          if (i > tb.n - 2) i = tb.n - 2;
-          const double w = f - (double)i;
-          chk = (1.0 - w) * __ldg(tb.rhoh + i) + w * __ldg(tb.rhoh + i + 1);
-        }
-      } else {
+        if (f >= 0.0 && f <= (double)(tb.n - 1)) hint = (int)f;
+      } else if (y[0] >= __ldg(tb.t) && y[0] <= __ldg(tb.t + tb.n - 1)) {
         int i1, i2;
         double w1;
         tab_bracket(tb.t, tb.n, y[0], i1, i2, w1);
-        chk = w1 * __ldg(tb.rhoh + i1) + (1.0 - w1) * __ldg(tb.rhoh + i2);
+        hint = i1;
       }
-      if (use_net) use_net = fabs(chk - rh) <= ck.tol * (tb.dhmax - tb.dhmin);
+      bool hit = false;
+      const CellProps p = props_from_dh(tb, rh, hint, ck.win, &hit);
+      fb = !hit;
+      h[c] = T(p.h);
+      t[c] = T(p.t);
+      k[c] = T(p.k);
+      d[c] = T(p.d);
+      m[c] = T(p.m);
+    } else if (valid) {
+      h[c] = T(rh / y[1]);
+      t[c] = T(y[0]);
+      d[c] = T(y[1]);
+      m[c] = T(y[2]);
+      k[c] = T(y[3]);
     }
-    const bool fb = valid && !use_net;
     const unsigned mask = __ballot_sync(0xffffffffu, fb);
     if (lane == 0 && mask) atomicAdd(nfallback, (unsigned long long)__popc(mask));
-    if (valid) {
-      if (use_net) {
-        h[c] = T(rh / y[1]);
-        t[c] = T(y[0]);
-        d[c] = T(y[1]);
-        m[c] = T(y[2]);
-        k[c] = T(y[3]);
-      } else {
-        const CellProps p = props_from_dh(tb, rh);
-        h[c] = T(p.h);
-        t[c] = T(p.t);
-        k[c] = T(p.k);
-        d[c] = T(p.d);
-        m[c] = T(p.m);
-      }
-    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();

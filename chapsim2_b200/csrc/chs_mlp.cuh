@@ -28,8 +28,11 @@ struct MlpSmall {
 };
 
 struct MlpCheck {
-  double tol;        // accept the network when |rho*h(T_net) - rho*h| <= tol * (dhmax - dhmin)
-  int uniform_t;     // the table's T column is uniform (O(1) check), else bisection on T
+  double tol;        // error bound on the network's T, as a fraction of the table's T range
+  int win;           // the same bound in table rows: the rho*h bracket is searched within +-win rows
+                     // of the row the network's T gives, else from scratch (fallback)
+  int raw;           // 1: the network's outputs as they are (no table; tests of the network)
+  int uniform_t;     // the table's T column is uniform (O(1) row from T), else bisection on T
   double t0, dt_tab;
 };
 

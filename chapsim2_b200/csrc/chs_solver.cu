@@ -1359,6 +1359,14 @@ void thermo_fill_t(chs_handle* H, const HostFtp& f, double t_ini) {
   run_op(H, 2, M1C2P, per, any, src(A(H->dDens)), s_ccc, A(H->gz), false, 1.0, O_MUL, A(H->qz));
 }
 
+// error bound of the network's T (fraction of the table's T range) and the same bound in table rows;
+// tol = 0: no network hint (every cell searches the table from scratch)
+void set_mlp_tol(MlpCheck& ck, double tol, int n) {
+  ck.tol = tol;
+  ck.raw = 0;
+  ck.win = tol > 0.0 ? std::max(1, (int)std::ceil(tol * (n - 1))) : -1;
+}
+
 void thermo_init(chs_handle* H, const chs_thermo* c) {
   if (H->periodic_y) throw std::invalid_argument("variable properties need the channel (y walls)");
   for (int v = V_QX; v <= V_QZ; ++v)
@@ -1443,7 +1451,7 @@ void thermo_init(chs_handle* H, const chs_thermo* c) {
     double dev = 0.0;
     for (int i = 0; i < n; ++i) dev = std::max(dev, std::fabs(c->t[i] - (ck.t0 + i * ck.dt_tab)));
     ck.uniform_t = dev <= 1e-9 * (c->t[n - 1] - c->t[0]) ? 1 : 0;
-    ck.tol = 1.0e-4;
+    set_mlp_tol(ck, 1.0e-4, n);
   }
   const size_t nc = H->n_ccc;
   for (double** p : {&H->rhoh, &H->hEnth, &H->tTemp, &H->kCond, &H->dDens, &H->mVisc, &H->erhs, &H->erhs0,
@@ -1584,7 +1592,8 @@ void mlp_eval(chs_handle* H, int n, const double* rhoh, double tol, double* out,
   CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
   CK(cudaMemcpyAsync(d, rhoh, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st));
   MlpCheck ck = H->mlp_check;
-  ck.tol = tol < 0.0 ? 1.0e300 : tol;
+  if (tol < 0.0) ck.raw = 1;
+  else set_mlp_tol(ck, tol, H->tab.n);
   double *t = d + n, *rho = d + 2 * (size_t)n, *mu = d + 3 * (size_t)n, *ka = d + 4 * (size_t)n, *h = d + 5 * (size_t)n;
   launch_mlp_props<double>(H->tab, H->mlp_norm, H->mlp_small, ck, H->mlp_wpack, d, h, t, ka, rho, mu, n, cnt, st);
   H->launches++;
@@ -2025,7 +2034,10 @@ int chs_mlp_set_mode(chs_handle* H, int mode, double tol) {
   if (!H || mode < 0 || mode > 1) return CHS_ERR_ARG;
   return guard(H, [&] {
     if (mode == 1 && !H->mlp_ready) throw std::invalid_argument("the MLP surrogate is not trained");
-    if (tol > 0.0) H->mlp_check.tol = tol;
+    if (tol > 0.0 && tol != H->mlp_check.tol) {
+      set_mlp_tol(H->mlp_check, tol, H->tab.n);
+      drop_graphs(H);  // the captured launches hold the check by value
+    }
     if (mode != H->mlp_mode) drop_graphs(H);
     H->mlp_mode = mode;
     if (H->mlp_nfb) CK(cudaMemsetAsync(H->mlp_nfb, 0, sizeof(unsigned long long), H->st));

@@ -39,24 +39,50 @@ __device__ __forceinline__ void tab_bracket_ix(const ThermoTab& tb, int c, const
   tab_bracket_from(col, a, b, x, i1, i2, w1);
 }
 
+// Search of a strictly increasing column started near row r: bisection from (r - w, r + w + 1)
+// when that range holds x.  Where x lies more than kBracketMargin from both ends of the bracket
+// found, every node of the column is that far from x, so each sign test of the full search
+// ((col[a]-x)*(col[m]-x) > 1e-20) takes the ordinary bisection branch and the full search ends in
+// the same bracket: the result is then exactly the full search's.  false: not verified (the
+// caller runs the full search).
+constexpr double kBracketMargin = 2.0e-10;
+__device__ __forceinline__ bool tab_bracket_near(const double* __restrict__ col, int n, int r, int w, double x,
+                                                 int& i1, int& i2, double& w1) {
+  int a = r - w, b = r + w + 1;
+  if (a < 0) a = 0;
+  if (b > n - 1) b = n - 1;
+  if (a >= b || !(__ldg(col + a) < x && x < __ldg(col + b))) return false;
+  tab_bracket_from(col, a, b, x, i1, i2, w1);
+  return (x - __ldg(col + i1)) > kBracketMargin && (__ldg(col + i2) - x) > kBracketMargin;
+}
+
 struct CellProps {
   double h, t, k, d, m;
 };
 
-__device__ __forceinline__ CellProps props_from_dh(const ThermoTab& tb, double rhoh) {
+// Property lookup from rho*h (ftp_refresh_thermal_properties_from_DH): rho*h -> h0 on the rho*h
+// column, h0 -> rho0 on the h column, h = rho*h/rho0, h -> properties on the h column.  hint >= 0:
+// a predicted row of the rho*h bracket (e.g. from the surrogate network's T), tried within
+// +-win rows; *hit tells whether it was verified.  The h-column searches start near the rho*h
+// bracket (the columns share the table's T order).  Every path returns the full search's result.
+__device__ __forceinline__ CellProps props_from_dh(const ThermoTab& tb, double rhoh, int hint = -1, int win = 0,
+                                                   bool* hit = nullptr) {
   if (rhoh < tb.dhmin) rhoh = tb.dhmin;
   else if (rhoh > tb.dhmax) rhoh = tb.dhmax;
   int i1, i2;
   double w1;
-  tab_bracket_ix(tb, 0, tb.rhoh, rhoh, i1, i2, w1);
+  const bool near = hint >= 0 && tab_bracket_near(tb.rhoh, tb.n, hint, win, rhoh, i1, i2, w1);
+  if (hit) *hit = near;
+  if (!near) tab_bracket_ix(tb, 0, tb.rhoh, rhoh, i1, i2, w1);
+  const int r0 = i1;
   double w2 = 1.0 - w1;
   const double h0 = w1 * __ldg(tb.h + i1) + w2 * __ldg(tb.h + i2);
-  tab_bracket_ix(tb, 1, tb.h, h0, i1, i2, w1);
+  if (!tab_bracket_near(tb.h, tb.n, r0, 4, h0, i1, i2, w1)) tab_bracket_ix(tb, 1, tb.h, h0, i1, i2, w1);
   w2 = 1.0 - w1;
   const double d0 = w1 * __ldg(tb.d + i1) + w2 * __ldg(tb.d + i2);
   CellProps p;
   p.h = rhoh / d0;
-  tab_bracket_ix(tb, 1, tb.h, p.h, i1, i2, w1);
+  if (!tab_bracket_near(tb.h, tb.n, r0, 4, p.h, i1, i2, w1)) tab_bracket_ix(tb, 1, tb.h, p.h, i1, i2, w1);
   w2 = 1.0 - w1;
   p.d = w1 * __ldg(tb.d + i1) + w2 * __ldg(tb.d + i2);
   p.m = w1 * __ldg(tb.m + i1) + w2 * __ldg(tb.m + i2);

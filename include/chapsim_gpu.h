@@ -176,10 +176,12 @@ int chs_energy_substep(chs_handle* h, int isub);
  * (src/eq_energy.f90:14-146): a 1 -> 64 -> 64 -> 64 -> 4 tanh network from rho*h
  * to (T, rho, mu, kappa), trained on the GPU by this library's own FP32
  * forward/backward/Adam kernels on seeded samples whose targets are the table
- * lookup, evaluated with BF16 tensor cores (FP32 accumulation).  In mode 1 each
- * cell's prediction is checked against the table (|rho*h(T_net) - rho*h| <=
- * tol * table range) and replaced by the table lookup when the check fails or
- * rho*h is outside the table.  No counterpart in the reference.
+ * lookup, evaluated with BF16 tensor cores (FP32 accumulation).  In mode 1 the
+ * network's T of each cell gives the table row where the rho*h search starts;
+ * the table judges it exactly (a start within tol of the T range that brackets
+ * the cell's rho*h is verified, else the search runs from scratch: the
+ * fallback), so the stored properties equal the table lookup's bit for bit.
+ * No counterpart in the reference.
  */
 typedef struct chs_mlp_train_cfg {
   int nsamples;                /* training samples (e.g. 1000000) */
@@ -196,7 +198,10 @@ typedef struct chs_mlp_report {
 } chs_mlp_report;
 
 int chs_mlp_train(chs_handle* h, const chs_mlp_train_cfg* cfg, chs_mlp_report* rep);
-/* mode 0: table lookups (the reference's method); 1: network with table fallback at tol (> 0 sets it) */
+/* mode 0: table lookups (the reference's method); 1: the network's T picks the table row where the
+ * rho*h search starts, within tol (> 0 sets it) of the table's T range; the table verifies that
+ * start and otherwise searches from scratch (fallback), so the properties are always exactly the
+ * table lookup's */
 int chs_mlp_set_mode(chs_handle* h, int mode, double tol);
 /* cells that took the table fallback since the last chs_mlp_set_mode */
 int chs_mlp_fallbacks(chs_handle* h, unsigned long long* count);
@@ -205,8 +210,9 @@ int chs_mlp_params(chs_handle* h, float* buf, int n, int set);
 /* loss and gradients of the FP32 network for B samples (normalised x[B], targets t[B][4]) */
 int chs_mlp_grad(chs_handle* h, const float* params, int B, const float* x, const float* t, float* grad,
                  float* loss);
-/* tensor-core inference on n host values of rho*h: out[5][n] = T, rho, mu, kappa, h; tol < 0 takes
- * every network value (no fallback); *nfallback = cells that took the table */
+/* tensor-core inference on n host values of rho*h: out[5][n] = T, rho, mu, kappa, h.  tol < 0: the
+ * network's own outputs (no table); tol = 0: the table search alone; tol > 0: as
+ * chs_mlp_set_mode; *nfallback = cells whose network start row was not verified */
 int chs_mlp_eval(chs_handle* h, int n, const double* rhoh, double tol, double* out, unsigned long long* nfallback);
 /* normalisation: out[10] = xa, xb (x = xa*rhoh + xb), ya[4], yb[4] (value = ya*y + yb) */
 int chs_mlp_norm(const chs_handle* h, double* out);

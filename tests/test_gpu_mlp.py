@@ -66,7 +66,10 @@ def test_tensor_core_inference_matches_fp32_network(trained):
         assert e < 2e-2, (j, e)
 
 
-def test_checked_inference_against_table(trained):
+def test_network_start_rows_judged_by_table(trained):
+    """Mode-1 inference: the network's T picks the row where the table search starts and the table
+    verifies it, so every output is the table lookup's; a wider error bound lets more starts
+    through (fewer fallbacks)."""
     cfg, tc, g, rep = trained
     o = po.Oracle(cfg)
     o.set_fields(*I.channel_fields(cfg))
@@ -75,26 +78,26 @@ def test_checked_inference_against_table(trained):
     rh_tab = tb["d"] * tb["h"]
     rng = np.random.default_rng(9)
     rh = rng.uniform(rh_tab.min(), rh_tab.max(), 20000)
-    tol = 1e-4
-    out, nfb = g.mlp_eval(rh, tol=tol)
     h, T, d, m, k, cp = o.ftp_from_dh(rh)
-    # every accepted cell satisfies the check; every rejected one is the table value
-    chk = np.interp(out[0], tb["t"], rh_tab)
-    exact = np.abs(out[0] - T) < 1e-12
-    acc = ~exact
-    assert np.all(np.abs(chk[acc] - rh[acc]) <= tol * (rh_tab.max() - rh_tab.min()) * (1 + 1e-9))
-    assert nfb >= np.count_nonzero(exact) - 5
     raw, _ = g.mlp_eval(rh, tol=-1.0)
     e_raw = np.abs(raw[0] - T)
-    e_chk = np.abs(out[0] - T)
-    print(f"T error vs table: raw network max {e_raw.max():.3e} rms {np.sqrt(np.mean(e_raw**2)):.3e}; "
-          f"checked max {e_chk.max():.3e}; fallback {nfb / rh.size:.3f}")
-    assert e_chk.max() <= e_raw.max() + 1e-12
+    fracs = []
+    for tol in (0.0, 1e-4, 1e-3, 1e-2):
+        out, nfb = g.mlp_eval(rh, tol=tol)
+        for name, got, ref in zip(("T", "rho", "mu", "kappa", "h"), out, (T, d, m, k, h)):
+            err = np.max(np.abs(got - ref))
+            assert err <= 1e-13 * (ref.max() - ref.min()), (tol, name, err)
+        fracs.append(nfb / rh.size)
+    print(f"network T error vs table: max {e_raw.max():.3e} rms {np.sqrt(np.mean(e_raw**2)):.3e}; "
+          f"fallback fraction at tol 0, 1e-4, 1e-3, 1e-2: {fracs}")
+    assert fracs[0] == 1.0
+    assert fracs[1] >= fracs[2] >= fracs[3]
+    assert fracs[3] < 0.5
 
 
 def test_network_in_the_time_loop(trained):
-    """Heated-channel substeps with the network property update against the table update: the
-    gain (time per property update) and the cost (error in the mean T profile)."""
+    """Heated-channel steps with the network-started property update give the table update's
+    state bit for bit; the fallback count shows how often the network's start row was right."""
     cfg, tc, g, rep = trained
     f = I.channel_fields(cfg)
     a = S.Solver(cfg)
@@ -108,11 +111,12 @@ def test_network_in_the_time_loop(trained):
         s.Solve_momentum_eq(0)
         s.step(3)
     ta, tb_ = a.get_thermo(), b.get_thermo()
-    sh = cfg.shapes()[3]
-    pa = ta["T"].reshape(sh).mean(axis=(0, 2))
-    pb = tb_["T"].reshape(sh).mean(axis=(0, 2))
-    err = np.linalg.norm(pb - pa) / np.linalg.norm(pa)
-    print(f"mean-T profile rel L2 (network vs table) after 3 steps: {err:.3e}; fallbacks {b.mlp_fallbacks()}")
-    assert err < 1e-3
+    for key in ta:
+        assert np.array_equal(ta[key], tb_[key]), key
+    for x, y in zip(a.get_fields(), b.get_fields()):
+        assert np.array_equal(x, y)
+    nfb = b.mlp_fallbacks()
+    print(f"fallbacks {nfb} of {3 * 3 * cfg.ncell} cell updates")
+    assert 0 <= nfb <= 3 * 3 * cfg.ncell
     a.close()
     b.close()
