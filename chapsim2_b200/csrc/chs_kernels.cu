@@ -437,7 +437,8 @@ __device__ __forceinline__ T bulk_win(const T* w, int b, T r1, T r2) {
   return v;
 }
 
-// one boundary row of the plan (as stencil_op_kernel), input values from f
+// one boundary row of the plan (as stencil_op_kernel), input values from f (out of line it costs
+// more than it saves: the call spills the captured state of f to the stack)
 template <typename T, typename F>
 __device__ __forceinline__ T boundary_row(const OpPlan& P, const LineIOT<T>& io, const F& f, int p, int L,
                                           int nlines) {
@@ -540,9 +541,13 @@ __global__ void __launch_bounds__(256) stencil_xseg_kernel(const __grid_constant
   T* s = tile[warp];
   for (int t = lane; t < kSegLen; t += 32) {
     int q = i0 - kSegHalo + t;
-    // lines shorter than the segment wrap more than once
-    if (wrap) q = ((q % nin) + nin) % nin;
-    else q = q < 0 ? 0 : (q >= nin ? nin - 1 : q);  // clamped slots are read by boundary rows only
+    if (wrap) {
+      // lines shorter than the segment wrap more than once
+      while (q < 0) q += nin;
+      while (q >= nin) q -= nin;
+    } else {
+      q = q < 0 ? 0 : (q >= nin ? nin - 1 : q);  // clamped slots are read by boundary rows only
+    }
     s[t] = expr_ro<M0, M1>(io, ibase + q);
   }
   __syncwarp();

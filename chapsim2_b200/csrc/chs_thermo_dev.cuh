@@ -63,8 +63,9 @@ struct CellProps {
 // Property lookup from rho*h (ftp_refresh_thermal_properties_from_DH): rho*h -> h0 on the rho*h
 // column, h0 -> rho0 on the h column, h = rho*h/rho0, h -> properties on the h column.  hint >= 0:
 // a predicted row of the rho*h bracket (e.g. from the surrogate network's T), tried within
-// +-win rows; *hit tells whether it was verified.  The h-column searches start near the rho*h
-// bracket (the columns share the table's T order).  Every path returns the full search's result.
+// +-win rows; *hit tells whether it was verified
+// (the h-column searches start from the bracket index).  Every path returns the full search's
+// result.
 __device__ __forceinline__ CellProps props_from_dh(const ThermoTab& tb, double rhoh, int hint = -1, int win = 0,
                                                    bool* hit = nullptr) {
   if (rhoh < tb.dhmin) rhoh = tb.dhmin;
@@ -74,15 +75,14 @@ __device__ __forceinline__ CellProps props_from_dh(const ThermoTab& tb, double r
   const bool near = hint >= 0 && tab_bracket_near(tb.rhoh, tb.n, hint, win, rhoh, i1, i2, w1);
   if (hit) *hit = near;
   if (!near) tab_bracket_ix(tb, 0, tb.rhoh, rhoh, i1, i2, w1);
-  const int r0 = i1;
   double w2 = 1.0 - w1;
   const double h0 = w1 * __ldg(tb.h + i1) + w2 * __ldg(tb.h + i2);
-  if (!tab_bracket_near(tb.h, tb.n, r0, 4, h0, i1, i2, w1)) tab_bracket_ix(tb, 1, tb.h, h0, i1, i2, w1);
+  tab_bracket_ix(tb, 1, tb.h, h0, i1, i2, w1);
   w2 = 1.0 - w1;
   const double d0 = w1 * __ldg(tb.d + i1) + w2 * __ldg(tb.d + i2);
   CellProps p;
   p.h = rhoh / d0;
-  if (!tab_bracket_near(tb.h, tb.n, r0, 4, p.h, i1, i2, w1)) tab_bracket_ix(tb, 1, tb.h, p.h, i1, i2, w1);
+  tab_bracket_ix(tb, 1, tb.h, p.h, i1, i2, w1);
   w2 = 1.0 - w1;
   p.d = w1 * __ldg(tb.d + i1) + w2 * __ldg(tb.d + i2);
   p.m = w1 * __ldg(tb.m + i1) + w2 * __ldg(tb.m + i2);

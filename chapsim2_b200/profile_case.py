@@ -25,6 +25,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--mlp-epochs", type=int, default=0,
                     help="heated case: train the property surrogate for this many epochs and use it")
+    ap.add_argument("--graph-profile", action="store_true",
+                    help="after the substeps, print a per-launch profile of substep 1 replayed as a graph")
     a = ap.parse_args()
     tc = None
     if a.case == "channel":
@@ -48,6 +50,13 @@ def main():
     g.Solve_momentum_eq(0)
     for i in range(a.substeps):
         g.substep(1 + i % 3)
+    if a.graph_profile:
+        kinds = ("line_op", "fft", "ysolve", "elementwise")
+        prof = g.profile_substep_graph(1)
+        for i, r in enumerate(prof):
+            print(f"{i:3d} {kinds[r['kind']]:11s} dir {r['dir']:2d} {r['bytes'] / 1e6:9.1f} MB {r['ms'] * 1e3:9.1f} us "
+                  f"{r['bytes'] / r['ms'] / 1e6:7.0f} GB/s")
+        print(f"substep total {sum(r['ms'] for r in prof):.3f} ms over {len(prof)} launches")
     d = g.diagnostics()
     print(f"{a.case} {cfg.nc} iacc={a.iacc}: {a.substeps} substeps, launches={g.kernel_launches()}, "
           f"max_div={d['max_div']:.3e}, nan={d['nan_flag']}")
