@@ -6,7 +6,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libchapsim_gpu.so")
-SOURCES = ["chs_plan.cpp", "chs_kernels.cu", "chs_solver.cu", "chs_static.cu", "chs_mlp.cu"]
+SOURCES = ["chs_plan.cpp", "chs_kernels.cu", "chs_stencil_f64.cu", "chs_stencil_f32.cu", "chs_solver.cu",
+           "chs_static.cu", "chs_mlp.cu"]
+OBJDIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -33,12 +35,26 @@ def needs_build():
 
 
 def build(verbose=False, force=False, extra=()):
-    """Compile all sources into chapsim2_b200/libchapsim_gpu.so."""
+    """Compile the sources (in parallel, one object each) and link chapsim2_b200/libchapsim_gpu.so."""
     if not force and not needs_build():
         return LIB
-    cmd = [_nvcc(), "-ccbin", _host_cxx(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared",
-           "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-o", LIB, *[os.path.join(CSRC, s) for s in SOURCES],
-           "-lcudart", *extra]
+    from concurrent.futures import ThreadPoolExecutor
+
+    os.makedirs(OBJDIR, exist_ok=True)
+    common = [_nvcc(), "-ccbin", _host_cxx(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-Xcompiler", "-O2", *extra]
+
+    def compile_one(src):
+        obj = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".o")
+        cmd = [*common, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
+    cmd = [_nvcc(), "-ccbin", _host_cxx(), *ARCH, "--shared", "-o", LIB, *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

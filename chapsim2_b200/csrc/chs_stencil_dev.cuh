@@ -1,0 +1,59 @@
+// Device helpers shared by the line-operator translation units: output store modes, the bulk
+// stencil of each family, the runtime-mode input expression, and the entry of the specialised
+// explicit-operator kernels (compiled in chs_stencil_f64.cu / chs_stencil_f32.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "chs_kernels.cuh"
+
+namespace chs {
+
+template <typename T>
+__device__ __forceinline__ void store_out(const LineIOT<T>& io, int64_t a, T g, T v) {
+  if (io.omode == O_DIV) io.out[a] = io.onum[a] / (g * v);
+  else if (io.omode == O_MUL) io.out[a] = io.onum[a] * (g * v);
+  else io.out[a] = io.accumulate ? io.out[a] + g * v : g * v;
+}
+
+template <int FAM, typename T, typename F>
+__device__ __forceinline__ T bulk_fn(const F& f, int i, T r1, T r2) {
+  T v;
+  if (FAM == M1P2C) v = r1 * (f(i) + f(i + 1));
+  else if (FAM == M1C2P) v = r1 * (f(i) + f(i - 1));
+  else if (FAM == D1C2C || FAM == D1P2P) v = r1 * (f(i + 1) - f(i - 1));
+  else if (FAM == D1C2P) v = r1 * (f(i) - f(i - 1));
+  else v = r1 * (f(i + 1) - f(i));  // D1P2C
+  if (r2 != T(0)) {
+    if (FAM == M1P2C) v += r2 * (f(i - 1) + f(i + 2));
+    else if (FAM == M1C2P) v += r2 * (f(i + 1) + f(i - 2));
+    else if (FAM == D1C2C || FAM == D1P2P) v += r2 * (f(i + 2) - f(i - 2));
+    else if (FAM == D1C2P) v += r2 * (f(i + 1) - f(i - 2));
+    else v += r2 * (f(i + 2) - f(i - 1));
+  }
+  return v;
+}
+
+// int32-offset evaluation of the input expression (arrays below 2^31 values)
+template <typename T>
+__device__ __forceinline__ T eval_term32(const TermT<T>& t, int a) {
+  switch (t.mode) {
+    case T_X: return T(t.s) * t.X[a];
+    case T_XY: return T(t.s) * (t.X[a] * t.Y[a]);
+    case T_XpY: return T(t.s) * (t.X[a] + T(t.c) * t.Y[a]);
+    case T_XpYZ: return T(t.s) * (t.X[a] + T(t.c) * t.Y[a]) * t.Z[a];
+    default: return T(0);
+  }
+}
+template <typename T>
+__device__ __forceinline__ T eval_expr32(const LineIOT<T>& io, int a) {
+  T v = eval_term32(io.t[0], a);
+  if (io.t[1].mode != T_NONE) v += eval_term32(io.t[1], a);
+  return v;
+}
+
+// specialised explicit operators for the expression signatures the substep forms; false: the
+// caller runs the generic stencil_op_kernel
+template <typename T, int DIR>
+bool try_launch_win(const OpPlan& P, const LineIOT<T>& io, const double* table, cudaStream_t st, int nlines);
+
+}  // namespace chs

@@ -1,0 +1,254 @@
+// Specialised explicit line operators (see chs_stencil_dev.cuh); included once per field type by
+// chs_stencil_f64.cu and chs_stencil_f32.cu with CHS_STENCIL_T defined.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+
+#include "chs_stencil_dev.cuh"
+
+namespace chs {
+
+// ---------------------------------------------------------------------------
+// Explicit operators, specialised: the input expression's term modes are template parameters
+// (read-only loads, no per-value mode switch) and no integer division maps threads to positions.
+//  * y and z lines: each thread forms kWin consecutive outputs of one line from a register window
+//    of the input expression (each input value loaded once per thread instead of once per stencil
+//    point);
+//  * x lines (contiguous): the expression of a whole line is staged in shared memory, then every
+//    output row (bulk, wrapped bulk or boundary row) reads it from there.
+// Rows outside the bulk range evaluate the plan's boundary rows exactly as stencil_op_kernel does.
+// ---------------------------------------------------------------------------
+constexpr int kWin = 4;
+
+template <int M, typename T>
+__device__ __forceinline__ T term_ro(const TermT<T>& t, int a) {
+  if (M == T_X) return T(t.s) * __ldg(t.X + a);
+  if (M == T_XY) return T(t.s) * (__ldg(t.X + a) * __ldg(t.Y + a));
+  if (M == T_XpY) return T(t.s) * (__ldg(t.X + a) + T(t.c) * __ldg(t.Y + a));
+  if (M == T_XpYZ) return T(t.s) * (__ldg(t.X + a) + T(t.c) * __ldg(t.Y + a)) * __ldg(t.Z + a);
+  return T(0);
+}
+template <int M0, int M1, typename T>
+__device__ __forceinline__ T expr_ro(const LineIOT<T>& io, int a) {
+  T v = term_ro<M0>(io.t[0], a);
+  if (M1 != T_NONE) v += term_ro<M1>(io.t[1], a);
+  return v;
+}
+
+// stencil reach of a family: offsets [lo4, hi4] of the 4-point (r2 != 0) bulk formula and
+// [lo2, hi2] of its 2-point part
+template <int FAM>
+struct Reach {
+  static constexpr int lo4 = (FAM == M1P2C || FAM == D1P2C) ? -1 : -2;
+  static constexpr int hi4 = (FAM == M1C2P || FAM == D1C2P) ? 1 : 2;
+  static constexpr int lo2 = (FAM == M1P2C || FAM == D1P2C) ? 0 : -1;
+  static constexpr int hi2 = (FAM == M1C2P || FAM == D1C2P) ? 0 : 1;
+};
+
+// bulk_fn on a register window: w[b + o] holds the expression at offset o of the output row
+template <int FAM, typename T>
+__device__ __forceinline__ T bulk_win(const T* w, int b, T r1, T r2) {
+  T v;
+  if (FAM == M1P2C) v = r1 * (w[b] + w[b + 1]);
+  else if (FAM == M1C2P) v = r1 * (w[b] + w[b - 1]);
+  else if (FAM == D1C2C || FAM == D1P2P) v = r1 * (w[b + 1] - w[b - 1]);
+  else if (FAM == D1C2P) v = r1 * (w[b] - w[b - 1]);
+  else v = r1 * (w[b + 1] - w[b]);  // D1P2C
+  if (r2 != T(0)) {
+    if (FAM == M1P2C) v += r2 * (w[b - 1] + w[b + 2]);
+    else if (FAM == M1C2P) v += r2 * (w[b + 1] + w[b - 2]);
+    else if (FAM == D1C2C || FAM == D1P2P) v += r2 * (w[b + 2] - w[b - 2]);
+    else if (FAM == D1C2P) v += r2 * (w[b + 1] - w[b - 2]);
+    else v += r2 * (w[b + 2] - w[b - 1]);
+  }
+  return v;
+}
+
+// one boundary row of the plan (as stencil_op_kernel), input values from f (out of line it costs
+// more than it saves: the call spills the captured state of f to the stack)
+template <typename T, typename F>
+__device__ __forceinline__ T boundary_row(const OpPlan& P, const LineIOT<T>& io, const F& f, int p, int L,
+                                          int nlines) {
+  T v = T(0);
+  for (int s = 0; s < P.nspec; ++s) {
+    if (P.sp[s].row != p) continue;
+    const SpecialRow& R = P.sp[s];
+    T acc = T(0);
+    for (int t = 0; t < R.nt; ++t) acc += T(R.w[t]) * f(R.idx[t]);
+    for (int u = 0; u < 4; ++u)
+      if (R.wb[u] != 0.0) acc += T(R.wb[u]) * io.fbc[u * nlines + L];
+    v = acc * T(P.dd);
+  }
+  return v;
+}
+
+// y metric, Neumann overrides and the store mode (as stencil_op_kernel)
+template <typename T>
+__device__ __forceinline__ void finish_row(const OpPlan& P, const LineIOT<T>& io, const double* __restrict__ table,
+                                           int p, int L, int nlines, int64_t a, T v) {
+  if (P.lmap >= 0) v *= T(table[P.lmap + p]);
+  if (P.neu1 && p == 0) v = io.fbc[L];
+  if (P.neu2 && p == P.nout - 1) v = io.fbc[nlines + L];
+  store_out(io, a, T(io.g), v);
+}
+
+// y (DIR 1) or z (DIR 2) lines: thread = (position in the cross plane, chunk of kWin rows)
+template <typename T, int DIR, int FAM, int M0, int M1>
+__global__ void __launch_bounds__(256) stencil_win_kernel(const __grid_constant__ OpPlan P,
+                                                          const __grid_constant__ LineIOT<T> io,
+                                                          const double* __restrict__ table, int nlines) {
+  using RC = Reach<FAM>;
+  constexpr int W = kWin + RC::hi4 - RC::lo4;
+  const int nin = P.nin, nout = P.nout, n1 = io.n1;
+  int L, ibase, istride, p0;
+  int64_t obase, ostride;
+  if (DIR == 1) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    p0 = (blockIdx.y * blockDim.y + threadIdx.y) * kWin;
+    const int k = blockIdx.z;
+    if (i >= n1 || p0 >= nout) return;
+    L = i + n1 * k;
+    ibase = k * nin * n1 + i;
+    istride = n1;
+    obase = (int64_t)k * nout * n1 + i;
+    ostride = n1;
+  } else {
+    const int plane = n1 * io.n2;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    p0 = blockIdx.y * kWin;
+    if (q >= plane) return;
+    L = q;
+    ibase = q;
+    istride = plane;
+    obase = q;
+    ostride = plane;
+  }
+  const T r1 = T(P.r1), r2 = T(P.r2), dd = T(P.dd);
+  const bool r2on = P.r2 != 0.0, wrap = P.wrap != 0;
+  T w[W];
+#pragma unroll
+  for (int s = 0; s < W; ++s) {
+    // the 2-point formula never reads the outermost slots
+    const bool need = r2on || (s >= RC::lo2 - RC::lo4 && s <= kWin - 1 + RC::hi2 - RC::lo4);
+    int q = p0 + RC::lo4 + s;
+    // wrapped (periodic) or clamped; clamped slots are read only by boundary rows, which do not
+    // use the window
+    if (wrap) q = q < 0 ? q + nin : (q >= nin ? q - nin : q);
+    else q = q < 0 ? 0 : (q >= nin ? nin - 1 : q);
+    w[s] = need ? expr_ro<M0, M1>(io, ibase + q * istride) : T(0);
+  }
+  auto f = [&](int qq) -> T { return expr_ro<M0, M1>(io, ibase + qq * istride); };
+#pragma unroll
+  for (int u = 0; u < kWin; ++u) {
+    const int p = p0 + u;
+    if (p >= nout) break;
+    T v;
+    if (wrap || (p >= P.b_lo && p <= P.b_hi)) v = bulk_win<FAM>(w, u - RC::lo4, r1, r2) * dd;
+    else v = boundary_row(P, io, f, p, L, nlines);
+    finish_row(P, io, table, p, L, nlines, obase + (int64_t)p * ostride, v);
+  }
+}
+
+// x lines (DIR 0): each warp forms a segment of kSeg consecutive outputs of one line from a
+// warp-private shared-memory copy of the input expression over the segment and two values either
+// side (wrapped for periodic lines); boundary rows of non-periodic lines read the input directly
+constexpr int kSeg = 128, kSegHalo = 2, kSegLen = kSeg + 2 * kSegHalo;
+template <typename T, int FAM, int M0, int M1>
+__global__ void __launch_bounds__(256) stencil_xseg_kernel(const __grid_constant__ OpPlan P,
+                                                           const __grid_constant__ LineIOT<T> io,
+                                                           const double* __restrict__ table, int nlines, int nseg) {
+  __shared__ T tile[8][kSegLen];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * 8 + warp;  // global warp = line * nseg + segment
+  if (gw >= nlines * nseg) return;
+  const int L = gw / nseg, i0 = (gw - L * nseg) * kSeg;
+  const int nin = P.nin, nout = P.nout;
+  const int ibase = L * nin;
+  const bool wrap = P.wrap != 0;
+  T* s = tile[warp];
+  for (int t = lane; t < kSegLen; t += 32) {
+    int q = i0 - kSegHalo + t;
+    if (wrap) {
+      // lines shorter than the segment wrap more than once
+      while (q < 0) q += nin;
+      while (q >= nin) q -= nin;
+    } else {
+      q = q < 0 ? 0 : (q >= nin ? nin - 1 : q);  // clamped slots are read by boundary rows only
+    }
+    s[t] = expr_ro<M0, M1>(io, ibase + q);
+  }
+  __syncwarp();
+  const T r1 = T(P.r1), r2 = T(P.r2), dd = T(P.dd);
+  auto fs = [&](int qq) -> T { return s[qq - i0 + kSegHalo]; };
+  auto f = [&](int qq) -> T { return expr_ro<M0, M1>(io, ibase + qq); };
+  const int64_t obase = (int64_t)L * nout;
+#pragma unroll
+  for (int m = 0; m < kSeg / 32; ++m) {
+    const int p = i0 + lane + 32 * m;
+    if (p >= nout) break;
+    T v;
+    if (wrap || (p >= P.b_lo && p <= P.b_hi)) v = bulk_fn<FAM>(fs, p, r1, r2) * dd;
+    else v = boundary_row(P, io, f, p, L, nlines);
+    finish_row(P, io, table, p, L, nlines, obase + p, v);
+  }
+}
+
+template <typename T, int DIR, int FAM, int M0, int M1>
+void launch_win(const OpPlan& P, const LineIOT<T>& io, const double* table, cudaStream_t st, int nlines) {
+  if (DIR == 0) {
+    const int nseg = (P.nout + kSeg - 1) / kSeg;
+    const int64_t warps = (int64_t)nlines * nseg;
+    if (warps >= 0x7fffffff) throw std::runtime_error("explicit operator: too many line segments");
+    stencil_xseg_kernel<T, FAM, M0, M1><<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(P, io, table, nlines, nseg);
+  } else if (DIR == 1) {
+    // wide rows of x per warp group (contiguous DRAM segments), the rest of the CTA along y
+    const int bx = io.n1 >= 128 ? 128 : (io.n1 >= 64 ? 64 : 32), by = 256 / bx;
+    const int chunks = (P.nout + kWin - 1) / kWin;
+    dim3 grid((unsigned)((io.n1 + bx - 1) / bx), (unsigned)((chunks + by - 1) / by), (unsigned)io.n3);
+    stencil_win_kernel<T, 1, FAM, M0, M1><<<grid, dim3(bx, by), 0, st>>>(P, io, table, nlines);
+  } else {
+    const int plane = io.n1 * io.n2;
+    dim3 grid((unsigned)((plane + 255) / 256), (unsigned)((P.nout + kWin - 1) / kWin));
+    stencil_win_kernel<T, 2, FAM, M0, M1><<<grid, 256, 0, st>>>(P, io, table, nlines);
+  }
+}
+
+// the specialised kernels cover the interpolations of single arrays and the derivative inputs the
+// substep forms (products, linear combinations, their sums); false: use stencil_op_kernel
+template <typename T, int DIR>
+bool try_launch_win(const OpPlan& P, const LineIOT<T>& io, const double* table, cudaStream_t st,
+                           int nlines) {
+  const int m0 = io.t[0].mode, m1 = io.t[1].mode;
+  const int sig = m0 * 8 + m1;
+#define CHS_WIN(F, A, B)                                        \
+  if (P.fam == F && sig == A * 8 + B) {                         \
+    launch_win<T, DIR, F, A, B>(P, io, table, st, nlines);      \
+    return true;                                                \
+  }
+  CHS_WIN(M1P2C, T_X, T_NONE)
+  CHS_WIN(M1C2P, T_X, T_NONE)
+#define CHS_WIN_D(F)                 \
+  CHS_WIN(F, T_X, T_NONE)            \
+  CHS_WIN(F, T_XY, T_NONE)           \
+  CHS_WIN(F, T_XpY, T_NONE)          \
+  CHS_WIN(F, T_XpYZ, T_NONE)         \
+  CHS_WIN(F, T_XY, T_XpY)            \
+  CHS_WIN(F, T_XY, T_XpYZ)           \
+  CHS_WIN(F, T_XY, T_XY)
+  CHS_WIN_D(D1C2P)
+  CHS_WIN_D(D1P2C)
+#undef CHS_WIN_D
+#undef CHS_WIN
+  return false;
+}
+
+
+template bool try_launch_win<CHS_STENCIL_T, 0>(const OpPlan&, const LineIOT<CHS_STENCIL_T>&, const double*, cudaStream_t,
+                                               int);
+template bool try_launch_win<CHS_STENCIL_T, 1>(const OpPlan&, const LineIOT<CHS_STENCIL_T>&, const double*, cudaStream_t,
+                                               int);
+template bool try_launch_win<CHS_STENCIL_T, 2>(const OpPlan&, const LineIOT<CHS_STENCIL_T>&, const double*, cudaStream_t,
+                                               int);
+
+}  // namespace chs
