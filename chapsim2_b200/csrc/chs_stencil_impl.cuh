@@ -65,17 +65,17 @@ __device__ __forceinline__ T bulk_win(const T* w, int b, T r1, T r2) {
   return v;
 }
 
-// one boundary row of the plan (as stencil_op_kernel), input values from f (out of line it costs
-// more than it saves: the call spills the captured state of f to the stack)
-template <typename T, typename F>
-__device__ __forceinline__ T boundary_row(const OpPlan& P, const LineIOT<T>& io, const F& f, int p, int L,
-                                          int nlines) {
+// one boundary row of the plan (as stencil_op_kernel), input expression at ibase + q * istride
+// (a call out of line measured slower than the registers it saves)
+template <typename T, int M0, int M1>
+__device__ __forceinline__ T boundary_row(const OpPlan& P, const LineIOT<T>& io, int ibase, int istride, int p, int L,
+                                       int nlines) {
   T v = T(0);
   for (int s = 0; s < P.nspec; ++s) {
     if (P.sp[s].row != p) continue;
     const SpecialRow& R = P.sp[s];
     T acc = T(0);
-    for (int t = 0; t < R.nt; ++t) acc += T(R.w[t]) * f(R.idx[t]);
+    for (int t = 0; t < R.nt; ++t) acc += T(R.w[t]) * expr_ro<M0, M1>(io, ibase + R.idx[t] * istride);
     for (int u = 0; u < 4; ++u)
       if (R.wb[u] != 0.0) acc += T(R.wb[u]) * io.fbc[u * nlines + L];
     v = acc * T(P.dd);
@@ -138,14 +138,13 @@ __global__ void __launch_bounds__(256) stencil_win_kernel(const __grid_constant_
     else q = q < 0 ? 0 : (q >= nin ? nin - 1 : q);
     w[s] = need ? expr_ro<M0, M1>(io, ibase + q * istride) : T(0);
   }
-  auto f = [&](int qq) -> T { return expr_ro<M0, M1>(io, ibase + qq * istride); };
 #pragma unroll
   for (int u = 0; u < kWin; ++u) {
     const int p = p0 + u;
     if (p >= nout) break;
     T v;
     if (wrap || (p >= P.b_lo && p <= P.b_hi)) v = bulk_win<FAM>(w, u - RC::lo4, r1, r2) * dd;
-    else v = boundary_row(P, io, f, p, L, nlines);
+    else v = boundary_row<T, M0, M1>(P, io, ibase, istride, p, L, nlines);
     finish_row(P, io, table, p, L, nlines, obase + (int64_t)p * ostride, v);
   }
 }
@@ -167,21 +166,34 @@ __global__ void __launch_bounds__(256) stencil_xseg_kernel(const __grid_constant
   const int ibase = L * nin;
   const bool wrap = P.wrap != 0;
   T* s = tile[warp];
-  for (int t = lane; t < kSegLen; t += 32) {
-    int q = i0 - kSegHalo + t;
+  // the segment: no wrap or clamp unless it runs past the end of the line
+  const bool full = i0 + kSeg <= nin;
+#pragma unroll
+  for (int m = 0; m < kSeg / 32; ++m) {
+    int q = i0 + lane + 32 * m;
+    if (!full) {
+      if (wrap) {
+        while (q >= nin) q -= nin;  // lines shorter than a segment wrap more than once
+      } else {
+        q = q >= nin ? nin - 1 : q;  // clamped slots are read by boundary rows only
+      }
+    }
+    s[kSegHalo + lane + 32 * m] = expr_ro<M0, M1>(io, ibase + q);
+  }
+  // two values either side (lanes 0-1 left, 2-3 right)
+  if (lane < 2 * kSegHalo) {
+    int q = lane < kSegHalo ? i0 - kSegHalo + lane : i0 + kSeg + (lane - kSegHalo);
     if (wrap) {
-      // lines shorter than the segment wrap more than once
       while (q < 0) q += nin;
       while (q >= nin) q -= nin;
     } else {
-      q = q < 0 ? 0 : (q >= nin ? nin - 1 : q);  // clamped slots are read by boundary rows only
+      q = q < 0 ? 0 : (q >= nin ? nin - 1 : q);
     }
-    s[t] = expr_ro<M0, M1>(io, ibase + q);
+    s[lane < kSegHalo ? lane : kSeg + lane] = expr_ro<M0, M1>(io, ibase + q);
   }
   __syncwarp();
   const T r1 = T(P.r1), r2 = T(P.r2), dd = T(P.dd);
   auto fs = [&](int qq) -> T { return s[qq - i0 + kSegHalo]; };
-  auto f = [&](int qq) -> T { return expr_ro<M0, M1>(io, ibase + qq); };
   const int64_t obase = (int64_t)L * nout;
 #pragma unroll
   for (int m = 0; m < kSeg / 32; ++m) {
@@ -189,7 +201,7 @@ __global__ void __launch_bounds__(256) stencil_xseg_kernel(const __grid_constant
     if (p >= nout) break;
     T v;
     if (wrap || (p >= P.b_lo && p <= P.b_hi)) v = bulk_fn<FAM>(fs, p, r1, r2) * dd;
-    else v = boundary_row(P, io, f, p, L, nlines);
+    else v = boundary_row<T, M0, M1>(P, io, ibase, 1, p, L, nlines);
     finish_row(P, io, table, p, L, nlines, obase + p, v);
   }
 }
