@@ -755,18 +755,27 @@ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_doub
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 
 // one radix-R butterfly column of a Stockham stage
+// x / d for 0 <= x < 2^23 from a float reciprocal of d with one correction step (the float
+// estimate is within one of the quotient there); avoids an integer division per butterfly
+__device__ __forceinline__ int fast_div(int x, int d, float inv) {
+  int q = __float2int_rz((float)x * inv);
+  const int r = x - q * d;
+  if (r >= d) ++q;
+  else if (r < 0) --q;
+  return q;
+}
+
+// one radix-R butterfly column of a Stockham stage: column j = jq * ns + k (k < ns), input stride
+// n / R, twiddle step n / (ns R); k * r * tstep < n, so the twiddle index needs no reduction
 template <int R>
-__device__ __forceinline__ void stockham_bfly(const double2* in, double2* out, int j, int n, int ns,
-                                              const double2* tw, int sign) {
+__device__ __forceinline__ void stockham_bfly(const double2* in, double2* out, int j, int jq, int k, int stride,
+                                              int ns, int tstep, const double2* tw, int sign) {
   double2 v[R];
-  const int stride = n / R;
-  const int k = j % ns;
-  const int tstep = n / (ns * R);
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     double2 x = in[j + r * stride];
     if (r > 0 && k > 0) {
-      double2 t = tw[(k * r * tstep) % n];
+      double2 t = tw[k * r * tstep];
       if (sign > 0) t.y = -t.y;
       x = cmul(x, t);
     }
@@ -794,7 +803,7 @@ __device__ __forceinline__ void stockham_bfly(const double2* in, double2* out, i
     v[1] = cadd(m, it2);
     v[2] = csub(m, it2);
   }
-  const int idxd = (j / ns) * ns * R + k;
+  const int idxd = jq * ns * R + k;
 #pragma unroll
   for (int r = 0; r < R; ++r) out[idxd + r * ns] = v[r];
 }
@@ -808,14 +817,16 @@ __device__ double2* smem_fft(double2* buf0, double2* buf1, int nl, const FftPlan
   double2* out = buf1;
   for (int s = 0; s < fp.nst; ++s) {
     const int R = fp.radix[s];
-    const int nb = n / R;
+    const int nb = n / R, tstep = n / (ns * R);
+    const float inb = 1.0f / (float)nb, ins = 1.0f / (float)ns;
     for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
-      const int line = t / nb, j = t - line * nb;
+      const int line = fast_div(t, nb, inb), j = t - line * nb;
+      const int jq = fast_div(j, ns, ins), k = j - jq * ns;
       const double2* li = in + line * n;
       double2* lo = out + line * n;
-      if (R == 4) stockham_bfly<4>(li, lo, j, n, ns, fp.tw, sign);
-      else if (R == 2) stockham_bfly<2>(li, lo, j, n, ns, fp.tw, sign);
-      else stockham_bfly<3>(li, lo, j, n, ns, fp.tw, sign);
+      if (R == 4) stockham_bfly<4>(li, lo, j, jq, k, nb, ns, tstep, fp.tw, sign);
+      else if (R == 2) stockham_bfly<2>(li, lo, j, jq, k, nb, ns, tstep, fp.tw, sign);
+      else stockham_bfly<3>(li, lo, j, jq, k, nb, ns, tstep, fp.tw, sign);
     }
     __syncthreads();
     ns *= R;
@@ -840,6 +851,7 @@ __global__ void rfft_x_kernel(const __grid_constant__ FftPlan fp, const R* __res
   double2* b0 = sh;
   double2* b1 = sh + (size_t)lpc * n;
   const int pair0 = blockIdx.x * lpc;
+  const float inn = 1.0f / (float)n, innh = 1.0f / (float)nh;
   for (int t0 = threadIdx.x; t0 < lpc * n; t0 += 4 * blockDim.x) {
     double a[4], b[4];
 #pragma unroll
@@ -848,7 +860,7 @@ __global__ void rfft_x_kernel(const __grid_constant__ FftPlan fp, const R* __res
       a[u] = 0.0;
       b[u] = 0.0;
       if (t < lpc * n) {
-        const int l = t / n, p = t - l * n;
+        const int l = fast_div(t, n, inn), p = t - l * n;
         const int ra = 2 * (pair0 + l), rb = ra + 1;
         if (ra < nrows) a[u] = (double)in[(int64_t)ra * n + p];
         if (rb < nrows) b[u] = (double)in[(int64_t)rb * n + p];
@@ -863,10 +875,10 @@ __global__ void rfft_x_kernel(const __grid_constant__ FftPlan fp, const R* __res
   __syncthreads();
   double2* r = smem_fft(b0, b1, lpc, fp, -1);
   for (int t = threadIdx.x; t < lpc * nh; t += blockDim.x) {
-    const int l = t / nh, k = t - l * nh;
+    const int l = fast_div(t, nh, innh), k = t - l * nh;
     const int ra = 2 * (pair0 + l), rb = ra + 1;
     const double2 z = r[l * n + k];
-    double2 zc = r[l * n + ((n - k) % n)];
+    double2 zc = r[l * n + (k == 0 ? 0 : n - k)];
     zc.y = -zc.y;
     const double2 xa = make_double2(0.5 * (z.x + zc.x), 0.5 * (z.y + zc.y));
     const double2 d = csub(z, zc);
@@ -884,6 +896,7 @@ __global__ void irfft_x_kernel(const __grid_constant__ FftPlan fp, const double2
   double2* b0 = sh;
   double2* b1 = sh + (size_t)lpc * n;
   const int pair0 = blockIdx.x * lpc;
+  const float inn = 1.0f / (float)n;
   for (int t0 = threadIdx.x; t0 < lpc * n; t0 += 4 * blockDim.x) {
     double2 xa[4], xb[4];
 #pragma unroll
@@ -892,7 +905,7 @@ __global__ void irfft_x_kernel(const __grid_constant__ FftPlan fp, const double2
       xa[u] = make_double2(0.0, 0.0);
       xb[u] = make_double2(0.0, 0.0);
       if (t < lpc * n) {
-        const int l = t / n, k = t - l * n;
+        const int l = fast_div(t, n, inn), k = t - l * n;
         const int ra = 2 * (pair0 + l), rb = ra + 1;
         const int kk = k > n / 2 ? n - k : k;
         if (ra < nrows) xa[u] = in[(int64_t)ra * nh + kk];
@@ -903,7 +916,7 @@ __global__ void irfft_x_kernel(const __grid_constant__ FftPlan fp, const double2
     for (int u = 0; u < 4; ++u) {
       const int t = t0 + u * blockDim.x;
       if (t < lpc * n) {
-        const int k = t % n;
+        const int k = t - fast_div(t, n, inn) * n;
         const bool hi = k > n / 2;
         const int kk = hi ? n - k : k;
         double2 A = xa[u], B = xb[u];
@@ -916,7 +929,7 @@ __global__ void irfft_x_kernel(const __grid_constant__ FftPlan fp, const double2
   __syncthreads();
   double2* r = smem_fft(b0, b1, lpc, fp, +1);
   for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
-    const int l = t / n, p = t - l * n;
+    const int l = fast_div(t, n, inn), p = t - l * n;
     const int ra = 2 * (pair0 + l), rb = ra + 1;
     const double2 z = r[t];
     if (ra < nrows) out[(int64_t)ra * n + p] = R(z.x * scale);
@@ -927,11 +940,23 @@ __global__ void irfft_x_kernel(const __grid_constant__ FftPlan fp, const double2
 __global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __restrict__ data, int na, int nb,
                                  int64_t bstride, int64_t stride, int sign, int lpc) {
   extern __shared__ double2 sh[];
+  __shared__ int64_t lbase[32];  // start of each of the CTA's lines (lpc <= 32), -1 past the end
   const int n = fp.n;
   double2* b0 = sh;
   double2* b1 = sh + (size_t)lpc * n;
   const int64_t g0 = (int64_t)blockIdx.x * lpc;
   const int64_t nlines = (int64_t)na * nb;
+  if (threadIdx.x < lpc) {
+    const int64_t g = g0 + threadIdx.x;
+    if (g < nlines) {
+      const int64_t b = g / na, a = g - b * na;
+      lbase[threadIdx.x] = a + b * bstride;
+    } else {
+      lbase[threadIdx.x] = -1;
+    }
+  }
+  __syncthreads();
+  const float ilpc = 1.0f / (float)lpc;
   for (int t0 = threadIdx.x; t0 < lpc * n; t0 += 4 * blockDim.x) {
     double2 v[4];
 #pragma unroll
@@ -939,19 +964,16 @@ __global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __
       const int t = t0 + u * blockDim.x;
       v[u] = make_double2(0.0, 0.0);
       if (t < lpc * n) {
-        const int p = t / lpc, l = t - p * lpc;
-        const int64_t g = g0 + l;
-        if (g < nlines) {
-          const int64_t b = g / na, a = g - b * na;
-          v[u] = data[a + b * bstride + p * stride];
-        }
+        const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
+        const int64_t base = lbase[l];
+        if (base >= 0) v[u] = data[base + p * stride];
       }
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int t = t0 + u * blockDim.x;
       if (t < lpc * n) {
-        const int p = t / lpc, l = t - p * lpc;
+        const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
         b0[l * n + p] = v[u];
       }
     }
@@ -959,12 +981,9 @@ __global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __
   __syncthreads();
   double2* r = smem_fft(b0, b1, lpc, fp, sign);
   for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
-    const int p = t / lpc, l = t - p * lpc;
-    const int64_t g = g0 + l;
-    if (g < nlines) {
-      const int64_t b = g / na, a = g - b * na;
-      data[a + b * bstride + p * stride] = r[l * n + p];
-    }
+    const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
+    const int64_t base = lbase[l];
+    if (base >= 0) data[base + p * stride] = r[l * n + p];
   }
 }
 
