@@ -1311,19 +1311,22 @@ void launch_fbcy_extract(T* fbc, const T* A, const T* B, const T* C, double c1, 
   fbcy_extract_kernel<T><<<148, 256, 0, st>>>(fbc, A, B, C, c1, s, c2, n1, n2, n3);
 }
 
+// out = sa*a + sb*b (+ sc*c), the terms added in that order
 template <typename T>
 __global__ void axpby_kernel(T* __restrict__ out, const T* __restrict__ a, double sa, const T* __restrict__ b,
-                             double sb, int64_t n) {
-  const T ta = T(sa), tb = T(sb);
+                             double sb, const T* __restrict__ c, double sc, int64_t n) {
+  const T ta = T(sa), tb = T(sb), tc = T(sc);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     T v = ta * a[i];
     if (b) v += tb * b[i];
+    if (c) v += tc * c[i];
     out[i] = v;
   }
 }
 template <typename T>
-void launch_axpby(T* out, const T* a, double sa, const T* b, double sb, int64_t n, cudaStream_t st) {
-  axpby_kernel<T><<<148 * 8, 256, 0, st>>>(out, a, sa, b, sb, n);
+void launch_axpby(T* out, const T* a, double sa, const T* b, double sb, int64_t n, cudaStream_t st, const T* c,
+                  double sc) {
+  axpby_kernel<T><<<148 * 8, 256, 0, st>>>(out, a, sa, b, sb, c, sc, n);
 }
 
 // conversion between the double host layout and a float device field
@@ -1352,7 +1355,7 @@ void launch_convert(double* out, const float* in, int64_t n, cudaStream_t st) {
   template void launch_fbcy_const<T>(T*, int, int, double, double, cudaStream_t);                             \
   template void launch_fbcy_extract<T>(T*, const T*, const T*, const T*, double, double, double, int, int, int, \
                                        cudaStream_t);                                                         \
-  template void launch_axpby<T>(T*, const T*, double, const T*, double, int64_t, cudaStream_t);
+  template void launch_axpby<T>(T*, const T*, double, const T*, double, int64_t, cudaStream_t, const T*, double);
 CHS_INST_ELEM(double)
 CHS_INST_ELEM(float)
 #undef CHS_INST_ELEM

@@ -157,7 +157,8 @@ void launch_fbcy_extract(T* fbc, const T* A, const T* B, const T* C, double c1, 
                          int n3, cudaStream_t st);
 // out = sa*a + sb*b (b optional)
 template <typename T>
-void launch_axpby(T* out, const T* a, double sa, const T* b, double sb, int64_t n, cudaStream_t st);
+void launch_axpby(T* out, const T* a, double sa, const T* b, double sb, int64_t n, cudaStream_t st,
+                  const T* c = nullptr, double sc = 0.0);
 // float <-> double field conversion
 void launch_convert(float* out, const double* in, int64_t n, cudaStream_t st);
 void launch_convert(double* out, const float* in, int64_t n, cudaStream_t st);

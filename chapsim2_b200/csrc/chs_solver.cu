@@ -1060,26 +1060,23 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
   const T* mu_yz = TH ? A(H->muiyz_cpp) : nullptr;
 
   // div = qxdx + qydy + qzdz (:512-534)
-  PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, bufs(H->qxdx, H->qydy), bufs(H->div),
-        launch_axpby(A(H->div), A(H->qxdx), 1.0, A(H->qydy), 1.0, (int64_t)H->n_ccc, st));
-  PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, bufs(H->qzdz), bufs(H->div),
-        launch_axpby(A(H->div), A(H->div), 1.0, A(H->qzdz), 1.0, (int64_t)H->n_ccc, st));
-  H->launches += 2;
+  PROFD(H, 3, 32.0 / 8.0 * sizeof(T) * H->n_ccc, bufs(H->qxdx, H->qydy, H->qzdz), bufs(H->div),
+        launch_axpby(A(H->div), A(H->qxdx), 1.0, A(H->qydy), 1.0, (int64_t)H->n_ccc, st, A(H->qzdz), 1.0));
+  H->launches += 1;
   if (H->fbcy_velo) {
     // wall divergence for the y-viscous boundary value (:374-442, :537-546)
     run_op(H, 0, D1P2C, bx_qx, nullptr, src(A(H->qxiy)), s_ppc, A(H->qxdx_cpc), false, 1.0);
     run_op(H, 1, D1C2P, by_qy, fyqy, src(A(H->qyiy)), s_ccc, A(H->qydy_cpc), false, 1.0);
     run_op(H, 2, D1P2C, bz_qz, nullptr, src(A(H->qziy)), s_cpp, A(H->qzdz_cpc), false, 1.0);
     // fbcy_div = walls of (qxdx + qydy + qzdz)_cpc; visc2 bc = (qydy_cpc - div/3) * 2 (:1156-1171)
-    PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc, bufs(H->qydy_cpc), bufs(H->qxdx_cpc),
-          launch_axpby(A(H->qxdx_cpc), A(H->qxdx_cpc), 1.0, A(H->qydy_cpc), 1.0, (int64_t)H->n_cpc, st));
-    PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc, bufs(H->qzdz_cpc), bufs(H->qxdx_cpc),
-          launch_axpby(A(H->qxdx_cpc), A(H->qxdx_cpc), 1.0, A(H->qzdz_cpc), 1.0, (int64_t)H->n_cpc, st));
+    PROFD(H, 3, 32.0 / 8.0 * sizeof(T) * H->n_cpc, bufs(H->qydy_cpc, H->qzdz_cpc), bufs(H->qxdx_cpc),
+          launch_axpby(A(H->qxdx_cpc), A(H->qxdx_cpc), 1.0, A(H->qydy_cpc), 1.0, (int64_t)H->n_cpc, st,
+                       A(H->qzdz_cpc), 1.0));
     PROFD(H, 3, 48.0 / 8.0 * sizeof(T) * nc0 * nc2, bufs(H->qydy_cpc, H->qxdx_cpc, TH ? H->muiy_cpc : nullptr),
           bufs(H->fb_visc2),
          launch_fbcy_extract<T>(A(H->fb_visc2), A(H->qydy_cpc), A(H->qxdx_cpc), TH ? A(H->muiy_cpc) : nullptr,
                                 -third, TH ? 2.0 : 1.0, 2.0, nc0, np1, nc2, st));
-    H->launches += 3;
+    H->launches += 2;
   }
 
   // ---- 2-3. momentum RHS and fractional step, one fused pass per component.  The convection and
