@@ -95,9 +95,8 @@ __device__ __forceinline__ void finish_row(const OpPlan& P, const LineIOT<T>& io
 
 // y (DIR 1) or z (DIR 2) lines: thread = (position in the cross plane, chunk of kWin rows)
 template <typename T, int DIR, int FAM, int M0, int M1>
-__global__ void __launch_bounds__(256) stencil_win_kernel(const __grid_constant__ OpPlan P,
-                                                          const __grid_constant__ LineIOT<T> io,
-                                                          const double* __restrict__ table, int nlines) {
+__device__ __forceinline__ void stencil_win_body(const OpPlan& P, const LineIOT<T>& io,
+                                                 const double* __restrict__ table, int nlines) {
   using RC = Reach<FAM>;
   constexpr int W = kWin + RC::hi4 - RC::lo4;
   const int nin = P.nin, nout = P.nout, n1 = io.n1;
@@ -147,6 +146,20 @@ __global__ void __launch_bounds__(256) stencil_win_kernel(const __grid_constant_
     else v = boundary_row<T, M0, M1>(P, io, ibase, istride, p, L, nlines);
     finish_row(P, io, table, p, L, nlines, obase + (int64_t)p * ostride, v);
   }
+}
+
+// the y kernel keeps at most 51 registers (five CTAs per SM); the z kernel needs no cap (measured)
+template <typename T, int FAM, int M0, int M1>
+__global__ void __launch_bounds__(256, 5) stencil_winy_kernel(const __grid_constant__ OpPlan P,
+                                                              const __grid_constant__ LineIOT<T> io,
+                                                              const double* __restrict__ table, int nlines) {
+  stencil_win_body<T, 1, FAM, M0, M1>(P, io, table, nlines);
+}
+template <typename T, int FAM, int M0, int M1>
+__global__ void __launch_bounds__(256) stencil_winz_kernel(const __grid_constant__ OpPlan P,
+                                                           const __grid_constant__ LineIOT<T> io,
+                                                           const double* __restrict__ table, int nlines) {
+  stencil_win_body<T, 2, FAM, M0, M1>(P, io, table, nlines);
 }
 
 // x lines (DIR 0): each warp forms a segment of kSeg consecutive outputs of one line from a
@@ -218,11 +231,11 @@ void launch_win(const OpPlan& P, const LineIOT<T>& io, const double* table, cuda
     const int bx = io.n1 >= 128 ? 128 : (io.n1 >= 64 ? 64 : 32), by = 256 / bx;
     const int chunks = (P.nout + kWin - 1) / kWin;
     dim3 grid((unsigned)((io.n1 + bx - 1) / bx), (unsigned)((chunks + by - 1) / by), (unsigned)io.n3);
-    stencil_win_kernel<T, 1, FAM, M0, M1><<<grid, dim3(bx, by), 0, st>>>(P, io, table, nlines);
+    stencil_winy_kernel<T, FAM, M0, M1><<<grid, dim3(bx, by), 0, st>>>(P, io, table, nlines);
   } else {
     const int plane = io.n1 * io.n2;
     dim3 grid((unsigned)((plane + 255) / 256), (unsigned)((P.nout + kWin - 1) / kWin));
-    stencil_win_kernel<T, 2, FAM, M0, M1><<<grid, 256, 0, st>>>(P, io, table, nlines);
+    stencil_winz_kernel<T, FAM, M0, M1><<<grid, 256, 0, st>>>(P, io, table, nlines);
   }
 }
 
