@@ -1486,12 +1486,40 @@ void launch_fill(T* a, double v, int64_t n, cudaStream_t st) {
   fill_kernel<T><<<148 * 4, 256, 0, st>>>(a, v, n);
 }
 
+template <typename T>
+__global__ void stats_update_kernel(const __grid_constant__ StatsIO<T> s) {
+  const double ac = s.ac, am = s.am;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double u0 = (double)s.u[0][i], u1 = (double)s.u[1][i], u2 = (double)s.u[2][i];
+    s.pm[i] = am * s.pm[i] + ac * (double)s.p[i];
+    s.um[0][i] = am * s.um[0][i] + ac * u0;
+    s.um[1][i] = am * s.um[1][i] + ac * u1;
+    s.um[2][i] = am * s.um[2][i] + ac * u2;
+    s.uu[0][i] = am * s.uu[0][i] + ac * u0 * u0;
+    s.uu[1][i] = am * s.uu[1][i] + ac * u1 * u1;
+    s.uu[2][i] = am * s.uu[2][i] + ac * u2 * u2;
+    s.uu[3][i] = am * s.uu[3][i] + ac * u0 * u1;
+    s.uu[4][i] = am * s.uu[4][i] + ac * u0 * u2;
+    s.uu[5][i] = am * s.uu[5][i] + ac * u1 * u2;
+    if (s.t) {
+      const double t = (double)s.t[i];
+      s.tm[i] = am * s.tm[i] + ac * t;
+      s.ttm[i] = am * s.ttm[i] + ac * t * t;
+    }
+  }
+}
+template <typename T>
+void launch_stats_update(const StatsIO<T>& s, cudaStream_t st) {
+  stats_update_kernel<T><<<148 * 8, 256, 0, st>>>(s);
+}
+
 #define CHS_INST_THERMO(T)                                                                                      \
   template void launch_property_update<T>(const ThermoTab&, const T*, T*, T*, T*, T*, T*, int64_t, cudaStream_t); \
   template void launch_wall_props<T>(const ThermoTab&, const T*, int, int, int, int, int, T*, T*, T*, T*,        \
                                      cudaStream_t);                                                             \
   template void launch_energy_advance<T>(T*, T*, T*, int64_t, double, double, double, cudaStream_t); \
-  template void launch_fill<T>(T*, double, int64_t, cudaStream_t);
+  template void launch_fill<T>(T*, double, int64_t, cudaStream_t);                                           \
+  template void launch_stats_update<T>(const StatsIO<T>&, cudaStream_t);
 CHS_INST_THERMO(double)
 CHS_INST_THERMO(float)
 #undef CHS_INST_THERMO

@@ -181,6 +181,25 @@ void launch_energy_advance(T* rhs, T* rhs0, T* rhoh, int64_t n, double dt, doubl
 template <typename T>
 void launch_fill(T* a, double v, int64_t n, cudaStream_t st);
 
+// running means of the flow and thermal statistics (update_statistics_flow/thermo,
+// src/post_statistics.f90:152-283): with ac = 1/nstat, am = (nstat-1)/nstat,
+// mean = am*mean + ac*x and product means am*m + (ac*a)*b; inputs at cell centres, FP64 sums
+template <typename T>
+struct StatsIO {
+  const T* p;
+  const T* u[3];   // cell-centre velocities (P2C interpolations)
+  const T* t;      // temperature or null
+  double* pm;
+  double* um[3];
+  double* uu[6];   // uu, vv, ww, uv, uw, vw
+  double* tm;
+  double* ttm;
+  double ac, am;
+  int64_t n;
+};
+template <typename T>
+void launch_stats_update(const StatsIO<T>& s, cudaStream_t st);
+
 // max |a| and NaN flag into out[0], out[1] (two-pass with partials)
 void launch_absmax(const double* a, int64_t n, double* partial, int npart, double* out, cudaStream_t st);
 // 0.5*(u^2+v^2+w^2) over ccc

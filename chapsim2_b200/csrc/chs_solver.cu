@@ -160,6 +160,8 @@ struct chs_handle {
   MlpSmall mlp_small{};
   MlpCheck mlp_check{};
   std::vector<double> tab_host_t, tab_host_rhoh;
+  // running statistics (post_statistics.f90): 0 pr, 1-3 u, 4-9 uu vv ww uv uw vw, 10 T, 11 TT
+  double* stat[12] = {};
   double vol = 0.0;
   int npart = 0;
   // Poisson
@@ -1682,6 +1684,118 @@ void d2h_field(chs_handle* H, double* host, const double* dev, size_t n) {
   CK(cudaMemcpyAsync(host, H->stage, n * sizeof(double), cudaMemcpyDeviceToHost, H->st));
 }
 
+// ---- restart files and running statistics (src/io_restart.f90:32-227, src/post_statistics.f90:152-300)
+const char* const kStatKey[12] = {"time_averaged_pr", "time_averaged_ux", "time_averaged_uy", "time_averaged_uz",
+                                  "time_averaged_uu", "time_averaged_vv", "time_averaged_ww", "time_averaged_uv",
+                                  "time_averaged_uw", "time_averaged_vw", "time_averaged_t",  "time_averaged_tt"};
+
+// generate_pathfile_name (src/io_tools.f90:44-61): <dir>/domain<idom>_<keyword>_<iter>.bin
+std::string data_file(const char* dir, int idom, const char* key, int iter) {
+  return std::string(dir) + "/domain" + std::to_string(idom) + "_" + key + "_" + std::to_string(iter) + ".bin";
+}
+
+// decomp_2d_write_one / _read_one of a full-domain x-pencil array on one rank: the raw FP64 values
+// in Fortran order (x fastest), no header
+void write_raw(const std::string& path, const double* a, size_t n) {
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) throw std::runtime_error("cannot open " + path + " for writing");
+  const size_t w = std::fwrite(a, sizeof(double), n, f);
+  const int rc = std::fclose(f);
+  if (w != n || rc != 0) throw std::runtime_error("short write to " + path);
+}
+void read_raw(const std::string& path, double* a, size_t n) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) throw std::runtime_error("cannot open " + path);
+  std::fseek(f, 0, SEEK_END);
+  const long sz = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
+  if (sz != (long)(n * sizeof(double))) {
+    std::fclose(f);
+    throw std::runtime_error(path + ": " + std::to_string(sz) + " bytes, expected " + std::to_string(n * sizeof(double)));
+  }
+  const size_t r = std::fread(a, sizeof(double), n, f);
+  std::fclose(f);
+  if (r != n) throw std::runtime_error("short read from " + path);
+}
+
+void save_field(chs_handle* H, int field, const std::string& path) {
+  size_t n = 0;
+  double* d = field_ptr(H, field, &n);
+  std::vector<double> h(n);
+  d2h_field(H, h.data(), d, n);
+  CK(cudaStreamSynchronize(H->st));
+  write_raw(path, h.data(), n);
+}
+void load_field(chs_handle* H, int field, const std::string& path) {
+  size_t n = 0;
+  double* d = field_ptr(H, field, &n);
+  std::vector<double> h(n);
+  read_raw(path, h.data(), n);
+  h2d_field(H, d, h.data(), n);
+  CK(cudaStreamSynchronize(H->st));  // the host copy is released on return
+}
+
+// Update_thermal_properties (src/eq_energy.f90:14-146) from the current rho*h, wall states
+// included, then g = q * rho_face (convert_primary_conservative IQ2G): the thermal part of
+// restore_thermo_variables_from_restart (src/io_restart.f90:208-226)
+template <typename T>
+void thermo_refresh_t(chs_handle* H) {
+  auto A = [](double* p) { return reinterpret_cast<T*>(p); };
+  const int nc0 = H->nc[0], nc2 = H->nc[2], np1 = H->np[1];
+  const int s_ccc[3] = {H->nc[0], H->nc[1], H->nc[2]};
+  launch_property_update<T>(H->tab, A(H->rhoh), A(H->hEnth), A(H->tTemp), A(H->kCond), A(H->dDens), A(H->mVisc),
+                            (int64_t)H->n_ccc, H->st);
+  H->launches++;
+  const auto& B = H->ibc;
+  const int s0 = B[1][V_TM][0] == BC_NEUMANN, s1 = B[1][V_TM][1] == BC_NEUMANN;
+  if (s0 || s1) {
+    run_op(H, 1, M1C2P, H->ftpy, nullptr, src(A(H->rhoh)), s_ccc, A(H->dh_cpc), false, 1.0);
+    launch_wall_props<T>(H->tab, A(H->dh_cpc), nc0, np1, nc2, s0, s1, A(H->fb_h), A(H->fb_k), A(H->fb_m), A(H->fb_d),
+                         H->st);
+    H->launches++;
+  }
+  const Pair per = P2(kPer2);
+  const T* any = A(H->fb_maxp);
+  run_op(H, 0, M1C2P, per, any, src(A(H->dDens)), s_ccc, A(H->gx), false, 1.0, O_MUL, A(H->qx));
+  run_op(H, 1, M1C2P, H->ftpy, A(H->fb_d), src(A(H->dDens)), s_ccc, A(H->gy), false, 1.0, O_MUL, A(H->qy));
+  run_op(H, 2, M1C2P, per, any, src(A(H->dDens)), s_ccc, A(H->gz), false, 1.0, O_MUL, A(H->qz));
+}
+
+// update_statistics_flow / _thermo (src/post_statistics.f90:152-283) for sample nstat
+template <typename T>
+void stats_update_t(chs_handle* H, int nstat) {
+  auto A = [](double* p) { return reinterpret_cast<T*>(p); };
+  const int nst = H->thermo ? 12 : 10;
+  for (int k = 0; k < nst; ++k)
+    if (!H->stat[k]) H->stat[k] = H->dalloc<double>(H->n_ccc);
+  const auto& B = H->ibc;
+  const int s_pcc[3] = {H->np[0], H->nc[1], H->nc[2]}, s_cpc[3] = {H->nc[0], H->np[1], H->nc[2]};
+  const int s_ccp[3] = {H->nc[0], H->nc[1], H->np[2]};
+  const T* any = A(H->fb_maxp);
+  const T* fyqy = H->periodic_y ? nullptr : A(H->fb_qy);
+  // cell-centre velocities: the P2C mid-point interpolations of the reference (the derived-quantity
+  // buffers serve as scratch between steps)
+  run_op(H, 0, M1P2C, P2(B[0][V_QX]), any, src(A(H->qx)), s_pcc, A(H->qxix), false, 1.0);
+  run_op(H, 1, M1P2C, P2(B[1][V_QY]), fyqy, src(A(H->qy)), s_cpc, A(H->qyiy), false, 1.0);
+  run_op(H, 2, M1P2C, P2(B[2][V_QZ]), any, src(A(H->qz)), s_ccp, A(H->qziz), false, 1.0);
+  StatsIO<T> io{};
+  io.p = A(H->pres);
+  io.u[0] = A(H->qxix);
+  io.u[1] = A(H->qyiy);
+  io.u[2] = A(H->qziz);
+  io.t = H->thermo ? A(H->tTemp) : nullptr;
+  io.pm = H->stat[0];
+  for (int k = 0; k < 3; ++k) io.um[k] = H->stat[1 + k];
+  for (int k = 0; k < 6; ++k) io.uu[k] = H->stat[4 + k];
+  io.tm = H->stat[10];
+  io.ttm = H->stat[11];
+  io.ac = 1.0 / (double)nstat;
+  io.am = (double)(nstat - 1) / (double)nstat;
+  io.n = (int64_t)H->n_ccc;
+  launch_stats_update<T>(io, H->st);
+  H->launches++;
+}
+
 void capture_graphs(chs_handle* H) {
   for (int isub = 1; isub <= 3; ++isub) {
     cudaGraph_t g;
@@ -2359,6 +2473,98 @@ int chs_poisson_solve_device(chs_handle* H, double* d_rhs) {
     poisson_device(H, d_rhs);
     CK(cudaGetLastError());
   });
+}
+
+int chs_write_restart(chs_handle* H, const char* dir, int idom, int iter) {
+  if (!H || !dir) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    // write_instantanous_flow / _thermo (src/io_restart.f90:71-108)
+    const int f[4] = {CHS_QX, CHS_QY, CHS_QZ, CHS_PRES};
+    const char* k[4] = {"qx", "qy", "qz", "pr"};
+    for (int i = 0; i < 4; ++i) save_field(H, f[i], data_file(dir, idom, k[i], iter));
+    if (H->thermo) {
+      save_field(H, CHS_RHOH, data_file(dir, idom, "rhoh", iter));
+      save_field(H, CHS_TTEMP, data_file(dir, idom, "temp", iter));
+    }
+  });
+}
+
+int chs_read_restart(chs_handle* H, const char* dir, int idom, int iter) {
+  if (!H || !dir) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    // read_instantanous_flow (src/io_restart.f90:112-129), restore_flow_variables_from_restart
+    // (:132-167: pcor = 0), read_instantanous_thermo (:170-204; T is recomputed from rho*h) and
+    // restore_thermo_variables_from_restart (:208-226)
+    const int f[4] = {CHS_QX, CHS_QY, CHS_QZ, CHS_PRES};
+    const char* k[4] = {"qx", "qy", "qz", "pr"};
+    for (int i = 0; i < 4; ++i) load_field(H, f[i], data_file(dir, idom, k[i], iter));
+    if (H->mixed) launch_fill(reinterpret_cast<float*>(H->pcor), 0.0, (int64_t)H->n_ccc, H->st);
+    else launch_fill(H->pcor, 0.0, (int64_t)H->n_ccc, H->st);
+    H->launches++;
+    if (H->thermo) {
+      load_field(H, CHS_RHOH, data_file(dir, idom, "rhoh", iter));
+      if (H->mixed) thermo_refresh_t<float>(H);
+      else thermo_refresh_t<double>(H);
+    }
+    CK(cudaStreamSynchronize(H->st));
+  });
+}
+
+int chs_stats_update(chs_handle* H, int nstat) {
+  if (!H || nstat < 1) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    if (H->mixed) stats_update_t<float>(H, nstat);
+    else stats_update_t<double>(H, nstat);
+    CK(cudaGetLastError());
+  });
+}
+
+int chs_stats_get(chs_handle* H, int which, double* host, size_t n) {
+  if (!H || !host || which < 0 || which > 11) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    if (!H->stat[which]) throw std::invalid_argument("no statistics of this kind yet (chs_stats_update)");
+    if (n != H->n_ccc) throw std::invalid_argument("statistics size mismatch");
+    CK(cudaMemcpyAsync(host, H->stat[which], n * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaStreamSynchronize(H->st));
+  });
+}
+
+int chs_write_statistics(chs_handle* H, const char* dir, int idom, int iter) {
+  if (!H || !dir) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    // write_statistics_flow / _thermo (src/post_statistics.f90:217-239, :285-296)
+    const int nst = H->thermo ? 12 : 10;
+    std::vector<double> h(H->n_ccc);
+    for (int k = 0; k < nst; ++k) {
+      if (!H->stat[k]) throw std::invalid_argument("no statistics yet (chs_stats_update)");
+      CK(cudaMemcpyAsync(h.data(), H->stat[k], H->n_ccc * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+      CK(cudaStreamSynchronize(H->st));
+      write_raw(data_file(dir, idom, kStatKey[k], iter), h.data(), H->n_ccc);
+    }
+  });
+}
+
+int chs_read_statistics(chs_handle* H, const char* dir, int idom, int iter) {
+  if (!H || !dir) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    // read_statistics_flow / _thermo (src/post_statistics.f90:98-148)
+    const int nst = H->thermo ? 12 : 10;
+    std::vector<double> h(H->n_ccc);
+    for (int k = 0; k < nst; ++k) {
+      if (!H->stat[k]) H->stat[k] = H->dalloc<double>(H->n_ccc);
+      read_raw(data_file(dir, idom, kStatKey[k], iter), h.data(), H->n_ccc);
+      CK(cudaMemcpyAsync(H->stat[k], h.data(), H->n_ccc * sizeof(double), cudaMemcpyHostToDevice, H->st));
+      CK(cudaStreamSynchronize(H->st));
+    }
+  });
+}
+
+int chs_data_file_name(const char* dir, int idom, const char* keyword, int iter, char* buf, size_t len) {
+  if (!dir || !keyword || !buf || len == 0) return CHS_ERR_ARG;
+  const std::string s = data_file(dir, idom, keyword, iter);
+  if (s.size() + 1 > len) return CHS_ERR_ARG;
+  std::memcpy(buf, s.c_str(), s.size() + 1);
+  return CHS_OK;
 }
 
 int chs_diagnostics(chs_handle* H, chs_diag* out) {

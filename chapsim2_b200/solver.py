@@ -69,7 +69,9 @@ EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field
             "chs_mlp_train", "chs_mlp_set_mode", "chs_mlp_fallbacks", "chs_mlp_params", "chs_mlp_grad",
             "chs_mlp_eval", "chs_mlp_norm", "chs_ensemble_create", "chs_ensemble_step", "chs_ensemble_time_steps",
             "chs_ensemble_kernel_launches", "chs_ensemble_destroy", "chs_autotune", "chs_set_launch_shape",
-            "chs_set_lanes", "chs_profile_substep_graph"]
+            "chs_set_lanes", "chs_profile_substep_graph", "chs_write_restart", "chs_read_restart",
+            "chs_stats_update", "chs_stats_get", "chs_write_statistics", "chs_read_statistics",
+            "chs_data_file_name"]
 
 
 class ChsKprof(ctypes.Structure):
@@ -125,6 +127,12 @@ def load():
     L.chs_mlp_norm.argtypes = [ctypes.c_void_p, _D]
     L.chs_set_launch_shape.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.chs_set_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    for fn in ("chs_write_restart", "chs_read_restart", "chs_write_statistics", "chs_read_statistics"):
+        getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+    L.chs_stats_update.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.chs_stats_get.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]
+    L.chs_data_file_name.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p,
+                                     ctypes.c_size_t]
     L.chs_ensemble_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
     L.chs_ensemble_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.chs_ensemble_time_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
@@ -181,6 +189,16 @@ def make_config(cfg, precision=CHS_FP64):
         s.fbcy_const[i] = float(fb[i])
     s.yp, s.yc, s.ymap_pt, s.ymap_cc = [_ptr(a) for a in keep]
     return s, keep
+
+
+def data_file_name(directory, idom, keyword, iteration):
+    """Restart/statistics file name of the reference's naming (host only)."""
+    L = load()
+    buf = ctypes.create_string_buffer(4096)
+    rc = L.chs_data_file_name(str(directory).encode(), int(idom), str(keyword).encode(), int(iteration), buf, 4096)
+    if rc != 0:
+        raise RuntimeError(f"chs_data_file_name failed ({rc})")
+    return buf.value.decode()
 
 
 def plan_inspect(cfg, d, fam, ibc, has_fbc):
@@ -427,6 +445,35 @@ class Solver:
         n = ctypes.c_int()
         self._check(self.L.chs_profile_substep(self.h, int(isub), arr, maxk, ctypes.byref(n)), "chs_profile_substep")
         return [dict(kind=arr[i].kind, dir=arr[i].dir, bytes=arr[i].bytes, ms=arr[i].ms) for i in range(n.value)]
+
+    # ---- restart files and running statistics
+    def write_restart(self, directory, idom, iteration):
+        self._check(self.L.chs_write_restart(self.h, str(directory).encode(), int(idom), int(iteration)),
+                    "chs_write_restart")
+
+    def read_restart(self, directory, idom, iteration):
+        self._check(self.L.chs_read_restart(self.h, str(directory).encode(), int(idom), int(iteration)),
+                    "chs_read_restart")
+
+    def stats_update(self, nstat):
+        self._check(self.L.chs_stats_update(self.h, int(nstat)), "chs_stats_update")
+
+    STATS = ("pr", "ux", "uy", "uz", "uu", "vv", "ww", "uv", "uw", "vw", "t", "tt")
+
+    def stats_get(self, which):
+        """Running mean `which` (index or name of STATS) as a (nz, ny, nx) array."""
+        k = self.STATS.index(which) if isinstance(which, str) else int(which)
+        out = np.zeros(self.shapes[3])
+        self._check(self.L.chs_stats_get(self.h, k, _ptr(out), out.size), "chs_stats_get")
+        return out
+
+    def write_statistics(self, directory, idom, iteration):
+        self._check(self.L.chs_write_statistics(self.h, str(directory).encode(), int(idom), int(iteration)),
+                    "chs_write_statistics")
+
+    def read_statistics(self, directory, idom, iteration):
+        self._check(self.L.chs_read_statistics(self.h, str(directory).encode(), int(idom), int(iteration)),
+                    "chs_read_statistics")
 
     def profile_substep_graph(self, isub=1, maxk=512):
         """Per-launch profile of one substep replayed as a CUDA graph (advances the state)."""

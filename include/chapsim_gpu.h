@@ -251,6 +251,35 @@ int chs_set_launch_shape(chs_handle* h, int block, int lt_max, int fused);
  * reference, which runs the operators one after another). */
 int chs_set_lanes(chs_handle* h, int lanes);
 
+/*
+ * Restart files and running statistics.  Files follow the reference's naming
+ * (generate_pathfile_name, src/io_tools.f90:44-61): <dir>/domain<idom>_<keyword>_<iter>.bin,
+ * each the raw FP64 full-domain array in Fortran order as decomp_2d_write_one writes it on one
+ * rank (no header).
+ *
+ * chs_write_restart: qx, qy, qz, pr (+ rhoh, temp with variable properties) -- replaces
+ *   write_instantanous_flow / _thermo (src/io_restart.f90:71-108).
+ * chs_read_restart: reads them, pcor = 0, and with variable properties the property update from
+ *   rho*h (wall states included) and g = q * rho_face -- replaces read_instantanous_flow /
+ *   _thermo and restore_*_variables_from_restart (src/io_restart.f90:112-226).  The next
+ *   substep 1 continues the run (its RK3 history weight is zero).
+ * chs_stats_update: running means of p, u_i (cell-centre P2C interpolations) and u_i u_j (+ T,
+ *   T^2), sample nstat = iteration - stat_istart + 1 -- replaces update_statistics_flow /
+ *   _thermo (src/post_statistics.f90:152-283); FP64 accumulation in every precision.
+ * chs_stats_get: which 0 pr, 1-3 ux uy uz, 4-9 uu vv ww uv uw vw, 10 T, 11 TT (n = nc1*nc2*nc3).
+ * chs_write_statistics / chs_read_statistics: the time_averaged_* files of
+ *   write_statistics_flow / _thermo and read_statistics_* (src/post_statistics.f90:98-148,
+ *   217-239, 285-296).
+ * chs_data_file_name: the file name for a keyword (host only).
+ */
+int chs_write_restart(chs_handle* h, const char* dir, int idom, int iter);
+int chs_read_restart(chs_handle* h, const char* dir, int idom, int iter);
+int chs_stats_update(chs_handle* h, int nstat);
+int chs_stats_get(chs_handle* h, int which, double* host, size_t n);
+int chs_write_statistics(chs_handle* h, const char* dir, int idom, int iter);
+int chs_read_statistics(chs_handle* h, const char* dir, int idom, int iter);
+int chs_data_file_name(const char* dir, int idom, const char* keyword, int iter, char* buf, size_t len);
+
 /* Same as chs_poisson_solve on a device buffer (no host copies). */
 int chs_poisson_solve_device(chs_handle* h, double* d_rhs_inout);
 

@@ -36,3 +36,9 @@ def test_create_rejects_bad_config_without_gpu_work():
     h = ctypes.c_void_p()
     rc = L.chs_create(ctypes.byref(s), -1, ctypes.byref(h))
     assert rc != 0 and not h.value
+
+
+def test_data_file_names_follow_the_reference():
+    # generate_pathfile_name (src/io_tools.f90:44-61): <dir>/domain<idom>_<keyword>_<iter>.bin
+    assert S.data_file_name("1_data", 1, "qx", 1000) == "1_data/domain1_qx_1000.bin"
+    assert S.data_file_name("out", 2, "time_averaged_uv", 7) == "out/domain2_time_averaged_uv_7.bin"
