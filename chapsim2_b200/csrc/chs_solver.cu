@@ -185,8 +185,9 @@ struct chs_handle {
   // Launches that name no buffers act as barriers.  Only active while a substep graph is
   // captured; eager runs stay on `st` in program order.
   static constexpr int kLanes = 8;
-  // lanes used by the next capture (1: one stream, program order).  Three measured fastest on the
-  // 128x96x128 channel and heated-channel substeps (8-10% over one lane; more lanes lose again).
+  // lanes used by the next capture (1: one stream, program order).  Measured fastest on the
+  // 128x96x128 channel and heated-channel substeps: three for FP64 fields, four for FP32 (20-25 %
+  // over one lane; more lanes lose again).  Set with the precision in setup_host.
   int dag_lanes = 3;
   cudaStream_t lane[kLanes] = {};
   bool dag_on = false;
@@ -756,6 +757,7 @@ void setup_host(chs_handle* H, const chs_config* c) {
   if (H->ifft == 3 && !H->periodic_y) throw std::invalid_argument("3D-FFT Poisson needs periodic y");
   if (c->precision != CHS_FP64 && c->precision != CHS_MIXED) throw std::invalid_argument("unknown precision mode");
   H->mixed = c->precision == CHS_MIXED;
+  H->dag_lanes = H->mixed ? 4 : 3;
   H->h[0] = c->lxx / H->nc[0];
   H->h[2] = c->lzz / H->nc[2];
   H->h[1] = H->stretch_y ? 1.0 / H->nc[1] : (c->lyt - c->lyb) / H->nc[1];

@@ -244,7 +244,8 @@ int chs_autotune(chs_handle* h, int nsteps, int* block, int* lt_max, int* fused,
  * handle of the same grid): block 0/128/256/512, lt_max 0/16/32/64, fused 0/1;
  * 0 selects the defaults. */
 int chs_set_launch_shape(chs_handle* h, int block, int lt_max, int fused);
-/* Streams a captured substep graph spreads its launches over (1..8, default 3).
+/* Streams a captured substep graph spreads its launches over (1..8; default 3
+ * for CHS_FP64, 4 for CHS_MIXED).
  * Each launch waits only for the launches whose buffers it reads or overwrites,
  * so independent operators run concurrently; 1 keeps program order on one
  * stream.  Results are identical for every setting (no counterpart in the
