@@ -188,6 +188,13 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
   return *reinterpret_cast<const uint32_t*>(&v);
 }
 
+// hardware tanh of two packed BF16 values (the activations that feed the next BF16 MMA)
+__device__ __forceinline__ uint32_t tanh_bf16x2(uint32_t x) {
+  uint32_t y;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(y) : "r"(x));
+  return y;
+}
+
 // shared-memory matrix descriptor, no swizzle, K-major: start, leading-dimension byte offset
 // (between the two 8-element K chunks of one MMA), stride byte offset (between 8-row groups),
 // descriptor version 1
@@ -213,9 +220,10 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t a, uint64_t b, 
       : "r"(tmem), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
                : "r"(taddr));
 }
 
@@ -250,7 +258,7 @@ __device__ __forceinline__ void issue_layer(uint32_t tmem, uint32_t sa, uint32_t
 }
 
 template <typename T>
-__global__ void __launch_bounds__(128) mlp_props_kernel(
+__global__ void __launch_bounds__(128, 6) mlp_props_kernel(
     const __grid_constant__ ThermoTab tb, const __grid_constant__ MlpNorm nm, const __grid_constant__ MlpSmall sm,
     const __grid_constant__ MlpCheck ck, const uint16_t* __restrict__ wpack, const T* __restrict__ rhoh,
     T* __restrict__ h, T* __restrict__ t, T* __restrict__ k, T* __restrict__ d, T* __restrict__ m, int64_t n,
@@ -295,51 +303,69 @@ __global__ void __launch_bounds__(128) mlp_props_kernel(
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int o = kc * 8 + 2 * j;
-        q[j] = pack_bf16x2(tanh_fast(fmaf(sm.w1[o], x, sm.b1[o])), tanh_fast(fmaf(sm.w1[o + 1], x, sm.b1[o + 1])));
+        q[j] = tanh_bf16x2(pack_bf16x2(fmaf(sm.w1[o], x, sm.b1[o]), fmaf(sm.w1[o + 1], x, sm.b1[o + 1])));
       }
       *reinterpret_cast<uint4*>(sA + kc * 2048 + rowoff) = make_uint4(q[0], q[1], q[2], q[3]);
     }
-    float acc[64];
+    // layers 2 and 3 on the tensor cores; the accumulators are read back in two halves of 32
+    // columns: layer 2's activations go to the A operand, layer 3's straight into layer 4 (CUDA
+    // cores), which forms T only unless the raw network outputs are asked for
+    float y4[MLP_NOUT];
+#pragma unroll
+    for (int j = 0; j < MLP_NOUT; ++j) y4[j] = sm.b4[j];
 #pragma unroll
     for (int layer = 0; layer < 2; ++layer) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncthreads();
       if (failed) break;
-      if (tid == 0) issue_layer(tmem, sa, sw + layer * 8192, bar);
-      if (!mbar_wait(bar, phase)) failed = 1;
+      // one thread issues the MMAs and waits for their commit; the others wait at the barrier
+      // (no issue slots spent polling)
+      if (tid == 0) {
+        issue_layer(tmem, sa, sw + layer * 8192, bar);
+        if (!mbar_wait(bar, phase)) failed = 1;
+      }
       phase ^= 1;
       // a wait that gave up leaves the accumulators unread: every thread sees the flag here
       __syncthreads();
       if (failed) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      uint32_t r[64];
-      tmem_ld64(tl, r);
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       const float* bias = layer == 0 ? sm.b2 : sm.b3;
 #pragma unroll
-      for (int o = 0; o < 64; ++o) acc[o] = tanh_fast(__uint_as_float(r[o]) + bias[o]);
-      if (layer == 0) {
+      for (int hh = 0; hh < 2; ++hh) {
+        uint32_t r[32];
+        tmem_ld32(tl + hh * 32, r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (layer == 0) {
 #pragma unroll
-        for (int kc = 0; kc < 8; ++kc) {
-          uint32_t q[4];
+          for (int kc = 0; kc < 4; ++kc) {
+            uint32_t q[4];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) q[j] = pack_bf16x2(acc[kc * 8 + 2 * j], acc[kc * 8 + 2 * j + 1]);
-          *reinterpret_cast<uint4*>(sA + kc * 2048 + rowoff) = make_uint4(q[0], q[1], q[2], q[3]);
+            for (int j = 0; j < 4; ++j) {
+              const int o = kc * 8 + 2 * j;
+              q[j] = tanh_bf16x2(pack_bf16x2(__uint_as_float(r[o]) + bias[hh * 32 + o],
+                                             __uint_as_float(r[o + 1]) + bias[hh * 32 + o + 1]));
+            }
+            *reinterpret_cast<uint4*>(sA + (hh * 4 + kc) * 2048 + rowoff) = make_uint4(q[0], q[1], q[2], q[3]);
+          }
+        } else {
+#pragma unroll
+          for (int o = 0; o < 32; ++o) {
+            const float v = tanh_fast(__uint_as_float(r[o]) + bias[hh * 32 + o]);
+            y4[0] = fmaf(sm.w4[hh * 32 + o], v, y4[0]);
+            if (ck.raw) {
+#pragma unroll
+              for (int j = 1; j < MLP_NOUT; ++j) y4[j] = fmaf(sm.w4[j * 64 + hh * 32 + o], v, y4[j]);
+            }
+          }
         }
       }
     }
     __syncthreads();
     if (failed) break;
-    // layer 4 (CUDA cores) and the properties
     double y[MLP_NOUT];
 #pragma unroll
-    for (int j = 0; j < MLP_NOUT; ++j) {
-      float s = sm.b4[j];
-#pragma unroll
-      for (int o = 0; o < 64; ++o) s = fmaf(sm.w4[j * 64 + o], acc[o], s);
-      y[j] = nm.ya[j] * (double)s + nm.yb[j];
-    }
+    for (int j = 0; j < MLP_NOUT; ++j) y[j] = nm.ya[j] * (double)y4[j] + nm.yb[j];
     // the network's T selects the table row where the rho*h search starts; the table judges it
     // exactly (the search from that row is verified, else it runs from scratch), so the stored
     // properties are always the table lookup's
@@ -435,7 +461,7 @@ void launch_mlp_props(const ThermoTab& tb, const MlpNorm& nm, const MlpSmall& sm
                       const uint16_t* wpack, const T* rhoh, T* h, T* t, T* k, T* d, T* m, int64_t n,
                       unsigned long long* nfallback, cudaStream_t st) {
   int64_t tiles = (n + 127) / 128;
-  if (tiles > 148 * 4) tiles = 148 * 4;
+  if (tiles > 148 * 6) tiles = 148 * 6;  // six CTAs per SM: 6 x 64 TMEM columns, 6 x 32 KB shared
   if (tiles < 1) tiles = 1;
   mlp_props_kernel<T><<<(unsigned)tiles, 128, 0, st>>>(tb, nm, sm, ck, wpack, rhoh, h, t, k, d, m, n, nfallback);
 }
