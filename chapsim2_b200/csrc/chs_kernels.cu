@@ -1476,6 +1476,36 @@ void launch_energy_advance(T* rhs, T* rhs0, T* rhoh, int64_t n, double dt, doubl
   energy_advance_kernel<T><<<148 * 8, 256, 0, st>>>(rhs, rhs0, rhoh, n, dt, gam, zeta);
 }
 
+// the energy fractional step and rho*h update followed by the property update of the new rho*h,
+// one pass (the same arithmetic as energy_advance_kernel then property_update_kernel)
+template <typename T>
+__global__ void energy_advance_props_kernel(const __grid_constant__ ThermoTab tb, T* __restrict__ rhs,
+                                            T* __restrict__ rhs0, T* __restrict__ rhoh, T* __restrict__ h,
+                                            T* __restrict__ t, T* __restrict__ k, T* __restrict__ d,
+                                            T* __restrict__ m, int64_t n, double dt, double gam, double zeta) {
+  const T tdt = T(dt), tg = T(gam), tz = T(zeta);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T cur = rhs[i], last = rhs0[i];
+    const T tot = tg * cur + tz * last;
+    rhs0[i] = cur;
+    const T r1 = tdt * tot;
+    rhs[i] = r1;
+    const T rn = rhoh[i] + r1;
+    rhoh[i] = rn;
+    const CellProps p = props_from_dh(tb, (double)rn);
+    h[i] = T(p.h);
+    t[i] = T(p.t);
+    k[i] = T(p.k);
+    d[i] = T(p.d);
+    m[i] = T(p.m);
+  }
+}
+template <typename T>
+void launch_energy_advance_props(const ThermoTab& tb, T* rhs, T* rhs0, T* rhoh, T* h, T* t, T* k, T* d, T* m,
+                                 int64_t n, double dt, double gam, double zeta, cudaStream_t st) {
+  energy_advance_props_kernel<T><<<148 * 8, 256, 0, st>>>(tb, rhs, rhs0, rhoh, h, t, k, d, m, n, dt, gam, zeta);
+}
+
 template <typename T>
 __global__ void fill_kernel(T* __restrict__ a, double v, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -1518,6 +1548,8 @@ void launch_stats_update(const StatsIO<T>& s, cudaStream_t st) {
   template void launch_wall_props<T>(const ThermoTab&, const T*, int, int, int, int, int, T*, T*, T*, T*,        \
                                      cudaStream_t);                                                             \
   template void launch_energy_advance<T>(T*, T*, T*, int64_t, double, double, double, cudaStream_t); \
+  template void launch_energy_advance_props<T>(const ThermoTab&, T*, T*, T*, T*, T*, T*, T*, T*, int64_t, double,    \
+                                               double, double, cudaStream_t);                                  \
   template void launch_fill<T>(T*, double, int64_t, cudaStream_t);                                           \
   template void launch_stats_update<T>(const StatsIO<T>&, cudaStream_t);
 CHS_INST_THERMO(double)

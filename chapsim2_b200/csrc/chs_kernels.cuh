@@ -177,6 +177,11 @@ template <typename T>
 void launch_energy_advance(T* rhs, T* rhs0, T* rhoh, int64_t n, double dt, double gam, double zeta,
                            cudaStream_t st);
 
+// launch_energy_advance followed by launch_property_update of the new rho*h, in one pass
+template <typename T>
+void launch_energy_advance_props(const ThermoTab& tb, T* rhs, T* rhs0, T* rhoh, T* h, T* t, T* k, T* d, T* m,
+                                 int64_t n, double dt, double gam, double zeta, cudaStream_t st);
+
 // a[i] = v
 template <typename T>
 void launch_fill(T* a, double v, int64_t n, cudaStream_t st);

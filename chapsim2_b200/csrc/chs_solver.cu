@@ -633,17 +633,18 @@ void run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const
          launch_fractional_step(out, rhs0, pfc_scratch, (int64_t)nout, H->dt, H->tGamma[isub], H->tZeta[isub],
                                 H->tAlpha[isub], st));
     H->launches++;
+  } else if (epilogue == EP_ENERGY && props) {
+    // fractional step, rho*h update and table property update in one pass
+    PROFD(H, 3, 10.0 * sizeof(T) * nout, bufs(), bufs(out, rhs0, rhoh, H->hEnth, H->tTemp, H->kCond, H->dDens, H->mVisc),
+          launch_energy_advance_props<T>(H->tab, out, rhs0, rhoh, reinterpret_cast<T*>(H->hEnth),
+                                         reinterpret_cast<T*>(H->tTemp), reinterpret_cast<T*>(H->kCond),
+                                         reinterpret_cast<T*>(H->dDens), reinterpret_cast<T*>(H->mVisc),
+                                         (int64_t)nout, H->dt, H->tGamma[isub], H->tZeta[isub], st));
+    H->launches++;
   } else if (epilogue == EP_ENERGY) {
     PROFD(H, 3, 5.0 * sizeof(T) * nout, bufs(), bufs(out, rhs0, rhoh),
          launch_energy_advance<T>(out, rhs0, rhoh, (int64_t)nout, H->dt, H->tGamma[isub], H->tZeta[isub], st));
     H->launches++;
-    if (props) {
-      PROFD(H, 3, 6.0 * sizeof(T) * nout, bufs(rhoh), bufs(H->hEnth, H->tTemp, H->kCond, H->dDens, H->mVisc),
-           launch_property_update<T>(H->tab, rhoh, reinterpret_cast<T*>(H->hEnth), reinterpret_cast<T*>(H->tTemp),
-                                     reinterpret_cast<T*>(H->kCond), reinterpret_cast<T*>(H->dDens),
-                                     reinterpret_cast<T*>(H->mVisc), (int64_t)nout, st));
-      H->launches++;
-    }
   }
 }
 
