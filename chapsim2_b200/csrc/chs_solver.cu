@@ -562,10 +562,9 @@ void pair_terms(std::vector<OpTerm<T>>& v, int d, int fam, Pair bc1, const typen
 // gradient in pfc_scratch.
 template <typename T>
 void run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const int m[3], int epilogue, T* rhs0,
-               int isub, T* pfc_scratch, T* rhoh = nullptr, bool props = false) {
-  cudaStream_t st = H->st;
+               int isub, T* pfc_scratch, T* rhoh = nullptr, bool props = false, bool prefer_fused = false) {
   const size_t tsz = H->book.table.size();
-  bool fuse = H->tune_fuse && !terms.empty() && (int)terms.size() <= kMaxFusedTerms;
+  bool fuse = (H->tune_fuse || prefer_fused) && !terms.empty() && (int)terms.size() <= kMaxFusedTerms;
   for (const auto& t : terms) {
     const OpPlan& P = H->plan(t.d, t.fam, t.bc, t.fbc != nullptr);
     if (P.tdma || (t.fam != D1C2P && t.fam != D1P2C)) fuse = false;
@@ -608,11 +607,24 @@ void run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const
     const double ob = epilogue == EP_STORE ? 1.0 : epilogue == EP_ACCUM ? 2.0 : epilogue == EP_FRAC ? 3.0
                                                                           : (props ? 9.0 : 4.0);
     bytes += (double)sizeof(T) * ob * nout;
-    H->dag_barrier_begin();
+    chs_handle::Bufs rd, wr;
+    for (const auto& t : terms) {
+      for (int q = 0; q < 2; ++q)
+        for (const void* a : {(const void*)t.in.t[q].X, (const void*)t.in.t[q].Y, (const void*)t.in.t[q].Z})
+          if (a) rd.p[rd.n++] = a;
+      if (t.fbc) rd.p[rd.n++] = t.fbc;
+    }
+    wr.p[wr.n++] = out;
+    for (const void* a : {(const void*)rhs0, (const void*)rhoh}) if (a) wr.p[wr.n++] = a;
+    if (props)
+      for (const void* a : {(const void*)H->hEnth, (const void*)H->tTemp, (const void*)H->kCond,
+                            (const void*)H->dDens, (const void*)H->mVisc})
+        wr.p[wr.n++] = a;
+    cudaStream_t ls = H->dag_begin(rd, wr);
     cudaEvent_t e0 = H->prof_begin();
-    launch_fused(F, H->table, st);
+    launch_fused(F, H->table, ls);
     H->prof_end(e0, 0, -1, bytes);
-    H->dag_barrier_end();
+    H->dag_end();
     H->launches++;
     return;
   }
@@ -1163,7 +1175,9 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
     std::vector<OpTerm<T>> t = {term<T>(0, D1P2C, bx_qx, any, src(A(ux)), s_pcc, coeff, 0),
                                 term<T>(1, D1P2C, by_qy, nullptr, src(A(uy)), s_cpc, coeff, 0),
                                 term<T>(2, D1P2C, bz_qz, nullptr, src(A(uz)), s_ccp, coeff, 0)};
-    run_fused<T>(H, t, A(H->pcor), s_ccc, EP_STORE, nullptr, isub, nullptr);
+    // the divergence of three single-array terms: one fused pass (measured faster than three
+    // accumulating operators; the momentum sums are not)
+    run_fused<T>(H, t, A(H->pcor), s_ccc, EP_STORE, nullptr, isub, nullptr, nullptr, false, true);
   }
   poisson_device<T>(H, A(H->pcor));
   PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, bufs(H->pcor), bufs(H->pres),
