@@ -21,13 +21,22 @@ namespace chs {
 // ---------------------------------------------------------------------------
 constexpr int kWin = 4;
 
+// the value of one input term from its array values (the one formula every path uses, so the
+// window, segment and vector paths give the same bits)
+template <int M, typename T>
+__device__ __forceinline__ T term_val(const TermT<T>& t, T x, T y, T z) {
+  if (M == T_X) return T(t.s) * x;
+  if (M == T_XY) return T(t.s) * (x * y);
+  if (M == T_XpY) return T(t.s) * (x + T(t.c) * y);
+  if (M == T_XpYZ) return T(t.s) * (x + T(t.c) * y) * z;
+  return T(0);
+}
 template <int M, typename T>
 __device__ __forceinline__ T term_ro(const TermT<T>& t, int a) {
-  if (M == T_X) return T(t.s) * __ldg(t.X + a);
-  if (M == T_XY) return T(t.s) * (__ldg(t.X + a) * __ldg(t.Y + a));
-  if (M == T_XpY) return T(t.s) * (__ldg(t.X + a) + T(t.c) * __ldg(t.Y + a));
-  if (M == T_XpYZ) return T(t.s) * (__ldg(t.X + a) + T(t.c) * __ldg(t.Y + a)) * __ldg(t.Z + a);
-  return T(0);
+  const T x = __ldg(t.X + a);
+  const T y = (M == T_XY || M == T_XpY || M == T_XpYZ) ? __ldg(t.Y + a) : T(0);
+  const T z = M == T_XpYZ ? __ldg(t.Z + a) : T(0);
+  return term_val<M>(t, x, y, z);
 }
 template <int M0, int M1, typename T>
 __device__ __forceinline__ T expr_ro(const LineIOT<T>& io, int a) {
@@ -165,12 +174,56 @@ __global__ void __launch_bounds__(256) stencil_winz_kernel(const __grid_constant
 // x lines (DIR 0): each warp forms a segment of kSeg consecutive outputs of one line from a
 // warp-private shared-memory copy of the input expression over the segment and two values either
 // side (wrapped for periodic lines); boundary rows of non-periodic lines read the input directly
-constexpr int kSeg = 128, kSegHalo = 2, kSegLen = kSeg + 2 * kSegHalo;
+constexpr int kSeg = 128, kSegHalo = 2;
+
+// 16-byte vectors of the field type: the main part of a segment is loaded with one vector load
+// per array and lane where the line start is 16-byte aligned
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int n = 4;
+};
+
+// the V array values of a term at a (a multiple of V, arrays 16-byte aligned)
+template <int M, typename T, int V>
+__device__ __forceinline__ void term_load_vec(const TermT<T>& t, int a, T (&x)[V], T (&y)[V], T (&z)[V]) {
+  using VT = typename Vec16<T>::type;
+  *reinterpret_cast<VT*>(x) = __ldg(reinterpret_cast<const VT*>(t.X + a));
+  if (M == T_XY || M == T_XpY || M == T_XpYZ) *reinterpret_cast<VT*>(y) = __ldg(reinterpret_cast<const VT*>(t.Y + a));
+  else
+#pragma unroll
+    for (int u = 0; u < V; ++u) y[u] = T(0);
+  if (M == T_XpYZ) *reinterpret_cast<VT*>(z) = __ldg(reinterpret_cast<const VT*>(t.Z + a));
+  else
+#pragma unroll
+    for (int u = 0; u < V; ++u) z[u] = T(0);
+}
+// expr_ro at V consecutive positions from a, element by element the same formula
+template <int M0, int M1, typename T, int V>
+__device__ __forceinline__ void expr_vec(const LineIOT<T>& io, int a, T (&v)[V]) {
+  T x0[V], y0[V], z0[V], x1[V], y1[V], z1[V];
+  term_load_vec<M0>(io.t[0], a, x0, y0, z0);
+  if (M1 != T_NONE) term_load_vec<M1>(io.t[1], a, x1, y1, z1);
+#pragma unroll
+  for (int u = 0; u < V; ++u) {
+    v[u] = term_val<M0>(io.t[0], x0[u], y0[u], z0[u]);
+    if (M1 != T_NONE) v[u] += term_val<M1>(io.t[1], x1[u], y1[u], z1[u]);
+  }
+}
 template <typename T, int FAM, int M0, int M1>
 __global__ void __launch_bounds__(256) stencil_xseg_kernel(const __grid_constant__ OpPlan P,
                                                            const __grid_constant__ LineIOT<T> io,
                                                            const double* __restrict__ table, int nlines, int nseg) {
-  __shared__ T tile[8][kSegLen];
+  constexpr int V = Vec16<T>::n;
+  constexpr int kO = V;  // slot of the segment's first value (16-byte aligned); halo at kO-2, kO-1
+  __shared__ __align__(16) T tile[8][kSeg + 2 * V];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gw = blockIdx.x * 8 + warp;  // global warp = line * nseg + segment
   if (gw >= nlines * nseg) return;
@@ -181,17 +234,30 @@ __global__ void __launch_bounds__(256) stencil_xseg_kernel(const __grid_constant
   T* s = tile[warp];
   // the segment: no wrap or clamp unless it runs past the end of the line
   const bool full = i0 + kSeg <= nin;
+  const uintptr_t al = reinterpret_cast<uintptr_t>(io.t[0].X) | reinterpret_cast<uintptr_t>(io.t[0].Y) |
+                       reinterpret_cast<uintptr_t>(io.t[0].Z) | reinterpret_cast<uintptr_t>(io.t[1].X) |
+                       reinterpret_cast<uintptr_t>(io.t[1].Y) | reinterpret_cast<uintptr_t>(io.t[1].Z);
+  if (full && (al & 15) == 0 && nin % V == 0) {
 #pragma unroll
-  for (int m = 0; m < kSeg / 32; ++m) {
-    int q = i0 + lane + 32 * m;
-    if (!full) {
-      if (wrap) {
-        while (q >= nin) q -= nin;  // lines shorter than a segment wrap more than once
-      } else {
-        q = q >= nin ? nin - 1 : q;  // clamped slots are read by boundary rows only
-      }
+    for (int m = 0; m < kSeg / (32 * V); ++m) {
+      const int c = lane + 32 * m;
+      T v[V];
+      expr_vec<M0, M1>(io, ibase + i0 + c * V, v);
+      *reinterpret_cast<typename Vec16<T>::type*>(s + kO + c * V) = *reinterpret_cast<const typename Vec16<T>::type*>(v);
     }
-    s[kSegHalo + lane + 32 * m] = expr_ro<M0, M1>(io, ibase + q);
+  } else {
+#pragma unroll
+    for (int m = 0; m < kSeg / 32; ++m) {
+      int q = i0 + lane + 32 * m;
+      if (!full) {
+        if (wrap) {
+          while (q >= nin) q -= nin;  // lines shorter than a segment wrap more than once
+        } else {
+          q = q >= nin ? nin - 1 : q;  // clamped slots are read by boundary rows only
+        }
+      }
+      s[kO + lane + 32 * m] = expr_ro<M0, M1>(io, ibase + q);
+    }
   }
   // two values either side (lanes 0-1 left, 2-3 right)
   if (lane < 2 * kSegHalo) {
@@ -202,11 +268,11 @@ __global__ void __launch_bounds__(256) stencil_xseg_kernel(const __grid_constant
     } else {
       q = q < 0 ? 0 : (q >= nin ? nin - 1 : q);
     }
-    s[lane < kSegHalo ? lane : kSeg + lane] = expr_ro<M0, M1>(io, ibase + q);
+    s[lane < kSegHalo ? kO - kSegHalo + lane : kO + kSeg + (lane - kSegHalo)] = expr_ro<M0, M1>(io, ibase + q);
   }
   __syncwarp();
   const T r1 = T(P.r1), r2 = T(P.r2), dd = T(P.dd);
-  auto fs = [&](int qq) -> T { return s[qq - i0 + kSegHalo]; };
+  auto fs = [&](int qq) -> T { return s[qq - i0 + kO]; };
   const int64_t obase = (int64_t)L * nout;
 #pragma unroll
   for (int m = 0; m < kSeg / 32; ++m) {
