@@ -102,80 +102,6 @@ __device__ __forceinline__ void finish_row(const OpPlan& P, const LineIOT<T>& io
   store_out(io, a, T(io.g), v);
 }
 
-// y (DIR 1) or z (DIR 2) lines: thread = (position in the cross plane, chunk of kWin rows)
-template <typename T, int DIR, int FAM, int M0, int M1>
-__device__ __forceinline__ void stencil_win_body(const OpPlan& P, const LineIOT<T>& io,
-                                                 const double* __restrict__ table, int nlines) {
-  using RC = Reach<FAM>;
-  constexpr int W = kWin + RC::hi4 - RC::lo4;
-  const int nin = P.nin, nout = P.nout, n1 = io.n1;
-  int L, ibase, istride, p0;
-  int64_t obase, ostride;
-  if (DIR == 1) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    p0 = (blockIdx.y * blockDim.y + threadIdx.y) * kWin;
-    const int k = blockIdx.z;
-    if (i >= n1 || p0 >= nout) return;
-    L = i + n1 * k;
-    ibase = k * nin * n1 + i;
-    istride = n1;
-    obase = (int64_t)k * nout * n1 + i;
-    ostride = n1;
-  } else {
-    const int plane = n1 * io.n2;
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    p0 = blockIdx.y * kWin;
-    if (q >= plane) return;
-    L = q;
-    ibase = q;
-    istride = plane;
-    obase = q;
-    ostride = plane;
-  }
-  const T r1 = T(P.r1), r2 = T(P.r2), dd = T(P.dd);
-  const bool r2on = P.r2 != 0.0, wrap = P.wrap != 0;
-  T w[W];
-#pragma unroll
-  for (int s = 0; s < W; ++s) {
-    // the 2-point formula never reads the outermost slots
-    const bool need = r2on || (s >= RC::lo2 - RC::lo4 && s <= kWin - 1 + RC::hi2 - RC::lo4);
-    int q = p0 + RC::lo4 + s;
-    // wrapped (periodic) or clamped; clamped slots are read only by boundary rows, which do not
-    // use the window
-    if (wrap) q = q < 0 ? q + nin : (q >= nin ? q - nin : q);
-    else q = q < 0 ? 0 : (q >= nin ? nin - 1 : q);
-    w[s] = need ? expr_ro<M0, M1>(io, ibase + q * istride) : T(0);
-  }
-#pragma unroll
-  for (int u = 0; u < kWin; ++u) {
-    const int p = p0 + u;
-    if (p >= nout) break;
-    T v;
-    if (wrap || (p >= P.b_lo && p <= P.b_hi)) v = bulk_win<FAM>(w, u - RC::lo4, r1, r2) * dd;
-    else v = boundary_row<T, M0, M1>(P, io, ibase, istride, p, L, nlines);
-    finish_row(P, io, table, p, L, nlines, obase + (int64_t)p * ostride, v);
-  }
-}
-
-// the y kernel keeps at most 51 registers (five CTAs per SM); the z kernel needs no cap (measured)
-template <typename T, int FAM, int M0, int M1>
-__global__ void __launch_bounds__(256, 5) stencil_winy_kernel(const __grid_constant__ OpPlan P,
-                                                              const __grid_constant__ LineIOT<T> io,
-                                                              const double* __restrict__ table, int nlines) {
-  stencil_win_body<T, 1, FAM, M0, M1>(P, io, table, nlines);
-}
-template <typename T, int FAM, int M0, int M1>
-__global__ void __launch_bounds__(256) stencil_winz_kernel(const __grid_constant__ OpPlan P,
-                                                           const __grid_constant__ LineIOT<T> io,
-                                                           const double* __restrict__ table, int nlines) {
-  stencil_win_body<T, 2, FAM, M0, M1>(P, io, table, nlines);
-}
-
-// x lines (DIR 0): each warp forms a segment of kSeg consecutive outputs of one line from a
-// warp-private shared-memory copy of the input expression over the segment and two values either
-// side (wrapped for periodic lines); boundary rows of non-periodic lines read the input directly
-constexpr int kSeg = 128, kSegHalo = 2;
-
 // 16-byte vectors of the field type: the main part of a segment is loaded with one vector load
 // per array and lane where the line start is 16-byte aligned
 template <typename T>
@@ -217,6 +143,121 @@ __device__ __forceinline__ void expr_vec(const LineIOT<T>& io, int a, T (&v)[V])
     if (M1 != T_NONE) v[u] += term_val<M1>(io.t[1], x1[u], y1[u], z1[u]);
   }
 }
+
+// y (DIR 1) or z (DIR 2) lines: each thread owns V = 16 / sizeof(T) adjacent x positions (one
+// 16-byte vector per load and store) and kWin consecutive rows of their lines; a register window
+// of the input expression along the line serves all kWin rows (each input value loaded once per
+// thread).  Needs n1 % V == 0 and 16-byte aligned arrays (checked by the launcher).
+template <typename T, int DIR, int FAM, int M0, int M1>
+__device__ __forceinline__ void stencil_win_body(const OpPlan& P, const LineIOT<T>& io,
+                                                 const double* __restrict__ table, int nlines) {
+  using RC = Reach<FAM>;
+  using VT = typename Vec16<T>::type;
+  constexpr int V = Vec16<T>::n;
+  constexpr int W = kWin + RC::hi4 - RC::lo4;
+  const int nin = P.nin, nout = P.nout, n1 = io.n1;
+  int L, ibase, istride, p0;
+  int64_t obase, ostride;
+  if (DIR == 1) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) * V;
+    p0 = (blockIdx.y * blockDim.y + threadIdx.y) * kWin;
+    const int k = blockIdx.z;
+    if (i >= n1 || p0 >= nout) return;
+    L = i + n1 * k;
+    ibase = k * nin * n1 + i;
+    istride = n1;
+    obase = (int64_t)k * nout * n1 + i;
+    ostride = n1;
+  } else {
+    const int plane = n1 * io.n2;
+    const int q = (blockIdx.x * blockDim.x + threadIdx.x) * V;
+    p0 = blockIdx.y * kWin;
+    if (q >= plane) return;
+    L = q;
+    ibase = q;
+    istride = plane;
+    obase = q;
+    ostride = plane;
+  }
+  const T r1 = T(P.r1), r2 = T(P.r2), dd = T(P.dd);
+  const bool r2on = P.r2 != 0.0, wrap = P.wrap != 0;
+  T w[W][V];
+#pragma unroll
+  for (int s = 0; s < W; ++s) {
+    // the 2-point formula never reads the outermost slots
+    const bool need = r2on || (s >= RC::lo2 - RC::lo4 && s <= kWin - 1 + RC::hi2 - RC::lo4);
+    int q = p0 + RC::lo4 + s;
+    // wrapped (periodic) or clamped; clamped slots are read only by boundary rows, which do not
+    // use the window
+    if (wrap) q = q < 0 ? q + nin : (q >= nin ? q - nin : q);
+    else q = q < 0 ? 0 : (q >= nin ? nin - 1 : q);
+    if (need) {
+      expr_vec<M0, M1>(io, ibase + q * istride, w[s]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < V; ++e) w[s][e] = T(0);
+    }
+  }
+  const bool plain = io.omode == O_STORE && !io.accumulate;
+  const T g = T(io.g);
+#pragma unroll
+  for (int u = 0; u < kWin; ++u) {
+    const int p = p0 + u;
+    if (p >= nout) break;
+    T v[V];
+    if (wrap || (p >= P.b_lo && p <= P.b_hi)) {
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        T col[W];
+#pragma unroll
+        for (int s = 0; s < W; ++s) col[s] = w[s][e];
+        v[e] = bulk_win<FAM>(col, u - RC::lo4, r1, r2) * dd;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < V; ++e) v[e] = boundary_row<T, M0, M1>(P, io, ibase + e, istride, p, L + e, nlines);
+    }
+    if (P.lmap >= 0) {
+      const T mp = T(table[P.lmap + p]);
+#pragma unroll
+      for (int e = 0; e < V; ++e) v[e] *= mp;
+    }
+    if ((P.neu1 && p == 0) || (P.neu2 && p == nout - 1)) {
+      const int off = p == 0 ? 0 : nlines;
+#pragma unroll
+      for (int e = 0; e < V; ++e) v[e] = io.fbc[off + L + e];
+    }
+    const int64_t a = obase + (int64_t)p * ostride;
+    if (plain) {
+      T o[V];
+#pragma unroll
+      for (int e = 0; e < V; ++e) o[e] = g * v[e];
+      *reinterpret_cast<VT*>(io.out + a) = *reinterpret_cast<const VT*>(o);
+    } else {
+#pragma unroll
+      for (int e = 0; e < V; ++e) store_out(io, a + e, g, v[e]);
+    }
+  }
+}
+
+template <typename T, int FAM, int M0, int M1>
+__global__ void __launch_bounds__(256) stencil_winy_kernel(const __grid_constant__ OpPlan P,
+                                                              const __grid_constant__ LineIOT<T> io,
+                                                              const double* __restrict__ table, int nlines) {
+  stencil_win_body<T, 1, FAM, M0, M1>(P, io, table, nlines);
+}
+template <typename T, int FAM, int M0, int M1>
+__global__ void __launch_bounds__(256) stencil_winz_kernel(const __grid_constant__ OpPlan P,
+                                                           const __grid_constant__ LineIOT<T> io,
+                                                           const double* __restrict__ table, int nlines) {
+  stencil_win_body<T, 2, FAM, M0, M1>(P, io, table, nlines);
+}
+
+// x lines (DIR 0): each warp forms a segment of kSeg consecutive outputs of one line from a
+// warp-private shared-memory copy of the input expression over the segment and two values either
+// side (wrapped for periodic lines); boundary rows of non-periodic lines read the input directly
+constexpr int kSeg = 128, kSegHalo = 2;
+
 template <typename T, int FAM, int M0, int M1>
 __global__ void __launch_bounds__(256) stencil_xseg_kernel(const __grid_constant__ OpPlan P,
                                                            const __grid_constant__ LineIOT<T> io,
@@ -294,13 +335,16 @@ void launch_win(const OpPlan& P, const LineIOT<T>& io, const double* table, cuda
     stencil_xseg_kernel<T, FAM, M0, M1><<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(P, io, table, nlines, nseg);
   } else if (DIR == 1) {
     // wide rows of x per warp group (contiguous DRAM segments), the rest of the CTA along y
-    const int bx = io.n1 >= 128 ? 128 : (io.n1 >= 64 ? 64 : 32), by = 256 / bx;
+    constexpr int V = Vec16<T>::n;
+    const int nv = io.n1 / V;
+    const int bx = nv >= 128 ? 128 : (nv >= 64 ? 64 : 32), by = 256 / bx;
     const int chunks = (P.nout + kWin - 1) / kWin;
-    dim3 grid((unsigned)((io.n1 + bx - 1) / bx), (unsigned)((chunks + by - 1) / by), (unsigned)io.n3);
+    dim3 grid((unsigned)((nv + bx - 1) / bx), (unsigned)((chunks + by - 1) / by), (unsigned)io.n3);
     stencil_winy_kernel<T, FAM, M0, M1><<<grid, dim3(bx, by), 0, st>>>(P, io, table, nlines);
   } else {
-    const int plane = io.n1 * io.n2;
-    dim3 grid((unsigned)((plane + 255) / 256), (unsigned)((P.nout + kWin - 1) / kWin));
+    constexpr int V = Vec16<T>::n;
+    const int nv = io.n1 * io.n2 / V;
+    dim3 grid((unsigned)((nv + 255) / 256), (unsigned)((P.nout + kWin - 1) / kWin));
     stencil_winz_kernel<T, FAM, M0, M1><<<grid, 256, 0, st>>>(P, io, table, nlines);
   }
 }
@@ -312,6 +356,15 @@ bool try_launch_win(const OpPlan& P, const LineIOT<T>& io, const double* table, 
                            int nlines) {
   const int m0 = io.t[0].mode, m1 = io.t[1].mode;
   const int sig = m0 * 8 + m1;
+  if (DIR != 0) {
+    // y and z kernels: V adjacent x positions per thread, 16-byte vectors
+    constexpr int V = Vec16<T>::n;
+    uintptr_t al = reinterpret_cast<uintptr_t>(io.out) | reinterpret_cast<uintptr_t>(io.onum);
+    for (int q = 0; q < 2; ++q)
+      al |= reinterpret_cast<uintptr_t>(io.t[q].X) | reinterpret_cast<uintptr_t>(io.t[q].Y) |
+            reinterpret_cast<uintptr_t>(io.t[q].Z);
+    if (io.n1 % V != 0 || (al & 15) != 0) return false;
+  }
 #define CHS_WIN(F, A, B)                                        \
   if (P.fam == F && sig == A * 8 + B) {                         \
     launch_win<T, DIR, F, A, B>(P, io, table, st, nlines);      \
