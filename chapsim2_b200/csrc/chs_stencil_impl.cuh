@@ -313,8 +313,29 @@ __global__ void __launch_bounds__(256) stencil_xseg_kernel(const __grid_constant
   }
   __syncwarp();
   const T r1 = T(P.r1), r2 = T(P.r2), dd = T(P.dd);
-  auto fs = [&](int qq) -> T { return s[qq - i0 + kO]; };
   const int64_t obase = (int64_t)L * nout;
+  // periodic full segments with a plain store: each lane forms V adjacent outputs from three
+  // 16-byte tile reads and stores them as one vector
+  const bool vout = wrap && i0 + kSeg <= nout && nout % V == 0 && io.omode == O_STORE && !io.accumulate &&
+                    (reinterpret_cast<uintptr_t>(io.out) & 15) == 0;
+  if (vout) {
+    using VT = typename Vec16<T>::type;
+    const T g = T(io.g);
+#pragma unroll
+    for (int m = 0; m < kSeg / (32 * V); ++m) {
+      const int c = lane + 32 * m;  // outputs i0 + c*V .. i0 + c*V + V-1
+      T win[3 * V];                 // input positions -V .. 2V-1 relative to the chunk
+      *reinterpret_cast<VT*>(win) = *reinterpret_cast<const VT*>(s + kO + (c - 1) * V);
+      *reinterpret_cast<VT*>(win + V) = *reinterpret_cast<const VT*>(s + kO + c * V);
+      *reinterpret_cast<VT*>(win + 2 * V) = *reinterpret_cast<const VT*>(s + kO + (c + 1) * V);
+      T o[V];
+#pragma unroll
+      for (int e = 0; e < V; ++e) o[e] = g * (bulk_win<FAM>(win, V + e, r1, r2) * dd);
+      *reinterpret_cast<VT*>(io.out + obase + i0 + c * V) = *reinterpret_cast<const VT*>(o);
+    }
+    return;
+  }
+  auto fs = [&](int qq) -> T { return s[qq - i0 + kO]; };
 #pragma unroll
   for (int m = 0; m < kSeg / 32; ++m) {
     const int p = i0 + lane + 32 * m;
