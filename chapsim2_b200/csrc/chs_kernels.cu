@@ -1187,11 +1187,57 @@ void launch_spectral_divide(double2* data, int nxh, int ny, int nz, const double
 // elementwise and reductions.  Field arrays are T (double, or float in the mixed-precision
 // form); scalars, reduction accumulators and results stay double.
 // ===========================================================================
+// 16-byte vectors for the streaming kernels: the elements are processed V at a time where every
+// array is 16-byte aligned (the same per-element arithmetic), the remainder one at a time
+template <typename T>
+struct EVec;
+template <>
+struct EVec<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
+template <>
+struct EVec<float> {
+  using type = float4;
+  static constexpr int n = 4;
+};
+__device__ __forceinline__ bool aligned16(const void* a, const void* b = nullptr, const void* c = nullptr,
+                                          const void* d = nullptr) {
+  return ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) | reinterpret_cast<uintptr_t>(c) |
+           reinterpret_cast<uintptr_t>(d)) & 15) == 0;
+}
+template <typename T>
+__device__ __forceinline__ typename EVec<T>::type vld(const T* p, int64_t iv) {
+  return reinterpret_cast<const typename EVec<T>::type*>(p)[iv];
+}
+template <typename T>
+__device__ __forceinline__ void vst(T* p, int64_t iv, const typename EVec<T>::type& v) {
+  reinterpret_cast<typename EVec<T>::type*>(p)[iv] = v;
+}
+
 template <typename T>
 __global__ void fractional_step_kernel(T* __restrict__ rhs1, T* __restrict__ rhs0, const T* __restrict__ pfc,
                                        int64_t n, double dt, double gam, double zeta, double alpha) {
   const T tdt = T(dt), tg = T(gam), tz = T(zeta), ta = T(alpha);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  constexpr int V = EVec<T>::n;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t nv = aligned16(rhs1, rhs0, pfc) ? n / V : 0;
+  for (int64_t iv = t0; iv < nv; iv += stride) {
+    typename EVec<T>::type c = vld(rhs1, iv), l = vld(rhs0, iv), f = vld(pfc, iv), o;
+    const T* cp = reinterpret_cast<const T*>(&c);
+    const T* lp = reinterpret_cast<const T*>(&l);
+    const T* fp = reinterpret_cast<const T*>(&f);
+    T* op = reinterpret_cast<T*>(&o);
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      T tot = tg * cp[e] + tz * lp[e];
+      tot = tot + ta * fp[e];
+      op[e] = tdt * tot;
+    }
+    vst(rhs0, iv, c);
+    vst(rhs1, iv, o);
+  }
+  for (int64_t i = nv * V + t0; i < n; i += stride) {
     const T cur = rhs1[i], last = rhs0[i];
     T tot = tg * cur + tz * last;
     rhs0[i] = cur;
@@ -1251,8 +1297,18 @@ template <typename T>
 __global__ void update_q_kernel(T* __restrict__ q, const T* __restrict__ rhs, const double* __restrict__ sub,
                                 int64_t n) {
   const T s = sub ? T(sub[0]) : T(0);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    q[i] = q[i] + (rhs[i] - s);
+  constexpr int V = EVec<T>::n;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t nv = aligned16(q, rhs) ? n / V : 0;
+  for (int64_t iv = t0; iv < nv; iv += stride) {
+    typename EVec<T>::type qv = vld(q, iv), rv = vld(rhs, iv);
+    T* qp = reinterpret_cast<T*>(&qv);
+    const T* rp = reinterpret_cast<const T*>(&rv);
+#pragma unroll
+    for (int e = 0; e < V; ++e) qp[e] = qp[e] + (rp[e] - s);
+    vst(q, iv, qv);
+  }
+  for (int64_t i = nv * V + t0; i < n; i += stride) q[i] = q[i] + (rhs[i] - s);
 }
 template <typename T>
 void launch_update_q(T* q, const T* rhs, const double* sub, int64_t n, cudaStream_t st) {
@@ -1316,7 +1372,25 @@ template <typename T>
 __global__ void axpby_kernel(T* __restrict__ out, const T* __restrict__ a, double sa, const T* __restrict__ b,
                              double sb, const T* __restrict__ c, double sc, int64_t n) {
   const T ta = T(sa), tb = T(sb), tc = T(sc);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  constexpr int V = EVec<T>::n;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t nv = aligned16(out, a, b, c) ? n / V : 0;
+  for (int64_t iv = t0; iv < nv; iv += stride) {
+    typename EVec<T>::type av = vld(a, iv), bv = b ? vld(b, iv) : av, cv = c ? vld(c, iv) : av, o;
+    const T* ap = reinterpret_cast<const T*>(&av);
+    const T* bp = reinterpret_cast<const T*>(&bv);
+    const T* cp = reinterpret_cast<const T*>(&cv);
+    T* op = reinterpret_cast<T*>(&o);
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      T v = ta * ap[e];
+      if (b) v += tb * bp[e];
+      if (c) v += tc * cp[e];
+      op[e] = v;
+    }
+    vst(out, iv, o);
+  }
+  for (int64_t i = nv * V + t0; i < n; i += stride) {
     T v = ta * a[i];
     if (b) v += tb * b[i];
     if (c) v += tc * c[i];
