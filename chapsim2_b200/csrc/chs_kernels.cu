@@ -1143,9 +1143,91 @@ __global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data,
     for (int j = tid / lt; j < ny; j += jstep) col[(int64_t)j * nxh] = sT[j * lt + l];
 }
 
+// The same solve with one thread per (kx, kz) line working in place in global memory: at a fixed
+// row j the threads of a warp (consecutive kx) read and write consecutive values, and each thread
+// loads eight rows ahead of its sweep, so the sequential recurrences of many lines overlap.  The
+// arithmetic and its order are those of ysolve_kernel.
+constexpr int kYsBatch = 8;
+__global__ void __launch_bounds__(128) ysolve_lines_kernel(double2* __restrict__ data, int nxh, int ny, int nz,
+                                                           const double* __restrict__ Zr,
+                                                           const double* __restrict__ D,
+                                                           const double* __restrict__ pa) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (int64_t)nxh * nz) return;
+  const int kz = (int)(g / nxh), kx = (int)(g - (int64_t)kz * nxh);
+  const int64_t base = (int64_t)kz * ny * nxh + kx;
+  double2* col = data + base;
+  const double* zr = Zr + base;
+  const double* dd = D + base;
+  const int64_t s = nxh;
+  double2 tp = col[0];
+  const double Z0 = zr[0];
+  tp.x *= Z0;
+  tp.y *= Z0;
+  col[0] = tp;
+  for (int j0 = 1; j0 < ny - 1; j0 += kYsBatch) {
+    double2 v[kYsBatch];
+    double z[kYsBatch];
+#pragma unroll
+    for (int u = 0; u < kYsBatch; ++u)
+      if (j0 + u < ny - 1) {
+        v[u] = col[(j0 + u) * s];
+        z[u] = zr[(j0 + u) * s];
+      }
+#pragma unroll
+    for (int u = 0; u < kYsBatch; ++u)
+      if (j0 + u < ny - 1) {
+        const double a = __ldg(pa + j0 + u);
+        v[u].x = (v[u].x - a * tp.x) * z[u];
+        v[u].y = (v[u].y - a * tp.y) * z[u];
+        tp = v[u];
+      }
+#pragma unroll
+    for (int u = 0; u < kYsBatch; ++u)
+      if (j0 + u < ny - 1) col[(j0 + u) * s] = v[u];
+  }
+  const double zl = zr[(ny - 1) * s];
+  double2 v = col[(ny - 1) * s];
+  // TRID0's singular-pivot pin: the last unknown is zero when the pivot vanishes
+  if (zl != 0.0) {
+    v.x = (v.x - __ldg(pa + ny - 1) * tp.x) / zl;
+    v.y = (v.y - __ldg(pa + ny - 1) * tp.y) / zl;
+  } else {
+    v.x = 0.0;
+    v.y = 0.0;
+  }
+  col[(ny - 1) * s] = v;
+  for (int j0 = ny - 2; j0 >= 0; j0 -= kYsBatch) {
+    double2 w[kYsBatch];
+    double d[kYsBatch];
+#pragma unroll
+    for (int u = 0; u < kYsBatch; ++u)
+      if (j0 - u >= 0) {
+        w[u] = col[(j0 - u) * s];
+        d[u] = dd[(j0 - u) * s];
+      }
+#pragma unroll
+    for (int u = 0; u < kYsBatch; ++u)
+      if (j0 - u >= 0) {
+        w[u].x = w[u].x - d[u] * v.x;
+        w[u].y = w[u].y - d[u] * v.y;
+        v = w[u];
+      }
+#pragma unroll
+    for (int u = 0; u < kYsBatch; ++u)
+      if (j0 - u >= 0) col[(j0 - u) * s] = w[u];
+  }
+}
+
 void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* Zr, const double* D, const double* pa,
                    cudaStream_t st) {
   if (ny < 2) throw std::runtime_error("ysolve: ny must be at least 2");
+  if (ny > 160) {
+    // tall columns: the shared-memory tile leaves too few solving threads per SM
+    const int64_t n = (int64_t)nxh * nz;
+    ysolve_lines_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(data, nxh, ny, nz, Zr, D, pa);
+    return;
+  }
   int lt = 32;
   while (lt > 4 && (size_t)ny * lt * 32 > 110 * 1024) lt /= 2;
   const size_t shm = (size_t)ny * lt * 32;

@@ -9,7 +9,7 @@ from oracle import pyoracle as po
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("nc", [(16, 12, 8), (24, 18, 36), (128, 96, 128)])
+@pytest.mark.parametrize("nc", [(16, 12, 8), (24, 18, 36), (128, 96, 128), (16, 192, 12), (24, 257, 8)])
 def test_fishpack_poisson(nc):
     cfg = C.channel(nc=nc, iacc=1)
     o = po.Oracle(cfg)
