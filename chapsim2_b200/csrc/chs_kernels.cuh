@@ -17,7 +17,10 @@ namespace chs {
 enum TermMode { T_NONE = 0, T_X = 1, T_XY = 2, T_XpY = 3, T_XpYZ = 4 };
 // Output of a line operator with result v: O_STORE out = g*v (or out += g*v when accumulating),
 // O_DIV out = num / (g*v), O_MUL out = num * (g*v)
-enum OutMode { O_STORE = 0, O_DIV = 1, O_MUL = 2 };
+enum OutMode { O_STORE = 0, O_DIV = 1, O_MUL = 2, O_FRAC = 3 };
+// O_FRAC: the operator value is the pressure-gradient term of the RK3 fractional step
+// (Calculate_momentum_fractional_step): with cur = out, last = rhs0,
+// rhs0 = cur, out = dt*(gam*cur + zeta*last + alpha*g*v), and, when qupd is set, qupd += out
 
 template <typename T>
 struct TermT {
@@ -41,6 +44,9 @@ struct LineIOT {
   const T* onum;      // numerator / factor of O_DIV / O_MUL (output layout)
   int block;          // launch shape chosen by the autotuner: explicit-operator CTA size (0 = 256)
   int lt_max;         // and lines per CTA of the compact-scheme tile kernel (0 = 64)
+  T* rhs0;            // O_FRAC: previous right-hand side (updated)
+  T* qupd;            // O_FRAC: field advanced by the new right-hand side, or null
+  double dt, gam, zeta, alpha;  // O_FRAC: RK3 coefficients of the substep
 };
 using LineIO = LineIOT<double>;
 

@@ -449,11 +449,19 @@ SrcT<T> plus(const SrcT<T>& a, const SrcT<T>& b, double w) {
   return x;
 }
 
+// the RK3 fractional step an O_FRAC operator applies to its output (see OutMode)
+template <typename T>
+struct FracStep {
+  T* rhs0;
+  T* qupd;
+  double dt, gam, zeta, alpha;
+};
+
 // run one operator: direction d, family fam, operation bc, boundary planes fbc (null = absent)
 template <typename T>
 void run_op(chs_handle* H, int d, int fam, Pair bc, const typename Id<T>::type* fbc, const SrcT<T>& in,
             const int n_in[3], T* out, bool accumulate, double g, int omode = O_STORE,
-            const typename Id<T>::type* onum = nullptr) {
+            const typename Id<T>::type* onum = nullptr, const FracStep<T>* frac = nullptr) {
   const size_t tsz = H->book.table.size();
   const OpPlan& P = H->plan(d, fam, bc, fbc != nullptr);
   if (H->book.table.size() != tsz) upload_table(H);
@@ -469,14 +477,21 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const typename Id<T>::type* 
   io.onum = onum;
   io.block = H->tune_block;
   io.lt_max = H->tune_lt;
+  if (omode == O_FRAC) {
+    if (!frac) throw std::logic_error("O_FRAC operator without its fractional-step data");
+    io.rhs0 = frac->rhs0;
+    io.qupd = frac->qupd;
+    io.dt = frac->dt; io.gam = frac->gam; io.zeta = frac->zeta; io.alpha = frac->alpha;
+  }
   const double nin_tot = (double)n_in[0] * n_in[1] * n_in[2];
   const double nout_tot = nin_tot / P.nin * P.nout;
   const int narr = in.narrays();
-  const double bytes =
-      (double)sizeof(T) * (narr * nin_tot + ((accumulate || omode != O_STORE) ? 2.0 : 1.0) * nout_tot);
+  const double nrw = omode == O_FRAC ? (io.qupd ? 6.0 : 4.0) : ((accumulate || omode != O_STORE) ? 2.0 : 1.0);
+  const double bytes = (double)sizeof(T) * (narr * nin_tot + nrw * nout_tot);
+  const bool rmw = accumulate || omode == O_FRAC;
   cudaStream_t s = H->dag_begin(bufs(io.t[0].X, io.t[0].Y, io.t[0].Z, io.t[1].X, io.t[1].Y, io.t[1].Z, io.fbc, io.onum,
-                                     accumulate ? out : nullptr),
-                                bufs(out));
+                                     rmw ? out : nullptr),
+                                bufs(out, io.rhs0, io.qupd));
   cudaEvent_t e0 = H->prof_begin();
   launch_line_op(d, P, io, H->table, s);
   H->prof_end(e0, 0, d, bytes);
@@ -561,8 +576,9 @@ void pair_terms(std::vector<OpTerm<T>>& v, int d, int fam, Pair bc1, const typen
 // the elementwise epilogue.  out has extents m; for EP_FRAC the fallback puts the pressure
 // gradient in pfc_scratch.
 template <typename T>
-void run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const int m[3], int epilogue, T* rhs0,
-               int isub, T* pfc_scratch, T* rhoh = nullptr, bool props = false, bool prefer_fused = false) {
+bool run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const int m[3], int epilogue, T* rhs0,
+               int isub, T* pfc_scratch, T* rhoh = nullptr, bool props = false, bool prefer_fused = false,
+               T* qupd = nullptr) {
   const size_t tsz = H->book.table.size();
   bool fuse = (H->tune_fuse || prefer_fused) && !terms.empty() && (int)terms.size() <= kMaxFusedTerms;
   for (const auto& t : terms) {
@@ -626,20 +642,29 @@ void run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const
     H->prof_end(e0, 0, -1, bytes);
     H->dag_end();
     H->launches++;
-    return;
+    return false;
   }
-  // fallback: one line operator per term, then the elementwise epilogue
+  // fallback: one line operator per term, then the elementwise epilogue.  A fractional step with
+  // one pressure-gradient term that comes last runs as that operator's O_FRAC store (no separate
+  // gradient array, no separate pass), and then also advances qupd when given.
+  int n1 = 0;
+  for (const auto& t : terms) n1 += t.group == 1 ? 1 : 0;
+  const bool frac_in_op = epilogue == EP_FRAC && n1 == 1 && terms.back().group == 1 && terms.front().group == 0;
   T* tgt0 = out;
   bool first0 = epilogue != EP_ACCUM, first1 = true;
   for (const auto& t : terms) {
     if (t.group == 0) {
       run_op<T>(H, t.d, t.fam, t.bc, t.fbc, t.in, t.n_in, tgt0, !first0, t.g);
       first0 = false;
+    } else if (frac_in_op) {
+      const FracStep<T> fs{rhs0, qupd, H->dt, H->tGamma[isub], H->tZeta[isub], H->tAlpha[isub]};
+      run_op<T>(H, t.d, t.fam, t.bc, t.fbc, t.in, t.n_in, out, false, t.g, O_FRAC, nullptr, &fs);
     } else {
       run_op<T>(H, t.d, t.fam, t.bc, t.fbc, t.in, t.n_in, pfc_scratch, !first1, t.g);
       first1 = false;
     }
   }
+  if (frac_in_op) return qupd != nullptr;
   if (epilogue == EP_FRAC) {
     PROFD(H, 3, 5.0 * sizeof(T) * nout, bufs(pfc_scratch), bufs(out, rhs0),
          launch_fractional_step(out, rhs0, pfc_scratch, (int64_t)nout, H->dt, H->tGamma[isub], H->tZeta[isub],
@@ -658,6 +683,7 @@ void run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const
          launch_energy_advance<T>(out, rhs0, rhoh, (int64_t)nout, H->dt, H->tGamma[isub], H->tZeta[isub], st));
     H->launches++;
   }
+  return false;
 }
 
 void build_bcs(chs_handle* H, const chs_config* c) {
@@ -1102,6 +1128,9 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
   // op(conv + rre*diff); the three directions, the pressure gradient and the fractional step
   // (:35-71) are summed per output value.
   const int m_pcc[3] = {np0, nc1, nc2}, m_cpc[3] = {nc0, np1, nc2}, m_ccp[3] = {nc0, nc1, np2};
+  // y and z: the fractional step's pressure-gradient operator also advances q (update_q with no
+  // mass-flux correction); x waits for the mass-flux mean
+  bool y_advanced = false, z_advanced = false;
   // x-momentum (:796-966)
   {
     std::vector<OpTerm<T>> t;
@@ -1130,7 +1159,8 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
     pair_terms(t, 2, D1P2C, H->mbcz_cov2, nullptr, prod(A(H->qyiz), c_ziy, -1.0), H->mbcz_tau2, nullptr,
                linm(A(H->qzdy), A(H->qydz), 1.0, 1.0, mu_yz), rre, s_cpp, nullptr, 0);
     t.push_back(term<T>(1, D1C2P, by_pr, fympr, src(A(H->pres), -1.0), s_ccc, 1.0, 1));
-    run_fused<T>(H, t, A(H->my), m_cpc, EP_FRAC, A(H->my0), isub, A(H->py));
+    y_advanced = run_fused<T>(H, t, A(H->my), m_cpc, EP_FRAC, A(H->my0), isub, A(H->py), nullptr, false, false,
+                              A(uy));
   }
   // z-momentum (:1262-1457)
   {
@@ -1142,7 +1172,8 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
     pair_terms(t, 2, D1C2P, H->mbcz_cov3, any, prod(c_ziz, A(H->qziz), -1.0), H->mbcz_tau3, any,
                linm(A(H->qzdz), A(H->div), -third, 2.0, mu_c), rre, s_ccc, nullptr, 0);
     t.push_back(term<T>(2, D1C2P, bz_pr, any, src(A(H->pres), -1.0), s_ccc, 1.0, 1));
-    run_fused<T>(H, t, A(H->mz), m_ccp, EP_FRAC, A(H->mz0), isub, A(H->pz));
+    z_advanced = run_fused<T>(H, t, A(H->mz), m_ccp, EP_FRAC, A(H->mz0), isub, A(H->pz), nullptr, false, false,
+                              A(uz));
   }
 
   // ---- 3b. mass flux
@@ -1156,11 +1187,17 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
   // ---- 4. q += rhs, walls
   PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_pcc, bufs(H->mx, bulk), bufs(ux),
         launch_update_q(A(ux), A(H->mx), bulk, (int64_t)H->n_pcc, st));
-  PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc, bufs(H->my), bufs(uy),
-        launch_update_q(A(uy), A(H->my), nullptr, (int64_t)H->n_cpc, st));
-  PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccp, bufs(H->mz), bufs(uz),
-        launch_update_q(A(uz), A(H->mz), nullptr, (int64_t)H->n_ccp, st));
-  H->launches += 3;
+  if (!y_advanced) {
+    PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_cpc, bufs(H->my), bufs(uy),
+          launch_update_q(A(uy), A(H->my), nullptr, (int64_t)H->n_cpc, st));
+    H->launches++;
+  }
+  if (!z_advanced) {
+    PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccp, bufs(H->mz), bufs(uz),
+          launch_update_q(A(uz), A(H->mz), nullptr, (int64_t)H->n_ccp, st));
+    H->launches++;
+  }
+  H->launches += 1;
   const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
   if (w0 || w1) {
     PROFD(H, 3, 16.0 / 8.0 * sizeof(T) * nc0 * nc2, bufs(), bufs(uy),

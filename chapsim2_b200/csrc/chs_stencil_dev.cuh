@@ -10,9 +10,24 @@ namespace chs {
 
 template <typename T>
 __device__ __forceinline__ void store_out(const LineIOT<T>& io, int64_t a, T g, T v) {
-  if (io.omode == O_DIV) io.out[a] = io.onum[a] / (g * v);
-  else if (io.omode == O_MUL) io.out[a] = io.onum[a] * (g * v);
-  else io.out[a] = io.accumulate ? io.out[a] + g * v : g * v;
+  if (io.omode == O_DIV) {
+    io.out[a] = io.onum[a] / (g * v);
+  } else if (io.omode == O_MUL) {
+    io.out[a] = io.onum[a] * (g * v);
+  } else if (io.omode == O_FRAC) {
+    // the arithmetic of fractional_step_kernel with pfc = g*v, then update_q_kernel's q += r
+    const T tdt = T(io.dt), tg = T(io.gam), tz = T(io.zeta), ta = T(io.alpha);
+    const T pfc = g * v;
+    const T cur = io.out[a], last = io.rhs0[a];
+    T tot = tg * cur + tz * last;
+    io.rhs0[a] = cur;
+    tot = tot + ta * pfc;
+    const T r = tdt * tot;
+    io.out[a] = r;
+    if (io.qupd) io.qupd[a] = io.qupd[a] + (r - T(0));
+  } else {
+    io.out[a] = io.accumulate ? io.out[a] + g * v : g * v;
+  }
 }
 
 template <int FAM, typename T, typename F>

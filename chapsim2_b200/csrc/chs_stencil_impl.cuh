@@ -199,7 +199,9 @@ __device__ __forceinline__ void stencil_win_body(const OpPlan& P, const LineIOT<
     }
   }
   const bool plain = io.omode == O_STORE && !io.accumulate;
+  const bool frac = io.omode == O_FRAC;
   const T g = T(io.g);
+  const T tdt = T(io.dt), tg = T(io.gam), tz = T(io.zeta), ta = T(io.alpha);
 #pragma unroll
   for (int u = 0; u < kWin; ++u) {
     const int p = p0 + u;
@@ -233,6 +235,27 @@ __device__ __forceinline__ void stencil_win_body(const OpPlan& P, const LineIOT<
 #pragma unroll
       for (int e = 0; e < V; ++e) o[e] = g * v[e];
       *reinterpret_cast<VT*>(io.out + a) = *reinterpret_cast<const VT*>(o);
+    } else if (frac) {
+      // store_out's O_FRAC arithmetic on vectors of the output, the previous right-hand side and q
+      T cur[V], last[V], r[V];
+      *reinterpret_cast<VT*>(cur) = *reinterpret_cast<const VT*>(io.out + a);
+      *reinterpret_cast<VT*>(last) = *reinterpret_cast<const VT*>(io.rhs0 + a);
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const T pfc = g * v[e];
+        T tot = tg * cur[e] + tz * last[e];
+        tot = tot + ta * pfc;
+        r[e] = tdt * tot;
+      }
+      *reinterpret_cast<VT*>(io.rhs0 + a) = *reinterpret_cast<const VT*>(cur);
+      *reinterpret_cast<VT*>(io.out + a) = *reinterpret_cast<const VT*>(r);
+      if (io.qupd) {
+        T q[V];
+        *reinterpret_cast<VT*>(q) = *reinterpret_cast<const VT*>(io.qupd + a);
+#pragma unroll
+        for (int e = 0; e < V; ++e) q[e] = q[e] + (r[e] - T(0));
+        *reinterpret_cast<VT*>(io.qupd + a) = *reinterpret_cast<const VT*>(q);
+      }
     } else {
 #pragma unroll
       for (int e = 0; e < V; ++e) store_out(io, a + e, g, v[e]);
@@ -380,7 +403,8 @@ bool try_launch_win(const OpPlan& P, const LineIOT<T>& io, const double* table, 
   if (DIR != 0) {
     // y and z kernels: V adjacent x positions per thread, 16-byte vectors
     constexpr int V = Vec16<T>::n;
-    uintptr_t al = reinterpret_cast<uintptr_t>(io.out) | reinterpret_cast<uintptr_t>(io.onum);
+    uintptr_t al = reinterpret_cast<uintptr_t>(io.out) | reinterpret_cast<uintptr_t>(io.onum) |
+                   reinterpret_cast<uintptr_t>(io.rhs0) | reinterpret_cast<uintptr_t>(io.qupd);
     for (int q = 0; q < 2; ++q)
       al |= reinterpret_cast<uintptr_t>(io.t[q].X) | reinterpret_cast<uintptr_t>(io.t[q].Y) |
             reinterpret_cast<uintptr_t>(io.t[q].Z);
