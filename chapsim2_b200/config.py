@@ -81,12 +81,15 @@ def taylor_green(n=64, iacc=IACCU_CP6, dt=1.0e-3, ren=1600.0):
 
 
 def channel(nc=(128, 96, 128), rstret=0.075, ren=2800.0, iacc=IACCU_CP6, dt=None, lxx=4 * np.pi,
-            lzz=4 * np.pi / 3):
+            lzz=4 * np.pi / 3, ifft=FFT_FISHPACK_2DFFT, istret=ISTRET_2SIDES):
     """Periodic turbulent channel with no-slip y walls and constant mass flux.
 
-    Stretching is the reference's tanh mapping with beta = 20 * rstret
-    (src/geometry.f90:237); rstret = 0.075 is beta = 1.5.  tanh stretching
-    selects the FISHPACK Poisson path (src/input_general.f90:552).
+    With the FISHPACK Poisson solver (default) the stretching is the reference's
+    tanh mapping with beta = 20 * rstret (src/geometry.f90:237); rstret = 0.075
+    is beta = 1.5.  With ifft = FFT_2DECOMP_3DFFT the mapping is the 3FMD one
+    (src/geometry.f90:287-408, beta = rstret, e.g. 0.25 as in the reference's
+    channel example) and the Poisson solver is poisson_010
+    (src/input_general.f90:552-553, src/poisson_1stderivcomp.f90:1457-1816).
     """
     bc = np.full((3, 5, 2), IBC_PERIODIC, np.int32)
     bc[1, V_QX] = IBC_DIRICHLET
@@ -94,8 +97,8 @@ def channel(nc=(128, 96, 128), rstret=0.075, ren=2800.0, iacc=IACCU_CP6, dt=None
     bc[1, V_QZ] = IBC_DIRICHLET
     bc[1, V_PR] = IBC_NEUMANN
     bc[1, V_TM] = IBC_DIRICHLET
-    cfg = DomainConfig(nc=tuple(nc), lxx=lxx, lyt=1.0, lyb=-1.0, lzz=lzz, istret=ISTRET_2SIDES, rstret=rstret,
-                       iacc=iacc, ifft=FFT_FISHPACK_2DFFT, idriven=IDRVF_X_MASSFLUX, ren=ren,
+    cfg = DomainConfig(nc=tuple(nc), lxx=lxx, lyt=1.0, lyb=-1.0, lzz=lzz, istret=istret, rstret=rstret,
+                       iacc=iacc, ifft=ifft, idriven=IDRVF_X_MASSFLUX, ren=ren,
                        dt=dt if dt is not None else 1.0e-3, nominal_bc=bc, name=f"channel{nc[0]}x{nc[1]}x{nc[2]}")
     return cfg
 
@@ -158,11 +161,12 @@ class ThermoConfig:
     qw: tuple = (-1.0, 1.0)  # dT/dy at the y walls: heat flux q_w = 1 into the fluid at both walls
 
 
-def heated_channel(nc=(128, 96, 128), iacc=IACCU_CD2, dt=None, rstret=0.075, ren=2800.0, table=None, t_ini=0.47):
+def heated_channel(nc=(128, 96, 128), iacc=IACCU_CD2, dt=None, rstret=0.075, ren=2800.0, table=None, t_ini=0.47,
+                   ifft=FFT_FISHPACK_2DFFT):
     """Heated channel with variable properties (same grid and flow as the channel) and isoflux
     y walls: T is Neumann at the walls, so the property BC is Dirichlet there
     (src/bc_general.f90:182-186).  Returns (DomainConfig, ThermoConfig)."""
-    cfg = channel(nc=nc, rstret=rstret, ren=ren, iacc=iacc, dt=dt)
+    cfg = channel(nc=nc, rstret=rstret, ren=ren, iacc=iacc, dt=dt, ifft=ifft)
     cfg.nominal_bc[1, V_TM] = IBC_NEUMANN
     cfg.name = f"heated{nc[0]}x{nc[1]}x{nc[2]}"
     tc = ThermoConfig(table=table if table is not None else synthetic_table(), t_ini=t_ini)
@@ -214,14 +218,47 @@ def _tanh_mapping(cfg, node, n):
     return (y - ymin) * ff + cfg.lyb, m1 / ff
 
 
+def _heaviside(r):
+    """heaviside_step (src/modules.f90:960-971)."""
+    return np.where(r > 1.0e-20, 1.0, np.where(r < -1.0e-20, 0.0, 0.5))
+
+
+def _fmd_mapping(cfg, node, n):
+    """Buildup_grid_mapping_1D_3fmd (src/geometry.f90:287-408): y and yMapping(:,1) = d eta/dy."""
+    if node:
+        shift, delta_eta = 0.0, 1.0 / (n - 1)
+    else:
+        shift, delta_eta = 0.5 / n, 1.0 / n
+    eta = shift + np.arange(n) * delta_eta
+    gamma, delta = {ISTRET_CENTRE: (1.0, 0.0), ISTRET_2SIDES: (1.0, 0.5), ISTRET_BOTTOM: (0.5, 0.5),
+                    ISTRET_TOP: (0.5, 0.0)}[cfg.istret]
+    beta = cfg.rstret
+    alpha = (-1.0 + np.sqrt(1.0 + 4.0 * np.pi * np.pi * beta * beta)) / beta * 0.5
+    cc = np.sqrt(alpha * beta + 1.0) / np.sqrt(beta)
+    dd = cc / np.sqrt(alpha)
+    ee = cc * np.sqrt(alpha)
+    st1 = (1.0 - 2.0 * delta) / gamma * 0.5
+    st2 = (3.0 - 2.0 * delta) / gamma * 0.5
+    mm = np.pi * (gamma * eta + delta)
+    y = (np.arctan(dd * np.tan(mm)) - np.arctan(dd * np.tan(np.pi * delta))
+         + np.pi * (_heaviside(eta - st1) + _heaviside(eta - st2)))
+    y = 1.0 / (gamma * ee) * y
+    if node:
+        y[0], y[-1] = 0.0, 1.0
+    ly = cfg.lyt - cfg.lyb
+    return y * ly + cfg.lyb, (alpha / np.pi + np.sin(mm) * np.sin(mm) / np.pi / beta) / ly
+
+
 def geometry(cfg):
     """Return dict with h(3), yp(np_geo), yc(nc), mppt, mpcc (yMapping(:,1))."""
     nc = cfg.nc
     h = np.array([cfg.lxx / nc[0], (cfg.lyt - cfg.lyb) / nc[1], cfg.lzz / nc[2]])
     if cfg.stretch_y:
         h[1] = 1.0 / nc[1]
-        yp, mppt = _tanh_mapping(cfg, True, nc[1] + 1)
-        yc, mpcc = _tanh_mapping(cfg, False, nc[1])
+        # the 3D-FFT solver selects the 3FMD mapping, FISHPACK the tanh one (src/input_general.f90:552-553)
+        mapping = _fmd_mapping if cfg.ifft == FFT_2DECOMP_3DFFT else _tanh_mapping
+        yp, mppt = mapping(cfg, True, nc[1] + 1)
+        yc, mpcc = mapping(cfg, False, nc[1])
     else:
         yp = np.arange(nc[1] + 1) * h[1] + cfg.lyb
         yc = np.arange(nc[1]) * h[1] + h[1] * 0.5 + cfg.lyb

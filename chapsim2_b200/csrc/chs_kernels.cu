@@ -1266,6 +1266,228 @@ void launch_spectral_divide(double2* data, int nxh, int ny, int nz, const double
 }
 
 // ===========================================================================
+// poisson_010 y stage (src/poisson_1stderivcomp.f90:1457-1816) per (kx, kz) column of the
+// x/z spectrum (layout (kz, j, kx)): the even/odd reordering in y (:1491-1501), the y FFT, the
+// cosine post-processing (:1557-1575), then either the wavenumber division (uniform grid,
+// :1591-1613) or the pentadiagonal solves of the odd and even cosine modes (matrice_refinement
+// :2718-3039 and inversion5_v1 :420-561), the backward post-processing (:1717-1735), the
+// inverse y FFT and the inverse reordering (:1772-1782).  The column stays in shared memory
+// from the first load to the last store.
+//
+// The x and z half-cell phase factors of the reference (:1527-1553, :1740-1767) multiply a
+// column by e^{-i theta} before this stage and by e^{+i theta} after it; the stage applies one
+// real operator to the real and the imaginary parts, so they cancel and are not applied.
+// ===========================================================================
+constexpr double kInv5Eps = 1.0e-16;  // epsilon of inversion5_v1 with DOUBLE_PREC
+
+template <int MODE>  // 0: uniform grid (wavenumber division), 1: stretched grid (pentadiagonal)
+__global__ void __launch_bounds__(256) dct_y_kernel(const __grid_constant__ FftPlan fp, double2* __restrict__ data,
+                                                    int nxh, int nz, int lpc, const double* __restrict__ ayby,
+                                                    const double* __restrict__ k2x, const double* __restrict__ k2z,
+                                                    const double* __restrict__ k2y, const double* __restrict__ ptab,
+                                                    double scale) {
+  extern __shared__ double2 sh[];
+  __shared__ int64_t lbase[32];
+  __shared__ double lkx[32], lkz[32];
+  const int ny = fp.n, h = ny / 2;
+  double2* b0 = sh;
+  double2* b1 = sh + (size_t)lpc * ny;
+  const int64_t g0 = (int64_t)blockIdx.x * lpc;
+  const int64_t nlines = (int64_t)nxh * nz;
+  if (threadIdx.x < lpc) {
+    const int64_t g = g0 + threadIdx.x;
+    if (g < nlines) {
+      const int kz = (int)(g / nxh), kx = (int)(g - (int64_t)kz * nxh);
+      lbase[threadIdx.x] = kx + (int64_t)kz * nxh * ny;
+      lkx[threadIdx.x] = k2x[kx];
+      lkz[threadIdx.x] = k2z[kz];
+    } else {
+      lbase[threadIdx.x] = -1;
+      lkx[threadIdx.x] = 0.0;
+      lkz[threadIdx.x] = 0.0;
+    }
+  }
+  __syncthreads();
+  const int ntot = lpc * ny;
+  const float ilpc = 1.0f / (float)lpc;
+  // load: row p of a column goes to position q of the reordered line (q < ny/2: row 2q;
+  // q >= ny/2: row 2ny-1-2q)
+  for (int t0 = threadIdx.x; t0 < ntot; t0 += 4 * blockDim.x) {
+    double2 v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = t0 + u * blockDim.x;
+      v[u] = make_double2(0.0, 0.0);
+      if (t < ntot) {
+        const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
+        const int64_t base = lbase[l];
+        if (base >= 0) v[u] = data[base + (int64_t)p * nxh];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < ntot) {
+        const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
+        const int q = (p & 1) ? ny - 1 - (p >> 1) : (p >> 1);
+        b0[l * ny + q] = v[u];
+      }
+    }
+  }
+  __syncthreads();
+  double2* r = smem_fft(b0, b1, lpc, fp, -1);
+  double2* o = (r == b0) ? b1 : b0;
+  const double* ay = ayby;
+  const double* by = ayby + ny;
+  // forward post-processing into o, layout [j][l]
+  for (int t = threadIdx.x; t < ntot; t += blockDim.x) {
+    const int j = fast_div(t, lpc, ilpc), l = t - j * lpc;
+    const double2 c = r[l * ny + j];
+    double2 v;
+    if (j == 0) {
+      v = make_double2(c.x * scale, c.y * scale);
+    } else {
+      const double2 d = r[l * ny + (ny - j)];
+      const double t1 = c.x * scale, t2 = c.y * scale, t3 = d.x * scale, t4 = d.y * scale;
+      const double yb = by[j], ya = ay[j];
+      const double xx1 = t1 * yb, xx2 = t1 * ya, xx3 = t2 * yb, xx4 = t2 * ya;
+      const double xx5 = t3 * yb, xx6 = t3 * ya, xx7 = t4 * yb, xx8 = t4 * ya;
+      v = make_double2(0.5 * (xx1 + xx4 + xx5 - xx8), 0.5 * (-xx2 + xx3 + xx6 + xx7));
+    }
+    if (MODE == 0) {
+      const double kk = lkx[l] + k2y[j] + lkz[l];
+      if (fabs(kk) < 1.0e-16) v = make_double2(0.0, 0.0);
+      else v = make_double2(v.x / (-kk), v.y / (-kk));
+    }
+    o[j * lpc + l] = v;
+  }
+  __syncthreads();
+  if (MODE == 1 && threadIdx.x < 2 * lpc) {
+    // one thread per (column, parity): inversion5_v1 on rows r = 0..h-1 (mode j = 2r + s), the
+    // rows generated from the tables as the elimination reaches them.  The modified diagonal
+    // and super-diagonal of each pivot row are kept for the back substitution in the free FFT
+    // buffer r, layout [row][thread].
+    const int tid = threadIdx.x, nt = 2 * lpc;
+    const int l = tid >> 1, s = tid & 1;
+    if (lbase[l] >= 0) {
+      double* f3 = reinterpret_cast<double*>(r);
+      double* f4 = f3 + (size_t)h * nt;
+      const double* A1 = ptab + (size_t)s * 6 * h;
+      const double* A2 = A1 + h;
+      const double* T1 = A1 + 2 * h;
+      const double* T2 = A1 + 3 * h;
+      const double* A4 = A1 + 4 * h;
+      const double* A5 = A1 + 5 * h;
+      const double sxz = lkx[l] + lkz[l];
+      const bool pin = s == 0 && lkx[l] == 0.0 && lkz[l] == 0.0;
+      auto diag = [&](int row) { return -((sxz + T1[row]) + T2[row]); };
+      auto sup2 = [&](int row) { return (pin && row == 0) ? 0.0 : A5[row]; };
+      auto E = [&](int row) -> double2& { return o[(2 * row + s) * lpc + l]; };
+      double P3 = pin ? 1.0 : diag(0), P4 = pin ? 0.0 : A4[0];
+      double R12 = A2[1], R13 = diag(1), R14 = A4[1];
+      double R21 = A1[2], R22 = A2[2], R23 = diag(2), R24 = A4[2];
+      double2 e0 = E(0), e1 = E(1), e2 = E(2);
+      double tmp = 0.0;  // a zero pivot keeps the previous multiplier, as the reference does
+      for (int m = 0; m <= h - 3; ++m) {
+        const double P5 = sup2(m);
+        if (P3 != 0.0) tmp = R12 / P3;
+        e1.x = e1.x - tmp * e0.x;
+        e1.y = e1.y - tmp * e0.y;
+        R13 = R13 - tmp * P4;
+        R14 = R14 - tmp * P5;
+        if (P3 != 0.0) tmp = R21 / P3;
+        e2.x = e2.x - tmp * e0.x;
+        e2.y = e2.y - tmp * e0.y;
+        R22 = R22 - tmp * P4;
+        R23 = R23 - tmp * P5;
+        f3[(size_t)m * nt + tid] = P3;
+        f4[(size_t)m * nt + tid] = P4;
+        E(m) = e0;
+        P3 = R13; P4 = R14; e0 = e1;
+        R12 = R22; R13 = R23; R14 = R24; e1 = e2;
+        if (m + 3 < h) {
+          R21 = A1[m + 3]; R22 = A2[m + 3]; R23 = diag(m + 3); R24 = A4[m + 3];
+          e2 = E(m + 3);
+        }
+      }
+      // rows h-2 (P) and h-1 (R1)
+      double t1 = fabs(P3) > kInv5Eps ? R12 / P3 : 0.0;
+      const double sr = t1;
+      double bb = R13 - t1 * P4;
+      double2 eh;
+      if (fabs(bb) > kInv5Eps) {
+        t1 = sr / bb;
+        eh = make_double2(e1.x / bb - t1 * e0.x, e1.y / bb - t1 * e0.y);
+      } else {
+        eh = make_double2(0.0, 0.0);
+      }
+      bb = fabs(P3) > kInv5Eps ? 1.0 / P3 : 0.0;
+      double a1 = P4 * bb;
+      const double2 ehm = make_double2(e0.x * bb - a1 * eh.x, e0.y * bb - a1 * eh.y);
+      E(h - 1) = eh;
+      E(h - 2) = ehm;
+      double2 x1 = ehm, x2 = eh;
+      for (int i = h - 3; i >= 0; --i) {
+        const double d3 = f3[(size_t)i * nt + tid], d4 = f4[(size_t)i * nt + tid];
+        const double q = fabs(d3) > kInv5Eps ? 1.0 / d3 : 0.0;
+        a1 = d4 * q;
+        bb = sup2(i) * q;
+        double2 ei = E(i);
+        ei.x = ei.x * q - a1 * x1.x - bb * x2.x;
+        ei.y = ei.y * q - a1 * x1.y - bb * x2.y;
+        E(i) = ei;
+        x2 = x1;
+        x1 = ei;
+      }
+    }
+  }
+  __syncthreads();
+  // backward post-processing from o ([j][l]) into r (line layout)
+  for (int t = threadIdx.x; t < ntot; t += blockDim.x) {
+    const int j = fast_div(t, lpc, ilpc), l = t - j * lpc;
+    const double2 c = o[j * lpc + l];
+    double2 v;
+    if (j == 0) {
+      v = c;
+    } else {
+      const double2 d = o[(ny - j) * lpc + l];
+      const double t1 = c.x, t2 = c.y, t3 = d.x, t4 = d.y;
+      const double yb = by[j], ya = ay[j];
+      const double xx1 = t1 * yb, xx2 = t1 * ya, xx3 = t2 * yb, xx4 = t2 * ya;
+      const double xx5 = t3 * yb, xx6 = t3 * ya, xx7 = t4 * yb, xx8 = t4 * ya;
+      v = make_double2(xx1 - xx4 + xx6 + xx7, -(-xx2 - xx3 + xx5 - xx8));
+    }
+    r[l * ny + j] = v;
+  }
+  __syncthreads();
+  double2* w = smem_fft(r, o, lpc, fp, +1);
+  // store: row p of the column takes position q of the line (the inverse reordering)
+  for (int t = threadIdx.x; t < ntot; t += blockDim.x) {
+    const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
+    const int64_t base = lbase[l];
+    const int q = (p & 1) ? ny - 1 - (p >> 1) : (p >> 1);
+    if (base >= 0) data[base + (int64_t)p * nxh] = w[l * ny + q];
+  }
+}
+
+void launch_dct_y(const FftPlan& fp, double2* data, int nxh, int nz, const double* ayby, const double* k2x,
+                  const double* k2z, const double* k2y, const double* ptab, double scale, cudaStream_t st) {
+  const int ny = fp.n;
+  if (ny % 2 || ny < 8) throw std::runtime_error("dct_y: ny must be even and at least 8");
+  const int lpc = fft_lines_per_cta(ny);
+  const int64_t nlines = (int64_t)nxh * nz;
+  const size_t shm = 2 * (size_t)lpc * ny * sizeof(double2);
+  const unsigned grid = (unsigned)((nlines + lpc - 1) / lpc);
+  if (ptab) {
+    cudaFuncSetAttribute(dct_y_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    dct_y_kernel<1><<<grid, 256, shm, st>>>(fp, data, nxh, nz, lpc, ayby, k2x, k2z, k2y, ptab, scale);
+  } else {
+    cudaFuncSetAttribute(dct_y_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    dct_y_kernel<0><<<grid, 256, shm, st>>>(fp, data, nxh, nz, lpc, ayby, k2x, k2z, k2y, ptab, scale);
+  }
+}
+
+// ===========================================================================
 // elementwise and reductions.  Field arrays are T (double, or float in the mixed-precision
 // form); scalars, reduction accumulators and results stay double.
 // ===========================================================================

@@ -134,6 +134,13 @@ void launch_ysolve_factor(double* Zr, double* D, int nxh, int ny, int nz, const 
 // y tridiagonal solve per (kx, kz) of the FISHPACK path (TRID0 with the singular-pivot pin)
 void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* Zr, const double* D, const double* pa,
                    cudaStream_t st);
+// poisson_010 y stage per (kx, kz) column: reordering, y FFT, cosine post-processing, the
+// pentadiagonal solves (ptab: per system s = 0 odd / 1 even cosine modes and row r < ny/2 the
+// rows [6][ny/2] sub-2, sub-1, t1, t2, super-1, super-2 with main diagonal
+// -(((kx2 + kz2) + t1) + t2)) or, with ptab null, the division by -(kx2 + k2y + kz2), and the
+// inverse steps; ayby holds sin and cos of (j pi / 2 ny), j < ny; scale the FFT normalisation
+void launch_dct_y(const FftPlan& fp, double2* data, int nxh, int nz, const double* ayby, const double* k2x,
+                  const double* k2z, const double* k2y, const double* ptab, double scale, cudaStream_t st);
 // 3D spectral division by -(kx'^2 + ky'^2 + kz'^2) (zero mode -> 0), with normalisation
 void launch_spectral_divide(double2* data, int nxh, int ny, int nz, const double* k2x, const double* k2y,
                             const double* k2z, double norm, cudaStream_t st);

@@ -170,6 +170,7 @@ struct chs_handle {
   double *lamx = nullptr, *lamz = nullptr, *pa = nullptr, *pb = nullptr, *pc = nullptr;
   double *yzr = nullptr, *yd = nullptr;  // precomputed y-solve factors
   double *k2x = nullptr, *k2y = nullptr, *k2z = nullptr;
+  double *ayby = nullptr, *ptab = nullptr;  // poisson_010 cosine factors and pentadiagonal rows
   // graphs per substep (1..3) and for a whole step
   cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
   long long kernels_per_sub[4] = {0, 0, 0, 0};
@@ -793,7 +794,13 @@ void setup_host(chs_handle* H, const chs_config* c) {
   if (H->iacc < 1 || H->iacc > 4) throw std::invalid_argument("iacc must be 1..4");
   if (H->ifft != 2 && H->ifft != 3) throw std::invalid_argument("ifft must be 2 or 3");
   if (H->ifft == 2 && H->periodic_y) throw std::invalid_argument("FISHPACK Poisson needs non-periodic y");
-  if (H->ifft == 3 && !H->periodic_y) throw std::invalid_argument("3D-FFT Poisson needs periodic y");
+  if (H->ifft == 3 && !H->periodic_y) {
+    // poisson_010 (src/poisson_1stderivcomp.f90:1457-1816): cosine modes in y, split odd/even
+    if (H->nc[1] % 2) throw std::invalid_argument("3D-FFT Poisson with y walls needs an even ny");
+    if (c->istret != 0 && c->istret != 1 && c->istret != 2)
+      throw std::invalid_argument("3D-FFT Poisson with y walls supports istret 0, 1 and 2");
+    if (c->istret != 0 && !(c->rstret > 0.0)) throw std::invalid_argument("3FMD stretching needs rstret > 0");
+  }
   if (c->precision != CHS_FP64 && c->precision != CHS_MIXED) throw std::invalid_argument("unknown precision mode");
   H->mixed = c->precision == CHS_MIXED;
   H->dag_lanes = H->mixed ? 4 : 3;
@@ -967,6 +974,75 @@ void setup_device(chs_handle* H, const chs_config* c) {
     auto ky = k2(nc1, c->lyt - c->lyb, H->h[1]);
     auto kz = k2(nc2, c->lzz, H->h[2]);
     kx.resize(nxh);
+    if (!H->periodic_y) {
+      // poisson_010.  abxyz for bcy = 1 (src/poisson_1stderivcomp.f90:2376-2382)
+      std::vector<double> ab(2 * (size_t)nc1);
+      for (int j = 1; j <= nc1; ++j) {
+        ab[j - 1] = std::sin(double(j - 1) * pi * 0.5 / double(nc1));
+        ab[nc1 + j - 1] = std::cos(double(j - 1) * pi * 0.5 / double(nc1));
+      }
+      H->ayby = H->dalloc<double>(ab.size());
+      CK(cudaMemcpyAsync(H->ayby, ab.data(), ab.size() * sizeof(double), cudaMemcpyHostToDevice, H->st));
+      // waves for bcy = 1 (:2484-2501): w = pi (j-1)/nym; yky = nym wp (stretched grid), yk2 = (nym wp / yly)^2
+      const double dy = H->h[1], yly = c->lyt - c->lyb;
+      const double ac = cs.rhs[2][0][BC_PERIODIC] / dy, bc = cs.rhs[2][1][BC_PERIODIC] / dy;
+      std::vector<double> yky(nc1, 0.0);
+      ky.assign(nc1, 0.0);
+      for (int j = 2; j <= nc1; ++j) {
+        const double w = 2.0 * pi * 0.5 * double(j - 1) / double(nc1);
+        double wp = ac * 2.0 * dy * std::sin(w * 0.5) + (bc * 2.0 * dy) * std::sin(3.0 * 0.5 * w);
+        wp = wp / (1.0 + 2.0 * alc * std::cos(w));
+        yky[j - 1] = H->stretch_y ? double(nc1) * wp : double(nc1) * wp / yly;
+        const double q = double(nc1) * wp / yly;
+        ky[j - 1] = q * q;
+      }
+      if (H->stretch_y) {
+        // matrice_refinement for istret 1 or 2 (:2718-3046) with unit transfer factors: per system
+        // (odd modes cw22 = yky(2j-1), even modes cw2 = yky(2j)) and row the diagonals a(.,1), a(.,2),
+        // the two added terms of the main diagonal, a(.,4) and a(.,5)
+        const int hh = nc1 / 2;
+        const double beta = c->rstret;
+        const double alpha = (-1.0 + std::sqrt(1.0 + 4.0 * pi * pi * beta * beta)) / beta * 0.5;
+        double xa0 = alpha / pi + 0.5 / beta / pi;
+        double xa1 = c->istret == 1 ? +1.0 / 4.0 / beta / pi : -1.0 / 4.0 / beta / pi;
+        xa0 = xa0 / yly;
+        xa1 = xa1 / yly;
+        const double xa0_2 = xa0 * xa0, xa1_2 = xa1 * xa1, xa01 = xa0 * xa1, xa0p1_2 = (xa0 + xa1) * (xa0 + xa1);
+        std::vector<double> tab(12 * (size_t)hh, 0.0);
+        for (int sy = 0; sy < 2; ++sy) {
+          std::vector<double> w(hh + 2, 0.0);  // 1-based
+          for (int j = 1; j <= hh; ++j) w[j] = yky[2 * j - 2 + sy];
+          double* A1 = tab.data() + (size_t)sy * 6 * hh;
+          double *A2 = A1 + hh, *T1 = A1 + 2 * hh, *T2 = A1 + 3 * hh, *A4 = A1 + 4 * hh, *A5 = A1 + 5 * hh;
+          for (int j = 1; j <= hh; ++j) {
+            const int r = j - 1;
+            if (j >= 2 && j <= hh - 1) {
+              T1[r] = xa0_2 * (w[j] * w[j]);
+              T2[r] = xa1_2 * w[j] * (w[j - 1] + w[j + 1]);
+            } else if (j == 1) {
+              T1[r] = (sy == 0 ? xa0_2 : xa0_2 - xa1_2) * (w[1] * w[1]);
+              T2[r] = xa1_2 * w[1] * w[2];
+            } else {
+              T1[r] = (sy == 0 ? xa0_2 : xa0p1_2) * (w[hh] * w[hh]);
+              T2[r] = xa1_2 * w[hh] * w[hh - 1];
+            }
+            if (j >= 2 && j <= hh - 1) A4[r] = xa01 * (w[j + 1] * (w[j] + w[j + 1]));
+            if (j == 1) A4[r] = sy == 0 ? 2.0 * xa01 * (w[1] * w[2] + w[2] * w[2])
+                                        : (xa0 - xa1) * xa1 * (w[1] * w[2]) + xa0 * xa1 * (w[2] * w[2]);
+            if (sy == 1 && j == hh - 1) A4[r] = xa0 * xa1 * w[hh - 1] * w[hh] + (xa0 + xa1) * xa1 * (w[hh] * w[hh]);
+            if (sy == 1 && j == hh) A4[r] = 0.0;
+            if (j <= hh - 2) A5[r] = xa1_2 * (-(w[j + 1] * w[j + 2]));
+            if (sy == 0 && j == 1) A5[r] = 2.0 * A5[r];
+            if (j >= 2) A2[r] = xa01 * (w[j - 1] * (w[j] + w[j - 1]));
+            if (sy == 1 && j == 2) A2[r] = xa0 * xa1 * (w[2] * w[1]) + (xa0 + xa1) * xa1 * (w[1] * w[1]);
+            if (sy == 1 && j == hh) A2[r] = (xa0 + xa1) * xa1 * (w[hh] * w[hh - 1]) + xa0 * xa1 * (w[hh - 1] * w[hh - 1]);
+            if (j >= 3) A1[r] = xa1_2 * (-(w[j - 1] * w[j - 2]));
+          }
+        }
+        H->ptab = H->dalloc<double>(tab.size());
+        CK(cudaMemcpyAsync(H->ptab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, H->st));
+      }
+    }
     H->k2x = H->dalloc<double>(nxh); H->k2y = H->dalloc<double>(nc1); H->k2z = H->dalloc<double>(nc2);
     CK(cudaMemcpyAsync(H->k2x, kx.data(), nxh * sizeof(double), cudaMemcpyHostToDevice, H->st));
     CK(cudaMemcpyAsync(H->k2y, ky.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice, H->st));
@@ -1004,6 +1080,15 @@ void poisson_device(chs_handle* H, T* rhs) {
     PROF(H, 2, 48.0 * nspec, launch_ysolve(H->spec, nxh, nc1, nc2, H->yzr, H->yd, H->pa, st));
     PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, H->spec, nxh, nc1, nxh, (int64_t)nxh * nc1, +1, st));
     PROF(H, 1, b_r2c, launch_irfft_x(H->fx, H->spec, rhs, nc1 * nc2, 1.0 / ((double)nc0 * (double)nc2), st));
+    H->launches += 5;
+  } else if (!H->periodic_y) {
+    // poisson_010 (src/poisson_1stderivcomp.f90:1457-1816): x and z transforms around the y
+    // stage (the FFT normalisation 1/(nx ny nz) is applied there, after the forward transforms)
+    PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, H->spec, nxh, nc1, nxh, (int64_t)nxh * nc1, -1, st));
+    PROF(H, 2, b_c2c, launch_dct_y(H->fy, H->spec, nxh, nc2, H->ayby, H->k2x, H->k2z, H->k2y, H->ptab,
+                                   1.0 / ((double)nc0 * (double)nc1 * (double)nc2), st));
+    PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, H->spec, nxh, nc1, nxh, (int64_t)nxh * nc1, +1, st));
+    PROF(H, 1, b_r2c, launch_irfft_x(H->fx, H->spec, rhs, nc1 * nc2, 1.0, st));
     H->launches += 5;
   } else {
     // poisson_000 (src/poisson_1stderivcomp.f90:1016-1195)

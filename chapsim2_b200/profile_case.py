@@ -27,14 +27,18 @@ def main():
                     help="heated case: train the property surrogate for this many epochs and use it")
     ap.add_argument("--graph-profile", action="store_true",
                     help="after the substeps, print a per-launch profile of substep 1 replayed as a graph")
+    ap.add_argument("--poisson", default="fishpack", choices=["fishpack", "3dfft"],
+                    help="channel cases: FISHPACK with tanh stretching, or the 3D-FFT solver (poisson_010) "
+                         "with 3FMD stretching (rstret 0.25)")
     a = ap.parse_args()
     tc = None
+    wall = {} if a.poisson == "fishpack" else dict(ifft=C.FFT_2DECOMP_3DFFT, rstret=0.25)
     if a.case == "channel":
-        cfg = C.channel(nc=tuple(a.nc), iacc=a.iacc)
+        cfg = C.channel(nc=tuple(a.nc), iacc=a.iacc, **wall)
         f = I.channel_fields(cfg)
         cfg.dt = I.cfl_dt(cfg, *f[:3], cfl=0.8)
     elif a.case == "heated":
-        cfg, tc = C.heated_channel(nc=tuple(a.nc), iacc=a.iacc)
+        cfg, tc = C.heated_channel(nc=tuple(a.nc), iacc=a.iacc, **wall)
         f = I.channel_fields(cfg)
         cfg.dt = I.cfl_dt(cfg, *f[:3], cfl=0.8)
     else:

@@ -10,6 +10,9 @@
 //   FISHPACK Poisson    src/poisson_fishpack.f90:20-490 with the RFFTF/RFFTB sums documented in
 //                       lib/fishpack4.1/fftpack.f:129-224 (evaluated here as direct DFT sums)
 //   3D-FFT Poisson      src/poisson_1stderivcomp.f90:1016-1195 (poisson_000), :2343-2714
+//   3FMD Poisson        src/poisson_1stderivcomp.f90:1457-1816 (poisson_010), :2718-3039
+//                       (matrice_refinement), :420-561 (inversion5_v1); the 3FMD mapping
+//                       src/geometry.f90:287-408
 //   correction          src/eq_momentum2.f90:1577-1660, :1799-1932
 //   KE monitor          src/io_monitor.f90:209-241
 //   energy equation     src/eq_energy.f90:148-458 (Compute_energy_rhs, Solve_energy_eq)
@@ -19,6 +22,7 @@
 //                       is_thermo branches of :796-1457, :1577-1660, :1799-1932
 // Restriction: x and z must be periodic (the channel and Taylor-Green configurations).
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -75,6 +79,49 @@ static void tanh_mapping(const Domain& dm, bool node, int n, std::vector<double>
   }
 }
 
+// heaviside_step (modules.f90:960-971)
+static double heaviside(double r) {
+  if (r > 1.0e-20) return 1.0;
+  if (r < -1.0e-20) return 0.0;
+  return 0.5;
+}
+
+static void fmd_mapping(const Domain& dm, bool node, int n, std::vector<double>& y, std::vector<double>& mp) {
+  // Buildup_grid_mapping_1D_3fmd (geometry.f90:287-408): the analytic stretching whose metric
+  // 1/h' has a single cosine mode, as the 3D-FFT Poisson solver requires
+  double eta_shift = 0.0, eta_delta = 1.0;
+  if (node) { eta_shift = 0.0; eta_delta = 1.0 / double(n - 1); }
+  else { eta_shift = 1.0 / double(n) * 0.5; eta_delta = 1.0 / double(n); }
+  std::vector<double> eta(n);
+  eta[0] = 0.0 + eta_shift;
+  for (int j = 2; j <= n; ++j) eta[j - 1] = eta[0] + double(j - 1) * eta_delta;
+  double gamma = 1.0, delta = 0.0;
+  if (dm.istret == 1) { gamma = 1.0; delta = 0.0; }
+  else if (dm.istret == 2) { gamma = 1.0; delta = 0.5; }
+  else if (dm.istret == 3) { gamma = 0.5; delta = 0.5; }
+  else if (dm.istret == 4) { gamma = 0.5; delta = 0.0; }
+  else throw std::runtime_error("unsupported istret");
+  const double beta = dm.rstret;
+  const double alpha = (-1.0 + std::sqrt(1.0 + 4.0 * PI * PI * beta * beta)) / beta * 0.5;
+  const double cc = std::sqrt(alpha * beta + 1.0) / std::sqrt(beta);
+  const double dd = cc / std::sqrt(alpha);
+  const double ee = cc * std::sqrt(alpha);
+  const double st1 = (1.0 - 2.0 * delta) / gamma * 0.5;
+  const double st2 = (3.0 - 2.0 * delta) / gamma * 0.5;
+  y.assign(n, 0.0);
+  mp.assign(n, 0.0);
+  for (int j = 1; j <= n; ++j) {
+    const double mm = PI * (gamma * eta[j - 1] + delta);
+    double yy = std::atan(dd * std::tan(mm)) - std::atan(dd * std::tan(PI * delta)) +
+                PI * (heaviside(eta[j - 1] - st1) + heaviside(eta[j - 1] - st2));
+    yy = 1.0 / (gamma * ee) * yy;
+    if (node && j == 1) yy = 0.0;
+    if (node && j == n) yy = 1.0;
+    y[j - 1] = yy * (dm.lyt - dm.lyb) + dm.lyb;
+    mp[j - 1] = (alpha / PI + std::sin(mm) * std::sin(mm) / PI / beta) / (dm.lyt - dm.lyb);
+  }
+}
+
 static void build_geometry(Domain& dm) {
   for (int d = 0; d < 3; ++d) {
     dm.np_geo[d] = dm.nc[d] + 1;
@@ -89,8 +136,14 @@ static void build_geometry(Domain& dm) {
   dm.mpcc.assign(dm.nc[1], 1.0);
   if (dm.stretch_y) {
     dm.h[1] = 1.0 / double(dm.nc[1]);
-    tanh_mapping(dm, true, dm.np_geo[1], dm.yp, dm.mppt);
-    tanh_mapping(dm, false, dm.nc[1], dm.yc, dm.mpcc);
+    // the 3D-FFT solver selects the 3FMD mapping, FISHPACK the tanh one (input_general.f90:552-553)
+    if (dm.ifft == 3) {
+      fmd_mapping(dm, true, dm.np_geo[1], dm.yp, dm.mppt);
+      fmd_mapping(dm, false, dm.nc[1], dm.yc, dm.mpcc);
+    } else {
+      tanh_mapping(dm, true, dm.np_geo[1], dm.yp, dm.mppt);
+      tanh_mapping(dm, false, dm.nc[1], dm.yc, dm.mpcc);
+    }
   } else {
     for (int j = 0; j < dm.np_geo[1]; ++j) dm.yp[j] = double(j) * dm.h[1] + dm.lyb;
     for (int j = 0; j < dm.nc[1]; ++j) dm.yc[j] = double(j) * dm.h[1] + dm.h[1] * 0.5 + dm.lyb;
@@ -782,6 +835,230 @@ static void poisson_3dfft(const Domain& dm, std::vector<double>& rhs) {
   for (size_t n = 0; n < rhs.size(); ++n) rhs[n] = a[n].real();
 }
 
+// ---------------------------------------------------------------------------
+// poisson_010: x and z periodic, y non-periodic (poisson_1stderivcomp.f90:1457-1816)
+// ---------------------------------------------------------------------------
+// waves() for bcy = 1 (poisson_1stderivcomp.f90:2484-2501): yky = nym*wp (stretched, in eta) and
+// yk2 = (nym*wp/yly)^2 at w = pi*(j-1)/nym, j = 1..ny
+static void waves_y_neumann(const Domain& dm, std::vector<double>& yky, std::vector<double>& yk2) {
+  const Family& c2p = dm.T.fam[FAM_D1C2P];
+  const int m = dm.iacc - 1;
+  const int ny = dm.nc[1], nym = dm.nc[1];
+  const double dy = dm.h[1], yly = dm.lyt - dm.lyb;
+  const double alc = c2p.f[2][0][BC_PERIODIC][m];
+  const double ac = c2p.r[2][0][BC_PERIODIC][m] / dy;
+  const double bc = c2p.r[2][1][BC_PERIODIC][m] / dy;
+  yky.assign(ny, 0.0);
+  yk2.assign(ny, 0.0);
+  for (int j = 1; j <= ny; ++j) {
+    const double w = 2.0 * PI * 0.5 * double(j - 1) / double(nym);
+    double wp = ac * 2.0 * dy * std::sin(w * 0.5) + (bc * 2.0 * dy) * std::sin(3.0 * 0.5 * w);
+    wp = wp / (1.0 + 2.0 * alc * std::cos(w));
+    yky[j - 1] = dm.stretch_y ? double(nym) * wp : double(nym) * wp / yly;
+    const double q = double(nym) * wp / yly;
+    yk2[j - 1] = q * q;
+  }
+  yky[0] = 0.0;
+  yk2[0] = 0.0;
+}
+
+// The pentadiagonal systems of matrice_refinement (poisson_1stderivcomp.f90:2718-3039, istret 1
+// or 2, with the compact-interpolation transfer factors switched off (ftr = .false.) so they are
+// 1): for the odd (sys 0, a) and even (sys 1, a2) cosine modes, row r = 0..ny/2-1, the five
+// diagonals c[0..4] = a(.,.,.,1..5) at the main-diagonal shift s = xk2 + zk2.
+struct Penta {
+  int h;
+  double xa0, xa1;
+  std::vector<double> c[2];  // cw22 = yky(2j-1) and cw2 = yky(2j), j = 1..h
+  void init(const Domain& dm, const std::vector<double>& yky) {
+    h = dm.nc[1] / 2;
+    const double beta = dm.rstret;
+    const double alpha = (-1.0 + std::sqrt(1.0 + 4.0 * PI * PI * beta * beta)) / beta * 0.5;
+    xa0 = alpha / PI + 0.5 / beta / PI;
+    xa1 = dm.istret == 1 ? +1.0 / 4.0 / beta / PI : -1.0 / 4.0 / beta / PI;
+    const double yly = dm.lyt - dm.lyb;
+    xa0 = xa0 / yly;
+    xa1 = xa1 / yly;
+    for (int s = 0; s < 2; ++s) {
+      c[s].assign(h + 1, 0.0);  // 1-based
+      for (int j = 1; j <= h; ++j) c[s][j] = yky[2 * j - 2 + s];
+    }
+  }
+  // row j (1-based) of system s into d[1..5]
+  void row(int s, int j, double sxz, bool pin, double d[6]) const {
+    const std::vector<double>& w = c[s];
+    const double xa0_2 = xa0 * xa0, xa1_2 = xa1 * xa1, xa01 = xa0 * xa1, xa0p1_2 = (xa0 + xa1) * (xa0 + xa1);
+    for (int q = 0; q < 6; ++q) d[q] = 0.0;
+    // main diagonal (:2846-2926)
+    if (j >= 2 && j <= h - 1) d[3] = -(sxz + xa0_2 * (w[j] * w[j]) + xa1_2 * w[j] * (w[j - 1] + w[j + 1]));
+    else if (j == 1) {
+      if (s == 0) d[3] = -(sxz + xa0_2 * (w[1] * w[1]) + xa1_2 * w[1] * w[2]);
+      else d[3] = -(sxz + (xa0_2 - xa1_2) * (w[1] * w[1]) + xa1_2 * w[1] * w[2]);
+    } else {
+      if (s == 0) d[3] = -(sxz + xa0_2 * (w[h] * w[h]) + xa1_2 * w[h] * w[h - 1]);
+      else d[3] = -(sxz + xa0p1_2 * (w[h] * w[h]) + xa1_2 * w[h] * w[h - 1]);
+    }
+    // super-diagonal +1 (:2930-2975)
+    if (j >= 2 && j <= h - 1) d[4] = xa01 * (w[j + 1] * (w[j] + w[j + 1]));
+    if (j == 1) {
+      if (s == 0) d[4] = 2.0 * xa01 * (w[1] * w[2] + w[2] * w[2]);
+      else d[4] = (xa0 - xa1) * xa1 * (w[1] * w[2]) + xa0 * xa1 * (w[2] * w[2]);
+    }
+    if (s == 1 && j == h - 1) d[4] = xa0 * xa1 * w[h - 1] * w[h] + (xa0 + xa1) * xa1 * (w[h] * w[h]);
+    if (s == 1 && j == h) d[4] = 0.0;
+    // super-diagonal +2 (:2977-2997)
+    if (j <= h - 2) d[5] = xa1_2 * (-(w[j + 1] * w[j + 2]));
+    if (s == 0 && j == 1) d[5] = 2.0 * d[5];
+    // sub-diagonal -1 (:2999-3023)
+    if (j >= 2) d[2] = xa01 * (w[j - 1] * (w[j] + w[j - 1]));
+    if (s == 1 && j == 2) d[2] = xa0 * xa1 * (w[2] * w[1]) + (xa0 + xa1) * xa1 * (w[1] * w[1]);
+    if (s == 1 && j == h) d[2] = (xa0 + xa1) * xa1 * (w[h] * w[h - 1]) + xa0 * xa1 * (w[h - 1] * w[h - 1]);
+    // sub-diagonal -2 (:3025-3036)
+    if (j >= 3) d[1] = xa1_2 * (-(w[j - 1] * w[j - 2]));
+    // the zero mode is pinned (:3038-3046)
+    if (pin && s == 0 && j == 1) { d[3] = 1.0; d[4] = 0.0; d[5] = 0.0; }
+  }
+};
+
+// inversion5_v1 (poisson_1stderivcomp.f90:420-561) for one real system (rows 1..h, diagonals
+// a[j][1..5]) and right-hand side e[1..h]; eps = 1e-16 (DOUBLE_PREC).  The real and imaginary
+// parts of the reference share the same real matrix, so one call handles one part.
+static void inversion5(std::vector<std::array<double, 6>> a, std::vector<double>& e, int h) {
+  const double eps = 1.0e-16;
+  double tmp = 0.0;  // a zero pivot keeps the previous multiplier, as the reference does
+  for (int m = 1; m <= h - 2; ++m) {
+    for (int i = 1; i <= 2; ++i) {
+      const int mi = m + i;
+      if (a[m][3] != 0.0) tmp = a[mi][3 - i] / a[m][3];
+      e[mi] = e[mi] - tmp * e[m];
+      for (int jc = 4 - i; jc <= 5 - i; ++jc) a[mi][jc] = a[mi][jc] - tmp * a[m][jc + i];
+    }
+  }
+  double t1 = std::fabs(a[h - 1][3]) > eps ? a[h][2] / a[h - 1][3] : 0.0;
+  const double sr = t1;
+  double b1 = a[h][3] - t1 * a[h - 1][4];
+  double t3;
+  if (std::fabs(b1) > eps) {
+    t1 = sr / b1;
+    t3 = e[h] / b1 - t1 * e[h - 1];
+  } else {
+    t1 = 0.0;
+    t3 = 0.0;
+  }
+  e[h] = t3;
+  b1 = std::fabs(a[h - 1][3]) > eps ? 1.0 / a[h - 1][3] : 0.0;
+  double a1 = a[h - 1][4] * b1;
+  e[h - 1] = e[h - 1] * b1 - a1 * e[h];
+  for (int i = h - 2; i >= 1; --i) {
+    const double s = std::fabs(a[i][3]) > eps ? 1.0 / a[i][3] : 0.0;
+    a1 = a[i][4] * s;
+    const double bb = a[i][5] * s;
+    e[i] = e[i] * s - a1 * e[i + 1] - bb * e[i + 2];
+  }
+}
+
+// poisson_010.  The reference's real-to-complex 3D FFT (z halved) is taken here as the full
+// complex DFT of the real data; the forward and backward x and z half-cell phase factors
+// (:1527-1553, :1740-1767) multiply each (kx, kz) column by e^{-i theta} and e^{+i theta} around
+// a y stage that applies one real operator to both real and imaginary parts, so they cancel and
+// are left out, as in poisson_000 above.
+static void poisson_010(const Domain& dm, std::vector<double>& rhs) {
+  const int nx = dm.nc[0], ny = dm.nc[1], nz = dm.nc[2];
+  if (ny % 2 || ny < 8) throw std::runtime_error("poisson_010 needs an even ny >= 8");
+  if (dm.stretch_y && dm.istret != 1 && dm.istret != 2) throw std::runtime_error("poisson_010: istret 1 or 2");
+  const int n3[3] = {nx, ny, nz};
+  auto at = [&](int i, int j, int k) { return ((size_t)k * ny + j) * nx + i; };
+  // even/odd reordering in y (:1491-1501)
+  std::vector<std::complex<double>> a(rhs.size());
+  for (int k = 0; k < nz; ++k)
+    for (int i = 0; i < nx; ++i) {
+      for (int j = 1; j <= ny / 2; ++j) a[at(i, j - 1, k)] = rhs[at(i, 2 * (j - 1), k)];
+      for (int j = ny / 2 + 1; j <= ny; ++j) a[at(i, j - 1, k)] = rhs[at(i, 2 * ny - 2 * j + 1, k)];
+    }
+  for (int ax = 0; ax < 3; ++ax) cdft_axis(a, n3, ax, -1);
+  for (auto& v : a) v = v / double(nx) / double(ny) / double(nz);
+  std::vector<double> ay(ny), by(ny);  // abxyz, bcy = 1 (:2376-2382)
+  for (int j = 1; j <= ny; ++j) {
+    ay[j - 1] = std::sin(double(j - 1) * PI * 0.5 / double(ny));
+    by[j - 1] = std::cos(double(j - 1) * PI * 0.5 / double(ny));
+  }
+  auto kx = mod_k2(dm, 0, nx, dm.lxx, dm.h[0]);
+  auto kz = mod_k2(dm, 2, nz, dm.lzz, dm.h[2]);
+  std::vector<double> yky, yk2;
+  waves_y_neumann(dm, yky, yk2);
+  Penta P;
+  if (dm.stretch_y) P.init(dm, yky);
+  const int h = ny / 2;
+#pragma omp parallel for collapse(2)
+  for (int k = 0; k < nz; ++k)
+    for (int i = 0; i < nx; ++i) {
+      std::vector<std::complex<double>> c(ny), b(ny);
+      for (int j = 0; j < ny; ++j) c[j] = a[at(i, j, k)];
+      // forward post-processing in y (:1557-1575)
+      b[0] = c[0];
+      for (int j = 2; j <= ny; ++j) {
+        const double t1 = c[j - 1].real(), t2 = c[j - 1].imag();
+        const double t3 = c[ny - j + 1].real(), t4 = c[ny - j + 1].imag();
+        const double yb = by[j - 1], ya = ay[j - 1];
+        const double xx1 = t1 * yb, xx2 = t1 * ya, xx3 = t2 * yb, xx4 = t2 * ya;
+        const double xx5 = t3 * yb, xx6 = t3 * ya, xx7 = t4 * yb, xx8 = t4 * ya;
+        b[j - 1] = 0.5 * std::complex<double>(xx1 + xx4 + xx5 - xx8, -xx2 + xx3 + xx6 + xx7);
+      }
+      if (!dm.stretch_y) {
+        // wavenumber division (:1591-1613), kxyz = xk2 + yk2 + zk2 with equal parts
+        for (int j = 0; j < ny; ++j) {
+          const double kk = kx[i] + yk2[j] + kz[k];
+          if (std::fabs(kk) < 1.0e-16) b[j] = 0.0;
+          else b[j] = std::complex<double>(b[j].real() / (-kk), b[j].imag() / (-kk));
+        }
+      } else {
+        // odd and even modes (:1650-1675), inversion5_v1 on each
+        const bool pin = kx[i] == 0.0 && kz[k] == 0.0;
+        const double sxz = kx[i] + kz[k];
+        for (int s = 0; s < 2; ++s) {
+          std::vector<std::array<double, 6>> mat(h + 1);
+          std::vector<double> er(h + 1), ei(h + 1);
+          for (int j = 1; j <= h; ++j) {
+            double d[6];
+            P.row(s, j, sxz, pin, d);
+            for (int q = 0; q < 6; ++q) mat[j][q] = d[q];
+            er[j] = b[2 * j - 2 + s].real();
+            ei[j] = b[2 * j - 2 + s].imag();
+          }
+          inversion5(mat, er, h);
+          inversion5(mat, ei, h);
+          for (int j = 1; j <= h; ++j) b[2 * j - 2 + s] = std::complex<double>(er[j], ei[j]);
+        }
+      }
+      // backward post-processing in y (:1717-1735)
+      c[0] = b[0];
+      for (int j = 2; j <= ny; ++j) {
+        const double t1 = b[j - 1].real(), t2 = b[j - 1].imag();
+        const double t3 = b[ny - j + 1].real(), t4 = b[ny - j + 1].imag();
+        const double yb = by[j - 1], ya = ay[j - 1];
+        const double xx1 = t1 * yb, xx2 = t1 * ya, xx3 = t2 * yb, xx4 = t2 * ya;
+        const double xx5 = t3 * yb, xx6 = t3 * ya, xx7 = t4 * yb, xx8 = t4 * ya;
+        c[j - 1] = std::complex<double>(xx1 - xx4 + xx6 + xx7, -(-xx2 - xx3 + xx5 - xx8));
+      }
+      for (int j = 0; j < ny; ++j) a[at(i, j, k)] = c[j];
+    }
+  for (int ax = 0; ax < 3; ++ax) cdft_axis(a, n3, ax, +1);
+  // undo the reordering (:1772-1782)
+  for (int k = 0; k < nz; ++k)
+    for (int i = 0; i < nx; ++i) {
+      for (int j = 1; j <= ny / 2; ++j) rhs[at(i, 2 * j - 2, k)] = a[at(i, j - 1, k)].real();
+      for (int j = 1; j <= ny / 2; ++j) rhs[at(i, 2 * j - 1, k)] = a[at(i, ny - j, k)].real();
+    }
+}
+
+static void poisson_dispatch(const Domain& dm, std::vector<double>& rhs) {
+  // solve_fft_poisson (poisson_interface.f90:119-149) and the poisson_000 / poisson_010 choice of
+  // decomp_2d_poisson_init (poisson_1stderivcomp.f90:794-820)
+  if (dm.ifft == 2) poisson_fishpack(dm, rhs);
+  else if (dm.periodic[1]) poisson_3dfft(dm, rhs);
+  else poisson_010(dm, rhs);
+}
+
 // Get_divergence_flow (eq_continuity.f90:91-161)
 static Arr divergence(const Domain& dm, const std::vector<double>& ux, const std::vector<double>& uy,
                       const std::vector<double>& uz) {
@@ -844,8 +1121,7 @@ void momentum_substep(Domain& dm, Flow& fl, int isub, double* bulk_out) {
   for (size_t n = 0; n < pcor.size(); ++n) pcor[n] = pcor[n] + div.v[n];
   const double coeff = 1.0 / (dm.tAlpha[isub] * dm.sigma2p * dm.dt);
   for (auto& v : pcor) v = v * coeff;
-  if (dm.ifft == 2) poisson_fishpack(dm, pcor);
-  else poisson_3dfft(dm, pcor);
+  poisson_dispatch(dm, pcor);
   for (size_t n = 0; n < fl.pres.size(); ++n) fl.pres[n] = fl.pres[n] + pcor[n];
   fl.pcor = pcor;
   // Correct_massflux (eq_momentum2.f90:1577-1660)
@@ -1365,8 +1641,7 @@ int orc_poisson(void* p, double* rhs) {
   auto* H = static_cast<OrcHandle*>(p);
   const Domain& dm = H->dm;
   std::vector<double> r(rhs, rhs + (size_t)dm.nc[0] * dm.nc[1] * dm.nc[2]);
-  if (dm.ifft == 2) poisson_fishpack(dm, r);
-  else poisson_3dfft(dm, r);
+  poisson_dispatch(dm, r);
   std::memcpy(rhs, r.data(), sizeof(double) * r.size());
   return 0;
 }

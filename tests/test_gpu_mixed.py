@@ -20,9 +20,13 @@ def rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
-@pytest.mark.parametrize("acc", [1, 3])
-def test_channel_mixed_profiles_vs_oracle(acc):
-    cfg = C.channel(nc=(32, 24, 16), iacc=acc, dt=0.004)
+@pytest.mark.parametrize("acc,ifft", [(1, C.FFT_FISHPACK_2DFFT), (3, C.FFT_FISHPACK_2DFFT),
+                                      (4, C.FFT_2DECOMP_3DFFT)])
+def test_channel_mixed_profiles_vs_oracle(acc, ifft):
+    if ifft == C.FFT_2DECOMP_3DFFT:
+        cfg = C.channel(nc=(32, 24, 16), iacc=acc, dt=0.004, rstret=0.25, ifft=ifft)
+    else:
+        cfg = C.channel(nc=(32, 24, 16), iacc=acc, dt=0.004)
     f = I.channel_fields(cfg)
     o = po.Oracle(cfg)
     o.set_fields(*f)

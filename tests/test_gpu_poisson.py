@@ -34,3 +34,20 @@ def test_poisson_000(n, acc):
     got = g.solve_fft_poisson(rhs)
     assert np.abs(ref - got).max() / np.abs(ref).max() < 1e-11
     g.close()
+
+
+@pytest.mark.parametrize("nc,acc,istret", [((16, 24, 12), 1, 2), ((32, 64, 24), 4, 2), ((24, 48, 16), 3, 1),
+                                          ((16, 32, 8), 4, 0), ((16, 256, 8), 1, 2), ((64, 96, 64), 4, 2),
+                                          ((18, 16, 27), 2, 2)])
+def test_poisson_010(nc, acc, istret):
+    """poisson_010 (y walls, 3FMD stretching or uniform) on the GPU vs the oracle, random rhs."""
+    cfg = C.channel(nc=nc, iacc=acc, rstret=0.25, ifft=C.FFT_2DECOMP_3DFFT, istret=istret)
+    o = po.Oracle(cfg)
+    g = S.Solver(cfg)
+    rng = np.random.default_rng(7)
+    rhs = rng.standard_normal(o.shape_ccc)
+    ref = o.poisson(rhs)
+    got = g.solve_fft_poisson(rhs)
+    assert np.abs(ref - got).max() / np.abs(ref).max() < 1e-11
+    g.close()
+
