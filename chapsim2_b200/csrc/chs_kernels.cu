@@ -1285,10 +1285,11 @@ __global__ void __launch_bounds__(256) dct_y_kernel(const __grid_constant__ FftP
                                                     int nxh, int nz, int lpc, const double* __restrict__ ayby,
                                                     const double* __restrict__ k2x, const double* __restrict__ k2z,
                                                     const double* __restrict__ k2y, const double* __restrict__ ptab,
-                                                    double scale) {
+                                                    const double* __restrict__ pfac, double scale) {
   extern __shared__ double2 sh[];
   __shared__ int64_t lbase[32];
   __shared__ double lkx[32], lkz[32];
+  __shared__ int64_t lfoff[32];  // start of the column's elimination factors in pfac, -1 past the end
   const int ny = fp.n, h = ny / 2;
   double2* b0 = sh;
   double2* b1 = sh + (size_t)lpc * ny;
@@ -1301,8 +1302,11 @@ __global__ void __launch_bounds__(256) dct_y_kernel(const __grid_constant__ FftP
       lbase[threadIdx.x] = kx + (int64_t)kz * nxh * ny;
       lkx[threadIdx.x] = k2x[kx];
       lkz[threadIdx.x] = k2z[kz];
+      const int kzf = kz <= nz - kz ? kz : nz - kz;
+      lfoff[threadIdx.x] = (int64_t)kzf * h * 8 * nxh + kx;
     } else {
       lbase[threadIdx.x] = -1;
+      lfoff[threadIdx.x] = -1;
       lkx[threadIdx.x] = 0.0;
       lkz[threadIdx.x] = 0.0;
     }
@@ -1362,79 +1366,85 @@ __global__ void __launch_bounds__(256) dct_y_kernel(const __grid_constant__ FftP
     o[j * lpc + l] = v;
   }
   __syncthreads();
-  if (MODE == 1 && threadIdx.x < 2 * lpc) {
-    // one thread per (column, parity): inversion5_v1 on rows r = 0..h-1 (mode j = 2r + s), the
-    // rows generated from the tables as the elimination reaches them.  The modified diagonal
-    // and super-diagonal of each pivot row are kept for the back substitution in the free FFT
-    // buffer r, layout [row][thread].
-    const int tid = threadIdx.x, nt = 2 * lpc;
-    const int l = tid >> 1, s = tid & 1;
-    if (lbase[l] >= 0) {
-      double* f3 = reinterpret_cast<double*>(r);
-      double* f4 = f3 + (size_t)h * nt;
-      const double* A1 = ptab + (size_t)s * 6 * h;
-      const double* A2 = A1 + h;
-      const double* T1 = A1 + 2 * h;
-      const double* T2 = A1 + 3 * h;
-      const double* A4 = A1 + 4 * h;
-      const double* A5 = A1 + 5 * h;
-      const double sxz = lkx[l] + lkz[l];
-      const bool pin = s == 0 && lkx[l] == 0.0 && lkz[l] == 0.0;
-      auto diag = [&](int row) { return -((sxz + T1[row]) + T2[row]); };
-      auto sup2 = [&](int row) { return (pin && row == 0) ? 0.0 : A5[row]; };
-      auto E = [&](int row) -> double2& { return o[(2 * row + s) * lpc + l]; };
-      double P3 = pin ? 1.0 : diag(0), P4 = pin ? 0.0 : A4[0];
-      double R12 = A2[1], R13 = diag(1), R14 = A4[1];
-      double R21 = A1[2], R22 = A2[2], R23 = diag(2), R24 = A4[2];
-      double2 e0 = E(0), e1 = E(1), e2 = E(2);
-      double tmp = 0.0;  // a zero pivot keeps the previous multiplier, as the reference does
-      for (int m = 0; m <= h - 3; ++m) {
-        const double P5 = sup2(m);
-        if (P3 != 0.0) tmp = R12 / P3;
-        e1.x = e1.x - tmp * e0.x;
-        e1.y = e1.y - tmp * e0.y;
-        R13 = R13 - tmp * P4;
-        R14 = R14 - tmp * P5;
-        if (P3 != 0.0) tmp = R21 / P3;
-        e2.x = e2.x - tmp * e0.x;
-        e2.y = e2.y - tmp * e0.y;
-        R22 = R22 - tmp * P4;
-        R23 = R23 - tmp * P5;
-        f3[(size_t)m * nt + tid] = P3;
-        f4[(size_t)m * nt + tid] = P4;
-        E(m) = e0;
-        P3 = R13; P4 = R14; e0 = e1;
-        R12 = R22; R13 = R23; R14 = R24; e1 = e2;
-        if (m + 3 < h) {
-          R21 = A1[m + 3]; R22 = A2[m + 3]; R23 = diag(m + 3); R24 = A4[m + 3];
-          e2 = E(m + 3);
+  if (MODE == 1) {
+    // one thread per (column, parity): inversion5_v1 on rows r = 0..h-1 (mode j = 2r + s) with
+    // the elimination factors of the column's matrix (dct_y_factor_kernel).  The factors are
+    // staged in the free FFT buffer r by all threads (coalesced across kx): the forward
+    // multipliers for the forward sweep, then the back-substitution factors, layout
+    // [row][field][thread] with thread = 2 l + s.
+    double* fs = reinterpret_cast<double*>(r);
+    const int nt = 2 * lpc;
+    const float intt = 1.0f / (float)nt;
+    auto stage = [&](int f0) {
+      // fields f0, f0+1 of every row for every (column, parity)
+      const int tot = h * 2 * nt;
+      constexpr int kB = 8;  // loads in flight per thread
+      for (int t0 = threadIdx.x; t0 < tot; t0 += kB * blockDim.x) {
+        double v[kB];
+#pragma unroll
+        for (int u = 0; u < kB; ++u) {
+          const int t = t0 + u * blockDim.x;
+          v[u] = 0.0;
+          if (t < tot) {
+            const int rf = fast_div(t, nt, intt), c = t - rf * nt;  // rf = row * 2 + field
+            const int row = rf >> 1, fld = f0 + (rf & 1);
+            const int64_t off = lfoff[c >> 1];
+            if (off >= 0) v[u] = __ldg(pfac + off + ((size_t)(row * 4 + fld) * 2 + (c & 1)) * nxh);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kB; ++u) {
+          const int t = t0 + u * blockDim.x;
+          if (t < tot) fs[t] = v[u];
         }
       }
-      // rows h-2 (P) and h-1 (R1)
-      double t1 = fabs(P3) > kInv5Eps ? R12 / P3 : 0.0;
-      const double sr = t1;
-      double bb = R13 - t1 * P4;
-      double2 eh;
-      if (fabs(bb) > kInv5Eps) {
-        t1 = sr / bb;
-        eh = make_double2(e1.x / bb - t1 * e0.x, e1.y / bb - t1 * e0.y);
-      } else {
-        eh = make_double2(0.0, 0.0);
+    };
+    stage(0);
+    __syncthreads();
+    const int tid = threadIdx.x;
+    const int l = tid >> 1, s = tid & 1;
+    const bool act = tid < nt && lbase[l >= 0 && l < 32 ? l : 0] >= 0;
+    auto E = [&](int row) -> double2& { return o[(2 * row + s) * lpc + l]; };
+    auto FS = [&](int row, int fld) { return fs[(row * 2 + fld) * nt + tid]; };
+    double2 e0 = make_double2(0.0, 0.0), e1 = e0;
+    if (act) {
+      e0 = E(0);
+      e1 = E(1);
+      double2 e2 = E(2);
+      for (int m = 0; m <= h - 3; ++m) {
+        const double L1 = FS(m, 0), L2 = FS(m, 1);
+        const double2 e3 = m + 3 < h ? E(m + 3) : make_double2(0.0, 0.0);
+        e1.x = e1.x - L1 * e0.x;
+        e1.y = e1.y - L1 * e0.y;
+        e2.x = e2.x - L2 * e0.x;
+        e2.y = e2.y - L2 * e0.y;
+        E(m) = e0;
+        e0 = e1;
+        e1 = e2;
+        e2 = e3;
       }
-      bb = fabs(P3) > kInv5Eps ? 1.0 / P3 : 0.0;
-      double a1 = P4 * bb;
-      const double2 ehm = make_double2(e0.x * bb - a1 * eh.x, e0.y * bb - a1 * eh.y);
+    }
+    __syncthreads();
+    stage(2);
+    __syncthreads();
+    if (act) {
+      // rows h-1 and h-2: (b1, tmp1/b1) and (1/a3, a4/a3) of the reference's last two steps
+      const double bb = FS(h - 1, 0), t1 = FS(h - 1, 1);
+      double2 eh = make_double2(0.0, 0.0);
+      if (fabs(bb) > kInv5Eps) eh = make_double2(e1.x / bb - t1 * e0.x, e1.y / bb - t1 * e0.y);
+      const double q2 = FS(h - 2, 0), a2 = FS(h - 2, 1);
+      const double2 ehm = make_double2(e0.x * q2 - a2 * eh.x, e0.y * q2 - a2 * eh.y);
       E(h - 1) = eh;
       E(h - 2) = ehm;
+      const double* A5 = ptab + (size_t)s * 6 * h + 5 * h;
+      const bool pin = s == 0 && lkx[l] == 0.0 && lkz[l] == 0.0;
       double2 x1 = ehm, x2 = eh;
       for (int i = h - 3; i >= 0; --i) {
-        const double d3 = f3[(size_t)i * nt + tid], d4 = f4[(size_t)i * nt + tid];
-        const double q = fabs(d3) > kInv5Eps ? 1.0 / d3 : 0.0;
-        a1 = d4 * q;
-        bb = sup2(i) * q;
+        const double q = FS(i, 0), a1 = FS(i, 1);
+        const double b1 = ((pin && i == 0) ? 0.0 : __ldg(A5 + i)) * q;
         double2 ei = E(i);
-        ei.x = ei.x * q - a1 * x1.x - bb * x2.x;
-        ei.y = ei.y * q - a1 * x1.y - bb * x2.y;
+        ei.x = ei.x * q - a1 * x1.x - b1 * x2.x;
+        ei.y = ei.y * q - a1 * x1.y - b1 * x2.y;
         E(i) = ei;
         x2 = x1;
         x1 = ei;
@@ -1470,8 +1480,78 @@ __global__ void __launch_bounds__(256) dct_y_kernel(const __grid_constant__ FftP
   }
 }
 
+// The elimination of inversion5_v1 depends on the column only through the main-diagonal shift
+// kx2 + kz2 (and the zero-mode pin), not on the right-hand side, so it is done once per
+// (kx, |kz|) and parity: per row r the forward multipliers of the step with pivot r (fields 0, 1;
+// a zero pivot keeps the previous multiplier, as the reference does), and the back-substitution
+// factors 1/a3 and a4/a3 (fields 2, 3; 0 for a pivot within eps), for the last row b1 and
+// tmp1/b1 of the reference's closing 2x2 step.  The arithmetic is the reference's, in its order.
+__global__ void dct_y_factor_kernel(double* __restrict__ pfac, int nxh, int nzh, int nz, int h,
+                                    const double* __restrict__ k2x, const double* __restrict__ k2z,
+                                    const double* __restrict__ ptab) {
+  const int64_t n = (int64_t)nxh * nzh * 2;
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const int kx = (int)(g % nxh);
+  const int64_t rr = g / nxh;
+  const int s = (int)(rr % 2);
+  const int kzf = (int)(rr / 2);
+  (void)nz;
+  double* F = pfac + ((size_t)kzf * h * 8 + s) * nxh + kx;
+  const size_t fst = (size_t)2 * nxh;
+  const double* A1 = ptab + (size_t)s * 6 * h;
+  const double* A2 = A1 + h;
+  const double* T1 = A1 + 2 * h;
+  const double* T2 = A1 + 3 * h;
+  const double* A4 = A1 + 4 * h;
+  const double* A5 = A1 + 5 * h;
+  const double sxz = k2x[kx] + k2z[kzf];
+  const bool pin = s == 0 && k2x[kx] == 0.0 && k2z[kzf] == 0.0;
+  auto diag = [&](int row) { return -((sxz + T1[row]) + T2[row]); };
+  auto sup2 = [&](int row) { return (pin && row == 0) ? 0.0 : A5[row]; };
+  auto put = [&](int row, int field, double v) { F[(size_t)row * 4 * fst + field * fst] = v; };
+  double P3 = pin ? 1.0 : diag(0), P4 = pin ? 0.0 : A4[0];
+  double R12 = A2[1], R13 = diag(1), R14 = A4[1];
+  double R21 = A1[2], R22 = A2[2], R23 = diag(2), R24 = A4[2];
+  double tmp = 0.0;
+  for (int m = 0; m <= h - 3; ++m) {
+    const double P5 = sup2(m);
+    if (P3 != 0.0) tmp = R12 / P3;
+    put(m, 0, tmp);
+    R13 = R13 - tmp * P4;
+    R14 = R14 - tmp * P5;
+    if (P3 != 0.0) tmp = R21 / P3;
+    put(m, 1, tmp);
+    R22 = R22 - tmp * P4;
+    R23 = R23 - tmp * P5;
+    const double q = fabs(P3) > kInv5Eps ? 1.0 / P3 : 0.0;
+    put(m, 2, q);
+    put(m, 3, P4 * q);
+    P3 = R13; P4 = R14;
+    R12 = R22; R13 = R23; R14 = R24;
+    if (m + 3 < h) { R21 = A1[m + 3]; R22 = A2[m + 3]; R23 = diag(m + 3); R24 = A4[m + 3]; }
+  }
+  double t1 = fabs(P3) > kInv5Eps ? R12 / P3 : 0.0;
+  const double sr = t1;
+  const double bb = R13 - t1 * P4;
+  t1 = fabs(bb) > kInv5Eps ? sr / bb : 0.0;
+  put(h - 1, 2, bb);
+  put(h - 1, 3, t1);
+  const double q = fabs(P3) > kInv5Eps ? 1.0 / P3 : 0.0;
+  put(h - 2, 2, q);
+  put(h - 2, 3, P4 * q);
+}
+
+void launch_dct_y_factor(double* pfac, int nxh, int nz, int ny, const double* k2x, const double* k2z,
+                         const double* ptab, cudaStream_t st) {
+  const int nzh = nz / 2 + 1;
+  const int64_t n = (int64_t)nxh * nzh * 2;
+  dct_y_factor_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(pfac, nxh, nzh, nz, ny / 2, k2x, k2z, ptab);
+}
+
 void launch_dct_y(const FftPlan& fp, double2* data, int nxh, int nz, const double* ayby, const double* k2x,
-                  const double* k2z, const double* k2y, const double* ptab, double scale, cudaStream_t st) {
+                  const double* k2z, const double* k2y, const double* ptab, const double* pfac, double scale,
+                  cudaStream_t st) {
   const int ny = fp.n;
   if (ny % 2 || ny < 8) throw std::runtime_error("dct_y: ny must be even and at least 8");
   const int lpc = fft_lines_per_cta(ny);
@@ -1479,11 +1559,12 @@ void launch_dct_y(const FftPlan& fp, double2* data, int nxh, int nz, const doubl
   const size_t shm = 2 * (size_t)lpc * ny * sizeof(double2);
   const unsigned grid = (unsigned)((nlines + lpc - 1) / lpc);
   if (ptab) {
+    if (!pfac) throw std::runtime_error("dct_y: the pentadiagonal factors are missing");
     cudaFuncSetAttribute(dct_y_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-    dct_y_kernel<1><<<grid, 256, shm, st>>>(fp, data, nxh, nz, lpc, ayby, k2x, k2z, k2y, ptab, scale);
+    dct_y_kernel<1><<<grid, 256, shm, st>>>(fp, data, nxh, nz, lpc, ayby, k2x, k2z, k2y, ptab, pfac, scale);
   } else {
     cudaFuncSetAttribute(dct_y_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-    dct_y_kernel<0><<<grid, 256, shm, st>>>(fp, data, nxh, nz, lpc, ayby, k2x, k2z, k2y, ptab, scale);
+    dct_y_kernel<0><<<grid, 256, shm, st>>>(fp, data, nxh, nz, lpc, ayby, k2x, k2z, k2y, ptab, pfac, scale);
   }
 }
 

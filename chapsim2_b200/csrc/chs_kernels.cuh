@@ -139,8 +139,14 @@ void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* Zr, con
 // rows [6][ny/2] sub-2, sub-1, t1, t2, super-1, super-2 with main diagonal
 // -(((kx2 + kz2) + t1) + t2)) or, with ptab null, the division by -(kx2 + k2y + kz2), and the
 // inverse steps; ayby holds sin and cos of (j pi / 2 ny), j < ny; scale the FFT normalisation
+// (pfac: the elimination factors of the pentadiagonal systems from launch_dct_y_factor)
 void launch_dct_y(const FftPlan& fp, double2* data, int nxh, int nz, const double* ayby, const double* k2x,
-                  const double* k2z, const double* k2y, const double* ptab, double scale, cudaStream_t st);
+                  const double* k2z, const double* k2y, const double* ptab, const double* pfac, double scale,
+                  cudaStream_t st);
+// elimination factors of the poisson_010 pentadiagonal systems per (kx, |kz|) and parity, computed
+// once: 8 * (ny/2) * (nz/2+1) * nxh doubles
+void launch_dct_y_factor(double* pfac, int nxh, int nz, int ny, const double* k2x, const double* k2z,
+                         const double* ptab, cudaStream_t st);
 // 3D spectral division by -(kx'^2 + ky'^2 + kz'^2) (zero mode -> 0), with normalisation
 void launch_spectral_divide(double2* data, int nxh, int ny, int nz, const double* k2x, const double* k2y,
                             const double* k2z, double norm, cudaStream_t st);

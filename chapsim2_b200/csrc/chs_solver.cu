@@ -171,6 +171,7 @@ struct chs_handle {
   double *yzr = nullptr, *yd = nullptr;  // precomputed y-solve factors
   double *k2x = nullptr, *k2y = nullptr, *k2z = nullptr;
   double *ayby = nullptr, *ptab = nullptr;  // poisson_010 cosine factors and pentadiagonal rows
+  double* pfac = nullptr;                   // and the elimination factors per (kx, |kz|)
   // graphs per substep (1..3) and for a whole step
   cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
   long long kernels_per_sub[4] = {0, 0, 0, 0};
@@ -1041,12 +1042,23 @@ void setup_device(chs_handle* H, const chs_config* c) {
         }
         H->ptab = H->dalloc<double>(tab.size());
         CK(cudaMemcpyAsync(H->ptab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, H->st));
+        H->k2x = H->dalloc<double>(nxh);
+        H->k2z = H->dalloc<double>(nc2);
+        CK(cudaMemcpyAsync(H->k2x, kx.data(), nxh * sizeof(double), cudaMemcpyHostToDevice, H->st));
+        CK(cudaMemcpyAsync(H->k2z, kz.data(), nc2 * sizeof(double), cudaMemcpyHostToDevice, H->st));
+        H->pfac = H->dalloc<double>((size_t)8 * hh * (nc2 / 2 + 1) * nxh);
+        launch_dct_y_factor(H->pfac, nxh, nc2, nc1, H->k2x, H->k2z, H->ptab, H->st);
+        H->launches++;
       }
     }
-    H->k2x = H->dalloc<double>(nxh); H->k2y = H->dalloc<double>(nc1); H->k2z = H->dalloc<double>(nc2);
-    CK(cudaMemcpyAsync(H->k2x, kx.data(), nxh * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    if (!H->k2x) {
+      H->k2x = H->dalloc<double>(nxh);
+      H->k2z = H->dalloc<double>(nc2);
+      CK(cudaMemcpyAsync(H->k2x, kx.data(), nxh * sizeof(double), cudaMemcpyHostToDevice, H->st));
+      CK(cudaMemcpyAsync(H->k2z, kz.data(), nc2 * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    }
+    H->k2y = H->dalloc<double>(nc1);
     CK(cudaMemcpyAsync(H->k2y, ky.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice, H->st));
-    CK(cudaMemcpyAsync(H->k2z, kz.data(), nc2 * sizeof(double), cudaMemcpyHostToDevice, H->st));
   }
 }
 
@@ -1085,7 +1097,7 @@ void poisson_device(chs_handle* H, T* rhs) {
     // poisson_010 (src/poisson_1stderivcomp.f90:1457-1816): x and z transforms around the y
     // stage (the FFT normalisation 1/(nx ny nz) is applied there, after the forward transforms)
     PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, H->spec, nxh, nc1, nxh, (int64_t)nxh * nc1, -1, st));
-    PROF(H, 2, b_c2c, launch_dct_y(H->fy, H->spec, nxh, nc2, H->ayby, H->k2x, H->k2z, H->k2y, H->ptab,
+    PROF(H, 2, b_c2c, launch_dct_y(H->fy, H->spec, nxh, nc2, H->ayby, H->k2x, H->k2z, H->k2y, H->ptab, H->pfac,
                                    1.0 / ((double)nc0 * (double)nc1 * (double)nc2), st));
     PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, H->spec, nxh, nc1, nxh, (int64_t)nxh * nc1, +1, st));
     PROF(H, 1, b_r2c, launch_irfft_x(H->fx, H->spec, rhs, nc1 * nc2, 1.0, st));
