@@ -52,8 +52,11 @@ enum chs_precision { CHS_FP64 = 0, CHS_MIXED = 1 };
 typedef struct chs_config {
   int nc[3];                /* cells in x, y, z */
   int iacc;                 /* 1 CD2, 2 CD4, 3 CP4, 4 CP6 (src/modules.f90:248-251) */
-  int istret;               /* 0 none, 2 two-sided, 3 bottom, 4 top */
-  int ifft;                 /* 2 FISHPACK x/z-FFT + y-TDMA, 3 3D FFT (src/modules.f90:169-170) */
+  int istret;               /* 0 none, 1 centre, 2 two-sided, 3 bottom, 4 top */
+  int ifft;                 /* 2 FISHPACK x/z-FFT + y-TDMA (tanh mapping), 3 3D FFT (src/modules.f90:169-170):
+                             * poisson_000 for periodic y, poisson_010 for y walls
+                             * (src/poisson_1stderivcomp.f90:794-820; even ny, istret 0, 1 or 2, whose
+                             * y arrays below must be the 3FMD mapping, src/geometry.f90:287-408) */
   int idriven;              /* 0 none, 1 constant x mass flux */
   int precision;            /* chs_precision */
   double lxx, lyt, lyb, lzz;
