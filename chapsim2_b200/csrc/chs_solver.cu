@@ -1816,23 +1816,31 @@ double* field_ptr(chs_handle* H, int field, size_t* n) {
 }
 
 // host (double) -> device field, converting to float in the mixed form (stream-ordered)
-void h2d_field(chs_handle* H, double* dev, const double* host, size_t n) {
+// host <-> device copy of one field on stream st; the mixed form converts through an FP64
+// staging buffer (one per stream that copies concurrently)
+void h2d_field(chs_handle* H, double* dev, const double* host, size_t n, cudaStream_t st = nullptr,
+               double* stage = nullptr) {
+  if (!st) st = H->st;
+  if (!stage) stage = H->stage;
   if (!H->mixed) {
-    CK(cudaMemcpyAsync(dev, host, n * sizeof(double), cudaMemcpyHostToDevice, H->st));
+    CK(cudaMemcpyAsync(dev, host, n * sizeof(double), cudaMemcpyHostToDevice, st));
     return;
   }
-  CK(cudaMemcpyAsync(H->stage, host, n * sizeof(double), cudaMemcpyHostToDevice, H->st));
-  launch_convert(reinterpret_cast<float*>(dev), H->stage, (int64_t)n, H->st);
+  CK(cudaMemcpyAsync(stage, host, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  launch_convert(reinterpret_cast<float*>(dev), stage, (int64_t)n, st);
   H->launches++;
 }
-void d2h_field(chs_handle* H, double* host, const double* dev, size_t n) {
+void d2h_field(chs_handle* H, double* host, const double* dev, size_t n, cudaStream_t st = nullptr,
+               double* stage = nullptr) {
+  if (!st) st = H->st;
+  if (!stage) stage = H->stage;
   if (!H->mixed) {
-    CK(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    CK(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, st));
     return;
   }
-  launch_convert(H->stage, reinterpret_cast<const float*>(dev), (int64_t)n, H->st);
+  launch_convert(stage, reinterpret_cast<const float*>(dev), (int64_t)n, st);
   H->launches++;
-  CK(cudaMemcpyAsync(host, H->stage, n * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+  CK(cudaMemcpyAsync(host, stage, n * sizeof(double), cudaMemcpyDeviceToHost, st));
 }
 
 // ---- restart files and running statistics (src/io_restart.f90:32-227, src/post_statistics.f90:152-300)
@@ -2501,22 +2509,72 @@ int chs_time_steps_host_fields(chs_handle* H, int nsteps, int nfields, const int
       dev[f] = field_ptr(H, ids[f], &cnt[f]);
     }
     if (!H->gexec[1]) capture_graphs(H);
-    cudaEvent_t a, b;
-    CK(cudaEventCreate(&a));
-    CK(cudaEventCreate(&b));
-    CK(cudaEventRecord(a, H->st));
-    for (int s = 0; s < nsteps; ++s)
-      for (int isub = 1; isub <= 3; ++isub) {
-        for (int f = 0; f < nfields; ++f) h2d_field(H, dev[f], bufs[f], cnt[f]);
-        CK(cudaGraphLaunch(H->gexec[isub], H->st));
-        H->launches += H->kernels_per_sub[isub];
-        for (int f = 0; f < nfields; ++f) d2h_field(H, bufs[f], dev[f], cnt[f]);
+    // Copies in and out of every substep on two copy streams, one per PCIe direction, ordered
+    // per field: the copy-in of a field for substep k+1 waits only for that field's copy-out of
+    // substep k (it reads the host array that copy wrote), so copy-out and copy-in of different
+    // fields run at the same time; each substep's graph waits for all of its copies-in, and the
+    // copies-out wait for the graph.
+    cudaStream_t sin = nullptr, sout = nullptr;
+    CK(cudaStreamCreateWithFlags(&sin, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&sout, cudaStreamNonBlocking));
+    std::vector<cudaEvent_t> out_done(nfields, nullptr);
+    cudaEvent_t a = nullptr, b = nullptr, in_done = nullptr, graph_done = nullptr;
+    double* stage_out = nullptr;
+    auto cleanup = [&] {
+      for (auto& e : out_done)
+        if (e) cudaEventDestroy(e);
+      for (cudaEvent_t e : {a, b, in_done, graph_done})
+        if (e) cudaEventDestroy(e);
+      if (stage_out) cudaFree(stage_out);
+      if (sin) cudaStreamDestroy(sin);
+      if (sout) cudaStreamDestroy(sout);
+    };
+    try {
+      for (auto& e : out_done) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&in_done, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&graph_done, cudaEventDisableTiming));
+      CK(cudaEventCreate(&a));
+      CK(cudaEventCreate(&b));
+      if (H->mixed) {
+        size_t m = 0;
+        for (size_t c : cnt) m = std::max(m, c);
+        CK(cudaMalloc(&stage_out, std::max<size_t>(m, 1) * sizeof(double)));
       }
-    CK(cudaEventRecord(b, H->st));
-    CK(cudaEventSynchronize(b));
-    CK(cudaEventElapsedTime(ms, a, b));
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
+      CK(cudaEventRecord(a, H->st));
+      CK(cudaStreamWaitEvent(sin, a, 0));
+      bool first = true;
+      for (int s = 0; s < nsteps; ++s)
+        for (int isub = 1; isub <= 3; ++isub) {
+          for (int f = 0; f < nfields; ++f) {
+            if (!first) CK(cudaStreamWaitEvent(sin, out_done[f], 0));
+            h2d_field(H, dev[f], bufs[f], cnt[f], sin, H->stage);
+          }
+          first = false;
+          CK(cudaEventRecord(in_done, sin));
+          CK(cudaStreamWaitEvent(H->st, in_done, 0));
+          CK(cudaGraphLaunch(H->gexec[isub], H->st));
+          H->launches += H->kernels_per_sub[isub];
+          CK(cudaEventRecord(graph_done, H->st));
+          CK(cudaStreamWaitEvent(sout, graph_done, 0));
+          for (int f = 0; f < nfields; ++f) {
+            d2h_field(H, bufs[f], dev[f], cnt[f], sout, stage_out);
+            CK(cudaEventRecord(out_done[f], sout));
+          }
+        }
+      // the timed region ends when the last copy-out has landed
+      CK(cudaEventRecord(graph_done, sout));
+      CK(cudaStreamWaitEvent(H->st, graph_done, 0));
+      CK(cudaEventRecord(b, H->st));
+      CK(cudaEventSynchronize(b));
+      CK(cudaEventElapsedTime(ms, a, b));
+    } catch (...) {
+      cudaStreamSynchronize(sin);
+      cudaStreamSynchronize(sout);
+      cudaStreamSynchronize(H->st);
+      cleanup();
+      throw;
+    }
+    cleanup();
   });
 }
 

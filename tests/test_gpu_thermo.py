@@ -120,3 +120,32 @@ def test_indexed_table_lookup_matches_oracle(nonuniform):
         err = np.max(np.abs(got - ref))
         assert err <= 1e-13 * (ref.max() - ref.min()), (name, err)
     g.close()
+
+
+@pytest.mark.parametrize("precision", [S.CHS_FP64, S.CHS_MIXED])
+def test_host_fields_pipeline_matches_device_steps(precision):
+    """chs_time_steps_host_fields (pinned host state copied in and out around every substep, the two
+    copy directions overlapped per field) gives the same state as device-resident steps."""
+    cfg, tc = C.heated_channel(nc=(32, 24, 16), iacc=1, dt=0.004, t_ini=0.49)
+    f = I.channel_fields(cfg)
+    a = S.Solver(cfg, precision=precision)
+    b = S.Solver(cfg, precision=precision)
+    for g in (a, b):
+        g.set_fields(*f)
+        g.thermo_init(tc)
+        g.substep(0)
+    ids = [S.CHS_QX, S.CHS_QY, S.CHS_QZ, S.CHS_PRES, S.CHS_GX, S.CHS_GY, S.CHS_GZ, S.CHS_RHOH]
+    host = {}
+    for k in ids:
+        x = b.download(k)
+        h = b.pinned(x.shape)
+        h[...] = x
+        host[k] = h
+    a.step(3)
+    b.time_steps_host_fields(3, host)
+    for k in ids:
+        ref = a.download(k)
+        assert np.array_equal(host[k], ref), k
+        assert np.array_equal(b.download(k), ref), k
+    a.close()
+    b.close()
