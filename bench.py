@@ -280,7 +280,8 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
     e2e = {"value": world * cfg.ncell * sub / (ms_e2e * 1e-3) / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": 3 * field_bytes, "d2h_bytes_per_step": 3 * field_bytes,
            "path": "chs_time_steps_host_fields: pinned host state copied in and out around every substep "
-                   f"({len(ids)} fields), substep graph in between"}
+                   f"({len(ids)} fields) on one copy stream per PCIe direction, ordered per field; the substep "
+                   "graph (energy and momentum parts with variable properties) in between"}
 
     # x-z-mean profiles after the same number of steps the other forms take (1 + warmup + 2 steps);
     # the profiling below advances this handle by two more substeps

@@ -174,6 +174,9 @@ struct chs_handle {
   double* pfac = nullptr;                   // and the elimination factors per (kx, |kz|)
   // graphs per substep (1..3) and for a whole step
   cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
+  // the energy and momentum parts of substeps 1..3 as separate graphs (host-array pipeline)
+  cudaGraphExec_t gpart[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
+  long long kernels_per_part[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
   long long kernels_per_sub[4] = {0, 0, 0, 0};
   bool capturing = false;
   // Dataflow scheduling of a captured substep.  Each launch names the buffers it reads and
@@ -1065,6 +1068,9 @@ void setup_device(chs_handle* H, const chs_config* c) {
 void drop_graphs(chs_handle* H) {
   for (auto& g : H->gexec)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto& row : H->gpart)
+    for (auto& g : row)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
 // plans are created lazily; the table must be on the device before any launch.  Captured
@@ -1955,28 +1961,39 @@ void stats_update_t(chs_handle* H, int nstat) {
   H->launches++;
 }
 
-void capture_graphs(chs_handle* H) {
-  for (int isub = 1; isub <= 3; ++isub) {
-    cudaGraph_t g;
-    const long long before = H->launches;
-    CK(cudaStreamBeginCapture(H->st, cudaStreamCaptureModeThreadLocal));
-    H->capturing = true;
-    try {
-      H->dag_start();
-      substep_body(H, isub);
-      H->dag_stop();
-    } catch (...) {
-      H->dag_stop();
-      H->capturing = false;
-      cudaStreamEndCapture(H->st, &g);
-      throw;
-    }
+// capture substep isub (parts PART_*) as one graph; returns its kernel count
+long long capture_one(chs_handle* H, int isub, int parts, cudaGraphExec_t* out) {
+  cudaGraph_t g;
+  const long long before = H->launches;
+  CK(cudaStreamBeginCapture(H->st, cudaStreamCaptureModeThreadLocal));
+  H->capturing = true;
+  try {
+    H->dag_start();
+    substep_body(H, isub, parts);
+    H->dag_stop();
+  } catch (...) {
+    H->dag_stop();
     H->capturing = false;
-    CK(cudaStreamEndCapture(H->st, &g));
-    H->kernels_per_sub[isub] = H->launches - before;
-    H->launches = before;
-    CK(cudaGraphInstantiate(&H->gexec[isub], g, 0));
-    CK(cudaGraphDestroy(g));
+    cudaStreamEndCapture(H->st, &g);
+    throw;
+  }
+  H->capturing = false;
+  CK(cudaStreamEndCapture(H->st, &g));
+  const long long n = H->launches - before;
+  H->launches = before;
+  CK(cudaGraphInstantiate(out, g, 0));
+  CK(cudaGraphDestroy(g));
+  return n;
+}
+
+void capture_graphs(chs_handle* H) {
+  for (int isub = 1; isub <= 3; ++isub) H->kernels_per_sub[isub] = capture_one(H, isub, PART_ALL, &H->gexec[isub]);
+}
+
+void capture_part_graphs(chs_handle* H) {
+  for (int isub = 1; isub <= 3; ++isub) {
+    H->kernels_per_part[0][isub] = capture_one(H, isub, PART_ENERGY, &H->gpart[0][isub]);
+    H->kernels_per_part[1][isub] = capture_one(H, isub, PART_MOMENTUM, &H->gpart[1][isub]);
   }
 }
 
@@ -2508,22 +2525,44 @@ int chs_time_steps_host_fields(chs_handle* H, int nsteps, int nfields, const int
       if (!bufs[f]) throw std::invalid_argument("null host buffer");
       dev[f] = field_ptr(H, ids[f], &cnt[f]);
     }
-    if (!H->gexec[1]) capture_graphs(H);
     // Copies in and out of every substep on two copy streams, one per PCIe direction, ordered
     // per field: the copy-in of a field for substep k+1 waits only for that field's copy-out of
     // substep k (it reads the host array that copy wrote), so copy-out and copy-in of different
-    // fields run at the same time; each substep's graph waits for all of its copies-in, and the
-    // copies-out wait for the graph.
+    // fields run at the same time.  With variable properties the substep runs as two graphs,
+    // energy then momentum: the energy graph waits only for the fields it reads (g and the
+    // thermal fields) while the rest are still coming in, and the fields final after it (rho*h,
+    // h, T, kappa, the energy rhs) go out while the momentum graph runs.  Every copy-out waits
+    // for the graph after which its field is final; rho and mu, which the momentum graph reads,
+    // go out after it.
+    const bool split = H->thermo;
+    if (split) {
+      if (!H->gpart[0][1]) capture_part_graphs(H);
+    } else if (!H->gexec[1]) {
+      capture_graphs(H);
+    }
+    auto energy_reads = [](int id) {
+      return id == CHS_GX || id == CHS_GY || id == CHS_GZ || id == CHS_RHOH || id == CHS_HENTH || id == CHS_TTEMP ||
+             id == CHS_KCOND || id == CHS_DDENS || id == CHS_MVISC || id == CHS_ENE_RHS0;
+    };
+    auto final_after_energy = [](int id) {
+      return id == CHS_RHOH || id == CHS_HENTH || id == CHS_TTEMP || id == CHS_KCOND || id == CHS_ENE_RHS0;
+    };
+    const int nph = split ? 2 : 1;
+    std::vector<int> in_ph(nfields), out_ph(nfields);
+    for (int f = 0; f < nfields; ++f) {
+      in_ph[f] = (split && !energy_reads(ids[f])) ? 1 : 0;
+      out_ph[f] = (split && !final_after_energy(ids[f])) ? 1 : 0;
+    }
     cudaStream_t sin = nullptr, sout = nullptr;
     CK(cudaStreamCreateWithFlags(&sin, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&sout, cudaStreamNonBlocking));
     std::vector<cudaEvent_t> out_done(nfields, nullptr);
-    cudaEvent_t a = nullptr, b = nullptr, in_done = nullptr, graph_done = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr, in_done[2] = {nullptr, nullptr}, graph_done[2] = {nullptr, nullptr};
     double* stage_out = nullptr;
     auto cleanup = [&] {
       for (auto& e : out_done)
         if (e) cudaEventDestroy(e);
-      for (cudaEvent_t e : {a, b, in_done, graph_done})
+      for (cudaEvent_t e : {a, b, in_done[0], in_done[1], graph_done[0], graph_done[1]})
         if (e) cudaEventDestroy(e);
       if (stage_out) cudaFree(stage_out);
       if (sin) cudaStreamDestroy(sin);
@@ -2531,8 +2570,10 @@ int chs_time_steps_host_fields(chs_handle* H, int nsteps, int nfields, const int
     };
     try {
       for (auto& e : out_done) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&in_done, cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&graph_done, cudaEventDisableTiming));
+      for (int p = 0; p < 2; ++p) {
+        CK(cudaEventCreateWithFlags(&in_done[p], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&graph_done[p], cudaEventDisableTiming));
+      }
       CK(cudaEventCreate(&a));
       CK(cudaEventCreate(&b));
       if (H->mixed) {
@@ -2545,25 +2586,35 @@ int chs_time_steps_host_fields(chs_handle* H, int nsteps, int nfields, const int
       bool first = true;
       for (int s = 0; s < nsteps; ++s)
         for (int isub = 1; isub <= 3; ++isub) {
-          for (int f = 0; f < nfields; ++f) {
-            if (!first) CK(cudaStreamWaitEvent(sin, out_done[f], 0));
-            h2d_field(H, dev[f], bufs[f], cnt[f], sin, H->stage);
+          for (int p = 0; p < nph; ++p) {
+            for (int f = 0; f < nfields; ++f) {
+              if (in_ph[f] != p) continue;
+              if (!first) CK(cudaStreamWaitEvent(sin, out_done[f], 0));
+              h2d_field(H, dev[f], bufs[f], cnt[f], sin, H->stage);
+            }
+            CK(cudaEventRecord(in_done[p], sin));
           }
           first = false;
-          CK(cudaEventRecord(in_done, sin));
-          CK(cudaStreamWaitEvent(H->st, in_done, 0));
-          CK(cudaGraphLaunch(H->gexec[isub], H->st));
-          H->launches += H->kernels_per_sub[isub];
-          CK(cudaEventRecord(graph_done, H->st));
-          CK(cudaStreamWaitEvent(sout, graph_done, 0));
-          for (int f = 0; f < nfields; ++f) {
-            d2h_field(H, bufs[f], dev[f], cnt[f], sout, stage_out);
-            CK(cudaEventRecord(out_done[f], sout));
+          for (int p = 0; p < nph; ++p) {
+            CK(cudaStreamWaitEvent(H->st, in_done[p], 0));
+            CK(cudaGraphLaunch(split ? H->gpart[p][isub] : H->gexec[isub], H->st));
+            H->launches += split ? H->kernels_per_part[p][isub] : H->kernels_per_sub[isub];
+            CK(cudaEventRecord(graph_done[p], H->st));
+          }
+          for (int p = 0; p < nph; ++p) {
+            CK(cudaStreamWaitEvent(sout, graph_done[p], 0));
+            // the fields the next substep copies in first go out first
+            for (int q = 0; q < nph; ++q)
+              for (int f = 0; f < nfields; ++f) {
+                if (out_ph[f] != p || in_ph[f] != q) continue;
+                d2h_field(H, bufs[f], dev[f], cnt[f], sout, stage_out);
+                CK(cudaEventRecord(out_done[f], sout));
+              }
           }
         }
       // the timed region ends when the last copy-out has landed
-      CK(cudaEventRecord(graph_done, sout));
-      CK(cudaStreamWaitEvent(H->st, graph_done, 0));
+      CK(cudaEventRecord(graph_done[0], sout));
+      CK(cudaStreamWaitEvent(H->st, graph_done[0], 0));
       CK(cudaEventRecord(b, H->st));
       CK(cudaEventSynchronize(b));
       CK(cudaEventElapsedTime(ms, a, b));
