@@ -1228,7 +1228,9 @@ void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* Zr, con
     ysolve_lines_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(data, nxh, ny, nz, Zr, D, pa);
     return;
   }
-  int lt = 32;
+  // 16 columns per CTA: a CTA's load, sweep and store phases run one after another, so several
+  // CTAs per SM are needed to keep loads in flight while others sweep
+  int lt = 16;
   while (lt > 4 && (size_t)ny * lt * 32 > 110 * 1024) lt /= 2;
   const size_t shm = (size_t)ny * lt * 32;
   if (shm > 200 * 1024) throw std::runtime_error("ysolve: ny too large for the shared-memory tile");
