@@ -808,10 +808,12 @@ __device__ __forceinline__ void stockham_bfly(const double2* in, double2* out, i
   for (int r = 0; r < R; ++r) out[idxd + r * ns] = v[r];
 }
 
-// FFT of `nl` lines of length n stored contiguously in buf0 (line stride n); result in buf0 or buf1
-// (returned).  All threads of the CTA take part.
-__device__ double2* smem_fft(double2* buf0, double2* buf1, int nl, const FftPlan& fp, int sign) {
+// FFT of `nl` lines of length n stored in buf0 with line stride ls (n, or n + 1 where the line
+// loads and stores run across lines: the padding moves consecutive lines to different banks);
+// result in buf0 or buf1 (returned).  All threads of the CTA take part.
+__device__ double2* smem_fft(double2* buf0, double2* buf1, int nl, const FftPlan& fp, int sign, int ls = 0) {
   const int n = fp.n;
+  if (ls == 0) ls = n;
   int ns = 1;
   double2* in = buf0;
   double2* out = buf1;
@@ -822,8 +824,8 @@ __device__ double2* smem_fft(double2* buf0, double2* buf1, int nl, const FftPlan
     for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
       const int line = fast_div(t, nb, inb), j = t - line * nb;
       const int jq = fast_div(j, ns, ins), k = j - jq * ns;
-      const double2* li = in + line * n;
-      double2* lo = out + line * n;
+      const double2* li = in + line * ls;
+      double2* lo = out + line * ls;
       if (R == 4) stockham_bfly<4>(li, lo, j, jq, k, nb, ns, tstep, fp.tw, sign);
       else if (R == 2) stockham_bfly<2>(li, lo, j, jq, k, nb, ns, tstep, fp.tw, sign);
       else stockham_bfly<3>(li, lo, j, jq, k, nb, ns, tstep, fp.tw, sign);
@@ -941,9 +943,9 @@ __global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __
                                  int64_t bstride, int64_t stride, int sign, int lpc) {
   extern __shared__ double2 sh[];
   __shared__ int64_t lbase[32];  // start of each of the CTA's lines (lpc <= 32), -1 past the end
-  const int n = fp.n;
+  const int n = fp.n, ls = n + 1;  // padded line stride: the loads and stores run across lines
   double2* b0 = sh;
-  double2* b1 = sh + (size_t)lpc * n;
+  double2* b1 = sh + (size_t)lpc * ls;
   const int64_t g0 = (int64_t)blockIdx.x * lpc;
   const int64_t nlines = (int64_t)na * nb;
   if (threadIdx.x < lpc) {
@@ -974,16 +976,16 @@ __global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __
       const int t = t0 + u * blockDim.x;
       if (t < lpc * n) {
         const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
-        b0[l * n + p] = v[u];
+        b0[l * ls + p] = v[u];
       }
     }
   }
   __syncthreads();
-  double2* r = smem_fft(b0, b1, lpc, fp, sign);
+  double2* r = smem_fft(b0, b1, lpc, fp, sign, ls);
   for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
     const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
     const int64_t base = lbase[l];
-    if (base >= 0) data[base + p * stride] = r[l * n + p];
+    if (base >= 0) data[base + p * stride] = r[l * ls + p];
   }
 }
 
@@ -1013,7 +1015,7 @@ void launch_cfft_axis(const FftPlan& fp, double2* data, int na, int nb, int64_t 
                       cudaStream_t st) {
   const int lpc = fft_lines_per_cta(fp.n);
   const int64_t nlines = (int64_t)na * nb;
-  const size_t shm = 2 * (size_t)lpc * fp.n * sizeof(double2);
+  const size_t shm = 2 * (size_t)lpc * (fp.n + 1) * sizeof(double2);
   cudaFuncSetAttribute(cfft_axis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
   cfft_axis_kernel<<<(unsigned)((nlines + lpc - 1) / lpc), 256, shm, st>>>(fp, data, na, nb, bstride, stride, sign,
                                                                             lpc);
