@@ -1295,8 +1295,9 @@ __global__ void __launch_bounds__(256) dct_y_kernel(const __grid_constant__ FftP
   __shared__ double lkx[32], lkz[32];
   __shared__ int64_t lfoff[32];  // start of the column's elimination factors in pfac, -1 past the end
   const int ny = fp.n, h = ny / 2;
+  const int ls = ny + 1;  // padded line stride: loads, stores and post-processing run across lines
   double2* b0 = sh;
-  double2* b1 = sh + (size_t)lpc * ny;
+  double2* b1 = sh + (size_t)lpc * ls;
   const int64_t g0 = (int64_t)blockIdx.x * lpc;
   const int64_t nlines = (int64_t)nxh * nz;
   if (threadIdx.x < lpc) {
@@ -1338,24 +1339,24 @@ __global__ void __launch_bounds__(256) dct_y_kernel(const __grid_constant__ FftP
       if (t < ntot) {
         const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
         const int q = (p & 1) ? ny - 1 - (p >> 1) : (p >> 1);
-        b0[l * ny + q] = v[u];
+        b0[l * ls + q] = v[u];
       }
     }
   }
   __syncthreads();
-  double2* r = smem_fft(b0, b1, lpc, fp, -1);
+  double2* r = smem_fft(b0, b1, lpc, fp, -1, ls);
   double2* o = (r == b0) ? b1 : b0;
   const double* ay = ayby;
   const double* by = ayby + ny;
   // forward post-processing into o, layout [j][l]
   for (int t = threadIdx.x; t < ntot; t += blockDim.x) {
     const int j = fast_div(t, lpc, ilpc), l = t - j * lpc;
-    const double2 c = r[l * ny + j];
+    const double2 c = r[l * ls + j];
     double2 v;
     if (j == 0) {
       v = make_double2(c.x * scale, c.y * scale);
     } else {
-      const double2 d = r[l * ny + (ny - j)];
+      const double2 d = r[l * ls + (ny - j)];
       const double t1 = c.x * scale, t2 = c.y * scale, t3 = d.x * scale, t4 = d.y * scale;
       const double yb = by[j], ya = ay[j];
       const double xx1 = t1 * yb, xx2 = t1 * ya, xx3 = t2 * yb, xx4 = t2 * ya;
@@ -1471,16 +1472,16 @@ __global__ void __launch_bounds__(256) dct_y_kernel(const __grid_constant__ FftP
       const double xx5 = t3 * yb, xx6 = t3 * ya, xx7 = t4 * yb, xx8 = t4 * ya;
       v = make_double2(xx1 - xx4 + xx6 + xx7, -(-xx2 - xx3 + xx5 - xx8));
     }
-    r[l * ny + j] = v;
+    r[l * ls + j] = v;
   }
   __syncthreads();
-  double2* w = smem_fft(r, o, lpc, fp, +1);
+  double2* w = smem_fft(r, o, lpc, fp, +1, ls);
   // store: row p of the column takes position q of the line (the inverse reordering)
   for (int t = threadIdx.x; t < ntot; t += blockDim.x) {
     const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
     const int64_t base = lbase[l];
     const int q = (p & 1) ? ny - 1 - (p >> 1) : (p >> 1);
-    if (base >= 0) data[base + (int64_t)p * nxh] = w[l * ny + q];
+    if (base >= 0) data[base + (int64_t)p * nxh] = w[l * ls + q];
   }
 }
 
@@ -1560,7 +1561,7 @@ void launch_dct_y(const FftPlan& fp, double2* data, int nxh, int nz, const doubl
   if (ny % 2 || ny < 8) throw std::runtime_error("dct_y: ny must be even and at least 8");
   const int lpc = fft_lines_per_cta(ny);
   const int64_t nlines = (int64_t)nxh * nz;
-  const size_t shm = 2 * (size_t)lpc * ny * sizeof(double2);
+  const size_t shm = 2 * (size_t)lpc * (ny + 1) * sizeof(double2);
   const unsigned grid = (unsigned)((nlines + lpc - 1) / lpc);
   if (ptab) {
     if (!pfac) throw std::runtime_error("dct_y: the pentadiagonal factors are missing");
