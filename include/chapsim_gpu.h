@@ -134,7 +134,11 @@ int chs_time_steps_host(chs_handle* h, int nsteps, double* qx, double* qy, doubl
  * copies the listed host arrays in, replays the substep graph (energy and
  * momentum for variable-property runs) and copies them back.  This is the
  * host-array drop-in of one time-loop substep (src/chapsim.f90:292-309) for a
- * caller that keeps those arrays on the host. */
+ * caller that keeps those arrays on the host.  The copies run on two internal
+ * streams, one per direction, ordered per field (a field's copy-in for the
+ * next substep follows its copy-out), so the host arrays must be page-locked
+ * (chs_host_alloc) for the directions to overlap and must not be touched by
+ * the caller until the call returns; all work is complete on return. */
 int chs_time_steps_host_fields(chs_handle* h, int nsteps, int nfields, const int* ids, double* const* bufs,
                                float* ms);
 
