@@ -1408,7 +1408,7 @@ __global__ void __launch_bounds__(256) dct_y_kernel(const __grid_constant__ FftP
     __syncthreads();
     const int tid = threadIdx.x;
     const int l = tid >> 1, s = tid & 1;
-    const bool act = tid < nt && lbase[l >= 0 && l < 32 ? l : 0] >= 0;
+    const bool act = tid < nt && lbase[l] >= 0;  // l < lpc <= 32 whenever tid < nt
     auto E = [&](int row) -> double2& { return o[(2 * row + s) * lpc + l]; };
     auto FS = [&](int row, int fld) { return fs[(row * 2 + fld) * nt + tid]; };
     double2 e0 = make_double2(0.0, 0.0), e1 = e0;
