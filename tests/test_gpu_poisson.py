@@ -51,3 +51,13 @@ def test_poisson_010(nc, acc, istret):
     assert np.abs(ref - got).max() / np.abs(ref).max() < 1e-11
     g.close()
 
+
+
+@pytest.mark.parametrize("nc,istret", [((16, 24, 12), C.ISTRET_BOTTOM), ((16, 24, 12), C.ISTRET_TOP),
+                                       ((16, 25, 12), C.ISTRET_2SIDES)])
+def test_poisson_010_rejects_unsupported_setups(nc, istret):
+    """chs_create refuses the 3D-FFT solver with y walls for istret 3 and 4 (whose reference matrices
+    are not built for poisson_010's odd/even solves) and for an odd number of y cells."""
+    cfg = C.channel(nc=nc, iacc=1, rstret=0.25, ifft=C.FFT_2DECOMP_3DFFT, istret=istret)
+    with pytest.raises(RuntimeError, match="chs_create"):
+        S.Solver(cfg)
