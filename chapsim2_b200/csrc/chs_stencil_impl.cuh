@@ -381,7 +381,7 @@ void launch_win(const OpPlan& P, const LineIOT<T>& io, const double* table, cuda
     // wide rows of x per warp group (contiguous DRAM segments), the rest of the CTA along y
     constexpr int V = Vec16<T>::n;
     const int nv = io.n1 / V;
-    const int bx = nv >= 128 ? 128 : (nv >= 64 ? 64 : 32), by = 256 / bx;
+    const int bx = nv >= 64 ? 64 : 32, by = 256 / bx;
     const int chunks = (P.nout + kWin - 1) / kWin;
     dim3 grid((unsigned)((nv + bx - 1) / bx), (unsigned)((chunks + by - 1) / by), (unsigned)io.n3);
     stencil_winy_kernel<T, FAM, M0, M1><<<grid, dim3(bx, by), 0, st>>>(P, io, table, nlines);
