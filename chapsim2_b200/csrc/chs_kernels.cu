@@ -1559,7 +1559,11 @@ void launch_dct_y(const FftPlan& fp, double2* data, int nxh, int nz, const doubl
                   cudaStream_t st) {
   const int ny = fp.n;
   if (ny % 2 || ny < 8) throw std::runtime_error("dct_y: ny must be even and at least 8");
-  const int lpc = fft_lines_per_cta(ny);
+  // tall columns: half the FFT kernels' lines per CTA.  The serial sweeps of a CTA leave most
+  // of its warps waiting, and smaller CTAs keep more sweeps in flight per SM (384x256x384:
+  // 1.06 -> 0.99 ms; at 96 rows the halving is slower, 44 -> 53 us)
+  int lpc = fft_lines_per_cta(ny);
+  if (ny >= 192 && lpc > 1) lpc /= 2;
   const int64_t nlines = (int64_t)nxh * nz;
   const size_t shm = 2 * (size_t)lpc * (ny + 1) * sizeof(double2);
   const unsigned grid = (unsigned)((nlines + lpc - 1) / lpc);
