@@ -6,11 +6,13 @@
 // modified wavenumbers of the periodic C2P derivative of the chosen scheme
 // (src/poisson_1stderivcomp.f90:2448-2503), and the inverse transforms.  The same kernels
 // run; only the spectrum and the tables live in `g_static_work` instead of handle memory.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <memory>
 #include <mutex>
 
 #include "../../include/chapsim_gpu.h"
@@ -29,23 +31,58 @@ constexpr int kMaxLen = 4096;
 constexpr size_t kTabTw = 3 * (size_t)kMaxLen;
 constexpr size_t kTabK2 = 3 * (size_t)kMaxLen / 2;
 constexpr size_t kWorkLen = kSpecMax + kTabTw + kTabK2;
+// 16 MiB of spectrum + 192 KiB of twiddles + 96 KiB of squared wavenumbers = 16 MiB + 288 KiB
+static_assert(kWorkLen * sizeof(double2) == (size_t(16) << 20) + (size_t(288) << 10), "work array size");
 
 __device__ __align__(256) double2 g_static_work[kWorkLen];
 
-// Tables currently held by g_static_work, per device (the module-level array exists once per
-// device context).  Guarded by g_mu.
+// Tables currently held by g_static_work, per device.  The array lives in the device context, so
+// the key also records the context's unique id: after cudaDeviceReset (or any new primary context)
+// the array comes back zeroed and the id differs, which forces the set-up to run again.
 struct Key {
   bool valid;
+  unsigned long long ctx_id;
   int nc[3];
   double len[3];
   int iacc;
 };
+// host staging of one device's tables (the set-up waits for the copies before it reuses them)
+struct Staging {
+  double2 tw[3][kMaxLen];
+  double k2[3][kMaxLen];
+};
 constexpr int kMaxDevices = 64;
 Key g_key[kMaxDevices];
-std::mutex g_mu;
-// host staging of the tables (fixed size; filled under g_mu)
-double2 g_tw_host[3][kMaxLen];
-double g_k2_host[3][kMaxLen];
+std::unique_ptr<Staging> g_stage[kMaxDevices];
+// one lock per device: a set-up that waits for its stream blocks only callers of the same device
+std::mutex g_mu[kMaxDevices];
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique id of the calling thread's current context, through the runtime's driver entry points
+// (the library does not link the driver library directly).
+cudaError_t current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  if (!get_current || !get_id) return cudaErrorNotSupported;
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return cudaErrorDeviceUninitialized;
+  if (get_id(ctx, id) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+  return cudaSuccess;
+}
 
 int fail(char* err, size_t errlen, int code, const char* fmt, ...) {
   if (err && errlen) {
@@ -129,29 +166,35 @@ extern "C" int chs_poisson_periodic_static(double* d_rhs, const int nc[3], const
   const double* k2y = k2 + kMaxLen;
   const double* k2z = k2 + 2 * kMaxLen;
 
+  unsigned long long ctx_id = 0;
+  e = current_context_id(&ctx_id);
+  if (e != cudaSuccess) return fail(err, errlen, CHS_ERR_CUDA, "context id: %s", cudaGetErrorString(e));
   {
-    // set-up: (re)write the tables when this device holds tables of another grid
-    std::lock_guard<std::mutex> lock(g_mu);
+    // set-up: (re)write the tables when this device's context holds tables of another grid, or
+    // none (a new context starts with a zeroed array)
+    std::lock_guard<std::mutex> lock(g_mu[dev]);
     Key& k = g_key[dev];
-    const bool same = k.valid && k.iacc == iacc && k.nc[0] == nc[0] && k.nc[1] == nc[1] && k.nc[2] == nc[2] &&
-                      k.len[0] == len[0] && k.len[1] == len[1] && k.len[2] == len[2];
+    const bool same = k.valid && k.ctx_id == ctx_id && k.iacc == iacc && k.nc[0] == nc[0] && k.nc[1] == nc[1] &&
+                      k.nc[2] == nc[2] && k.len[0] == len[0] && k.len[1] == len[1] && k.len[2] == len[2];
     if (!same) {
       k.valid = false;
+      if (!g_stage[dev]) g_stage[dev] = std::make_unique<Staging>();
+      Staging& sg = *g_stage[dev];
       const FftPlan* fp[3] = {&fx, &fy, &fz};
       for (int d = 0; d < 3; ++d) {
-        twiddles(nc[d], g_tw_host[d]);
-        mod_k2(nc[d], len[d], len[d] / nc[d], iacc, g_k2_host[d]);
-        e = cudaMemcpyAsync(const_cast<double2*>(fp[d]->tw), g_tw_host[d], nc[d] * sizeof(double2),
+        twiddles(nc[d], sg.tw[d]);
+        mod_k2(nc[d], len[d], len[d] / nc[d], iacc, sg.k2[d]);
+        e = cudaMemcpyAsync(const_cast<double2*>(fp[d]->tw), sg.tw[d], nc[d] * sizeof(double2),
                             cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess)
-          e = cudaMemcpyAsync(k2 + (size_t)d * kMaxLen, g_k2_host[d], nc[d] * sizeof(double), cudaMemcpyHostToDevice,
-                              st);
+          e = cudaMemcpyAsync(k2 + (size_t)d * kMaxLen, sg.k2[d], nc[d] * sizeof(double), cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return fail(err, errlen, CHS_ERR_CUDA, "table upload: %s", cudaGetErrorString(e));
       }
-      // the host staging arrays are reused by the next set-up
+      // the staging arrays are reused by this device's next set-up
       e = cudaStreamSynchronize(st);
       if (e != cudaSuccess) return fail(err, errlen, CHS_ERR_CUDA, "table upload: %s", cudaGetErrorString(e));
       k.valid = true;
+      k.ctx_id = ctx_id;
       k.iacc = iacc;
       for (int d = 0; d < 3; ++d) {
         k.nc[d] = nc[d];
