@@ -211,7 +211,7 @@ def run_reference(args, cfg, fields, tc, world, rank, dist):
 def roofline(prof, peak, peak_kind, workload):
     by = {}
     for r in prof:
-        k = ("line_op", "fft", "ysolve", "elementwise")[r["kind"]]
+        k = ("line_op", "fft", "ysolve", "elementwise", "fused_momentum")[r["kind"]]
         a = by.setdefault(k, {"ms": 0.0, "bytes": 0.0, "n": 0})
         a["ms"] += r["ms"]
         a["bytes"] += r["bytes"]

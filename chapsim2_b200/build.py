@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libchapsim_gpu.so")
 SOURCES = ["chs_plan.cpp", "chs_kernels.cu", "chs_stencil_f64.cu", "chs_stencil_f32.cu", "chs_solver.cu",
-           "chs_static.cu", "chs_mlp.cu"]
+           "chs_static.cu", "chs_mlp.cu", "chs_fused.cu"]
 OBJDIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "../../include/chapsim_gpu.h"
+#include "chs_fused.cuh"
 #include "chs_kernels.cuh"
 #include "chs_mlp.cuh"
 #include "chs_plan.h"
@@ -122,6 +123,11 @@ struct chs_handle {
   std::vector<std::pair<void*, size_t>> allocs;
   int tune_block = 0, tune_lt = 0;  // launch shapes picked by chs_autotune (0 = defaults)
   int tune_fuse = 0;                // 1: fused operator sums (chs_autotune decides; off by default)
+  // fused substep kernels for the explicit schemes (chs_fused.cu): 1 on by default, 0 the
+  // operator-by-operator path (chs_set_fusion)
+  int kfuse = 1;
+  OpPlan* fz_plans = nullptr;                                    // device copies of every plan
+  std::map<std::tuple<int, int, int, int, int>, int> fz_index;  // plan key -> slot in fz_plans
   long long launches = 0;
   std::string err;
 
@@ -1084,6 +1090,24 @@ void upload_table(chs_handle* H) {
                      H->st));
 }
 
+// every plan built so far as one device array, so the fused kernels can read the boundary rows
+// of any plan they use (slot per plan key in fz_index)
+void upload_fz_plans(chs_handle* H) {
+  drop_graphs(H);
+  std::vector<OpPlan> v;
+  H->fz_index.clear();
+  for (const auto& kv : H->plans) {
+    H->fz_index[kv.first] = (int)v.size();
+    v.push_back(kv.second);
+  }
+  if (H->fz_plans) { CK(cudaFreeAsync(H->fz_plans, H->st)); H->fz_plans = nullptr; }
+  if (v.empty()) return;
+  CK(cudaMallocAsync(&H->fz_plans, v.size() * sizeof(OpPlan), H->st));
+  CK(cudaMemcpyAsync(H->fz_plans, v.data(), v.size() * sizeof(OpPlan), cudaMemcpyHostToDevice, H->st));
+  // the host vector goes out of scope: wait for the copy
+  CK(cudaStreamSynchronize(H->st));
+}
+
 template <typename T>
 void poisson_device(chs_handle* H, T* rhs) {
   const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
@@ -1122,6 +1146,187 @@ void poisson_device(chs_handle* H, T* rhs) {
 }
 
 // the substep body (enqueued on H->st; capturable); T is the field type
+// ---- fused momentum path for the explicit schemes (chs_fused.cu)
+// The descriptor names, for every inner and outer operator of the momentum equation, the same plan
+// the operator path below launches (direction, family, boundary pair, whether boundary planes are
+// given); a plan that is not an explicit one, or an x/z plan that is not periodic with the bulk
+// formula everywhere, sends the substep down the operator path.
+struct FzBuild {
+  chs_handle* H;
+  bool ok = true;
+  FzOp op(int d, int fam, Pair bc, bool has_fbc) {
+    FzOp o{};
+    auto key = std::make_tuple(d, fam, bc.v[0], bc.v[1], has_fbc ? 1 : 0);
+    auto it = H->plans.find(key);
+    auto ix = H->fz_index.find(key);
+    if (it == H->plans.end() || ix == H->fz_index.end()) { ok = false; return o; }
+    const OpPlan& P = it->second;
+    // CD2 only: every bulk formula two-point; x and z periodic (bulk formula everywhere); y plans
+    // with walls: bulk range covering rows 2 .. nout-3, so that the rows kFzEdge .. n-1-kFzEdge of
+    // every fused output use the bulk formula at every level
+    if (P.tdma || P.r2 != 0.0 || (d != 1 && !P.wrap) || (d == 1 && H->periodic_y != (P.wrap != 0))) ok = false;
+    if (d == 1 && !P.wrap && (P.b_lo > 2 || P.b_hi < P.nout - 3)) ok = false;
+    o.kind = P.wrap ? 0 : 1;
+    o.b_lo = P.b_lo;
+    o.b_hi = P.b_hi;
+    o.lmap = (int)P.lmap;
+    o.neu = (P.neu1 ? 1 : 0) | (P.neu2 ? 2 : 0);
+    o.nout = P.nout;
+    o.plan = ix->second;
+    o.r1 = P.r1;
+    o.r2 = P.r2;
+    o.dd = P.dd;
+    return o;
+  }
+  // pair_terms' rule: one operator on the combined expression when both terms share the plan
+  template <typename T>
+  FzPair<T> pair(int d, int fam, Pair bc1, const T* f1, Pair bc2, const T* f2, const T* fcomb) {
+    FzPair<T> p{};
+    const bool same = bc1.v[0] == bc2.v[0] && bc1.v[1] == bc2.v[1] && ((f1 == nullptr) == (f2 == nullptr)) &&
+                      (f1 == f2 || fcomb != nullptr);
+    if (same) {
+      const T* f = (f1 == f2) ? f1 : fcomb;
+      p.a = op(d, fam, bc1, f != nullptr);
+      p.fa = f;
+      p.merged = 1;
+    } else {
+      p.a = op(d, fam, bc1, f1 != nullptr);
+      p.fa = f1;
+      p.b = op(d, fam, bc2, f2 != nullptr);
+      p.fb = f2;
+      p.merged = 0;
+    }
+    return p;
+  }
+};
+
+// Momentum right-hand sides, fractional step, mass-flux mean and advance of the substep in four
+// launches (wall planes, fused momentum, mean, advance) instead of the ~50 of the operator path.
+// Returns false (nothing launched) when the configuration needs the operator path.
+template <typename T>
+bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz) {
+  if (!H->kfuse || H->iacc != ACC_CD2 || !H->fz_plans) return false;
+  auto A = [](double* p) { return reinterpret_cast<T*>(p); };
+  const auto& B = H->ibc;
+  const bool TH = H->thermo;
+  const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2], np1 = H->np[1];
+  const T* any = A(H->fb_maxp);
+  const T* fyqx = H->periodic_y ? nullptr : A(H->fb_qx);
+  const T* fyqy = H->periodic_y ? nullptr : A(H->fb_qy);
+  const T* fyqz = H->periodic_y ? nullptr : A(H->fb_qz);
+  const T* fympr = H->periodic_y ? nullptr : A(H->fb_mpr);
+  const T* fz = TH ? A(H->fb_zero) : nullptr;
+  const Pair bx_qx = P2(B[0][V_QX]), by_qx = P2(B[1][V_QX]), bz_qx = P2(B[2][V_QX]);
+  const Pair bx_qy = P2(B[0][V_QY]), by_qy = P2(B[1][V_QY]), bz_qy = P2(B[2][V_QY]);
+  const Pair bx_qz = P2(B[0][V_QZ]), by_qz = P2(B[1][V_QZ]), bz_qz = P2(B[2][V_QZ]);
+  const Pair bx_pr = P2(B[0][V_PR]), by_pr = P2(B[1][V_PR]), bz_pr = P2(B[2][V_PR]);
+  const Pair per = P2(kPer2);
+  FzBuild b{H};
+  FzMomentum<T> F{};
+  F.n0 = nc0; F.nc1 = nc1; F.np1 = np1; F.n2 = nc2;
+  F.thermo = TH ? 1 : 0;
+  F.periodic_y = H->periodic_y ? 1 : 0;
+  if (TH && H->periodic_y) return false;
+  F.qx = A(H->qx); F.qy = A(H->qy); F.qz = A(H->qz); F.p = A(H->pres);
+  if (TH) { F.gx = A(H->gx); F.gy = A(H->gy); F.gz = A(H->gz); F.mu = A(H->mVisc); F.fm = A(H->fb_m); }
+  F.fyqx = fyqx; F.fyqy = fyqy; F.fyqz = fyqz; F.fz = fz;
+  // inner operators: the derived quantities of the operator path (same plan keys)
+  F.in[FI_QX_MX] = b.op(0, M1P2C, bx_qx, true);
+  F.in[FI_QX_DX] = b.op(0, D1P2C, bx_qx, true);
+  F.in[FI_QX_DY] = b.op(1, D1C2P, by_qx, fyqx != nullptr);
+  F.in[FI_QX_MY] = b.op(1, M1C2P, by_qx, fyqx != nullptr);
+  F.in[FI_QX_MZ] = b.op(2, M1C2P, bz_qx, true);
+  F.in[FI_QX_DZ] = b.op(2, D1C2P, bz_qx, true);
+  F.in[FI_QY_DX] = b.op(0, D1C2P, bx_qy, true);
+  F.in[FI_QY_MX] = b.op(0, M1C2P, bx_qy, true);
+  F.in[FI_QY_DY] = b.op(1, D1P2C, by_qy, false);
+  F.in[FI_QY_MY] = b.op(1, M1P2C, by_qy, fyqy != nullptr);
+  F.in[FI_QY_DZ] = b.op(2, D1C2P, bz_qy, true);
+  F.in[FI_QY_MZ] = b.op(2, M1C2P, bz_qy, true);
+  F.in[FI_QZ_DX] = b.op(0, D1C2P, bx_qz, true);
+  F.in[FI_QZ_MX] = b.op(0, M1C2P, bx_qz, true);
+  F.in[FI_QZ_MY] = b.op(1, M1C2P, by_qz, fyqz != nullptr);
+  F.in[FI_QZ_DY] = b.op(1, D1C2P, by_qz, fyqz != nullptr);
+  F.in[FI_QZ_MZ] = b.op(2, M1P2C, bz_qz, true);
+  F.in[FI_QZ_DZ] = b.op(2, D1P2C, bz_qz, false);
+  if (TH) {
+    F.in[FI_GX_MX] = b.op(0, M1P2C, bx_qx, true);
+    F.in[FI_GX_MY] = b.op(1, M1C2P, by_qx, true);
+    F.in[FI_GX_MZ] = b.op(2, M1C2P, bz_qx, true);
+    F.in[FI_GY_MX] = b.op(0, M1C2P, bx_qy, true);
+    F.in[FI_GY_MY] = b.op(1, M1P2C, by_qy, true);
+    F.in[FI_GY_MZ] = b.op(2, M1C2P, bz_qy, true);
+    F.in[FI_GZ_MX] = b.op(0, M1C2P, bx_qz, true);
+    F.in[FI_GZ_MY] = b.op(1, M1C2P, by_qz, true);
+    F.in[FI_GZ_MZ] = b.op(2, M1P2C, bz_qz, true);
+    F.in[FI_MU_Y] = b.op(1, M1C2P, H->ftpy, true);
+    F.in[FI_MU_YX] = b.op(0, M1C2P, per, true);
+    F.in[FI_MU_X] = b.op(0, M1C2P, per, true);
+    F.in[FI_MU_XZ] = b.op(2, M1C2P, per, false);
+    F.in[FI_MU_YZ] = b.op(2, M1C2P, per, false);
+  }
+  if (H->fbcy_velo) {
+    F.in[FI_W_DX] = b.op(0, D1P2C, bx_qx, false);
+    F.in[FI_W_DY] = b.op(1, D1C2P, by_qy, fyqy != nullptr);
+    F.in[FI_W_DZ] = b.op(2, D1P2C, bz_qz, false);
+  }
+  // outer operators of the three components, as the operator path pairs them
+  const T* fconv2 = H->fbcy_velo ? A(H->fb_conv2) : A(H->fb_maxp);
+  const T* fvisc2 = H->fbcy_velo ? A(H->fb_visc2) : A(H->fb_maxp);
+  F.term[0][0] = b.pair<T>(0, D1C2P, H->mbcx_cov1, any, H->mbcx_tau1, any, (const T*)nullptr);
+  F.term[0][1] = b.pair<T>(1, D1P2C, H->mbcy_cov1, (const T*)nullptr, H->mbcy_tau1, (const T*)nullptr, (const T*)nullptr);
+  F.term[0][2] = b.pair<T>(2, D1P2C, H->mbcz_cov1, (const T*)nullptr, H->mbcz_tau1, (const T*)nullptr, (const T*)nullptr);
+  F.term[1][0] = b.pair<T>(0, D1P2C, H->mbcx_cov2, (const T*)nullptr, H->mbcx_tau2, (const T*)nullptr, (const T*)nullptr);
+  F.term[1][1] = b.pair<T>(1, D1C2P, H->mbcy_cov2, fconv2, H->mbcy_tau2, fvisc2, (const T*)A(H->fb_comb));
+  F.term[1][2] = b.pair<T>(2, D1P2C, H->mbcz_cov2, (const T*)nullptr, H->mbcz_tau2, (const T*)nullptr, (const T*)nullptr);
+  F.term[2][0] = b.pair<T>(0, D1P2C, H->mbcx_cov3, (const T*)nullptr, H->mbcx_tau3, (const T*)nullptr, (const T*)nullptr);
+  F.term[2][1] = b.pair<T>(1, D1P2C, H->mbcy_cov3, (const T*)nullptr, H->mbcy_tau3, (const T*)nullptr, (const T*)nullptr);
+  F.term[2][2] = b.pair<T>(2, D1C2P, H->mbcz_cov3, any, H->mbcz_tau3, any, (const T*)nullptr);
+  F.pres[0] = b.op(0, D1C2P, bx_pr, true);
+  F.pres[1] = b.op(1, D1C2P, by_pr, fympr != nullptr);
+  F.pres[2] = b.op(2, D1C2P, bz_pr, true);
+  F.fpres[0] = any; F.fpres[1] = fympr; F.fpres[2] = any;
+  if (!b.ok) return false;
+  F.m[0] = A(H->mx); F.m[1] = A(H->my); F.m[2] = A(H->mz);
+  F.m0[0] = A(H->mx0); F.m0[1] = A(H->my0); F.m0[2] = A(H->mz0);
+  F.rre = H->rre;
+  F.dt = H->dt; F.gam = H->tGamma[isub]; F.zeta = H->tZeta[isub]; F.alpha = H->tAlpha[isub];
+  F.plans = H->fz_plans;
+  F.table = H->table;
+  const double nf = (double)sizeof(T) * H->n_ccc;
+  if (H->fbcy_velo) {
+    PROFD(H, 3, (double)sizeof(T) * 16.0 * nc0 * nc2,
+          bufs(H->qx, H->qy, H->qz, H->fb_qy, H->fb_conv2, TH ? H->mVisc : nullptr, TH ? H->fb_m : nullptr),
+          bufs(H->fb_visc2, H->fb_comb), launch_fz_wall_visc<T>(F, A(H->fb_visc2), A(H->fb_comb), fconv2, st));
+    H->launches++;
+  }
+  // per component: rhs0 read and written, rhs written, and a third of the shared inputs q (3), p
+  // [+ g (3), mu] (the three components together read each input once); the three run concurrently
+  // on the dataflow lanes
+  double* mo[3] = {H->mx, H->my, H->mz};
+  double* m0[3] = {H->mx0, H->my0, H->mz0};
+  for (int c = 0; c < 3; ++c) {
+    PROFD(H, 4, nf * ((TH ? 8.0 : 4.0) / 3.0 + 3.0),
+          bufs(H->qx, H->qy, H->qz, H->pres, TH ? H->gx : nullptr, TH ? H->gy : nullptr, TH ? H->gz : nullptr,
+               TH ? H->mVisc : nullptr, H->fb_comb, H->fb_visc2, H->fb_qx, H->fb_qz),
+          bufs(mo[c], m0[c]), launch_fz_momentum<T>(F, c, st));
+    H->launches++;
+  }
+  const double* bulk = nullptr;
+  if (H->idriven == 1) {
+    PROFD(H, 3, 8.0 / 8.0 * sizeof(T) * H->n_pcc, bufs(H->mx, H->wy), bufs(H->partial, H->scal),
+         launch_weighted_mean(A(H->mx), H->wy, nc0, nc1, nc2, H->partial, H->npart, H->scal + 0, H->vol, st));
+    bulk = H->scal + 0;
+    H->launches += 2;
+  }
+  const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
+  PROFD(H, 3, nf * 9.0, bufs(H->mx, H->my, H->mz, bulk), bufs(ux, uy, uz),
+        launch_fz_update<T>(A(ux), A(uy), A(uz), A(H->mx), A(H->my), A(H->mz), bulk, nc0, nc1, np1, nc2, w0,
+                            H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+  H->launches++;
+  return true;
+}
+
 template <typename T>
 void energy_body_t(chs_handle* H, int isub);
 template <typename T>
@@ -1152,6 +1357,8 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
   double* uy = TH ? H->gy : H->qy;
   double* uz = TH ? H->gz : H->qz;
 
+  const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
+  if (!fused_momentum<T>(H, isub, ux, uy, uz)) {
   // ---- 1. derived quantities (src/eq_momentum2.f90:347-508)
   run_op(H, 0, M1P2C, bx_qx, any, src(A(H->qx)), s_pcc, A(H->qxix), false, 1.0);
   run_op(H, 0, D1P2C, bx_qx, any, src(A(H->qx)), s_pcc, A(H->qxdx), false, 1.0);
@@ -1301,12 +1508,12 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
     H->launches++;
   }
   H->launches += 1;
-  const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
   if (w0 || w1) {
     PROFD(H, 3, 16.0 / 8.0 * sizeof(T) * nc0 * nc2, bufs(), bufs(uy),
           launch_set_yrows(A(uy), nc0, np1, nc2, w0, H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
     H->launches++;
   }
+  }  // operator path
   // ---- 5. Poisson RHS, solve, pressure and projection.  For variable properties the reference
   // adds (rho - rho_m1)/dt (Calculate_drhodt, src/eq_continuity.f90:26-78), but
   // Update_thermal_properties has already set rho_m1 = rho, so the term is zero and left out.
@@ -1442,6 +1649,7 @@ void prepare_plans(chs_handle* H) {
   }
   for (const auto& x : r) H->plan(x.d, x.fam, x.bc, x.f);
   upload_table(H);
+  upload_fz_plans(H);
 }
 
 // operator plans of the variable-property path (energy equation, g and mu interpolations,
@@ -1464,6 +1672,7 @@ void prepare_thermo_plans(chs_handle* H) {
   };
   for (const auto& x : r) H->plan(x.d, x.fam, x.bc, x.f);
   upload_table(H);
+  upload_fz_plans(H);
 }
 
 // host-side lookup of the initial state from T (ftp_refresh_thermal_properties_from_T_undim,
@@ -2165,6 +2374,14 @@ int chs_set_launch_shape(chs_handle* H, int block, int lt_max, int fused) {
   });
 }
 
+int chs_set_fusion(chs_handle* H, int on) {
+  if (!H || on < 0 || on > 1) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    H->kfuse = on;
+    drop_graphs(H);
+  });
+}
+
 int chs_set_lanes(chs_handle* H, int lanes) {
   if (!H || lanes < 1 || lanes > chs_handle::kLanes) return CHS_ERR_ARG;
   return guard(H, [&] {
@@ -2273,6 +2490,7 @@ int chs_destroy(chs_handle* H) {
   if (H->st) cudaStreamSynchronize(H->st);
   drop_graphs(H);
   if (H->table) cudaFree(H->table);
+  if (H->fz_plans) cudaFree(H->fz_plans);
   for (auto& a : H->allocs) cudaFree(a.first);
   for (int l = 1; l < chs_handle::kLanes; ++l)
     if (H->lane[l]) cudaStreamDestroy(H->lane[l]);

@@ -71,7 +71,7 @@ EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field
             "chs_ensemble_kernel_launches", "chs_ensemble_destroy", "chs_autotune", "chs_set_launch_shape",
             "chs_set_lanes", "chs_profile_substep_graph", "chs_write_restart", "chs_read_restart",
             "chs_stats_update", "chs_stats_get", "chs_write_statistics", "chs_read_statistics",
-            "chs_data_file_name"]
+            "chs_data_file_name", "chs_set_fusion"]
 
 
 class ChsKprof(ctypes.Structure):
@@ -127,6 +127,7 @@ def load():
     L.chs_mlp_norm.argtypes = [ctypes.c_void_p, _D]
     L.chs_set_launch_shape.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.chs_set_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.chs_set_fusion.argtypes = [ctypes.c_void_p, ctypes.c_int]
     for fn in ("chs_write_restart", "chs_read_restart", "chs_write_statistics", "chs_read_statistics"):
         getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
     L.chs_stats_update.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -306,6 +307,10 @@ class Solver:
     def set_lanes(self, lanes):
         """Streams a captured substep spreads its independent launches over (1..8)."""
         self._check(self.L.chs_set_lanes(self.h, int(lanes)), "chs_set_lanes")
+
+    def set_fusion(self, on):
+        """Fused substep kernels for the explicit schemes (True, the default) or the operator path."""
+        self._check(self.L.chs_set_fusion(self.h, 1 if on else 0), "chs_set_fusion")
 
     # ---- MLP surrogate of the property update
     def mlp_train(self, nsamples=1000000, batch=4096, epochs=20, lr=2e-3, seed=20250101):

@@ -147,7 +147,8 @@ void* chs_host_alloc(size_t bytes);
 void chs_host_free(void* p);
 
 /* Per-kernel profile of one substep (not graph-replayed): for each launch, its
- * class (0 line op, 1 FFT, 2 y solve, 3 elementwise/reduction), direction
+ * class (0 line op, 1 FFT, 2 y solve, 3 elementwise/reduction, 4 fused CD2
+ * momentum component), direction
  * (-1 if none), algorithmic bytes moved and CUDA-event duration. */
 typedef struct chs_kprof {
   int kind;
@@ -258,6 +259,15 @@ int chs_set_launch_shape(chs_handle* h, int block, int lt_max, int fused);
  * stream.  Results are identical for every setting (no counterpart in the
  * reference, which runs the operators one after another). */
 int chs_set_lanes(chs_handle* h, int lanes);
+/* Fused substep kernels for the explicit schemes (CD2, CD4): on = 1 (the
+ * default) forms the momentum right-hand sides of all three components with
+ * the fractional step in one pass that evaluates every interpolation and
+ * derivative where it is needed (the same plans, boundary rows and arithmetic
+ * as the operator path of Compute_momentum_rhs, src/eq_momentum2.f90:101-1571,
+ * without writing them to device memory); on = 0 runs one operator per
+ * derived quantity.  Compact schemes (CP4, CP6) always take the operator
+ * path.  No counterpart in the reference, which has only the operator path. */
+int chs_set_fusion(chs_handle* h, int on);
 
 /*
  * Restart files and running statistics.  Files follow the reference's naming
@@ -331,14 +341,17 @@ int chs_last_error(const chs_handle* h, char* buf, size_t len);
  * of the same grid and scheme.  Kernels run on `stream` (a cudaStream_t; NULL
  * is the legacy default stream).
  *
- * Work memory is a fixed module-level device array of 16 MiB + 144 KiB, so the
+ * Work memory is a fixed module-level device array of 16 MiB + 288 KiB (spectrum
+ * 16 MiB, twiddles 192 KiB, squared wavenumbers 96 KiB), so the
  * limits are (nc[0]/2+1)*nc[1]*nc[2] <= 1048576 complex values and each nc[d]
  * <= 4096, each of the form 2^a 3^b; larger grids return CHS_ERR_ARG with a
  * message.  Nothing in it needs to start at zero: every value is written before
  * it is read.  The first call on a device, and any call whose nc, len or iacc
  * differ from the previous call's, does set-up: it writes the FFT and
  * wavenumber tables with a host-to-device copy on `stream` and synchronizes
- * that stream, so make such a call before any stream capture.  All calls on one
+ * that stream, so make such a call before any stream capture.  The tables are
+ * tied to the device context: after cudaDeviceReset the next call sets up
+ * again.  A set-up holds a per-device lock only.  All calls on one
  * device share the one work array: calls that overlap in time (on different
  * streams, or from threads that do not order them) race and corrupt each other;
  * order them on one stream.  Errors are written to err (errlen bytes, may be
