@@ -1,7 +1,7 @@
-// Fused momentum right-hand side for the explicit schemes (see chs_fused.cuh).
+// Fused CD2 substep kernels (see chs_fused.cuh).
 //
-// Compute_momentum_rhs (src/eq_momentum2.f90:101-1571, Cartesian branches) with the fractional
-// step Calculate_momentum_fractional_step (:35-71), per output value:
+// Momentum: Compute_momentum_rhs (src/eq_momentum2.f90:101-1571, Cartesian branches) with the
+// fractional step Calculate_momentum_fractional_step (:35-71), per output value:
 //   x: d/dx[-u u + 2 mu/Re (du/dx - div/3)] + d/dy[-v u + mu/Re (du/dy + dv/dx)]
 //      + d/dz[-w u + mu/Re (du/dz + dw/dx)] - dp/dx            (:796-966)
 //   y: d/dx[-u v + mu/Re (du/dy + dv/dx)] + d/dy[-v v + 2 mu/Re (dv/dy - div/3)]
@@ -9,109 +9,120 @@
 //   z: d/dx[-u w + mu/Re (du/dz + dw/dx)] + d/dy[-v w + mu/Re (dv/dz + dw/dy)]
 //      + d/dz[-w w + 2 mu/Re (dw/dz - div/3)] - dp/dz          (:1262-1457)
 // with the first velocity factor of each convective product replaced by the interpolated momentum
-// g and the viscosity interpolated to the stress points for variable properties (:576-703).  Every
-// interpolation and derivative is the plan the operator path launches (same coefficients, same
-// boundary rows, same arithmetic order), evaluated in registers where the sum needs it.
+// g and the viscosity interpolated to the stress points for variable properties (:576-703).
+// Energy: Compute_energy_rhs and Calculate_energy_fractional_step (src/eq_energy.f90:148-401).
+// Projection: Correct_massflux (src/eq_momentum2.f90:1577-1660) and convert_primary_conservative
+// (src/para_conversion.f90:5-227).
 #include <cuda_runtime.h>
 
 #include <stdexcept>
 
 #include "chs_fused.cuh"
-#include "chs_stencil_dev.cuh"
 
 namespace chs {
 
 namespace {
 
-// CD2 bulk formula of family FAM at row p (bulk_fn with r2 = 0)
-template <int FAM, typename T, typename F>
-__device__ __forceinline__ T fz_bulk(const F& f, int p, T r1) {
-  if (FAM == M1P2C) return r1 * (f(p) + f(p + 1));
-  if (FAM == M1C2P) return r1 * (f(p) + f(p - 1));
-  if (FAM == D1C2P) return r1 * (f(p) - f(p - 1));
-  return r1 * (f(p + 1) - f(p));  // D1P2C
-}
-
-// periodic line: every row the bulk formula with wrapped indices (the plan's wrap flag)
-template <int FAM, typename T, typename F>
-__device__ __forceinline__ T fz_per(const FzOp& o, int p, int nin, const F& f) {
-  auto w = [&](int q) -> T { return f(q < 0 ? q + nin : (q >= nin ? q - nin : q)); };
-  return fz_bulk<FAM, T>(w, p, T(o.r1)) * T(o.dd);
-}
-
-// the plan's boundary row p over the input f and the boundary planes (out of line: boundary rows are
-// a few wall rows, and inlining them into every composed expression multiplies the code)
-template <typename T, typename F>
-__device__ __forceinline__ T fz_special(const OpPlan* __restrict__ P, int p, const T* __restrict__ fbc, int nl, int L,
-                                     F f) {
-  T v = T(0);
-  const int ns = P->nspec;
-  for (int s = 0; s < ns; ++s) {
-    if (P->sp[s].row != p) continue;
-    const SpecialRow& R = P->sp[s];
-    T acc = T(0);
-    const int nt = R.nt;
-    for (int t = 0; t < nt; ++t) acc += T(R.w[t]) * f(R.idx[t]);
-    for (int u = 0; u < 4; ++u)
-      if (R.wb[u] != 0.0) acc += T(R.wb[u]) * fbc[u * nl + L];
-    v = acc * T(P->dd);
-  }
-  return v;
-}
-
-// the y metric and the Neumann overrides of stencil_op_kernel
+// Every array of the fused kernels has x extent n0 and z extent n2 (periodic: points = cells) and y
+// extent nc1 (cell rows) or np1 (point rows); index (k, j, i), x fastest, below 2^31 values.
 template <typename T>
-__device__ __forceinline__ T fz_finish(const FzOp& o, const double* __restrict__ table, const T* __restrict__ fbc,
-                                       int nl, int L, int p, T v) {
-  if (o.lmap >= 0) v *= T(table[o.lmap + p]);
-  if ((o.neu & 1) && p == 0) v = fbc[L];
-  if ((o.neu & 2) && p == o.nout - 1) v = fbc[nl + L];
-  return v;
+__device__ __forceinline__ T ld(const T* __restrict__ a, int n0, int ny, int i, int j, int k) {
+  return __ldg(a + (k * ny + j) * n0 + i);
 }
 
-// y line with walls, a row in the bulk range: the bulk formula and the y metric
+// periodic CD2 operator of family FAM at row p: the bulk formula of stencil_op_kernel (bulk_fn with
+// r2 = 0) on wrapped indices, times dd
 template <int FAM, typename T, typename F>
-__device__ __forceinline__ T fz_ybulk(const FzOp& o, const double* __restrict__ table, int p, const F& f) {
-  T v = fz_bulk<FAM, T>(f, p, T(o.r1)) * T(o.dd);
-  if (o.lmap >= 0) v *= T(table[o.lmap + p]);
-  return v;
-}
-
-// y line with walls: bulk rows or the plan's boundary rows
-template <int FAM, typename T, typename F>
-__device__ __forceinline__ T fz_wall(const FzOp& o, const OpPlan* __restrict__ plans, const double* __restrict__ table,
-                                     const T* __restrict__ fbc, int nl, int L, int p, const F& f) {
+__device__ __forceinline__ T fz_per(const FzOp& o, int p, int n, const F& f) {
+  const T r1 = T(o.r1);
   T v;
-  if (p >= o.b_lo && p <= o.b_hi) v = fz_bulk<FAM, T>(f, p, T(o.r1)) * T(o.dd);
-  else v = fz_special<T>(plans + o.plan, p, fbc, nl, L, f);
-  return fz_finish<T>(o, table, fbc, nl, L, p, v);
+  if (FAM == M1P2C) v = r1 * (f(p) + f(p + 1 < n ? p + 1 : 0));
+  else if (FAM == M1C2P) v = r1 * (f(p) + f(p > 0 ? p - 1 : n - 1));
+  else if (FAM == D1C2P) v = r1 * (f(p) - f(p > 0 ? p - 1 : n - 1));
+  else v = r1 * (f(p + 1 < n ? p + 1 : 0) - f(p));  // D1P2C
+  return v * T(o.dd);
 }
 
-// The inner operators at one position.  Arrays all have x extent n0 and z extent n2; their y
-// extent is nc1 (cell rows: qx, qz, p, gx, gz, mu) or np1 (point rows: qy, gy).  PY: periodic y.
-// E: rows near the walls, where y operators may take their plans' boundary rows; the interior rows
-// (every y operator of every level in its bulk range, checked by the host) compile without them.
+// y operator with walls at output row p from its row table
+template <typename T, typename F>
+__device__ __forceinline__ T fz_row(const FzRow* __restrict__ rows, const FzOp& o, int p, const T* __restrict__ fbc,
+                                    int nl, int L, const F& f) {
+  const FzRow& r = rows[o.row + p];
+  const int fl = r.flags;
+  T v = T(r.w[0]) * f(p + r.o[0]);
+  v += T(r.w[1]) * f(p + r.o[1]);
+  if (fl & 1) v += T(r.w[2]) * f(p + r.o[2]);
+  if (fl & 2) v += T(r.wb[0]) * fbc[L];
+  if (fl & 4) v += T(r.wb[1]) * fbc[nl + L];
+  return v;
+}
+
+// input offsets of the two taps of a family's bulk formula (bulk_fn)
+template <int FAM>
+struct FzTap {
+  static constexpr int o0 = FAM == D1P2C ? 1 : 0;
+  static constexpr int o1 = (FAM == M1P2C) ? 1 : (FAM == D1P2C ? 0 : -1);
+};
+
+// y operator: periodic (PY); with walls in the interior rows (E false: the row's two bulk weights at
+// the family's fixed offsets, so loads shared between taps are shared in the code); with walls near
+// them (E: the row's own taps and wall planes)
+template <int FAM, bool PY, bool E, typename T, typename F>
+__device__ __forceinline__ T fz_y(const FzRow* __restrict__ rows, const FzOp& o, int p, int nin,
+                                  const T* __restrict__ fbc, int nl, int L, const F& f) {
+  if (PY) return fz_per<FAM, T>(o, p, nin, f);
+  if (!E) {
+    const FzRow& r = rows[o.row + p];
+    T v = T(r.w[0]) * f(p + FzTap<FAM>::o0);
+    v += T(r.w[1]) * f(p + FzTap<FAM>::o1);
+    return v;
+  }
+  return fz_row<T>(rows, o, p, fbc, nl, L, f);
+}
+
+// op(conv) + w*op(visc) of one direction.  x and z are periodic with one bulk formula for both
+// terms (checked by the host), so one operator runs on conv + (s*w)*visc; a y pair runs on the
+// combined expression when it merges (as the operator path does) and term by term otherwise.
+template <int FAM, int DIR, bool PY, bool E, typename T, typename FC, typename FV>
+__device__ __forceinline__ T fz_pair(const FzPair<T>& pr, const FzRow* __restrict__ rows, int nl, int n0, int i, int j,
+                                     int k, int nin, double sv, double w, const FC& conv, const FV& visc) {
+  const double sr = sv * w;
+  auto comb = [&](int q) -> T {
+    T e = conv(q);
+    e += visc(sr, q);
+    return e;
+  };
+  if (DIR == 0) return fz_per<FAM, T>(pr.a, i, nin, comb);
+  if (DIR == 2) return fz_per<FAM, T>(pr.a, k, nin, comb);
+  if (PY) return fz_per<FAM, T>(pr.a, j, nin, comb);
+  const int L = i + n0 * k;
+  // interior rows: both terms' plans share the bulk weights (checked by the host)
+  if (!E || pr.merged) return fz_y<FAM, false, E, T>(rows, pr.a, j, nin, pr.fa, nl, L, comb);
+  const T va = fz_row<T>(rows, pr.a, j, pr.fa, nl, L, [&](int q) { return conv(q); });
+  const T vb = fz_row<T>(rows, pr.b, j, pr.fb, nl, L, [&](int q) { return visc(sv, q); });
+  return va + T(w) * vb;
+}
+
+// rows at each y wall whose outputs may reach a boundary row of some plan at some level: a block
+// whose rows all lie in [kFzEdge, nc1 - kFzEdge) takes the bulk formulas only (the host checked
+// that every y plan's bulk range covers rows 2 .. nout-3)
+constexpr int kFzEdge = 4;
+__device__ __forceinline__ bool fz_interior_block(int nc1) {
+  const int j0 = blockIdx.y * blockDim.y;
+  return j0 >= kFzEdge && j0 + (int)blockDim.y <= nc1 - kFzEdge;
+}
+
+// the inner operators of the momentum equation at one position (E: the row may be near a wall)
 template <typename T, bool TH, bool PY, bool E>
 struct FzCtx {
   const FzMomentum<T>& f;
   int nl;  // lines of a y operator (n0 * n2)
 
-  __device__ __forceinline__ T at(const T* a, int ny, int i, int j, int k) const {
-    return __ldg(a + ((int64_t)k * ny + j) * f.n0 + i);
-  }
-  template <int FAM, typename F>
-  __device__ __forceinline__ T xop(int s, int i, const F& g) const { return fz_per<FAM, T>(f.in[s], i, f.n0, g); }
-  template <int FAM, typename F>
-  __device__ __forceinline__ T zop(int s, int k, const F& g) const { return fz_per<FAM, T>(f.in[s], k, f.n2, g); }
-  template <int FAM, typename F>
-  __device__ __forceinline__ T yop(int s, const T* fbc, int i, int j, int k, int nin, const F& g) const {
-    if (PY) return fz_per<FAM, T>(f.in[s], j, nin, g);
-    if (!E) return fz_ybulk<FAM, T>(f.in[s], f.table, j, g);
-    return fz_wall<FAM, T>(f.in[s], f.plans, f.table, fbc, nl, i + f.n0 * k, j, g);
-  }
-#define FZ_X(FAM, S, A, NY) xop<FAM>(S, i, [&](int q) { return at(A, NY, q, j, k); })
-#define FZ_Z(FAM, S, A, NY) zop<FAM>(S, k, [&](int q) { return at(A, NY, i, j, q); })
-#define FZ_Y(FAM, S, A, NY, FB) yop<FAM>(S, FB, i, j, k, NY, [&](int q) { return at(A, NY, i, q, k); })
+  __device__ __forceinline__ T at(const T* a, int ny, int i, int j, int k) const { return ld(a, f.n0, ny, i, j, k); }
+#define FZ_X(FAM, S, A, NY) fz_per<FAM, T>(f.in[S], i, f.n0, [&](int q) { return at(A, NY, q, j, k); })
+#define FZ_Z(FAM, S, A, NY) fz_per<FAM, T>(f.in[S], k, f.n2, [&](int q) { return at(A, NY, i, j, q); })
+#define FZ_Y(FAM, S, A, NY, FB) \
+  fz_y<FAM, PY, E, T>(f.rows, f.in[S], j, NY, FB, nl, i + f.n0 * k, [&](int q) { return at(A, NY, i, q, k); })
   // velocity interpolations and derivatives (src/eq_momentum2.f90:347-508)
   __device__ __forceinline__ T qxix(int i, int j, int k) const { return FZ_X(M1P2C, FI_QX_MX, f.qx, f.nc1); }
   __device__ __forceinline__ T qxdx(int i, int j, int k) const { return FZ_X(D1P2C, FI_QX_DX, f.qx, f.nc1); }
@@ -121,7 +132,9 @@ struct FzCtx {
   __device__ __forceinline__ T qxdz(int i, int j, int k) const { return FZ_Z(D1C2P, FI_QX_DZ, f.qx, f.nc1); }
   __device__ __forceinline__ T qydx(int i, int j, int k) const { return FZ_X(D1C2P, FI_QY_DX, f.qy, f.np1); }
   __device__ __forceinline__ T qyix(int i, int j, int k) const { return FZ_X(M1C2P, FI_QY_MX, f.qy, f.np1); }
-  __device__ __forceinline__ T qydy(int i, int j, int k) const { return FZ_Y(D1P2C, FI_QY_DY, f.qy, f.np1, (const T*)nullptr); }
+  __device__ __forceinline__ T qydy(int i, int j, int k) const {
+    return FZ_Y(D1P2C, FI_QY_DY, f.qy, f.np1, (const T*)nullptr);
+  }
   __device__ __forceinline__ T qyiy(int i, int j, int k) const { return FZ_Y(M1P2C, FI_QY_MY, f.qy, f.np1, f.fyqy); }
   __device__ __forceinline__ T qydz(int i, int j, int k) const { return FZ_Z(D1C2P, FI_QY_DZ, f.qy, f.np1); }
   __device__ __forceinline__ T qyiz(int i, int j, int k) const { return FZ_Z(M1C2P, FI_QY_MZ, f.qy, f.np1); }
@@ -144,13 +157,13 @@ struct FzCtx {
   __device__ __forceinline__ T muy(int i, int j, int k) const { return FZ_Y(M1C2P, FI_MU_Y, f.mu, f.nc1, f.fm); }
   __device__ __forceinline__ T mux(int i, int j, int k) const { return FZ_X(M1C2P, FI_MU_X, f.mu, f.nc1); }
   __device__ __forceinline__ T muyx(int i, int j, int k) const {
-    return xop<M1C2P>(FI_MU_YX, i, [&](int q) { return muy(q, j, k); });
+    return fz_per<M1C2P, T>(f.in[FI_MU_YX], i, f.n0, [&](int q) { return muy(q, j, k); });
   }
   __device__ __forceinline__ T muxz(int i, int j, int k) const {
-    return zop<M1C2P>(FI_MU_XZ, k, [&](int q) { return mux(i, j, q); });
+    return fz_per<M1C2P, T>(f.in[FI_MU_XZ], k, f.n2, [&](int q) { return mux(i, j, q); });
   }
   __device__ __forceinline__ T muyz(int i, int j, int k) const {
-    return zop<M1C2P>(FI_MU_YZ, k, [&](int q) { return muy(i, j, q); });
+    return fz_per<M1C2P, T>(f.in[FI_MU_YZ], k, f.n2, [&](int q) { return muy(i, j, q); });
   }
 #undef FZ_X
 #undef FZ_Z
@@ -164,11 +177,12 @@ struct FzCtx {
     v += qzdz(i, j, k);
     return v;
   }
-  // s*(a + c*b), times m with variable properties (linm)
+  // s*(a + c*b) (linm; times the viscosity with variable properties)
   __device__ __forceinline__ T lin(double s, T a, double c, T b) const { return T(s) * (a + T(c) * b); }
 
-  // ---- the viscous and convective expressions at the stress points
-  // cell centre, component c (0 x, 1 y, 2 z): conv -(ci*qi), visc s*(qidi - div/3)[*mu]
+  // ---- the convective and viscous expressions at the stress points
+  // cell centre, component C: conv -(c*qi) with c the interpolated momentum (or qi), visc
+  // s*(qidi - div/3)[*mu]
   template <int C>
   __device__ __forceinline__ T conv_c(int i, int j, int k) const {
     if (C == 0) { const T a = qxix(i, j, k); const T b = TH ? gxix(i, j, k) : a; return T(-1.0) * (b * a); }
@@ -179,15 +193,12 @@ struct FzCtx {
   }
   template <int C>
   __device__ __forceinline__ T visc_c(double s, int i, int j, int k) const {
-    T d;
-    T dv;
-    if (C == 0) { d = qxdx(i, j, k); dv = divc(d, i, j, k); }
-    else if (C == 1) { d = qydy(i, j, k); dv = divc(qxdx(i, j, k), i, j, k); }
-    else { d = qzdz(i, j, k); dv = divc(qxdx(i, j, k), i, j, k); }
-    const T v = lin(s, d, -1.0 / 3.0, dv);
+    const T dx = qxdx(i, j, k);
+    const T d = C == 0 ? dx : (C == 1 ? qydy(i, j, k) : qzdz(i, j, k));
+    const T v = lin(s, d, -1.0 / 3.0, divc(dx, i, j, k));
     return TH ? v * muc(i, j, k) : v;
   }
-  // xy point (ppc): conv of x-momentum -(gyix*qxiy), of y-momentum -(gxiy*qyix); visc shared
+  // xy edge (ppc): x-momentum -(gyix*qxiy), y-momentum -(gxiy*qyix); the viscous part is shared
   template <int C>
   __device__ __forceinline__ T conv_xy(int i, int j, int k) const {
     if (C == 0) { const T a = qxiy(i, j, k); const T b = TH ? gyix(i, j, k) : qyix(i, j, k); return T(-1.0) * (b * a); }
@@ -199,7 +210,7 @@ struct FzCtx {
     const T v = lin(s, qxdy(i, j, k), 1.0, qydx(i, j, k));
     return TH ? v * muyx(i, j, k) : v;
   }
-  // xz point (pcp): x-momentum -(gzix*qxiz), z-momentum -(gxiz*qzix)
+  // xz edge (pcp): x-momentum -(gzix*qxiz), z-momentum -(gxiz*qzix)
   template <int C>
   __device__ __forceinline__ T conv_xz(int i, int j, int k) const {
     if (C == 0) { const T a = qxiz(i, j, k); const T b = TH ? gzix(i, j, k) : qzix(i, j, k); return T(-1.0) * (b * a); }
@@ -211,7 +222,7 @@ struct FzCtx {
     const T v = lin(s, qxdz(i, j, k), 1.0, qzdx(i, j, k));
     return TH ? v * muxz(i, j, k) : v;
   }
-  // yz point (cpp): y-momentum -(qyiz*gziy), z-momentum -(gyiz*qziy)
+  // yz edge (cpp): y-momentum -(qyiz*gziy), z-momentum -(gyiz*qziy)
   template <int C>
   __device__ __forceinline__ T conv_yz(int i, int j, int k) const {
     if (C == 1) { const T a = qyiz(i, j, k); const T b = TH ? gziy(i, j, k) : qziy(i, j, k); return T(-1.0) * (a * b); }
@@ -224,43 +235,8 @@ struct FzCtx {
     return TH ? v * muyz(i, j, k) : v;
   }
 
-  // op(conv) + rre*op(visc) of one direction, added to acc (`first`: stored).  x and z are periodic
-  // with identical bulk plans for both terms, so one operator runs on conv + (s*rre)*visc; in y the
-  // bulk rows do the same, and a boundary row applies each term's own plan (the combined planes
-  // when the pair merges, as the operator path does)
-  template <int FAM, int DIR, typename FC, typename FV>
-  __device__ __forceinline__ T pair(const FzPair<T>& pr, T acc, bool first, int i, int j, int k, int nin, double sv,
-                                    const FC& conv, const FV& visc) const {
-    const double sr = sv * f.rre;
-    auto comb = [&](int q) -> T {
-      T e = conv(q);
-      e += visc(sr, q);
-      return e;
-    };
-    T v;
-    if (DIR != 1 || PY) {
-      v = fz_per<FAM, T>(pr.a, DIR == 0 ? i : (DIR == 1 ? j : k), nin, comb);
-    } else if (!E) {
-      v = fz_ybulk<FAM, T>(pr.a, f.table, j, comb);
-    } else {
-      const int L = i + f.n0 * k;
-      if (j >= pr.a.b_lo && j <= pr.a.b_hi) {
-        v = fz_finish<T>(pr.a, f.table, pr.fa, nl, L, j, fz_bulk<FAM, T>(comb, j, T(pr.a.r1)) * T(pr.a.dd));
-      } else if (pr.merged) {
-        v = fz_finish<T>(pr.a, f.table, pr.fa, nl, L, j, fz_special<T>(f.plans + pr.a.plan, j, pr.fa, nl, L, comb));
-      } else {
-        const T va = fz_finish<T>(pr.a, f.table, pr.fa, nl, L, j,
-                                  fz_special<T>(f.plans + pr.a.plan, j, pr.fa, nl, L, [&](int q) { return conv(q); }));
-        const T vb = fz_finish<T>(pr.b, f.table, pr.fb, nl, L, j,
-                                  fz_special<T>(f.plans + pr.b.plan, j, pr.fb, nl, L, [&](int q) { return visc(sv, q); }));
-        v = va + T(f.rre) * vb;
-      }
-    }
-    return first ? v : acc + v;
-  }
-
   // the fractional step of the operator path's O_FRAC store (pfc = 1 * v)
-  __device__ __forceinline__ void frac(int c, int64_t a, T F, T v) const {
+  __device__ __forceinline__ void frac(int c, int a, T F, T v) const {
     const T tdt = T(f.dt), tg = T(f.gam), tz = T(f.zeta), ta = T(f.alpha);
     const T pfc = T(1.0) * v;
     const T last = f.m0[c][a];
@@ -271,64 +247,66 @@ struct FzCtx {
   }
 };
 
-// one momentum component C (0 x, 1 y, 2 z) per thread and output value.  Interior launch (E
-// false): rows [row0, row0 + gridDim.y * blockDim.y) of the component's grid; edge launch (E
-// true): blockIdx.y indexes the edge rows, [0, row0) then [row1, ny).
+// one momentum component C (0 x, 1 y, 2 z) at (i, j, k)
 template <typename T, bool TH, bool PY, int C, bool E>
-__global__ void __launch_bounds__(256) fz_momentum_kernel(const __grid_constant__ FzMomentum<T> f, int row0, int row1) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+__device__ __forceinline__ void fz_momentum_body(const FzMomentum<T>& f, int i, int j, int k) {
   const int n0 = f.n0, nc1 = f.nc1, np1 = f.np1, n2 = f.n2;
-  int j;
-  if (E) j = blockIdx.y < row0 ? (int)blockIdx.y : row1 + ((int)blockIdx.y - row0);
-  else j = row0 + blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= n0 || j >= (E ? (C == 1 ? np1 : nc1) : row1) || k >= n2) return;
   const FzCtx<T, TH, PY, E> c{f, n0 * n2};
-  const int L = i + n0 * k;
+  const int nl = c.nl, L = i + n0 * k;
+  const double r = f.rre;
   T F, v;
   if (C == 0) {
     // x-momentum at (i, j, k) of the qx grid
-    F = c.template pair<D1C2P, 0>(
-        f.term[0][0], T(0), true, i, j, k, n0, 2.0, [&](int q) { return c.template conv_c<0>(q, j, k); },
+    F = fz_pair<D1C2P, 0, PY, E, T>(
+        f.term[0][0], f.rows, nl, n0, i, j, k, n0, 2.0, r, [&](int q) { return c.template conv_c<0>(q, j, k); },
         [&](double s, int q) { return c.template visc_c<0>(s, q, j, k); });
-    F = c.template pair<D1P2C, 1>(
-        f.term[0][1], F, false, i, j, k, np1, 1.0, [&](int q) { return c.template conv_xy<0>(i, q, k); },
+    F += fz_pair<D1P2C, 1, PY, E, T>(
+        f.term[0][1], f.rows, nl, n0, i, j, k, np1, 1.0, r, [&](int q) { return c.template conv_xy<0>(i, q, k); },
         [&](double s, int q) { return c.visc_xy(s, i, q, k); });
-    F = c.template pair<D1P2C, 2>(
-        f.term[0][2], F, false, i, j, k, n2, 1.0, [&](int q) { return c.template conv_xz<0>(i, j, q); },
+    F += fz_pair<D1P2C, 2, PY, E, T>(
+        f.term[0][2], f.rows, nl, n0, i, j, k, n2, 1.0, r, [&](int q) { return c.template conv_xz<0>(i, j, q); },
         [&](double s, int q) { return c.visc_xz(s, i, j, q); });
     v = fz_per<D1C2P, T>(f.pres[0], i, n0, [&](int q) { return T(-1.0) * c.pr(q, j, k); });
-    c.frac(0, ((int64_t)k * nc1 + j) * n0 + i, F, v);
+    c.frac(0, (k * nc1 + j) * n0 + i, F, v);
   } else if (C == 1) {
     // y-momentum at (i, j, k) of the qy grid
-    F = c.template pair<D1P2C, 0>(
-        f.term[1][0], T(0), true, i, j, k, n0, 1.0, [&](int q) { return c.template conv_xy<1>(q, j, k); },
+    F = fz_pair<D1P2C, 0, PY, E, T>(
+        f.term[1][0], f.rows, nl, n0, i, j, k, n0, 1.0, r, [&](int q) { return c.template conv_xy<1>(q, j, k); },
         [&](double s, int q) { return c.visc_xy(s, q, j, k); });
-    F = c.template pair<D1C2P, 1>(
-        f.term[1][1], F, false, i, j, k, nc1, 2.0, [&](int q) { return c.template conv_c<1>(i, q, k); },
+    F += fz_pair<D1C2P, 1, PY, E, T>(
+        f.term[1][1], f.rows, nl, n0, i, j, k, nc1, 2.0, r, [&](int q) { return c.template conv_c<1>(i, q, k); },
         [&](double s, int q) { return c.template visc_c<1>(s, i, q, k); });
-    F = c.template pair<D1P2C, 2>(
-        f.term[1][2], F, false, i, j, k, n2, 1.0, [&](int q) { return c.template conv_yz<1>(i, j, q); },
+    F += fz_pair<D1P2C, 2, PY, E, T>(
+        f.term[1][2], f.rows, nl, n0, i, j, k, n2, 1.0, r, [&](int q) { return c.template conv_yz<1>(i, j, q); },
         [&](double s, int q) { return c.visc_yz(s, i, j, q); });
-    auto pf = [&](int q) { return T(-1.0) * c.pr(i, q, k); };
-    if (PY) v = fz_per<D1C2P, T>(f.pres[1], j, nc1, pf);
-    else if (!E) v = fz_ybulk<D1C2P, T>(f.pres[1], f.table, j, pf);
-    else v = fz_wall<D1C2P, T>(f.pres[1], f.plans, f.table, f.fpres[1], c.nl, L, j, pf);
-    c.frac(1, ((int64_t)k * np1 + j) * n0 + i, F, v);
+    v = fz_y<D1C2P, PY, E, T>(f.rows, f.pres[1], j, nc1, f.fpres[1], nl, L,
+                           [&](int q) { return T(-1.0) * c.pr(i, q, k); });
+    c.frac(1, (k * np1 + j) * n0 + i, F, v);
   } else {
     // z-momentum at (i, j, k) of the qz grid
-    F = c.template pair<D1P2C, 0>(
-        f.term[2][0], T(0), true, i, j, k, n0, 1.0, [&](int q) { return c.template conv_xz<2>(q, j, k); },
+    F = fz_pair<D1P2C, 0, PY, E, T>(
+        f.term[2][0], f.rows, nl, n0, i, j, k, n0, 1.0, r, [&](int q) { return c.template conv_xz<2>(q, j, k); },
         [&](double s, int q) { return c.visc_xz(s, q, j, k); });
-    F = c.template pair<D1P2C, 1>(
-        f.term[2][1], F, false, i, j, k, np1, 1.0, [&](int q) { return c.template conv_yz<2>(i, q, k); },
+    F += fz_pair<D1P2C, 1, PY, E, T>(
+        f.term[2][1], f.rows, nl, n0, i, j, k, np1, 1.0, r, [&](int q) { return c.template conv_yz<2>(i, q, k); },
         [&](double s, int q) { return c.visc_yz(s, i, q, k); });
-    F = c.template pair<D1C2P, 2>(
-        f.term[2][2], F, false, i, j, k, n2, 2.0, [&](int q) { return c.template conv_c<2>(i, j, q); },
+    F += fz_pair<D1C2P, 2, PY, E, T>(
+        f.term[2][2], f.rows, nl, n0, i, j, k, n2, 2.0, r, [&](int q) { return c.template conv_c<2>(i, j, q); },
         [&](double s, int q) { return c.template visc_c<2>(s, i, j, q); });
     v = fz_per<D1C2P, T>(f.pres[2], k, n2, [&](int q) { return T(-1.0) * c.pr(i, j, q); });
-    c.frac(2, ((int64_t)k * nc1 + j) * n0 + i, F, v);
+    c.frac(2, (k * nc1 + j) * n0 + i, F, v);
   }
+}
+
+// one momentum component C (0 x, 1 y, 2 z) per thread and output value
+template <typename T, bool TH, bool PY, int C>
+__global__ void __launch_bounds__(256) fz_momentum_kernel(const __grid_constant__ FzMomentum<T> f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= f.n0 || j >= (C == 1 ? f.np1 : f.nc1) || k >= f.n2) return;
+  if (PY || fz_interior_block(f.nc1)) fz_momentum_body<T, TH, PY, C, false>(f, i, j, k);
+  else fz_momentum_body<T, TH, PY, C, true>(f, i, j, k);
 }
 
 // the wall rows of the y-viscous boundary value (fbcy_velo: src/eq_momentum2.f90:374-442, :537-546,
@@ -343,8 +321,7 @@ __global__ void fz_wall_visc_kernel(const __grid_constant__ FzMomentum<T> f, T* 
     for (int side = 0; side < 2; ++side) {
       const int j = side == 0 ? 0 : f.np1 - 1;
       const T ddx = fz_per<D1P2C, T>(f.in[FI_W_DX], i, f.n0, [&](int q) { return c.qxiy(q, j, k); });
-      const T ddy = fz_wall<D1C2P, T>(f.in[FI_W_DY], f.plans, f.table, f.fyqy, nl, g, j,
-                                      [&](int q) { return c.qyiy(i, q, k); });
+      const T ddy = fz_row<T>(f.rows, f.in[FI_W_DY], j, f.fyqy, nl, g, [&](int q) { return c.qyiy(i, q, k); });
       const T ddz = fz_per<D1P2C, T>(f.in[FI_W_DZ], k, f.n2, [&](int q) { return c.qziy(i, j, q); });
       T sum = T(1.0) * ddx;
       sum += T(1.0) * ddy;
@@ -374,44 +351,161 @@ __global__ void fz_update_kernel(T* __restrict__ ux, T* __restrict__ uy, T* __re
   const int k = blockIdx.z;
   if (i >= n0) return;
   if (j < nc1) {
-    const int64_t a = ((int64_t)k * nc1 + j) * n0 + i;
+    const int a = (k * nc1 + j) * n0 + i;
     const T s = bulk ? T(bulk[0]) : T(0);
     ux[a] = ux[a] + (mx[a] - s);
     uz[a] = uz[a] + (mz[a] - T(0));
   }
-  const int64_t b = ((int64_t)k * np1 + j) * n0 + i;
+  const int b = (k * np1 + j) * n0 + i;
   T v = uy[b] + (my[b] - T(0));
   if (s0 && j == 0) v = T(v0);
   if (s1 && j == np1 - 1) v = T(v1);
   uy[b] = v;
 }
 
-}  // namespace
-
-template <typename T, bool TH, bool PY, int C>
-void launch_fz_c(const FzMomentum<T>& f, cudaStream_t st) {
-  const int ny = C == 1 ? f.np1 : f.nc1;
-  // interior rows [m, ny - m) without boundary-row code (all rows when y is periodic); the host
-  // checked that every y plan's bulk range covers rows 2 .. n-3 of its output
-  const int m = PY ? 0 : (ny > 2 * kFzEdge ? kFzEdge : ny / 2);
-  const int r0 = m, r1 = ny - m;
-  if (r1 > r0) {
-    const dim3 bs(32, 4, 2);
-    const dim3 grid((f.n0 + bs.x - 1) / bs.x, (r1 - r0 + bs.y - 1) / bs.y, (f.n2 + bs.z - 1) / bs.z);
-    fz_momentum_kernel<T, TH, PY, C, false><<<grid, bs, 0, st>>>(f, r0, r1);
+// ---- energy equation: thread per cell (i, j, k)
+template <typename T, bool E>
+struct FzECtx {
+  const FzEnergy<T>& f;
+  int nl;
+  __device__ __forceinline__ T at(const T* a, int ny, int i, int j, int k) const { return ld(a, f.n0, ny, i, j, k); }
+  template <int FAM>
+  __device__ __forceinline__ T xop(int s, const T* a, int i, int j, int k) const {
+    return fz_per<FAM, T>(f.in[s], i, f.n0, [&](int q) { return at(a, f.nc1, q, j, k); });
   }
-  if (!PY && m > 0) {
-    const dim3 bs(32, 1, 8);
-    const dim3 grid((f.n0 + bs.x - 1) / bs.x, r0 + (ny - r1), (f.n2 + bs.z - 1) / bs.z);
-    fz_momentum_kernel<T, TH, PY, C, true><<<grid, bs, 0, st>>>(f, r0, r1);
+  template <int FAM>
+  __device__ __forceinline__ T zop(int s, const T* a, int i, int j, int k) const {
+    return fz_per<FAM, T>(f.in[s], k, f.n2, [&](int q) { return at(a, f.nc1, i, j, q); });
+  }
+  template <int FAM>
+  __device__ __forceinline__ T yop(int s, const T* a, const T* fbc, int i, int j, int k) const {
+    return fz_y<FAM, false, E, T>(f.rows, f.in[s], j, f.nc1, fbc, nl, i + f.n0 * k,
+                                  [&](int q) { return at(a, f.nc1, i, q, k); });
+  }
+};
+
+template <typename T, bool E>
+__device__ __forceinline__ void fz_energy_body(const FzEnergy<T>& f, int i, int j, int k) {
+  const int n0 = f.n0, nc1 = f.nc1, np1 = f.np1, n2 = f.n2;
+  const FzECtx<T, E> c{f, n0 * n2};
+  const int nl = c.nl;
+  // x: faces (q, j, k) of the qx grid
+  T F = fz_pair<D1P2C, 0, false, E, T>(
+      f.term[0], f.rows, nl, n0, i, j, k, n0, 1.0, f.rpr,
+      [&](int q) { return T(-1.0) * (c.at(f.gx, nc1, q, j, k) * c.template xop<M1C2P>(FE_H_X, f.h, q, j, k)); },
+      [&](double s, int q) {
+        return T(s) * (c.template xop<D1C2P>(FE_T_X, f.t, q, j, k) * c.template xop<M1C2P>(FE_K_X, f.k, q, j, k));
+      });
+  // y: faces (i, q, k) of the qy grid
+  F += fz_pair<D1P2C, 1, false, E, T>(
+      f.term[1], f.rows, nl, n0, i, j, k, np1, 1.0, f.rpr,
+      [&](int q) { return T(-1.0) * (c.at(f.gy, np1, i, q, k) * c.template yop<M1C2P>(FE_H_Y, f.h, f.fh, i, q, k)); },
+      [&](double s, int q) {
+        return T(s) * (c.template yop<D1C2P>(FE_T_Y, f.t, f.fqw, i, q, k) *
+                       c.template yop<M1C2P>(FE_K_Y, f.k, f.fk, i, q, k));
+      });
+  // z: faces (i, j, q) of the qz grid
+  F += fz_pair<D1P2C, 2, false, E, T>(
+      f.term[2], f.rows, nl, n0, i, j, k, n2, 1.0, f.rpr,
+      [&](int q) { return T(-1.0) * (c.at(f.gz, nc1, i, j, q) * c.template zop<M1C2P>(FE_H_Z, f.h, i, j, q)); },
+      [&](double s, int q) {
+        return T(s) * (c.template zop<D1C2P>(FE_T_Z, f.t, i, j, q) * c.template zop<M1C2P>(FE_K_Z, f.k, i, j, q));
+      });
+  // energy_advance_kernel: rhs0 = F, rho*h += dt*(gam*F + zeta*rhs0)
+  const int a = (k * nc1 + j) * n0 + i;
+  const T tdt = T(f.dt), tg = T(f.gam), tz = T(f.zeta);
+  const T last = f.rhs0[a];
+  const T tot = tg * F + tz * last;
+  f.rhs0[a] = F;
+  const T r1 = tdt * tot;
+  f.rhoh[a] = f.rhoh[a] + r1;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) fz_energy_kernel(const __grid_constant__ FzEnergy<T> f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= f.n0 || j >= f.nc1 || k >= f.n2) return;
+  if (fz_interior_block(f.nc1)) fz_energy_body<T, false>(f, i, j, k);
+  else fz_energy_body<T, true>(f, i, j, k);
+}
+
+template <typename T>
+__global__ void fz_energy_walls_kernel(const __grid_constant__ FzEnergy<T> f, int mode, T* __restrict__ out) {
+  const int nl = f.n0 * f.n2;
+  const FzECtx<T, true> c{f, nl};
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nl; g += gridDim.x * blockDim.x) {
+    const int k = g / f.n0, i = g - k * f.n0;
+    for (int side = 0; side < 2; ++side) {
+      const int j = side == 0 ? 0 : f.np1 - 1;
+      if (mode == 0) {
+        // launch_fbcy_extract(A = dT/dy, B none, C = kappa_y, s = 1): (A*1)*C
+        T v = c.template yop<D1C2P>(FE_T_Y, f.t, f.fqw, i, j, k);
+        v = v * T(1.0);
+        v = v * c.template yop<M1C2P>(FE_K_Y, f.k, f.fk, i, j, k);
+        out[side * nl + g] = v;
+        out[(side + 2) * nl + g] = v;
+      } else {
+        out[(k * f.np1 + j) * f.n0 + i] = c.template yop<M1C2P>(FE_RH_Y, f.rhoh, (const T*)nullptr, i, j, k);
+      }
+    }
   }
 }
 
+// ---- pressure update, projection and q = g / rho_face: thread per (i, j, k), j over the y points
+template <typename T, bool TH>
+__global__ void __launch_bounds__(256) fz_project_kernel(const __grid_constant__ FzProject<T> f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int n0 = f.n0, nc1 = f.nc1, np1 = f.np1, n2 = f.n2;
+  if (i >= n0 || j >= np1 || k >= n2) return;
+  const int nl = n0 * n2, L = i + n0 * k;
+  auto phi = [&](int ii, int jj, int kk) { return ld(f.phi, n0, nc1, ii, jj, kk); };
+  auto rho = [&](int ii, int jj, int kk) { return ld(f.rho, n0, nc1, ii, jj, kk); };
+  const T cf = T(f.coef);
+  if (j < nc1) {
+    const int a = (k * nc1 + j) * n0 + i;
+    // p += phi (axpby with unit weights)
+    T pv = T(1.0) * f.p[a];
+    pv += T(1.0) * phi(i, j, k);
+    f.p[a] = pv;
+    const T vx = fz_per<D1C2P, T>(f.in[FP_DX], i, n0, [&](int q) { return phi(q, j, k); });
+    const T gxn = f.ux[a] + cf * vx;
+    f.ux[a] = gxn;
+    const T vz = fz_per<D1C2P, T>(f.in[FP_DZ], k, n2, [&](int q) { return phi(i, j, q); });
+    const T gzn = f.uz[a] + cf * vz;
+    f.uz[a] = gzn;
+    if (TH) {
+      f.qx[a] = gxn / (T(1.0) * fz_per<M1C2P, T>(f.in[FP_PX], i, n0, [&](int q) { return rho(q, j, k); }));
+      f.qz[a] = gzn / (T(1.0) * fz_per<M1C2P, T>(f.in[FP_PZ], k, n2, [&](int q) { return rho(i, j, q); }));
+    }
+  }
+  const int b = (k * np1 + j) * n0 + i;
+  T vy;
+  if (f.periodic_y) vy = fz_per<D1C2P, T>(f.in[FP_DY], j, nc1, [&](int q) { return phi(i, q, k); });
+  else vy = fz_row<T>(f.rows, f.in[FP_DY], j, f.fphi, nl, L, [&](int q) { return phi(i, q, k); });
+  T gyn = f.uy[b] + cf * vy;
+  if (f.s0 && j == 0) gyn = T(f.v0);
+  if (f.s1 && j == np1 - 1) gyn = T(f.v1);
+  f.uy[b] = gyn;
+  if (TH) {
+    const T ry = fz_row<T>(f.rows, f.in[FP_PY], j, f.fd, nl, L, [&](int q) { return rho(i, q, k); });
+    f.qy[b] = gyn / (T(1.0) * ry);
+  }
+}
+
+}  // namespace
+
 template <typename T, bool TH, bool PY>
 void launch_fz_c(const FzMomentum<T>& f, int c, cudaStream_t st) {
-  if (c == 0) launch_fz_c<T, TH, PY, 0>(f, st);
-  else if (c == 1) launch_fz_c<T, TH, PY, 1>(f, st);
-  else launch_fz_c<T, TH, PY, 2>(f, st);
+  const dim3 bs(32, 4, 2);
+  const int ny = c == 1 ? f.np1 : f.nc1;
+  const dim3 grid((f.n0 + bs.x - 1) / bs.x, (ny + bs.y - 1) / bs.y, (f.n2 + bs.z - 1) / bs.z);
+  if (c == 0) fz_momentum_kernel<T, TH, PY, 0><<<grid, bs, 0, st>>>(f);
+  else if (c == 1) fz_momentum_kernel<T, TH, PY, 1><<<grid, bs, 0, st>>>(f);
+  else fz_momentum_kernel<T, TH, PY, 2><<<grid, bs, 0, st>>>(f);
 }
 
 template <typename T>
@@ -437,6 +531,28 @@ void launch_fz_update(T* ux, T* uy, T* uz, const T* mx, const T* my, const T* mz
   fz_update_kernel<T><<<grid, 128, 0, st>>>(ux, uy, uz, mx, my, mz, bulk, n0, nc1, np1, n2, s0, v0, s1, v1);
 }
 
+template <typename T>
+void launch_fz_energy(const FzEnergy<T>& f, cudaStream_t st) {
+  const dim3 bs(32, 4, 2);
+  const dim3 grid((f.n0 + bs.x - 1) / bs.x, (f.nc1 + bs.y - 1) / bs.y, (f.n2 + bs.z - 1) / bs.z);
+  fz_energy_kernel<T><<<grid, bs, 0, st>>>(f);
+}
+
+template <typename T>
+void launch_fz_energy_walls(const FzEnergy<T>& f, int mode, T* out, cudaStream_t st) {
+  const int nl = f.n0 * f.n2;
+  const int blocks = (nl + 255) / 256 < 148 ? (nl + 255) / 256 : 148;
+  fz_energy_walls_kernel<T><<<blocks, 256, 0, st>>>(f, mode, out);
+}
+
+template <typename T>
+void launch_fz_project(const FzProject<T>& f, cudaStream_t st) {
+  const dim3 bs(32, 4, 2);
+  const dim3 grid((f.n0 + bs.x - 1) / bs.x, (f.np1 + bs.y - 1) / bs.y, (f.n2 + bs.z - 1) / bs.z);
+  if (f.thermo) fz_project_kernel<T, true><<<grid, bs, 0, st>>>(f);
+  else fz_project_kernel<T, false><<<grid, bs, 0, st>>>(f);
+}
+
 template void launch_fz_momentum<double>(const FzMomentum<double>&, int, cudaStream_t);
 template void launch_fz_momentum<float>(const FzMomentum<float>&, int, cudaStream_t);
 template void launch_fz_wall_visc<double>(const FzMomentum<double>&, double*, double*, const double*, cudaStream_t);
@@ -445,5 +561,11 @@ template void launch_fz_update<double>(double*, double*, double*, const double*,
                                        const double*, int, int, int, int, int, double, int, double, cudaStream_t);
 template void launch_fz_update<float>(float*, float*, float*, const float*, const float*, const float*,
                                       const double*, int, int, int, int, int, double, int, double, cudaStream_t);
+template void launch_fz_energy<double>(const FzEnergy<double>&, cudaStream_t);
+template void launch_fz_energy<float>(const FzEnergy<float>&, cudaStream_t);
+template void launch_fz_energy_walls<double>(const FzEnergy<double>&, int, double*, cudaStream_t);
+template void launch_fz_energy_walls<float>(const FzEnergy<float>&, int, float*, cudaStream_t);
+template void launch_fz_project<double>(const FzProject<double>&, cudaStream_t);
+template void launch_fz_project<float>(const FzProject<float>&, cudaStream_t);
 
 }  // namespace chs

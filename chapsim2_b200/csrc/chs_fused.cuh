@@ -1,15 +1,16 @@
 // Fused substep kernels for the CD2 scheme: the momentum right-hand side of each component with the
-// RK3 fractional step in one pass, the wall planes it needs, and the advance of the velocities.
+// RK3 fractional step in one pass, the energy equation with its advance in one pass, and the pressure
+// update with the projection (and q = g / rho_face) in one pass.
 //
 // The operator-by-operator substep (chs_solver.cu) writes every interpolated velocity and every
 // velocity derivative to HBM and reads it back in the component sums.  Here each output value
-// evaluates those inner operators where it needs them, from the velocities (and momenta and
-// viscosity with variable properties) themselves, so only the primary fields are read and only
-// the right-hand sides are written.  Every operator is the same plan as the operator path's (the
-// host builds this descriptor from the plans the substep would launch): x and z operators are
-// periodic and use the bulk formula with wrapped indices; y operators use the bulk formula in
-// their bulk range and the plan's boundary rows (sparse forms over the line and the wall planes)
-// outside it, then the y metric and the Neumann overrides, exactly as stencil_op_kernel does.
+// evaluates those inner operators where it needs them, from the primary fields themselves, so only
+// the primary fields are read and only the right-hand sides are written.  Every operator is the same
+// plan as the operator path's (the host builds these descriptors from the plans the substep would
+// launch): x and z are periodic and every row is the two-point bulk formula with wrapped indices; a y
+// operator with walls is a table of rows (FzRow), each at most three taps over the input line and
+// the two wall planes, built from the plan's bulk formula, its boundary rows, the y metric and the
+// Neumann overrides.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -19,17 +20,21 @@
 
 namespace chs {
 
-// One explicit operator inside a fused kernel.  kind 0: periodic line whose every row is the bulk
-// formula with wrapped indices; kind 1: bulk formula on rows [b_lo, b_hi], the plan's boundary
-// rows (plans[plan]) elsewhere.
+// One output row p of a y operator with walls:
+//   v = w[0] f(p + o[0]) + w[1] f(p + o[1]) (+ w[2] f(p + o[2])) (+ wb[0] fbc0 + wb[1] fbc1)
+// with the operator's 1/h and the row's y metric folded into the weights; a Neumann row is wb = 1.
+struct FzRow {
+  double w[3];
+  double wb[2];
+  int o[3];
+  int flags;  // bit 0: tap 2 used; bit 1: wall plane 0 used; bit 2: wall plane 1 used
+};
+
+// One explicit CD2 operator.  row < 0: periodic line, every row r1*(two-point formula)*dd with
+// wrapped indices; row >= 0: a y line with walls whose output row p is rows[row + p].
 struct FzOp {
-  int kind;
-  int b_lo, b_hi;
-  int lmap;   // offset of the y metric in the operator table, or -1
-  int neu;    // bit 0: first row = fbc plane 0; bit 1: last row = fbc plane 1
-  int nout;
-  int plan;   // index of the full plan (boundary rows) in the device plan array
-  double r1, r2, dd;
+  int row;
+  double r1, dd;
 };
 
 // op(conv) + w*op(visc) of one direction of one momentum component: one application of `a` on the
@@ -63,7 +68,7 @@ struct FzMomentum {
   int thermo;
   int periodic_y;
   const T *qx, *qy, *qz, *p;
-  const T *gx, *gy, *gz, *mu;           // variable properties (else null)
+  const T *gx, *gy, *gz, *mu;             // variable properties (else null)
   const T *fyqx, *fyqy, *fyqz, *fz, *fm;  // y wall planes of qx, qy, qz, zero momentum, viscosity
   FzOp in[FI_COUNT];
   FzPair<T> term[3][3];  // [component][direction]
@@ -71,17 +76,11 @@ struct FzMomentum {
   const T* fpres[3];
   T *m[3], *m0[3];       // right-hand sides (fractional-step increments) and their histories
   double rre, dt, gam, zeta, alpha;
-  const OpPlan* plans;   // device array of the full plans
-  const double* table;   // operator table (y metric)
+  const FzRow* rows;     // row tables of the y operators
 };
 
-// rows at each y wall that take the launch with the plans' boundary rows (the others compile the
-// bulk formulas only); valid when every y plan's bulk range covers rows 2 .. nout-3
-constexpr int kFzEdge = 4;
-
 // the right-hand side of momentum component c (0 x, 1 y, 2 z) with the fractional step
-// (m = dt*(gam*F + zeta*m0 + alpha*pfc), m0 = F); the advance q += m is left to launch_fz_update.
-// CD2 plans only (every bulk formula two-point); x and z periodic.
+// (m = dt*(gam*F + zeta*m0 + alpha*pfc), m0 = F); the advance q += m is left to launch_fz_update
 template <typename T>
 void launch_fz_momentum(const FzMomentum<T>& f, int c, cudaStream_t st);
 
@@ -96,5 +95,50 @@ void launch_fz_wall_visc(const FzMomentum<T>& f, T* fvisc2, T* fcomb, const T* f
 template <typename T>
 void launch_fz_update(T* ux, T* uy, T* uz, const T* mx, const T* my, const T* mz, const double* bulk, int n0,
                       int nc1, int np1, int n2, int s0, double v0, int s1, double v1, cudaStream_t st);
+
+// ---- energy equation (Solve_energy_eq, src/eq_energy.f90:148-458): per cell the sum over the three
+// directions of d/dx_j[-g_j h_face + rPrRen kappa_face dT/dx_j] (face interpolations of h and
+// kappa, temperature gradients), the fractional step and the rho*h update in one pass
+enum FzEInner { FE_H_X, FE_H_Y, FE_H_Z, FE_K_X, FE_K_Y, FE_K_Z, FE_T_X, FE_T_Y, FE_T_Z, FE_RH_Y, FE_COUNT };
+template <typename T>
+struct FzEnergy {
+  int n0, nc1, np1, n2;
+  const T *gx, *gy, *gz, *h, *k, *t;
+  const T *fh, *fk, *fqw, *fdtk;  // y wall planes: h, kappa, the wall gradient of T, kappa*dT/dy
+  FzOp in[FE_COUNT];
+  FzPair<T> term[3];              // conv + rPrRen*diffusion per direction (y: never merged)
+  T *rhoh, *rhs0;
+  double rpr, dt, gam, zeta;
+  const FzRow* rows;
+};
+// rhs0 <- F, rho*h += dt*(gam*F + zeta*rhs0) (energy_advance_kernel's arithmetic)
+template <typename T>
+void launch_fz_energy(const FzEnergy<T>& f, cudaStream_t st);
+// wall rows, before the energy pass (mode 0): kappa*dT/dy into planes side and side + 2 of out;
+// after it (mode 1): rho*h interpolated to the y faces into rows 0 and np1-1 of out (the dh_cpc
+// array launch_wall_props reads)
+template <typename T>
+void launch_fz_energy_walls(const FzEnergy<T>& f, int mode, T* out, cudaStream_t st);
+
+// ---- pressure update and projection (src/eq_momentum2.f90:1577-1660, :1890) with, for variable
+// properties, q = g / rho_face (convert_primary_conservative, src/para_conversion.f90:5-227)
+enum FzPInner { FP_PX, FP_PY, FP_PZ, FP_DX, FP_DY, FP_DZ, FP_COUNT };
+template <typename T>
+struct FzProject {
+  int n0, nc1, np1, n2;
+  int thermo, periodic_y;
+  const T* phi;
+  T *p, *ux, *uy, *uz;            // pressure, advanced variables (g with variable properties, else q)
+  T *qx, *qy, *qz;                // velocities (variable properties)
+  const T* rho;
+  const T *fphi, *fd;             // y planes of the pressure-correction gradient and of rho
+  FzOp in[FP_COUNT];              // rho to the faces (3), d/dx_i phi (3)
+  double coef;                    // -dt*alpha*sigma
+  int s0, s1;                     // y walls of uy set to v0 / v1
+  double v0, v1;
+  const FzRow* rows;
+};
+template <typename T>
+void launch_fz_project(const FzProject<T>& f, cudaStream_t st);
 
 }  // namespace chs

@@ -1863,6 +1863,31 @@ void launch_absmax(const double* a, int64_t n, double* partial, int npart, doubl
   absmax_final_kernel<<<1, 32, 0, st>>>(partial, npart, out);
 }
 
+// the three x-slab maxima of |a| of Check_element_mass_conservation (src/eq_continuity.f90:379-389):
+// slabs i in [0, 4), [4, n1 - 4), [n1 - 6, n1) of an (n1, n2, n3) array; out[0..2] hold the bit
+// patterns of non-negative doubles (their order is the values' order) and start at zero
+__global__ void absmax_slabs_kernel(const double* __restrict__ a, int n1, int64_t nrows,
+                                    unsigned long long* __restrict__ out) {
+  double m[3] = {0.0, 0.0, 0.0};
+  const int64_t n = nrows * n1;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(g % n1);
+    const double v = fabs(a[g]);
+    if (i < 4) m[0] = fmax(m[0], v);
+    if (i >= 4 && i < n1 - 4) m[1] = fmax(m[1], v);
+    if (i >= n1 - 6) m[2] = fmax(m[2], v);
+  }
+  for (int s = 0; s < 3; ++s) {
+    double v = m[s];
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out + s, (unsigned long long)__double_as_longlong(v));
+  }
+}
+void launch_absmax_slabs(const double* a, int n1, int64_t nrows, unsigned long long* out, cudaStream_t st) {
+  cudaMemsetAsync(out, 0, 3 * sizeof(unsigned long long), st);
+  absmax_slabs_kernel<<<148 * 4, 256, 0, st>>>(a, n1, nrows, out);
+}
+
 __global__ void ke_density_kernel(double* __restrict__ out, const double* __restrict__ u, const double* __restrict__ v,
                                   const double* __restrict__ w, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)

@@ -226,6 +226,9 @@ void launch_stats_update(const StatsIO<T>& s, cudaStream_t st);
 
 // max |a| and NaN flag into out[0], out[1] (two-pass with partials)
 void launch_absmax(const double* a, int64_t n, double* partial, int npart, double* out, cudaStream_t st);
+// max |a| over the x slabs [0, 4), [4, n1 - 4), [n1 - 6, n1) of nrows rows of length n1 (the three
+// monitors of Check_element_mass_conservation) as the bit patterns of the three doubles in out
+void launch_absmax_slabs(const double* a, int n1, int64_t nrows, unsigned long long* out, cudaStream_t st);
 // 0.5*(u^2+v^2+w^2) over ccc
 void launch_ke_density(double* out, const double* u, const double* v, const double* w, int64_t n, cudaStream_t st);
 

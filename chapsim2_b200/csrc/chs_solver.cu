@@ -126,8 +126,9 @@ struct chs_handle {
   // fused substep kernels for the explicit schemes (chs_fused.cu): 1 on by default, 0 the
   // operator-by-operator path (chs_set_fusion)
   int kfuse = 1;
-  OpPlan* fz_plans = nullptr;                                    // device copies of every plan
-  std::map<std::tuple<int, int, int, int, int>, int> fz_index;  // plan key -> slot in fz_plans
+  FzRow* fz_rows = nullptr;  // device row tables of the y operators (chs_fused.cuh)
+  // plan key -> first row of its table in fz_rows (-1: no table: periodic, or not representable)
+  std::map<std::tuple<int, int, int, int, int>, int> fz_index;
   long long launches = 0;
   std::string err;
 
@@ -212,7 +213,7 @@ struct chs_handle {
   std::vector<cudaEvent_t> evpool;
   int lane_last[kLanes];
   int fence = -1, cur_node = -1;
-  struct Bufs { const void* p[12]; int n = 0; };
+  struct Bufs { const void* p[16]; int n = 0; };
   std::vector<int> pend_r, pend_w, deps;
   int buf_id(const void* q) const {
     const uintptr_t a = reinterpret_cast<uintptr_t>(q);
@@ -408,7 +409,7 @@ struct chs_handle {
 // buffers a launch reads or writes (null entries are ignored)
 template <class... Ps>
 chs_handle::Bufs bufs(Ps... ps) {
-  static_assert(sizeof...(Ps) <= 12, "too many buffers");
+  static_assert(sizeof...(Ps) <= 16, "too many buffers");
   chs_handle::Bufs b;
   ((b.p[b.n++] = static_cast<const void*>(ps)), ...);
   return b;
@@ -1090,20 +1091,77 @@ void upload_table(chs_handle* H) {
                      H->st));
 }
 
-// every plan built so far as one device array, so the fused kernels can read the boundary rows
-// of any plan they use (slot per plan key in fz_index)
-void upload_fz_plans(chs_handle* H) {
+// The row table of a y operator with walls for the fused kernels: every output row as at most three
+// taps over the input line plus the two wall planes, with 1/h and the row's y metric folded into the
+// weights (the plan's bulk formula on its bulk rows, its boundary rows elsewhere, the Neumann
+// overrides as a unit wall weight).  False when the plan does not fit that form.
+bool fz_rows_of(const chs_handle* H, int fam, const OpPlan& P, std::vector<FzRow>& out) {
+  if (P.tdma || P.r2 != 0.0) return false;
+  const int nin = P.nin, nout = P.nout;
+  const std::vector<double>& tab = H->book.table;
+  for (int p = 0; p < nout; ++p) {
+    FzRow r{};
+    const int pc = p < 0 ? 0 : (p > nin - 1 ? nin - 1 : p);  // a valid input row for unused taps
+    for (int t = 0; t < 3; ++t) r.o[t] = pc - p;
+    if (P.neu1 && p == 0) {
+      r.wb[0] = 1.0;
+      r.flags = 2;
+    } else if (P.neu2 && p == nout - 1) {
+      r.wb[1] = 1.0;
+      r.flags = 4;
+    } else {
+      const double sc = P.dd * (P.lmap >= 0 ? tab[P.lmap + p] : 1.0);
+      if (p >= P.b_lo && p <= P.b_hi) {
+        const double r1 = P.r1;
+        if (fam == M1P2C) { r.o[0] = 0; r.o[1] = 1; r.w[0] = r1 * sc; r.w[1] = r1 * sc; }
+        else if (fam == M1C2P) { r.o[0] = 0; r.o[1] = -1; r.w[0] = r1 * sc; r.w[1] = r1 * sc; }
+        else if (fam == D1C2P) { r.o[0] = 0; r.o[1] = -1; r.w[0] = r1 * sc; r.w[1] = -r1 * sc; }
+        else if (fam == D1P2C) { r.o[0] = 1; r.o[1] = 0; r.w[0] = r1 * sc; r.w[1] = -r1 * sc; }
+        else return false;
+      } else {
+        for (int s = 0; s < P.nspec; ++s) {
+          const SpecialRow& R = P.sp[s];
+          if (R.row != p) continue;
+          if (R.nt > 3 || R.wb[2] != 0.0 || R.wb[3] != 0.0) return false;
+          for (int t = 0; t < R.nt; ++t) {
+            r.o[t] = R.idx[t] - p;
+            r.w[t] = R.w[t] * sc;
+          }
+          if (R.nt == 3) r.flags |= 1;
+          if (R.wb[0] != 0.0) { r.wb[0] = R.wb[0] * sc; r.flags |= 2; }
+          if (R.wb[1] != 0.0) { r.wb[1] = R.wb[1] * sc; r.flags |= 4; }
+        }
+      }
+    }
+    for (int t = 0; t < 3; ++t)
+      if (p + r.o[t] < 0 || p + r.o[t] >= nin) return false;
+    out.push_back(r);
+  }
+  return true;
+}
+
+// the row tables of every y plan built so far, uploaded as one device array (fz_index gives each
+// plan's first row)
+void upload_fz_rows(chs_handle* H) {
   drop_graphs(H);
-  std::vector<OpPlan> v;
+  std::vector<FzRow> v;
   H->fz_index.clear();
   for (const auto& kv : H->plans) {
-    H->fz_index[kv.first] = (int)v.size();
-    v.push_back(kv.second);
+    const int d = std::get<0>(kv.first), fam = std::get<1>(kv.first);
+    int at = -1;
+    if (d == 1 && !kv.second.wrap) {
+      std::vector<FzRow> r;
+      if (fz_rows_of(H, fam, kv.second, r)) {
+        at = (int)v.size();
+        v.insert(v.end(), r.begin(), r.end());
+      }
+    }
+    H->fz_index[kv.first] = at;
   }
-  if (H->fz_plans) { CK(cudaFreeAsync(H->fz_plans, H->st)); H->fz_plans = nullptr; }
-  if (v.empty()) return;
-  CK(cudaMallocAsync(&H->fz_plans, v.size() * sizeof(OpPlan), H->st));
-  CK(cudaMemcpyAsync(H->fz_plans, v.data(), v.size() * sizeof(OpPlan), cudaMemcpyHostToDevice, H->st));
+  if (H->fz_rows) { CK(cudaFreeAsync(H->fz_rows, H->st)); H->fz_rows = nullptr; }
+  if (v.empty()) v.push_back(FzRow{});  // periodic y: no tables, a valid pointer all the same
+  CK(cudaMallocAsync(&H->fz_rows, v.size() * sizeof(FzRow), H->st));
+  CK(cudaMemcpyAsync(H->fz_rows, v.data(), v.size() * sizeof(FzRow), cudaMemcpyHostToDevice, H->st));
   // the host vector goes out of scope: wait for the copy
   CK(cudaStreamSynchronize(H->st));
 }
@@ -1154,6 +1212,7 @@ void poisson_device(chs_handle* H, T* rhs) {
 struct FzBuild {
   chs_handle* H;
   bool ok = true;
+  const OpPlan* plan = nullptr;  // the plan of the last op()
   FzOp op(int d, int fam, Pair bc, bool has_fbc) {
     FzOp o{};
     auto key = std::make_tuple(d, fam, bc.v[0], bc.v[1], has_fbc ? 1 : 0);
@@ -1161,20 +1220,17 @@ struct FzBuild {
     auto ix = H->fz_index.find(key);
     if (it == H->plans.end() || ix == H->fz_index.end()) { ok = false; return o; }
     const OpPlan& P = it->second;
-    // CD2 only: every bulk formula two-point; x and z periodic (bulk formula everywhere); y plans
-    // with walls: bulk range covering rows 2 .. nout-3, so that the rows kFzEdge .. n-1-kFzEdge of
-    // every fused output use the bulk formula at every level
-    if (P.tdma || P.r2 != 0.0 || (d != 1 && !P.wrap) || (d == 1 && H->periodic_y != (P.wrap != 0))) ok = false;
+    // CD2 only: every bulk formula two-point; x and z periodic (bulk formula everywhere); a y
+    // plan either periodic too or with a row table
+    if (P.tdma || P.r2 != 0.0) ok = false;
+    if (d != 1 && !P.wrap) ok = false;
+    if (d == 1 && (H->periodic_y != (P.wrap != 0) || (!P.wrap && ix->second < 0))) ok = false;
+    // the fused kernels' interior blocks (rows 4 .. n-5) take every y operator's bulk formula at
+    // every level: each bulk range must cover rows 2 .. nout-3
     if (d == 1 && !P.wrap && (P.b_lo > 2 || P.b_hi < P.nout - 3)) ok = false;
-    o.kind = P.wrap ? 0 : 1;
-    o.b_lo = P.b_lo;
-    o.b_hi = P.b_hi;
-    o.lmap = (int)P.lmap;
-    o.neu = (P.neu1 ? 1 : 0) | (P.neu2 ? 2 : 0);
-    o.nout = P.nout;
-    o.plan = ix->second;
+    o.row = P.wrap ? -1 : ix->second;
+    plan = &P;
     o.r1 = P.r1;
-    o.r2 = P.r2;
     o.dd = P.dd;
     return o;
   }
@@ -1192,9 +1248,14 @@ struct FzBuild {
     } else {
       p.a = op(d, fam, bc1, f1 != nullptr);
       p.fa = f1;
+      const OpPlan* pa = plan;
       p.b = op(d, fam, bc2, f2 != nullptr);
       p.fb = f2;
       p.merged = 0;
+      // the interior rows run one operator on the combined expression: one bulk formula
+      if (pa && plan && (pa->r1 != plan->r1 || pa->dd != plan->dd || pa->lmap != plan->lmap)) ok = false;
+      // periodic directions run one operator on the combined expression: one bulk formula
+      if ((d != 1 || H->periodic_y) && (p.a.r1 != p.b.r1 || p.a.dd != p.b.dd)) ok = false;
     }
     return p;
   }
@@ -1205,7 +1266,7 @@ struct FzBuild {
 // Returns false (nothing launched) when the configuration needs the operator path.
 template <typename T>
 bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz) {
-  if (!H->kfuse || H->iacc != ACC_CD2 || !H->fz_plans) return false;
+  if (!H->kfuse || H->iacc != ACC_CD2 || !H->fz_rows) return false;
   auto A = [](double* p) { return reinterpret_cast<T*>(p); };
   const auto& B = H->ibc;
   const bool TH = H->thermo;
@@ -1291,8 +1352,7 @@ bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz)
   F.m0[0] = A(H->mx0); F.m0[1] = A(H->my0); F.m0[2] = A(H->mz0);
   F.rre = H->rre;
   F.dt = H->dt; F.gam = H->tGamma[isub]; F.zeta = H->tZeta[isub]; F.alpha = H->tAlpha[isub];
-  F.plans = H->fz_plans;
-  F.table = H->table;
+  F.rows = H->fz_rows;
   const double nf = (double)sizeof(T) * H->n_ccc;
   if (H->fbcy_velo) {
     PROFD(H, 3, (double)sizeof(T) * 16.0 * nc0 * nc2,
@@ -1300,17 +1360,20 @@ bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz)
           bufs(H->fb_visc2, H->fb_comb), launch_fz_wall_visc<T>(F, A(H->fb_visc2), A(H->fb_comb), fconv2, st));
     H->launches++;
   }
-  // per component: rhs0 read and written, rhs written, and a third of the shared inputs q (3), p
-  // [+ g (3), mu] (the three components together read each input once); the three run concurrently
-  // on the dataflow lanes
-  double* mo[3] = {H->mx, H->my, H->mz};
-  double* m0[3] = {H->mx0, H->my0, H->mz0};
-  for (int c = 0; c < 3; ++c) {
-    PROFD(H, 4, nf * ((TH ? 8.0 : 4.0) / 3.0 + 3.0),
-          bufs(H->qx, H->qy, H->qz, H->pres, TH ? H->gx : nullptr, TH ? H->gy : nullptr, TH ? H->gz : nullptr,
-               TH ? H->mVisc : nullptr, H->fb_comb, H->fb_visc2, H->fb_qx, H->fb_qz),
-          bufs(mo[c], m0[c]), launch_fz_momentum<T>(F, c, st));
-    H->launches++;
+  {
+    // one pass per component: rhs0 read and written, rhs written, and a third of the shared inputs
+    // q (3), p [+ g (3), mu] (the three components together read each input once); the three run
+    // concurrently on the dataflow lanes
+    double* mo[3] = {H->mx, H->my, H->mz};
+    double* m0[3] = {H->mx0, H->my0, H->mz0};
+    for (int c = 0; c < 3; ++c) {
+      PROFD(H, 4, nf * ((TH ? 8.0 : 4.0) / 3.0 + 3.0),
+            bufs(H->qx, H->qy, H->qz, H->pres, TH ? H->gx : nullptr, TH ? H->gy : nullptr, TH ? H->gz : nullptr,
+                 TH ? H->mVisc : nullptr, H->fb_comb, H->fb_visc2, H->fb_qx, H->fb_qz, H->fb_qy,
+                 TH ? H->fb_m : nullptr),
+            bufs(mo[c], m0[c]), launch_fz_momentum<T>(F, c, st));
+      H->launches++;
+    }
   }
   const double* bulk = nullptr;
   if (H->idriven == 1) {
@@ -1323,6 +1386,124 @@ bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz)
   PROFD(H, 3, nf * 9.0, bufs(H->mx, H->my, H->mz, bulk), bufs(ux, uy, uz),
         launch_fz_update<T>(A(ux), A(uy), A(uz), A(H->mx), A(H->my), A(H->mz), bulk, nc0, nc1, np1, nc2, w0,
                             H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+  H->launches++;
+  return true;
+}
+
+// Energy equation in four launches (wall gradients, fused energy pass, property update, wall
+// states) instead of the ~14 of the operator path; false when it needs the operator path.
+template <typename T>
+bool fused_energy(chs_handle* H, int isub) {
+  if (!H->kfuse || H->iacc != ACC_CD2 || !H->fz_rows || H->periodic_y) return false;
+  auto A = [](double* p) { return reinterpret_cast<T*>(p); };
+  const auto& B = H->ibc;
+  const T* any = A(H->fb_maxp);
+  const Pair per = P2(kPer2);
+  FzBuild b{H};
+  FzEnergy<T> F{};
+  F.n0 = H->nc[0]; F.nc1 = H->nc[1]; F.np1 = H->np[1]; F.n2 = H->nc[2];
+  F.gx = A(H->gx); F.gy = A(H->gy); F.gz = A(H->gz);
+  F.h = A(H->hEnth); F.k = A(H->kCond); F.t = A(H->tTemp);
+  F.fh = A(H->fb_h); F.fk = A(H->fb_k); F.fqw = A(H->fb_qw); F.fdtk = A(H->fb_dtk);
+  // the operator path's energy_body_t plans
+  F.in[FE_H_X] = b.op(0, M1C2P, per, true);
+  F.in[FE_H_Y] = b.op(1, M1C2P, H->ftpy, true);
+  F.in[FE_H_Z] = b.op(2, M1C2P, per, true);
+  F.in[FE_K_X] = b.op(0, M1C2P, per, true);
+  F.in[FE_K_Y] = b.op(1, M1C2P, H->ftpy, true);
+  F.in[FE_K_Z] = b.op(2, M1C2P, per, true);
+  F.in[FE_T_X] = b.op(0, D1C2P, P2(B[0][V_TM]), true);
+  F.in[FE_T_Y] = b.op(1, D1C2P, P2(B[1][V_TM]), true);
+  F.in[FE_T_Z] = b.op(2, D1C2P, P2(B[2][V_TM]), true);
+  F.in[FE_RH_Y] = b.op(1, M1C2P, H->ftpy, false);
+  F.term[0] = b.pair<T>(0, D1P2C, H->ebcx_conv, any, H->ebcx_difu, any, (const T*)nullptr);
+  F.term[1].a = b.op(1, D1P2C, H->ebcy_conv, false);
+  F.term[1].fa = nullptr;
+  F.term[1].b = b.op(1, D1P2C, H->ebcy_difu, true);
+  F.term[1].fb = A(H->fb_dtk);
+  F.term[1].merged = 0;
+  F.term[2] = b.pair<T>(2, D1P2C, H->ebcz_conv, (const T*)nullptr, H->ebcz_difu, (const T*)nullptr,
+                        (const T*)nullptr);
+  if (!b.ok) return false;
+  F.rhoh = A(H->rhoh);
+  F.rhs0 = A(H->erhs0);
+  F.rpr = H->rPrRen;
+  F.dt = H->dt; F.gam = H->tGamma[isub]; F.zeta = H->tZeta[isub];
+  F.rows = H->fz_rows;
+  const int nc0 = H->nc[0], nc2 = H->nc[2], np1 = H->np[1];
+  const double nf = (double)sizeof(T) * H->n_ccc;
+  PROFD(H, 3, (double)sizeof(T) * 12.0 * nc0 * nc2, bufs(H->tTemp, H->kCond, H->fb_qw, H->fb_k), bufs(H->fb_dtk),
+        launch_fz_energy_walls<T>(F, 0, A(H->fb_dtk), st));
+  H->launches++;
+  // read g (3), h, kappa, T, rhs0, rho*h; write rhs0, rho*h
+  PROFD(H, 4, nf * 10.0,
+        bufs(H->gx, H->gy, H->gz, H->hEnth, H->kCond, H->tTemp, H->fb_h, H->fb_k, H->fb_qw, H->fb_dtk),
+        bufs(H->rhoh, H->erhs0), launch_fz_energy<T>(F, st));
+  H->launches++;
+  if (H->mlp_mode != 1) {
+    PROFD(H, 3, nf * 6.0, bufs(H->rhoh), bufs(H->hEnth, H->tTemp, H->kCond, H->dDens, H->mVisc),
+          launch_property_update<T>(H->tab, A(H->rhoh), A(H->hEnth), A(H->tTemp), A(H->kCond), A(H->dDens),
+                                    A(H->mVisc), (int64_t)H->n_ccc, st));
+  } else {
+    PROFD(H, 3, 6.0 * sizeof(T) * H->n_ccc, bufs(H->rhoh, H->mlp_wpack),
+          bufs(H->hEnth, H->tTemp, H->kCond, H->dDens, H->mVisc, H->mlp_nfb),
+          launch_mlp_props<T>(H->tab, H->mlp_norm, H->mlp_small, H->mlp_check, H->mlp_wpack, A(H->rhoh),
+                              A(H->hEnth), A(H->tTemp), A(H->kCond), A(H->dDens), A(H->mVisc), (int64_t)H->n_ccc,
+                              H->mlp_nfb, st));
+  }
+  H->launches++;
+  const int s0 = B[1][V_TM][0] == BC_NEUMANN, s1 = B[1][V_TM][1] == BC_NEUMANN;
+  if (s0 || s1) {
+    PROFD(H, 3, (double)sizeof(T) * 8.0 * nc0 * nc2, bufs(H->rhoh), bufs(H->dh_cpc),
+          launch_fz_energy_walls<T>(F, 1, A(H->dh_cpc), st));
+    PROFD(H, 3, 10.0 * sizeof(T) * nc0 * nc2, bufs(H->dh_cpc), bufs(H->fb_h, H->fb_k, H->fb_m, H->fb_d),
+          launch_wall_props<T>(H->tab, A(H->dh_cpc), nc0, np1, nc2, s0, s1, A(H->fb_h), A(H->fb_k), A(H->fb_m),
+                               A(H->fb_d), st));
+    H->launches += 2;
+  }
+  return true;
+}
+
+// Pressure update, projection, wall enforcement and (variable properties) q = g / rho_face in one
+// launch instead of up to nine; false when the configuration needs the operator path.
+template <typename T>
+bool fused_project(chs_handle* H, int isub, double* ux, double* uy, double* uz, int w0, int w1) {
+  if (!H->kfuse || H->iacc != ACC_CD2 || !H->fz_rows) return false;
+  auto A = [](double* p) { return reinterpret_cast<T*>(p); };
+  const auto& B = H->ibc;
+  const bool TH = H->thermo;
+  const T* fypr = H->periodic_y ? nullptr : A(H->fb_pr);
+  FzBuild b{H};
+  FzProject<T> F{};
+  F.n0 = H->nc[0]; F.nc1 = H->nc[1]; F.np1 = H->np[1]; F.n2 = H->nc[2];
+  F.thermo = TH ? 1 : 0;
+  F.periodic_y = H->periodic_y ? 1 : 0;
+  F.phi = A(H->pcor);
+  F.p = A(H->pres);
+  F.ux = A(ux); F.uy = A(uy); F.uz = A(uz);
+  F.fphi = fypr;
+  F.in[FP_DX] = b.op(0, D1C2P, P2(B[0][V_PR]), true);
+  F.in[FP_DY] = b.op(1, D1C2P, P2(B[1][V_PR]), fypr != nullptr);
+  F.in[FP_DZ] = b.op(2, D1C2P, P2(B[2][V_PR]), true);
+  if (TH) {
+    if (H->periodic_y) return false;
+    const Pair per = P2(kPer2);
+    F.qx = A(H->qx); F.qy = A(H->qy); F.qz = A(H->qz);
+    F.rho = A(H->dDens);
+    F.fd = A(H->fb_d);
+    F.in[FP_PX] = b.op(0, M1C2P, per, true);
+    F.in[FP_PY] = b.op(1, M1C2P, H->ftpy, true);
+    F.in[FP_PZ] = b.op(2, M1C2P, per, true);
+  }
+  if (!b.ok) return false;
+  F.coef = -(H->dt * H->tAlpha[isub] * H->sigma2p);
+  F.s0 = w0; F.s1 = w1;
+  F.v0 = H->fbcy[V_QY][0]; F.v1 = H->fbcy[V_QY][1];
+  F.rows = H->fz_rows;
+  const double nf = (double)sizeof(T) * H->n_ccc;
+  PROFD(H, 3, nf * (TH ? 13.0 : 9.0), bufs(H->pcor, H->fb_pr, TH ? H->dDens : nullptr, TH ? H->fb_d : nullptr),
+        bufs(H->pres, ux, uy, uz, TH ? H->qx : nullptr, TH ? H->qy : nullptr, TH ? H->qz : nullptr),
+        launch_fz_project<T>(F, st));
   H->launches++;
   return true;
 }
@@ -1527,6 +1708,7 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
     run_fused<T>(H, t, A(H->pcor), s_ccc, EP_STORE, nullptr, isub, nullptr, nullptr, false, true);
   }
   poisson_device<T>(H, A(H->pcor));
+  if (fused_project<T>(H, isub, ux, uy, uz, w0, w1)) return;
   PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, bufs(H->pcor), bufs(H->pres),
         launch_axpby(A(H->pres), A(H->pres), 1.0, A(H->pcor), 1.0, (int64_t)H->n_ccc, st));
   H->launches++;
@@ -1556,6 +1738,7 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
 // rho*h (the reference indexes np(1)).
 template <typename T>
 void energy_body_t(chs_handle* H, int isub) {
+  if (fused_energy<T>(H, isub)) return;
   auto A = [](double* p) { return reinterpret_cast<T*>(p); };
   const int nc0 = H->nc[0], nc1 = H->nc[1], nc2 = H->nc[2];
   const int np0 = H->np[0], np1 = H->np[1], np2 = H->np[2];
@@ -1649,7 +1832,7 @@ void prepare_plans(chs_handle* H) {
   }
   for (const auto& x : r) H->plan(x.d, x.fam, x.bc, x.f);
   upload_table(H);
-  upload_fz_plans(H);
+  upload_fz_rows(H);
 }
 
 // operator plans of the variable-property path (energy equation, g and mu interpolations,
@@ -1672,7 +1855,7 @@ void prepare_thermo_plans(chs_handle* H) {
   };
   for (const auto& x : r) H->plan(x.d, x.fam, x.bc, x.f);
   upload_table(H);
-  upload_fz_plans(H);
+  upload_fz_rows(H);
 }
 
 // host-side lookup of the initial state from T (ftp_refresh_thermal_properties_from_T_undim,
@@ -2490,7 +2673,7 @@ int chs_destroy(chs_handle* H) {
   if (H->st) cudaStreamSynchronize(H->st);
   drop_graphs(H);
   if (H->table) cudaFree(H->table);
-  if (H->fz_plans) cudaFree(H->fz_plans);
+  if (H->fz_rows) cudaFree(H->fz_rows);
   for (auto& a : H->allocs) cudaFree(a.first);
   for (int l = 1; l < chs_handle::kLanes; ++l)
     if (H->lane[l]) cudaStreamDestroy(H->lane[l]);
@@ -3079,6 +3262,10 @@ int chs_diagnostics(chs_handle* H, chs_diag* out) {
     run_op(H, 1, D1P2C, by, nullptr, src(uy), s_cpc, H->div, true, 1.0);
     run_op(H, 2, D1P2C, bz, nullptr, src(uz), s_ccp, H->div, true, 1.0);
     launch_absmax(H->div, (int64_t)H->n_ccc, H->partial, H->npart, H->scal + 2, H->st);
+    // the reference's three x-slab monitors of the same divergence (Check_element_mass_conservation,
+    // src/eq_continuity.f90:379-389; its d(rho)/dt term is zero there, rho_m1 = rho after the
+    // property update)
+    launch_absmax_slabs(H->div, nc0, (int64_t)nc1 * nc2, reinterpret_cast<unsigned long long*>(H->scal + 8), H->st);
     // kinetic energy of the P2C-interpolated velocities (src/io_monitor.f90:209-241)
     run_op(H, 0, M1P2C, bx, fmaxp, src(qx), s_pcc, H->qxix, false, 1.0);
     run_op(H, 1, M1P2C, by, H->periodic_y ? nullptr : fqy, src(qy), s_cpc, H->qyiy, false, 1.0);
@@ -3086,10 +3273,11 @@ int chs_diagnostics(chs_handle* H, chs_diag* out) {
     launch_ke_density(H->qxdx, H->qxix, H->qyiy, H->qziz, (int64_t)H->n_ccc, H->st);
     launch_weighted_mean(H->qxdx, H->wy, nc0, nc1, nc2, H->partial, H->npart, H->scal + 4, H->vol, H->st);
     launch_weighted_mean(qx, H->wy, H->np[0], nc1, nc2, H->partial, H->npart, H->scal + 5, H->vol, H->st);
-    H->launches += 7;
-    double s[8];
-    CK(cudaMemcpyAsync(s, H->scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, H->st));
+    H->launches += 8;
+    double s[11];
+    CK(cudaMemcpyAsync(s, H->scal, 11 * sizeof(double), cudaMemcpyDeviceToHost, H->st));
     CK(cudaStreamSynchronize(H->st));
+    for (int m = 0; m < 3; ++m) out->mcon[m] = s[8 + m];
     out->max_div = s[2];
     out->nan_flag = s[3] != 0.0 ? 1 : 0;
     out->bulk_ke = s[4];

@@ -27,6 +27,8 @@ def main():
                     help="heated case: train the property surrogate for this many epochs and use it")
     ap.add_argument("--graph-profile", action="store_true",
                     help="after the substeps, print a per-launch profile of substep 1 replayed as a graph")
+    ap.add_argument("--fusion", type=int, default=1, choices=[0, 1],
+                    help="CD2 fused substep kernels (1, the default) or the operator path (0)")
     ap.add_argument("--poisson", default="fishpack", choices=["fishpack", "3dfft"],
                     help="channel cases: FISHPACK with tanh stretching, or the 3D-FFT solver (poisson_010) "
                          "with 3FMD stretching (rstret 0.25)")
@@ -45,6 +47,7 @@ def main():
         cfg = C.taylor_green(a.nc[0], iacc=a.iacc)
         f = I.taylor_green_fields(cfg)
     g = S.Solver(cfg, precision=S.CHS_MIXED if a.precision == "mixed" else S.CHS_FP64)
+    g.set_fusion(a.fusion)
     g.set_fields(*f)
     if tc is not None:
         g.thermo_init(tc)
@@ -55,7 +58,7 @@ def main():
     for i in range(a.substeps):
         g.substep(1 + i % 3)
     if a.graph_profile:
-        kinds = ("line_op", "fft", "ysolve", "elementwise")
+        kinds = ("line_op", "fft", "ysolve", "elementwise", "fused_momentum")
         prof = g.profile_substep_graph(1)
         for i, r in enumerate(prof):
             print(f"{i:3d} {kinds[r['kind']]:11s} dir {r['dir']:2d} {r['bytes'] / 1e6:9.1f} MB {r['ms'] * 1e3:9.1f} us "

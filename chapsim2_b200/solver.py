@@ -58,7 +58,7 @@ MLP_NPARAM = 8708
 
 class ChsDiag(ctypes.Structure):
     _fields_ = [("max_div", ctypes.c_double), ("bulk_ke", ctypes.c_double), ("bulk_u", ctypes.c_double),
-                ("last_bulk_rhs", ctypes.c_double), ("nan_flag", ctypes.c_int)]
+                ("last_bulk_rhs", ctypes.c_double), ("nan_flag", ctypes.c_int), ("mcon", ctypes.c_double * 3)]
 
 
 EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field", "chs_momentum_substep",
@@ -309,7 +309,7 @@ class Solver:
         self._check(self.L.chs_set_lanes(self.h, int(lanes)), "chs_set_lanes")
 
     def set_fusion(self, on):
-        """Fused substep kernels for the explicit schemes (True, the default) or the operator path."""
+        """Fused CD2 substep kernels (True, the default) or the operator path (False)."""
         self._check(self.L.chs_set_fusion(self.h, 1 if on else 0), "chs_set_fusion")
 
     # ---- MLP surrogate of the property update
@@ -392,7 +392,7 @@ class Solver:
         d = ChsDiag()
         self._check(self.L.chs_diagnostics(self.h, ctypes.byref(d)), "chs_diagnostics")
         return dict(max_div=d.max_div, bulk_ke=d.bulk_ke, bulk_u=d.bulk_u, last_bulk_rhs=d.last_bulk_rhs,
-                    nan_flag=d.nan_flag)
+                    nan_flag=d.nan_flag, mcon=[d.mcon[0], d.mcon[1], d.mcon[2]])
 
     def op3d(self, d, fam, ibc, fi, fbc2d=None):
         fi = np.ascontiguousarray(fi, np.float64)

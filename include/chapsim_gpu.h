@@ -88,6 +88,8 @@ typedef struct chs_diag {
   double bulk_u;       /* volume-averaged qx */
   double last_bulk_rhs;/* last mass-flux correction removed from mx_rhs */
   int nan_flag;        /* 1 if a NaN/Inf was found */
+  double mcon[3];      /* Check_element_mass_conservation's monitors (src/eq_continuity.f90:379-389): max |div|
+                          over the x slabs i = 1:4, 5:n-4 and n-5:n (1-based), the fl%mcon(1:3) of the reference */
 } chs_diag;
 
 /* Replaces initialise_fft / Prepare_LHS_coeffs_for_operations / allocation

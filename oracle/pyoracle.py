@@ -213,6 +213,15 @@ class Oracle:
         lib().orc_divergence(self.h, _p(d))
         return d
 
+    def mass_conservation(self):
+        """Check_element_mass_conservation (src/eq_continuity.f90:337-397): max |div + drho/dt| over
+        the x slabs 1:4, 5:n-4 and n-5:n (1-based, :379-389), i.e. fl%mcon(1:3).  drho/dt is zero
+        there: the property update has already set rho_m1 = rho (src/eq_energy.f90:48-49)."""
+        import numpy as np
+        d = np.abs(self.divergence())
+        n = d.shape[2]
+        return [float(d[:, :, 0:4].max()), float(d[:, :, 4:n - 4].max()), float(d[:, :, n - 6:n].max())]
+
     def bulk_ke(self):
         return lib().orc_bulk_ke(self.h)
 
