@@ -11,7 +11,10 @@ frozen.  --workload channel runs the flow-only channel instead; --workload
 large the Re_tau ~ 395 heated channel, 384 x 256 x 384 cells (37.7M), beta =
 1.8, Re_b = 6875 (its CPU sample is one substep per step); --workload
 channel3fmd the flow-only channel on the 3FMD grid (beta = 0.25) with the
-3D-FFT Poisson solver for y walls (poisson_010).
+3D-FFT Poisson solver for y walls (poisson_010); --workload tgv the Taylor-Green
+vortex 64^3 at Re 1600 with the CP6 compact operators (line solves) and the 3D-FFT
+Poisson solver (poisson_000).  --iacc picks another scheme (CP4/CP6 channels run
+the compact operators with their line solves).
 
 `value` is the plain FP64 path (the drop-in).  `forms` adds the mixed form
 (FP32 fields, operators and RHS; FP64 Poisson, mass-flux mean and checks) on
@@ -52,11 +55,18 @@ METRIC = "Mcell-RK3-substeps/s on 1 B200: mixed+MLP vs plain FP64 at ≤1e-5 L2;
 UNIT = "Mcell-substeps/s"
 # compulsory traffic per cell per RK3 substep: flow-only FP64 (30 words), variable-property FP64
 # (57 words: + energy 10, property update 7, momentum with g and mu 4, drho/dt 2, g->q 4)
-BYTES_PER_CELL_SUBSTEP = {"channel": 240.0, "heated": 456.0, "large": 456.0, "channel3fmd": 240.0}
+BYTES_PER_CELL_SUBSTEP = {"channel": 240.0, "heated": 456.0, "large": 456.0, "channel3fmd": 240.0, "tgv": 240.0}
 
 
-def workload(kind="heated", nc=(128, 96, 128), iacc=C.IACCU_CD2):
-    """(cfg, fields, thermo config or None)."""
+def workload(kind="heated", nc=(128, 96, 128), iacc=None):
+    """(cfg, fields, thermo config or None).  iacc None: CP6 for the Taylor-Green box, CD2 otherwise."""
+    if iacc is None:
+        iacc = C.IACCU_CP6 if kind == "tgv" else C.IACCU_CD2
+    if kind == "tgv":
+        # Taylor-Green vortex 64^3, Re 1600, dt 1e-3, 3D-FFT Poisson dividing by the compact scheme's
+        # modified wavenumbers: the compact (line-solve) operators on the timed path
+        cfg = C.taylor_green(nc[0] if tuple(nc) != (128, 96, 128) else 64, iacc=iacc, dt=1e-3)
+        return cfg, I.taylor_green_fields(cfg), None
     if kind == "heated":
         cfg, tc = C.heated_channel(nc=nc, iacc=iacc)
     elif kind == "large":
@@ -71,16 +81,22 @@ def workload(kind="heated", nc=(128, 96, 128), iacc=C.IACCU_CD2):
     return cfg, fields, tc
 
 
+ACC_NAMES = {C.IACCU_CD2: "CD2", C.IACCU_CD4: "CD4", C.IACCU_CP4: "CP4", C.IACCU_CP6: "CP6"}
+
+
 def describe(cfg, tc):
     n = f"{cfg.nc[0]}x{cfg.nc[1]}x{cfg.nc[2]}"
+    acc = ACC_NAMES[cfg.iacc]
+    if cfg.periodic_y:
+        return f"Taylor-Green vortex {n}, Re={cfg.ren:g}, dt={cfg.dt:g}, 3D-FFT Poisson (poisson_000), {acc}"
     if tc is None and cfg.ifft == C.FFT_2DECOMP_3DFFT:
         return (f"channel {n} flow-only, 3FMD stretching beta={cfg.rstret:g}, 3D-FFT Poisson (poisson_010), "
-                f"Re_b={cfg.ren:g}, CD2")
+                f"Re_b={cfg.ren:g}, {acc}")
     if tc is None:
-        return f"channel {n} flow-only, beta={20.0 * cfg.rstret:g}, Re_b={cfg.ren:g}, CD2"
+        return f"channel {n} flow-only, beta={20.0 * cfg.rstret:g}, Re_b={cfg.ren:g}, {acc}"
     beta, reb = 20.0 * cfg.rstret, cfg.ren
     return (f"heated channel {n}, variable properties (synthetic 4096-row table), isoflux walls, beta={beta:g}, "
-            f"Re_b={reb:g}, CD2")
+            f"Re_b={reb:g}, {acc}")
 
 
 def measured_peaks():
@@ -208,14 +224,24 @@ def run_reference(args, cfg, fields, tc, world, rank, dist):
     }
 
 
-def roofline(prof, peak, peak_kind, workload):
+CLASSES = ("line_op", "fft", "ysolve", "elementwise", "fused")
+
+
+def roofline(prof, peak, peak_kind, workload, class_ms=None):
+    """Roofline of the dominant kernel class.  prof: the per-launch profile of one substep (algorithmic
+    bytes of every launch); class_ms: per class, the time of one replay of the substep's graph holding
+    only that class's launches (no per-launch event nodes), which then replaces the event sums."""
     by = {}
     for r in prof:
-        k = ("line_op", "fft", "ysolve", "elementwise", "fused_momentum")[r["kind"]]
+        k = CLASSES[r["kind"]]
         a = by.setdefault(k, {"ms": 0.0, "bytes": 0.0, "n": 0})
         a["ms"] += r["ms"]
         a["bytes"] += r["bytes"]
         a["n"] += 1
+    if class_ms:
+        for k in by:
+            by[k]["ms_events"] = by[k]["ms"]
+            by[k]["ms"] = class_ms[k]
     dom = max(by, key=lambda k: by[k]["ms"])
     a = by[dom]
     achieved = a["bytes"] / (a["ms"] * 1e-3) / 1e9
@@ -231,7 +257,7 @@ def roofline(prof, peak, peak_kind, workload):
             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
             "bytes_per_launch": a["bytes"] / a["n"], "ms_per_launch": a["ms"] / a["n"], "launches": a["n"],
             "share_of_substep": a["ms"] / sum(v["ms"] for v in by.values()),
-            "classes": {k: {"ms": v["ms"], "launches": v["n"]} for k, v in by.items()}}
+            "classes": {k: {"ms": v["ms"], "launches": v["n"], "bytes": v["bytes"]} for k, v in by.items()}}
 
 
 def make_solver(S, cfg, fields, tc, local, precision):
@@ -302,10 +328,17 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
     # per-launch CUDA events inside a one-stream graph replay of substep 1 (the timed path, without
     # the concurrency of the dataflow lanes), and the same after eager launches for comparison
     prof = g.profile_substep_graph(1)
-    rl = roofline(prof, peak, peak_kind, args.workload)
-    rl["timing"] = "CUDA events around each launch in a one-stream graph replay of one substep"
-    eager = roofline(g.profile_substep(1), peak, peak_kind, args.workload)
-    rl["eager"] = {"achieved": eager["achieved"], "frac": eager["frac"], "ms_per_launch": eager["ms_per_launch"]}
+    kinds = sorted({r["kind"] for r in prof})
+    class_ms = {CLASSES[k]: g.profile_class(k, 1, reps=20) for k in kinds}
+    substep_ms = g.profile_class(-1, 1, reps=20)
+    rl = roofline(prof, peak, peak_kind, args.workload, class_ms)
+    rl["timing"] = ("per class: one replay of substep 1's graph (dataflow lanes as timed) holding only that class's "
+                    "launches, mean of 20 replays; bytes: algorithmic bytes of each launch")
+    rl["substep_ms_in_graph"] = substep_ms
+    rl["sum_of_class_ms"] = sum(class_ms.values())
+    events = roofline(prof, peak, peak_kind, args.workload)
+    rl["per_launch_events"] = {"kernel": events["kernel"], "achieved": events["achieved"], "frac": events["frac"],
+                               "ms_per_launch": events["ms_per_launch"]}
     bpc = BYTES_PER_CELL_SUBSTEP[args.workload]
     step_model = {"bytes_per_cell_substep": bpc, "achieved_gbs": bpc * cfg.ncell * sub / (ms * 1e-3) / 1e9}
     step_model["frac"] = step_model["achieved_gbs"] / peak
@@ -427,10 +460,12 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="heated", choices=["heated", "channel", "large", "ensemble", "channel3fmd"])
+    ap.add_argument("--workload", default="heated",
+                    choices=["heated", "channel", "large", "ensemble", "channel3fmd", "tgv"])
     ap.add_argument("--members", type=int, default=48)
     ap.add_argument("--nc", type=int, nargs=3, default=[128, 96, 128])
-    ap.add_argument("--iacc", type=int, default=C.IACCU_CD2)
+    ap.add_argument("--iacc", type=int, default=None,
+                    help="1 CD2, 2 CD4, 3 CP4, 4 CP6 (default: CP6 for tgv, CD2 otherwise)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mlp", action="store_true")
     ap.add_argument("--mlp-epochs", type=int, default=200)

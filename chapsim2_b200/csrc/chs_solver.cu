@@ -126,6 +126,8 @@ struct chs_handle {
   // fused substep kernels for the explicit schemes (chs_fused.cu): 1 on by default, 0 the
   // operator-by-operator path (chs_set_fusion)
   int kfuse = 1;
+  // >= 0 while chs_profile_class captures a substep: launches of other kernel classes are left out
+  int only_kind = -1;
   FzRow* fz_rows = nullptr;  // device row tables of the y operators (chs_fused.cuh)
   // plan key -> first row of its table in fz_rows (-1: no table: periodic, or not representable)
   std::map<std::tuple<int, int, int, int, int>, int> fz_index;
@@ -501,6 +503,7 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const typename Id<T>::type* 
   const double nrw = omode == O_FRAC ? (io.qupd ? 6.0 : 4.0) : ((accumulate || omode != O_STORE) ? 2.0 : 1.0);
   const double bytes = (double)sizeof(T) * (narr * nin_tot + nrw * nout_tot);
   const bool rmw = accumulate || omode == O_FRAC;
+  if (H->only_kind >= 0 && H->only_kind != 0) return;
   cudaStream_t s = H->dag_begin(bufs(io.t[0].X, io.t[0].Y, io.t[0].Z, io.t[1].X, io.t[1].Y, io.t[1].Z, io.fbc, io.onum,
                                      rmw ? out : nullptr),
                                 bufs(out, io.rhs0, io.qupd));
@@ -515,6 +518,7 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const typename Id<T>::type* 
 // the dataflow schedule
 #define PROF(H, kind, bytes, ...)                       \
   do {                                                   \
+    if ((H)->only_kind >= 0 && (H)->only_kind != (kind)) break; \
     (H)->dag_barrier_begin();                            \
     cudaEvent_t e0_ = (H)->prof_begin();                 \
     __VA_ARGS__;                                         \
@@ -525,6 +529,7 @@ void run_op(chs_handle* H, int d, int fam, Pair bc, const typename Id<T>::type* 
 // names the lane the schedule picked
 #define PROFD(H, kind, bytes, R, W, ...)                 \
   do {                                                   \
+    if ((H)->only_kind >= 0 && (H)->only_kind != (kind)) break; \
     cudaStream_t st = (H)->dag_begin(R, W);              \
     cudaEvent_t e0_ = (H)->prof_begin();                 \
     __VA_ARGS__;                                         \
@@ -648,6 +653,7 @@ bool run_fused(chs_handle* H, const std::vector<OpTerm<T>>& terms, T* out, const
       for (const void* a : {(const void*)H->hEnth, (const void*)H->tTemp, (const void*)H->kCond,
                             (const void*)H->dDens, (const void*)H->mVisc})
         wr.p[wr.n++] = a;
+    if (H->only_kind >= 0 && H->only_kind != 0) return false;
     cudaStream_t ls = H->dag_begin(rd, wr);
     cudaEvent_t e0 = H->prof_begin();
     launch_fused(F, H->table, ls);
@@ -3064,6 +3070,44 @@ int chs_profile_substep(chs_handle* H, int isub, chs_kprof* out, int max, int* n
     }
     H->recs.clear();
     *n = k;
+  });
+}
+
+int chs_profile_class(chs_handle* H, int isub, int kind, int reps, float* ms) {
+  if (!H || !ms || isub < 1 || isub > 3 || kind < -1 || kind > 4 || reps < 1) return CHS_ERR_ARG;
+  return guard(H, [&] {
+    // the partial substep leaves the state inconsistent: save it and put it back afterwards
+    size_t tot = 0;
+    for (const auto& a : H->allocs) tot += a.second;
+    char* buf = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void**>(&buf), tot, H->st));
+    snapshot(H, buf, true);
+    cudaGraphExec_t ge = nullptr;
+    H->only_kind = kind;
+    try {
+      capture_one(H, isub, PART_ALL, &ge);
+    } catch (...) {
+      H->only_kind = -1;
+      throw;
+    }
+    H->only_kind = -1;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaGraphLaunch(ge, H->st));  // warm-up
+    CK(cudaEventRecord(a, H->st));
+    for (int r = 0; r < reps; ++r) CK(cudaGraphLaunch(ge, H->st));
+    CK(cudaEventRecord(b, H->st));
+    CK(cudaEventSynchronize(b));
+    float t = 0.0f;
+    CK(cudaEventElapsedTime(&t, a, b));
+    *ms = t / reps;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaGraphExecDestroy(ge);
+    snapshot(H, buf, false);
+    CK(cudaFreeAsync(buf, H->st));
+    CK(cudaStreamSynchronize(H->st));
   });
 }
 

@@ -71,7 +71,7 @@ EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field
             "chs_ensemble_kernel_launches", "chs_ensemble_destroy", "chs_autotune", "chs_set_launch_shape",
             "chs_set_lanes", "chs_profile_substep_graph", "chs_write_restart", "chs_read_restart",
             "chs_stats_update", "chs_stats_get", "chs_write_statistics", "chs_read_statistics",
-            "chs_data_file_name", "chs_set_fusion"]
+            "chs_data_file_name", "chs_set_fusion", "chs_profile_class"]
 
 
 class ChsKprof(ctypes.Structure):
@@ -128,6 +128,8 @@ def load():
     L.chs_set_launch_shape.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.chs_set_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.chs_set_fusion.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.chs_profile_class.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_float)]
     for fn in ("chs_write_restart", "chs_read_restart", "chs_write_statistics", "chs_read_statistics"):
         getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
     L.chs_stats_update.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -487,6 +489,13 @@ class Solver:
         self._check(self.L.chs_profile_substep_graph(self.h, int(isub), arr, maxk, ctypes.byref(n)),
                     "chs_profile_substep_graph")
         return [dict(kind=arr[i].kind, dir=arr[i].dir, bytes=arr[i].bytes, ms=arr[i].ms) for i in range(n.value)]
+
+    def profile_class(self, kind, isub=1, reps=20):
+        """ms of one graph replay of substep isub holding only kernel class `kind` (-1: all)."""
+        ms = ctypes.c_float()
+        self._check(self.L.chs_profile_class(self.h, int(isub), int(kind), int(reps), ctypes.byref(ms)),
+                    "chs_profile_class")
+        return ms.value
 
     def sync(self):
         self._check(self.L.chs_sync(self.h), "chs_sync")

@@ -150,7 +150,7 @@ void chs_host_free(void* p);
 
 /* Per-kernel profile of one substep (not graph-replayed): for each launch, its
  * class (0 line op, 1 FFT, 2 y solve, 3 elementwise/reduction, 4 fused CD2
- * momentum component), direction
+ * kernel: a momentum component or the energy equation), direction
  * (-1 if none), algorithmic bytes moved and CUDA-event duration. */
 typedef struct chs_kprof {
   int kind;
@@ -165,6 +165,15 @@ int chs_profile_substep(chs_handle* h, int isub, chs_kprof* out, int max, int* n
  * replay (the timed path) rather than after an eager launch.  Advances the
  * state by that substep, like chs_momentum_substep. */
 int chs_profile_substep_graph(chs_handle* h, int isub, chs_kprof* out, int max, int* n);
+/* In-step time of one kernel class: the substep isub (1..3) is captured as the
+ * timed path captures it (dataflow lanes included) with only the launches of
+ * class `kind` (0 line op, 1 FFT, 2 y solve, 3 elementwise/reduction, 4 fused
+ * CD2 kernels; -1 all of them), the graph is replayed reps times after one
+ * warm-up, and *ms is the mean time of one replay: the class's time without
+ * the per-launch event nodes of chs_profile_substep_graph.  The state is saved
+ * before and restored after (device memory for one copy of the handle's fields
+ * is allocated for the duration of the call).  No counterpart in the reference. */
+int chs_profile_class(chs_handle* h, int isub, int kind, int reps, float* ms);
 
 /* Replaces Buildup_thermo_mapping_relations + initialise_thermal_properties
  * (src/chapsim.f90:103-108, src/input_thermo.f90:1070-1103) and the q -> g

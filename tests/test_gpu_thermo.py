@@ -149,3 +149,52 @@ def test_host_fields_pipeline_matches_device_steps(precision):
         assert np.array_equal(b.download(k), ref), k
     a.close()
     b.close()
+
+
+def _full_field_compare(o, g, tol):
+    """u, v, w, p and rho*h, h, T, rho, mu, kappa, g against the oracle (p on its own scale)."""
+    ref, got = o.get_fields(), g.get_fields()
+    for name, a, b in zip(("qx", "qy", "qz", "p"), got[:4], ref[:4]):
+        assert rel(a, b) < tol, (name, rel(a, b))
+    th_o, th_g = o.get_thermo(), g.get_thermo()
+    for k in ("rhoh", "h", "T", "d", "m", "k", "gx", "gy", "gz"):
+        assert rel(th_g[k], th_o[k]) < tol, (k, rel(th_g[k], th_o[k]))
+
+
+def test_heated_benchmark_workload_one_step_vs_oracle():
+    """The benchmark's workload itself (heated channel 128x96x128, CD2, beta 1.5, Re_b 2800, isoflux
+    walls, dt from CFL 0.8): the initial step and one RK3 step against the oracle, every field."""
+    import bench
+    cfg, f, tc = bench.workload("heated")
+    o = po.Oracle(cfg)
+    o.set_fields(*f)
+    o.thermo_init(tc)
+    g = S.Solver(cfg)
+    g.set_fields(*f)
+    g.thermo_init(tc)
+    for isub in (0, 1, 2, 3):
+        o.substep(isub)
+    g.substep(0)
+    g.step(1)
+    _full_field_compare(o, g, 1e-10)
+    d = g.diagnostics()
+    assert d["max_div"] < 1e-10 and d["nan_flag"] == 0
+    g.close()
+
+
+def test_large_heated_channel_substep_vs_oracle():
+    """Config 5 (384x256x384, beta 1.8, Re_b 6875, variable properties): the initial step and one
+    substep against the oracle, every field (the oracle takes ~20 s per substep on 16 host cores)."""
+    import bench
+    cfg, f, tc = bench.workload("large")
+    o = po.Oracle(cfg)
+    o.set_fields(*f)
+    o.thermo_init(tc)
+    g = S.Solver(cfg)
+    g.set_fields(*f)
+    g.thermo_init(tc)
+    for isub in (0, 1):
+        o.substep(isub)
+        g.substep(isub)
+    _full_field_compare(o, g, 1e-10)
+    g.close()
