@@ -421,13 +421,80 @@ __device__ __forceinline__ void fz_energy_body(const FzEnergy<T>& f, int i, int 
   f.rhoh[a] = f.rhoh[a] + r1;
 }
 
+// The interior rows of the energy pass with every input loaded up front (27 values of the 3D
+// cross around the cell, independent loads in flight together), then the arithmetic of
+// fz_energy_body<T, false> in the same order.
+template <typename T>
+__device__ __forceinline__ void fz_energy_interior(const FzEnergy<T>& f, int i, int j, int k) {
+  const int n0 = f.n0, nc1 = f.nc1, np1 = f.np1, n2 = f.n2;
+  const int im = i > 0 ? i - 1 : n0 - 1, ip = i + 1 < n0 ? i + 1 : 0;
+  const int km = k > 0 ? k - 1 : n2 - 1, kp = k + 1 < n2 ? k + 1 : 0;
+  const int c = (k * nc1 + j) * n0 + i;
+  const int xm = c - i + im, xp = c - i + ip;
+  const int ym = c - n0, yp = c + n0;
+  const int zm = c + (km - k) * nc1 * n0, zp = c + (kp - k) * nc1 * n0;
+  const int pc = (k * np1 + j) * n0 + i;
+  const T h0 = __ldg(f.h + c), hxm = __ldg(f.h + xm), hxp = __ldg(f.h + xp), hym = __ldg(f.h + ym),
+          hyp = __ldg(f.h + yp), hzm = __ldg(f.h + zm), hzp = __ldg(f.h + zp);
+  const T t0 = __ldg(f.t + c), txm = __ldg(f.t + xm), txp = __ldg(f.t + xp), tym = __ldg(f.t + ym),
+          typ = __ldg(f.t + yp), tzm = __ldg(f.t + zm), tzp = __ldg(f.t + zp);
+  const T k0 = __ldg(f.k + c), kxm = __ldg(f.k + xm), kxp = __ldg(f.k + xp), kym = __ldg(f.k + ym),
+          kyp = __ldg(f.k + yp), kzm = __ldg(f.k + zm), kzp = __ldg(f.k + zp);
+  const T gx0 = __ldg(f.gx + c), gx1 = __ldg(f.gx + xp);
+  const T gy0 = __ldg(f.gy + pc), gy1 = __ldg(f.gy + pc + n0);
+  const T gz0 = __ldg(f.gz + c), gz1 = __ldg(f.gz + zp);
+  const FzRow& rh0 = f.rows[f.in[FE_H_Y].row + j];
+  const FzRow& rh1 = f.rows[f.in[FE_H_Y].row + j + 1];
+  const FzRow& rt0 = f.rows[f.in[FE_T_Y].row + j];
+  const FzRow& rt1 = f.rows[f.in[FE_T_Y].row + j + 1];
+  const FzRow& rk0 = f.rows[f.in[FE_K_Y].row + j];
+  const FzRow& rk1 = f.rows[f.in[FE_K_Y].row + j + 1];
+  const FzRow& ro = f.rows[f.term[1].a.row + j];
+  const double sr = 1.0 * f.rpr;
+  // periodic M1C2P / D1C2P (fz_per): r1*(f(p) + f(p-1))*dd, r1*(f(p) - f(p-1))*dd
+  auto m12 = [](const FzOp& o, T a, T b) { return T(o.r1) * (a + b) * T(o.dd); };
+  auto d12 = [](const FzOp& o, T a, T b) { return T(o.r1) * (a - b) * T(o.dd); };
+  // y with walls, interior (fz_y): w0*f(p) + w1*f(p-1)
+  auto y12 = [](const FzRow& r, T a, T b) {
+    T v = T(r.w[0]) * a;
+    v += T(r.w[1]) * b;
+    return v;
+  };
+  auto face = [&](T g, T hf, T dt, T kf) {
+    T e = T(-1.0) * (g * hf);
+    e += T(sr) * (dt * kf);
+    return e;
+  };
+  // x: faces i and i+1 (D1P2C: r1*(f(p+1) - f(p))*dd)
+  const T ex0 = face(gx0, m12(f.in[FE_H_X], h0, hxm), d12(f.in[FE_T_X], t0, txm), m12(f.in[FE_K_X], k0, kxm));
+  const T ex1 = face(gx1, m12(f.in[FE_H_X], hxp, h0), d12(f.in[FE_T_X], txp, t0), m12(f.in[FE_K_X], kxp, k0));
+  T F = T(f.term[0].a.r1) * (ex1 - ex0) * T(f.term[0].a.dd);
+  // y: faces j and j+1 (D1P2C interior: w0*f(j+1) + w1*f(j))
+  const T ey0 = face(gy0, y12(rh0, h0, hym), y12(rt0, t0, tym), y12(rk0, k0, kym));
+  const T ey1 = face(gy1, y12(rh1, hyp, h0), y12(rt1, typ, t0), y12(rk1, kyp, k0));
+  T vy = T(ro.w[0]) * ey1;
+  vy += T(ro.w[1]) * ey0;
+  F += vy;
+  // z: faces k and k+1
+  const T ez0 = face(gz0, m12(f.in[FE_H_Z], h0, hzm), d12(f.in[FE_T_Z], t0, tzm), m12(f.in[FE_K_Z], k0, kzm));
+  const T ez1 = face(gz1, m12(f.in[FE_H_Z], hzp, h0), d12(f.in[FE_T_Z], tzp, t0), m12(f.in[FE_K_Z], kzp, k0));
+  F += T(f.term[2].a.r1) * (ez1 - ez0) * T(f.term[2].a.dd);
+  // energy_advance_kernel: rhs0 = F, rho*h += dt*(gam*F + zeta*rhs0)
+  const T tdt = T(f.dt), tg = T(f.gam), tz = T(f.zeta);
+  const T last = f.rhs0[c];
+  const T tot = tg * F + tz * last;
+  f.rhs0[c] = F;
+  const T r1 = tdt * tot;
+  f.rhoh[c] = f.rhoh[c] + r1;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) fz_energy_kernel(const __grid_constant__ FzEnergy<T> f) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
   if (i >= f.n0 || j >= f.nc1 || k >= f.n2) return;
-  if (fz_interior_block(f.nc1)) fz_energy_body<T, false>(f, i, j, k);
+  if (fz_interior_block(f.nc1)) fz_energy_interior<T>(f, i, j, k);
   else fz_energy_body<T, true>(f, i, j, k);
 }
 
