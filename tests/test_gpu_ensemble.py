@@ -6,6 +6,7 @@ import pytest
 from chapsim2_b200 import config as C
 from chapsim2_b200 import initial as I
 from chapsim2_b200 import solver as S
+from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu
 
@@ -73,6 +74,7 @@ def test_fused_sums_match_separate_operators(heated, precision):
     out = []
     for fused in (0, 1):
         g = S.Solver(cfg, precision=precision)
+        g.set_fusion(False)  # the operator path, where the autotuner's fused sums apply
         g.set_fields(*f)
         if tc is not None:
             g.thermo_init(tc)
@@ -84,3 +86,33 @@ def test_fused_sums_match_separate_operators(heated, precision):
     tol = 1e-12 if precision == S.CHS_FP64 else 1e-5
     for a, b in zip(*out):
         assert np.linalg.norm(a - b) <= tol * max(np.linalg.norm(b), 1e-30)
+
+
+def test_ensemble_members_match_the_oracle():
+    """Members of different grids and Reynolds numbers advanced together by the ensemble graph agree
+    with the oracle stepping each member alone (FP64, two RK3 steps)."""
+    cfgs = C.ensemble_members(n=3, seed=11, nx=(16, 24), ny=(16, 12), nz=(16, 8))
+    members, oracles = [], []
+    for cfg in cfgs:
+        f = I.channel_fields(cfg)
+        cfg.dt = I.cfl_dt(cfg, *f[:3], cfl=0.5)
+        g = S.Solver(cfg)
+        g.set_fields(*f)
+        g.Solve_momentum_eq(0)
+        members.append(g)
+        o = po.Oracle(cfg)
+        o.set_fields(*f)
+        o.substep(0)
+        oracles.append(o)
+    e = S.Ensemble(members)
+    e.step(2)
+    for g, o in zip(members, oracles):
+        o.step()
+        o.step()
+        got, ref = g.get_fields(), o.get_fields()
+        for name, a, b in zip(("qx", "qy", "qz", "p"), got[:4], ref[:4]):
+            err = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+            assert err < 1e-10, (g.cfg.nc, name, err)
+    e.close()
+    for g in members:
+        g.close()
