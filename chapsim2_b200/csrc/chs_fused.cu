@@ -236,20 +236,22 @@ struct FzCtx {
   }
 
   // the fractional step of the operator path's O_FRAC store (pfc = 1 * v)
-  __device__ __forceinline__ void frac(int c, int a, T F, T v) const {
+  __device__ __forceinline__ T frac(int c, int a, T F, T v) const {
     const T tdt = T(f.dt), tg = T(f.gam), tz = T(f.zeta), ta = T(f.alpha);
     const T pfc = T(1.0) * v;
     const T last = f.m0[c][a];
     T tot = tg * F + tz * last;
     f.m0[c][a] = F;
     tot = tot + ta * pfc;
-    f.m[c][a] = tdt * tot;
+    const T r = tdt * tot;
+    f.m[c][a] = r;
+    return r;
   }
 };
 
 // one momentum component C (0 x, 1 y, 2 z) at (i, j, k)
 template <typename T, bool TH, bool PY, int C, bool E>
-__device__ __forceinline__ void fz_momentum_body(const FzMomentum<T>& f, int i, int j, int k) {
+__device__ __forceinline__ T fz_momentum_body(const FzMomentum<T>& f, int i, int j, int k) {
   const int n0 = f.n0, nc1 = f.nc1, np1 = f.np1, n2 = f.n2;
   const FzCtx<T, TH, PY, E> c{f, n0 * n2};
   const int nl = c.nl, L = i + n0 * k;
@@ -267,7 +269,7 @@ __device__ __forceinline__ void fz_momentum_body(const FzMomentum<T>& f, int i, 
         f.term[0][2], f.rows, nl, n0, i, j, k, n2, 1.0, r, [&](int q) { return c.template conv_xz<0>(i, j, q); },
         [&](double s, int q) { return c.visc_xz(s, i, j, q); });
     v = fz_per<D1C2P, T>(f.pres[0], i, n0, [&](int q) { return T(-1.0) * c.pr(q, j, k); });
-    c.frac(0, (k * nc1 + j) * n0 + i, F, v);
+    return c.frac(0, (k * nc1 + j) * n0 + i, F, v);
   } else if (C == 1) {
     // y-momentum at (i, j, k) of the qy grid
     F = fz_pair<D1P2C, 0, PY, E, T>(
@@ -281,7 +283,7 @@ __device__ __forceinline__ void fz_momentum_body(const FzMomentum<T>& f, int i, 
         [&](double s, int q) { return c.visc_yz(s, i, j, q); });
     v = fz_y<D1C2P, PY, E, T>(f.rows, f.pres[1], j, nc1, f.fpres[1], nl, L,
                            [&](int q) { return T(-1.0) * c.pr(i, q, k); });
-    c.frac(1, (k * np1 + j) * n0 + i, F, v);
+    return c.frac(1, (k * np1 + j) * n0 + i, F, v);
   } else {
     // z-momentum at (i, j, k) of the qz grid
     F = fz_pair<D1P2C, 0, PY, E, T>(
@@ -294,7 +296,7 @@ __device__ __forceinline__ void fz_momentum_body(const FzMomentum<T>& f, int i, 
         f.term[2][2], f.rows, nl, n0, i, j, k, n2, 2.0, r, [&](int q) { return c.template conv_c<2>(i, j, q); },
         [&](double s, int q) { return c.template visc_c<2>(s, i, j, q); });
     v = fz_per<D1C2P, T>(f.pres[2], k, n2, [&](int q) { return T(-1.0) * c.pr(i, j, q); });
-    c.frac(2, (k * nc1 + j) * n0 + i, F, v);
+    return c.frac(2, (k * nc1 + j) * n0 + i, F, v);
   }
 }
 
@@ -304,9 +306,27 @@ __global__ void __launch_bounds__(256) fz_momentum_kernel(const __grid_constant_
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
-  if (i >= f.n0 || j >= (C == 1 ? f.np1 : f.nc1) || k >= f.n2) return;
-  if (PY || fz_interior_block(f.nc1)) fz_momentum_body<T, TH, PY, C, false>(f, i, j, k);
-  else fz_momentum_body<T, TH, PY, C, true>(f, i, j, k);
+  const bool valid = i < f.n0 && j < (C == 1 ? f.np1 : f.nc1) && k < f.n2;
+  T m = T(0);
+  if (valid) {
+    if (PY || fz_interior_block(f.nc1)) m = fz_momentum_body<T, TH, PY, C, false>(f, i, j, k);
+    else m = fz_momentum_body<T, TH, PY, C, true>(f, i, j, k);
+  }
+  if (C == 0 && f.part) {
+    // the CTA's share of the mass-flux mean: sum of wy[j] * m (fixed order, so the mean is
+    // deterministic), reduced over the warp by shuffles and over the CTA's 8 warps in shared memory
+    __shared__ double red[8];
+    double s = valid ? f.wy[j] * (double)m : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    if ((tid & 31) == 0) red[tid >> 5] = s;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x * blockDim.y * blockDim.z) / 32; ++w) t += red[w];
+      f.part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = t;
+    }
+  }
 }
 
 // the wall rows of the y-viscous boundary value (fbcy_velo: src/eq_momentum2.f90:374-442, :537-546,
@@ -316,9 +336,10 @@ __global__ void fz_wall_visc_kernel(const __grid_constant__ FzMomentum<T> f, T* 
                                     T* __restrict__ fcomb, const T* __restrict__ fconv2) {
   const int nl = f.n0 * f.n2;
   const FzCtx<T, TH, false, true> c{f, nl};
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nl; g += gridDim.x * blockDim.x) {
+  for (int gs = blockIdx.x * blockDim.x + threadIdx.x; gs < 2 * nl; gs += gridDim.x * blockDim.x) {
+    const int side = gs < nl ? 0 : 1, g = gs - side * nl;
     const int k = g / f.n0, i = g - k * f.n0;
-    for (int side = 0; side < 2; ++side) {
+    {
       const int j = side == 0 ? 0 : f.np1 - 1;
       const T ddx = fz_per<D1P2C, T>(f.in[FI_W_DX], i, f.n0, [&](int q) { return c.qxiy(q, j, k); });
       const T ddy = fz_row<T>(f.rows, f.in[FI_W_DY], j, f.fyqy, nl, g, [&](int q) { return c.qyiy(i, q, k); });
@@ -502,9 +523,10 @@ template <typename T>
 __global__ void fz_energy_walls_kernel(const __grid_constant__ FzEnergy<T> f, int mode, T* __restrict__ out) {
   const int nl = f.n0 * f.n2;
   const FzECtx<T, true> c{f, nl};
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nl; g += gridDim.x * blockDim.x) {
+  for (int gs = blockIdx.x * blockDim.x + threadIdx.x; gs < 2 * nl; gs += gridDim.x * blockDim.x) {
+    const int side = gs < nl ? 0 : 1, g = gs - side * nl;
     const int k = g / f.n0, i = g - k * f.n0;
-    for (int side = 0; side < 2; ++side) {
+    {
       const int j = side == 0 ? 0 : f.np1 - 1;
       if (mode == 0) {
         // launch_fbcy_extract(A = dT/dy, B none, C = kappa_y, s = 1): (A*1)*C
@@ -513,8 +535,16 @@ __global__ void fz_energy_walls_kernel(const __grid_constant__ FzEnergy<T> f, in
         v = v * c.template yop<M1C2P>(FE_K_Y, f.k, f.fk, i, j, k);
         out[side * nl + g] = v;
         out[(side + 2) * nl + g] = v;
-      } else {
-        out[(k * f.np1 + j) * f.n0 + i] = c.template yop<M1C2P>(FE_RH_Y, f.rhoh, (const T*)nullptr, i, j, k);
+      } else if (side == 0 ? f.ws0 : f.ws1) {
+        // wall_props_kernel on the wall row of rho*h interpolated to the y faces
+        const T dh = c.template yop<M1C2P>(FE_RH_Y, f.rhoh, (const T*)nullptr, i, j, k);
+        const CellProps p = props_from_dh(f.tab, (double)dh);
+        for (int u = side; u < 4; u += 2) {
+          f.wh[u * nl + g] = T(p.h);
+          f.wk[u * nl + g] = T(p.k);
+          f.wm[u * nl + g] = T(p.m);
+          f.wd[u * nl + g] = T(p.d);
+        }
       }
     }
   }
@@ -565,6 +595,8 @@ __global__ void __launch_bounds__(256) fz_project_kernel(const __grid_constant__
 
 }  // namespace
 
+int fz_momentum_x_blocks(int n0, int nc1, int n2) { return ((n0 + 31) / 32) * ((nc1 + 3) / 4) * ((n2 + 1) / 2); }
+
 template <typename T, bool TH, bool PY>
 void launch_fz_c(const FzMomentum<T>& f, int c, cudaStream_t st) {
   const dim3 bs(32, 4, 2);
@@ -586,9 +618,9 @@ void launch_fz_momentum(const FzMomentum<T>& f, int c, cudaStream_t st) {
 template <typename T>
 void launch_fz_wall_visc(const FzMomentum<T>& f, T* fvisc2, T* fcomb, const T* fconv2, cudaStream_t st) {
   const int nl = f.n0 * f.n2;
-  const int blocks = (nl + 255) / 256 < 148 ? (nl + 255) / 256 : 148;
-  if (f.thermo) fz_wall_visc_kernel<T, true><<<blocks, 256, 0, st>>>(f, fvisc2, fcomb, fconv2);
-  else fz_wall_visc_kernel<T, false><<<blocks, 256, 0, st>>>(f, fvisc2, fcomb, fconv2);
+  const int blocks = (2 * nl + 127) / 128;
+  if (f.thermo) fz_wall_visc_kernel<T, true><<<blocks, 128, 0, st>>>(f, fvisc2, fcomb, fconv2);
+  else fz_wall_visc_kernel<T, false><<<blocks, 128, 0, st>>>(f, fvisc2, fcomb, fconv2);
 }
 
 template <typename T>
@@ -608,8 +640,7 @@ void launch_fz_energy(const FzEnergy<T>& f, cudaStream_t st) {
 template <typename T>
 void launch_fz_energy_walls(const FzEnergy<T>& f, int mode, T* out, cudaStream_t st) {
   const int nl = f.n0 * f.n2;
-  const int blocks = (nl + 255) / 256 < 148 ? (nl + 255) / 256 : 148;
-  fz_energy_walls_kernel<T><<<blocks, 256, 0, st>>>(f, mode, out);
+  fz_energy_walls_kernel<T><<<(2 * nl + 127) / 128, 128, 0, st>>>(f, mode, out);
 }
 
 template <typename T>

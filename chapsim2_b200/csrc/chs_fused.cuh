@@ -17,6 +17,7 @@
 #include <cstdint>
 
 #include "chs_kernels.cuh"
+#include "chs_thermo_dev.cuh"
 
 namespace chs {
 
@@ -77,12 +78,18 @@ struct FzMomentum {
   T *m[3], *m0[3];       // right-hand sides (fractional-step increments) and their histories
   double rre, dt, gam, zeta, alpha;
   const FzRow* rows;     // row tables of the y operators
+  // constant mass flux: the x component also writes, per CTA, the y-weighted sum of its outputs
+  // (wy[j] * m, the numerator of the volume mean), for launch_finalize_mean; null otherwise
+  const double* wy;
+  double* part;
 };
 
 // the right-hand side of momentum component c (0 x, 1 y, 2 z) with the fractional step
 // (m = dt*(gam*F + zeta*m0 + alpha*pfc), m0 = F); the advance q += m is left to launch_fz_update
 template <typename T>
 void launch_fz_momentum(const FzMomentum<T>& f, int c, cudaStream_t st);
+// CTAs of the x component's launch (the length of f.part)
+int fz_momentum_x_blocks(int n0, int nc1, int n2);
 
 // wall planes of the y-viscous boundary value (fbcy_velo): fvisc2 = walls of
 // s*(qydy_cpc - (qxdx_cpc + qydy_cpc + qzdz_cpc)/3)*(mu_y or c2) and fcomb = fconv2 + rre*fvisc2,
@@ -110,13 +117,18 @@ struct FzEnergy {
   T *rhoh, *rhs0;
   double rpr, dt, gam, zeta;
   const FzRow* rows;
+  // wall states after the update (walls flagged ws0 / ws1): the property lookup of rho*h
+  // interpolated to each wall, into planes side and side + 2 of wh, wk, wm, wd
+  ThermoTab tab;
+  int ws0, ws1;
+  T *wh, *wk, *wm, *wd;
 };
 // rhs0 <- F, rho*h += dt*(gam*F + zeta*rhs0) (energy_advance_kernel's arithmetic)
 template <typename T>
 void launch_fz_energy(const FzEnergy<T>& f, cudaStream_t st);
 // wall rows, before the energy pass (mode 0): kappa*dT/dy into planes side and side + 2 of out;
-// after it (mode 1): rho*h interpolated to the y faces into rows 0 and np1-1 of out (the dh_cpc
-// array launch_wall_props reads)
+// after it (mode 1): the wall states (rho*h interpolated to each flagged wall and looked up in the
+// table: launch_wall_props on the wall rows of that interpolation); out unused
 template <typename T>
 void launch_fz_energy_walls(const FzEnergy<T>& f, int mode, T* out, cudaStream_t st);
 

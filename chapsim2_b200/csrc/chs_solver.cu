@@ -129,6 +129,7 @@ struct chs_handle {
   // >= 0 while chs_profile_class captures a substep: launches of other kernel classes are left out
   int only_kind = -1;
   FzRow* fz_rows = nullptr;  // device row tables of the y operators (chs_fused.cuh)
+  double* fz_part = nullptr;  // per-CTA partial sums of the mass-flux mean from the fused x pass
   // plan key -> first row of its table in fz_rows (-1: no table: periodic, or not representable)
   std::map<std::tuple<int, int, int, int, int>, int> fz_index;
   long long launches = 0;
@@ -905,6 +906,7 @@ void setup_device(chs_handle* H, const chs_config* c) {
   CK(cudaMemcpyAsync(H->wy, wy.data(), nc1 * sizeof(double), cudaMemcpyHostToDevice, H->st));
   H->npart = 148 * 4;
   H->partial = H->dalloc<double>(2 * H->npart);
+  H->fz_part = H->dalloc<double>(fz_momentum_x_blocks(nc0, nc1, nc2));
   H->scal = H->dalloc<double>(16);
 
   // Poisson tables
@@ -1354,6 +1356,10 @@ bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz)
   F.pres[2] = b.op(2, D1C2P, bz_pr, true);
   F.fpres[0] = any; F.fpres[1] = fympr; F.fpres[2] = any;
   if (!b.ok) return false;
+  if (H->idriven == 1) {
+    F.wy = H->wy;
+    F.part = H->fz_part;
+  }
   F.m[0] = A(H->mx); F.m[1] = A(H->my); F.m[2] = A(H->mz);
   F.m0[0] = A(H->mx0); F.m0[1] = A(H->my0); F.m0[2] = A(H->mz0);
   F.rre = H->rre;
@@ -1377,16 +1383,18 @@ bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz)
             bufs(H->qx, H->qy, H->qz, H->pres, TH ? H->gx : nullptr, TH ? H->gy : nullptr, TH ? H->gz : nullptr,
                  TH ? H->mVisc : nullptr, H->fb_comb, H->fb_visc2, H->fb_qx, H->fb_qz, H->fb_qy,
                  TH ? H->fb_m : nullptr),
-            bufs(mo[c], m0[c]), launch_fz_momentum<T>(F, c, st));
+            bufs(mo[c], m0[c], c == 0 && F.part ? H->fz_part : nullptr), launch_fz_momentum<T>(F, c, st));
       H->launches++;
     }
   }
   const double* bulk = nullptr;
   if (H->idriven == 1) {
-    PROFD(H, 3, 8.0 / 8.0 * sizeof(T) * H->n_pcc, bufs(H->mx, H->wy), bufs(H->partial, H->scal),
-         launch_weighted_mean(A(H->mx), H->wy, nc0, nc1, nc2, H->partial, H->npart, H->scal + 0, H->vol, st));
+    // the mass-flux mean from the x pass's per-CTA sums
+    const int nblk = fz_momentum_x_blocks(nc0, nc1, nc2);
+    PROFD(H, 3, 8.0 * nblk, bufs(H->fz_part), bufs(H->scal),
+          launch_finalize_mean(H->fz_part, nblk, H->scal + 0, H->vol, st));
     bulk = H->scal + 0;
-    H->launches += 2;
+    H->launches++;
   }
   const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
   PROFD(H, 3, nf * 9.0, bufs(H->mx, H->my, H->mz, bulk), bufs(ux, uy, uz),
@@ -1436,7 +1444,7 @@ bool fused_energy(chs_handle* H, int isub) {
   F.rpr = H->rPrRen;
   F.dt = H->dt; F.gam = H->tGamma[isub]; F.zeta = H->tZeta[isub];
   F.rows = H->fz_rows;
-  const int nc0 = H->nc[0], nc2 = H->nc[2], np1 = H->np[1];
+  const int nc0 = H->nc[0], nc2 = H->nc[2];
   const double nf = (double)sizeof(T) * H->n_ccc;
   PROFD(H, 3, (double)sizeof(T) * 12.0 * nc0 * nc2, bufs(H->tTemp, H->kCond, H->fb_qw, H->fb_k), bufs(H->fb_dtk),
         launch_fz_energy_walls<T>(F, 0, A(H->fb_dtk), st));
@@ -1460,12 +1468,12 @@ bool fused_energy(chs_handle* H, int isub) {
   H->launches++;
   const int s0 = B[1][V_TM][0] == BC_NEUMANN, s1 = B[1][V_TM][1] == BC_NEUMANN;
   if (s0 || s1) {
-    PROFD(H, 3, (double)sizeof(T) * 8.0 * nc0 * nc2, bufs(H->rhoh), bufs(H->dh_cpc),
-          launch_fz_energy_walls<T>(F, 1, A(H->dh_cpc), st));
-    PROFD(H, 3, 10.0 * sizeof(T) * nc0 * nc2, bufs(H->dh_cpc), bufs(H->fb_h, H->fb_k, H->fb_m, H->fb_d),
-          launch_wall_props<T>(H->tab, A(H->dh_cpc), nc0, np1, nc2, s0, s1, A(H->fb_h), A(H->fb_k), A(H->fb_m),
-                               A(H->fb_d), st));
-    H->launches += 2;
+    F.tab = H->tab;
+    F.ws0 = s0; F.ws1 = s1;
+    F.wh = A(H->fb_h); F.wk = A(H->fb_k); F.wm = A(H->fb_m); F.wd = A(H->fb_d);
+    PROFD(H, 3, (double)sizeof(T) * 12.0 * nc0 * nc2, bufs(H->rhoh), bufs(H->fb_h, H->fb_k, H->fb_m, H->fb_d),
+          launch_fz_energy_walls<T>(F, 1, (T*)nullptr, st));
+    H->launches++;
   }
   return true;
 }
