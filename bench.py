@@ -227,10 +227,11 @@ def run_reference(args, cfg, fields, tc, world, rank, dist):
 CLASSES = ("line_op", "fft", "ysolve", "elementwise", "fused")
 
 
-def roofline(prof, peak, peak_kind, workload, class_ms=None):
+def roofline(prof, peak, peak_kind, workload, class_ms=None, compact=False):
     """Roofline of the dominant kernel class.  prof: the per-launch profile of one substep (algorithmic
     bytes of every launch); class_ms: per class, the time of one replay of the substep's graph holding
-    only that class's launches (no per-launch event nodes), which then replaces the event sums."""
+    only that class's launches (no per-launch event nodes), which then replaces the event sums; compact:
+    the workload runs a compact (CP4/CP6) scheme."""
     by = {}
     for r in prof:
         k = CLASSES[r["kind"]]
@@ -249,9 +250,12 @@ def roofline(prof, peak, peak_kind, workload, class_ms=None):
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
-            # channel3fmd runs the channel's operator kernels on the same array sizes (only the
-            # y metric values differ), so it shares the channel's captured per-launch traffic
+            # channel3fmd with CD2 runs the channel's operator kernels on the same array sizes (only
+            # the y metric values differ), so it shares the channel's captured per-launch traffic; the
+            # compact schemes' line solves have their own capture
             key = "channel" if workload == "channel3fmd" else workload
+            if compact:
+                key = workload + "_compact"
             traffic = json.load(f).get(key, {}).get(dom)
     return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
@@ -270,13 +274,21 @@ def make_solver(S, cfg, fields, tc, local, precision):
 
 
 def xz_profiles(g, cfg, tc):
-    """x-z-mean profiles of u and (variable properties) T."""
+    """x-z-mean profiles of u and (variable properties) T; with periodic y (the Taylor-Green box, whose
+    x-z mean of u vanishes) the whole u field instead."""
     sh = cfg.shapes()
+    if cfg.periodic_y:
+        return {"u_field": g.download(0)}
     out = {"u": g.download(0).reshape(sh[0]).mean(axis=(0, 2))}
     if tc is not None:
         from chapsim2_b200 import solver as S
         out["T"] = g.download(S.CHS_TTEMP).reshape(sh[3]).mean(axis=(0, 2))
     return out
+
+
+def form_key(k):
+    """JSON key of one accuracy figure of a precision form against the FP64 path."""
+    return f"{k}_rel_l2_vs_fp64" if k.endswith("_field") else f"{k}_mean_profile_rel_l2_vs_fp64"
 
 
 def run_ours(args, cfg, fields, tc, world, rank, local, dist):
@@ -331,12 +343,13 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
     kinds = sorted({r["kind"] for r in prof})
     class_ms = {CLASSES[k]: g.profile_class(k, 1, reps=20) for k in kinds}
     substep_ms = g.profile_class(-1, 1, reps=20)
-    rl = roofline(prof, peak, peak_kind, args.workload, class_ms)
+    compact = cfg.iacc in (C.IACCU_CP4, C.IACCU_CP6)
+    rl = roofline(prof, peak, peak_kind, args.workload, class_ms, compact)
     rl["timing"] = ("per class: one replay of substep 1's graph (dataflow lanes as timed) holding only that class's "
                     "launches, mean of 20 replays; bytes: algorithmic bytes of each launch")
     rl["substep_ms_in_graph"] = substep_ms
     rl["sum_of_class_ms"] = sum(class_ms.values())
-    events = roofline(prof, peak, peak_kind, args.workload)
+    events = roofline(prof, peak, peak_kind, args.workload, compact=compact)
     rl["per_launch_events"] = {"kernel": events["kernel"], "achieved": events["achieved"], "frac": events["frac"],
                                "ms_per_launch": events["ms_per_launch"]}
     bpc = BYTES_PER_CELL_SUBSTEP[args.workload]
@@ -372,7 +385,7 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
     mixed = {"value": world * cfg.ncell * sub / (ms_m * 1e-3) / 1e6, "ms_per_step": ms_m / args.steps,
              "speedup_vs_fp64": ms_max / ms_m, "steps_compared": steps_done}
     for k in pd:
-        mixed[f"{k}_mean_profile_rel_l2_vs_fp64"] = float(np.linalg.norm(pm[k] - pd[k]) / np.linalg.norm(pd[k]))
+        mixed[form_key(k)] = float(np.linalg.norm(pm[k] - pd[k]) / np.linalg.norm(pd[k]))
     out["forms"] = {"fp64": {"value": value, "ms_per_step": ms_max / args.steps}, "mixed": mixed}
     m.close()
     if tc is not None and not args.no_mlp:
@@ -395,7 +408,7 @@ def run_ours(args, cfg, fields, tc, world, rank, local, dist):
               "t_error_bound": args.mlp_tol, "table_fallback_fraction": fb / float(cfg.ncell * 3 * (2 * args.steps + args.warmup)),
               "training": rep}
         for k in pd:
-            ml[f"{k}_mean_profile_rel_l2_vs_fp64"] = float(np.linalg.norm(pn[k] - pd[k]) / np.linalg.norm(pd[k]))
+            ml[form_key(k)] = float(np.linalg.norm(pn[k] - pd[k]) / np.linalg.norm(pd[k]))
         out["forms"]["mixed+mlp"] = ml
         n.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
