@@ -270,14 +270,15 @@ int chs_set_launch_shape(chs_handle* h, int block, int lt_max, int fused);
  * stream.  Results are identical for every setting (no counterpart in the
  * reference, which runs the operators one after another). */
 int chs_set_lanes(chs_handle* h, int lanes);
-/* Fused substep kernels for the explicit schemes (CD2, CD4): on = 1 (the
- * default) forms the momentum right-hand sides of all three components with
- * the fractional step in one pass that evaluates every interpolation and
- * derivative where it is needed (the same plans, boundary rows and arithmetic
- * as the operator path of Compute_momentum_rhs, src/eq_momentum2.f90:101-1571,
- * without writing them to device memory); on = 0 runs one operator per
- * derived quantity.  Compact schemes (CP4, CP6) always take the operator
- * path.  No counterpart in the reference, which has only the operator path. */
+/* Fused substep kernels for the CD2 scheme: on = 1 (the default) forms the
+ * momentum right-hand sides of all three components with the fractional step
+ * in one pass that evaluates every interpolation and derivative where it is
+ * needed (the same plans, boundary rows and arithmetic as the operator path
+ * of Compute_momentum_rhs, src/eq_momentum2.f90:101-1571, without writing
+ * them to device memory), likewise the energy right-hand side and the
+ * projection; on = 0 runs one operator per derived quantity.  The other
+ * schemes (CD4, CP4, CP6) always take the operator path.  No counterpart in
+ * the reference, which has only the operator path. */
 int chs_set_fusion(chs_handle* h, int on);
 
 /*
