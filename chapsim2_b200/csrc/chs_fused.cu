@@ -235,11 +235,11 @@ struct FzCtx {
     return TH ? v * muyz(i, j, k) : v;
   }
 
-  // the fractional step of the operator path's O_FRAC store (pfc = 1 * v)
-  __device__ __forceinline__ T frac(int c, int a, T F, T v) const {
+  // the fractional step of the operator path's O_FRAC store (pfc = 1 * v); last = m0[c][a], loaded
+  // by the caller before the stencil loads so that no load waits behind the stores
+  __device__ __forceinline__ T frac(int c, int a, T F, T v, T last) const {
     const T tdt = T(f.dt), tg = T(f.gam), tz = T(f.zeta), ta = T(f.alpha);
     const T pfc = T(1.0) * v;
-    const T last = f.m0[c][a];
     T tot = tg * F + tz * last;
     f.m0[c][a] = F;
     tot = tot + ta * pfc;
@@ -256,6 +256,8 @@ __device__ __forceinline__ T fz_momentum_body(const FzMomentum<T>& f, int i, int
   const FzCtx<T, TH, PY, E> c{f, n0 * n2};
   const int nl = c.nl, L = i + n0 * k;
   const double r = f.rre;
+  const int a = (k * (C == 1 ? np1 : nc1) + j) * n0 + i;
+  const T last = f.m0[C][a];
   T F, v;
   if (C == 0) {
     // x-momentum at (i, j, k) of the qx grid
@@ -269,7 +271,7 @@ __device__ __forceinline__ T fz_momentum_body(const FzMomentum<T>& f, int i, int
         f.term[0][2], f.rows, nl, n0, i, j, k, n2, 1.0, r, [&](int q) { return c.template conv_xz<0>(i, j, q); },
         [&](double s, int q) { return c.visc_xz(s, i, j, q); });
     v = fz_per<D1C2P, T>(f.pres[0], i, n0, [&](int q) { return T(-1.0) * c.pr(q, j, k); });
-    return c.frac(0, (k * nc1 + j) * n0 + i, F, v);
+    return c.frac(0, a, F, v, last);
   } else if (C == 1) {
     // y-momentum at (i, j, k) of the qy grid
     F = fz_pair<D1P2C, 0, PY, E, T>(
@@ -283,7 +285,7 @@ __device__ __forceinline__ T fz_momentum_body(const FzMomentum<T>& f, int i, int
         [&](double s, int q) { return c.visc_yz(s, i, j, q); });
     v = fz_y<D1C2P, PY, E, T>(f.rows, f.pres[1], j, nc1, f.fpres[1], nl, L,
                            [&](int q) { return T(-1.0) * c.pr(i, q, k); });
-    return c.frac(1, (k * np1 + j) * n0 + i, F, v);
+    return c.frac(1, a, F, v, last);
   } else {
     // z-momentum at (i, j, k) of the qz grid
     F = fz_pair<D1P2C, 0, PY, E, T>(
@@ -296,7 +298,7 @@ __device__ __forceinline__ T fz_momentum_body(const FzMomentum<T>& f, int i, int
         f.term[2][2], f.rows, nl, n0, i, j, k, n2, 2.0, r, [&](int q) { return c.template conv_c<2>(i, j, q); },
         [&](double s, int q) { return c.template visc_c<2>(s, i, j, q); });
     v = fz_per<D1C2P, T>(f.pres[2], k, n2, [&](int q) { return T(-1.0) * c.pr(i, j, q); });
-    return c.frac(2, (k * nc1 + j) * n0 + i, F, v);
+    return c.frac(2, a, F, v, last);
   }
 }
 
@@ -410,6 +412,8 @@ __device__ __forceinline__ void fz_energy_body(const FzEnergy<T>& f, int i, int 
   const int n0 = f.n0, nc1 = f.nc1, np1 = f.np1, n2 = f.n2;
   const FzECtx<T, E> c{f, n0 * n2};
   const int nl = c.nl;
+  const int a = (k * nc1 + j) * n0 + i;
+  const T last = f.rhs0[a], rh = f.rhoh[a];
   // x: faces (q, j, k) of the qx grid
   T F = fz_pair<D1P2C, 0, false, E, T>(
       f.term[0], f.rows, nl, n0, i, j, k, n0, 1.0, f.rpr,
@@ -433,13 +437,11 @@ __device__ __forceinline__ void fz_energy_body(const FzEnergy<T>& f, int i, int 
         return T(s) * (c.template zop<D1C2P>(FE_T_Z, f.t, i, j, q) * c.template zop<M1C2P>(FE_K_Z, f.k, i, j, q));
       });
   // energy_advance_kernel: rhs0 = F, rho*h += dt*(gam*F + zeta*rhs0)
-  const int a = (k * nc1 + j) * n0 + i;
   const T tdt = T(f.dt), tg = T(f.gam), tz = T(f.zeta);
-  const T last = f.rhs0[a];
   const T tot = tg * F + tz * last;
   f.rhs0[a] = F;
   const T r1 = tdt * tot;
-  f.rhoh[a] = f.rhoh[a] + r1;
+  f.rhoh[a] = rh + r1;
 }
 
 // The interior rows of the energy pass with every input loaded up front (27 values of the 3D
@@ -455,6 +457,7 @@ __device__ __forceinline__ void fz_energy_interior(const FzEnergy<T>& f, int i, 
   const int ym = c - n0, yp = c + n0;
   const int zm = c + (km - k) * nc1 * n0, zp = c + (kp - k) * nc1 * n0;
   const int pc = (k * np1 + j) * n0 + i;
+  const T last = f.rhs0[c], rh = f.rhoh[c];
   const T h0 = __ldg(f.h + c), hxm = __ldg(f.h + xm), hxp = __ldg(f.h + xp), hym = __ldg(f.h + ym),
           hyp = __ldg(f.h + yp), hzm = __ldg(f.h + zm), hzp = __ldg(f.h + zp);
   const T t0 = __ldg(f.t + c), txm = __ldg(f.t + xm), txp = __ldg(f.t + xp), tym = __ldg(f.t + ym),
@@ -502,11 +505,10 @@ __device__ __forceinline__ void fz_energy_interior(const FzEnergy<T>& f, int i, 
   F += T(f.term[2].a.r1) * (ez1 - ez0) * T(f.term[2].a.dd);
   // energy_advance_kernel: rhs0 = F, rho*h += dt*(gam*F + zeta*rhs0)
   const T tdt = T(f.dt), tg = T(f.gam), tz = T(f.zeta);
-  const T last = f.rhs0[c];
   const T tot = tg * F + tz * last;
   f.rhs0[c] = F;
   const T r1 = tdt * tot;
-  f.rhoh[c] = f.rhoh[c] + r1;
+  f.rhoh[c] = rh + r1;
 }
 
 template <typename T>
@@ -562,28 +564,31 @@ __global__ void __launch_bounds__(256) fz_project_kernel(const __grid_constant__
   auto phi = [&](int ii, int jj, int kk) { return ld(f.phi, n0, nc1, ii, jj, kk); };
   auto rho = [&](int ii, int jj, int kk) { return ld(f.rho, n0, nc1, ii, jj, kk); };
   const T cf = T(f.coef);
+  // every read-modify-write value is loaded before the first store, so that no load waits behind one
+  const int b = (k * np1 + j) * n0 + i;
+  const T uy0 = f.uy[b];
   if (j < nc1) {
     const int a = (k * nc1 + j) * n0 + i;
+    const T p0 = f.p[a], ux0 = f.ux[a], uz0 = f.uz[a];
     // p += phi (axpby with unit weights)
-    T pv = T(1.0) * f.p[a];
+    T pv = T(1.0) * p0;
     pv += T(1.0) * phi(i, j, k);
     f.p[a] = pv;
     const T vx = fz_per<D1C2P, T>(f.in[FP_DX], i, n0, [&](int q) { return phi(q, j, k); });
-    const T gxn = f.ux[a] + cf * vx;
+    const T gxn = ux0 + cf * vx;
     f.ux[a] = gxn;
     const T vz = fz_per<D1C2P, T>(f.in[FP_DZ], k, n2, [&](int q) { return phi(i, j, q); });
-    const T gzn = f.uz[a] + cf * vz;
+    const T gzn = uz0 + cf * vz;
     f.uz[a] = gzn;
     if (TH) {
       f.qx[a] = gxn / (T(1.0) * fz_per<M1C2P, T>(f.in[FP_PX], i, n0, [&](int q) { return rho(q, j, k); }));
       f.qz[a] = gzn / (T(1.0) * fz_per<M1C2P, T>(f.in[FP_PZ], k, n2, [&](int q) { return rho(i, j, q); }));
     }
   }
-  const int b = (k * np1 + j) * n0 + i;
   T vy;
   if (f.periodic_y) vy = fz_per<D1C2P, T>(f.in[FP_DY], j, nc1, [&](int q) { return phi(i, q, k); });
   else vy = fz_row<T>(f.rows, f.in[FP_DY], j, f.fphi, nl, L, [&](int q) { return phi(i, q, k); });
-  T gyn = f.uy[b] + cf * vy;
+  T gyn = uy0 + cf * vy;
   if (f.s0 && j == 0) gyn = T(f.v0);
   if (f.s1 && j == np1 - 1) gyn = T(f.v1);
   f.uy[b] = gyn;
