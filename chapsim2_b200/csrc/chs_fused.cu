@@ -302,9 +302,10 @@ __device__ __forceinline__ T fz_momentum_body(const FzMomentum<T>& f, int i, int
   }
 }
 
-// one momentum component C (0 x, 1 y, 2 z) per thread and output value
+// one momentum component C (0 x, 1 y, 2 z) per thread and output value; at most 64 registers, so that
+// four CTAs fit an SM (the loads of more warps in flight)
 template <typename T, bool TH, bool PY, int C>
-__global__ void __launch_bounds__(256) fz_momentum_kernel(const __grid_constant__ FzMomentum<T> f) {
+__global__ void __launch_bounds__(256, 4) fz_momentum_kernel(const __grid_constant__ FzMomentum<T> f) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
@@ -323,10 +324,34 @@ __global__ void __launch_bounds__(256) fz_momentum_kernel(const __grid_constant_
     const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
     if ((tid & 31) == 0) red[tid >> 5] = s;
     __syncthreads();
+    const int nthr = blockDim.x * blockDim.y * blockDim.z;
+    const int nblk = gridDim.x * gridDim.y * gridDim.z;
+    __shared__ int last;
     if (tid == 0) {
       double t = 0.0;
-      for (int w = 0; w < (int)(blockDim.x * blockDim.y * blockDim.z) / 32; ++w) t += red[w];
+      for (int w = 0; w < nthr / 32; ++w) t += red[w];
       f.part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = t;
+      __threadfence();
+      last = atomicAdd(f.count, 1u) == (unsigned)(nblk - 1);
+    }
+    __syncthreads();
+    if (last) {
+      // every CTA's sum is written: the mean over them in index order (thread t takes t, t + nthr,
+      // ..., then a tree over the threads), read past L1; the counter is left at zero
+      __threadfence();
+      __shared__ double acc[256];
+      double a = 0.0;
+      for (int q = tid; q < nblk; q += nthr) a += __ldcg(f.part + q);
+      acc[tid] = a;
+      __syncthreads();
+      for (int h = nthr / 2; h > 0; h >>= 1) {
+        if (tid < h) acc[tid] += acc[tid + h];
+        __syncthreads();
+      }
+      if (tid == 0) {
+        f.bulk[0] = acc[0] / f.vol;
+        *f.count = 0u;
+      }
     }
   }
 }

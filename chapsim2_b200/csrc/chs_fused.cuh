@@ -79,9 +79,13 @@ struct FzMomentum {
   double rre, dt, gam, zeta, alpha;
   const FzRow* rows;     // row tables of the y operators
   // constant mass flux: the x component also writes, per CTA, the y-weighted sum of its outputs
-  // (wy[j] * m, the numerator of the volume mean), for launch_finalize_mean; null otherwise
+  // (wy[j] * m, the numerator of the volume mean), and the last CTA to finish (count, zero between
+  // launches) writes their sum / vol to bulk[0]; part null otherwise
   const double* wy;
   double* part;
+  unsigned* count;
+  double* bulk;
+  double vol;
 };
 
 // the right-hand side of momentum component c (0 x, 1 y, 2 z) with the fractional step

@@ -1680,9 +1680,6 @@ __global__ void finalize_mean_kernel(const double* __restrict__ partial, int npa
   }
   if (threadIdx.x == 0) out[0] = red[0] / vol;
 }
-void launch_finalize_mean(const double* partial, int npart, double* out, double vol, cudaStream_t st) {
-  finalize_mean_kernel<<<1, 256, 0, st>>>(partial, npart, out, vol);
-}
 template <typename T>
 void launch_weighted_mean(const T* a, const double* wy, int n1, int n2, int n3, double* partial, int npart,
                           double* out, double vol, cudaStream_t st) {

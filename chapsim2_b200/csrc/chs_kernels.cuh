@@ -161,8 +161,6 @@ void launch_fractional_step(T* rhs1, T* rhs0, const T* pfc, int64_t n, double dt
 template <typename T>
 void launch_weighted_mean(const T* a, const double* wy, int n1, int n2, int n3, double* partial, int npart,
                           double* out, double vol, cudaStream_t st);
-// out[0] = sum of partial[0 .. npart) / vol, in a fixed order
-void launch_finalize_mean(const double* partial, int npart, double* out, double vol, cudaStream_t st);
 // q <- q + rhs - (sub ? *sub : 0)
 template <typename T>
 void launch_update_q(T* q, const T* rhs, const double* sub, int64_t n, cudaStream_t st);
