@@ -754,7 +754,6 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 
-// one radix-R butterfly column of a Stockham stage
 // x / d for 0 <= x < 2^23 from a float reciprocal of d with one correction step (the float
 // estimate is within one of the quotient there); avoids an integer division per butterfly
 __device__ __forceinline__ int fast_div(int x, int d, float inv) {
