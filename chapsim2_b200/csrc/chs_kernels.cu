@@ -170,8 +170,19 @@ __global__ void __launch_bounds__(256) line_op_kernel(const __grid_constant__ Op
       T w0 = T(0), w1 = T(0), w2 = col[0], w3 = col[ld], w4;
       T yprev = T(0);
       const T b1 = T(P.b1);
+      // shared-memory values are loaded one or two rows ahead of the recurrence (the input rows
+      // i + 3 and i + 4 are not yet overwritten at row i), so that no load sits on its chain
+      T wa = (2 < nin) ? col[2 * ld] : T(0), wb = (3 < nin) ? col[3 * ld] : T(0);
+      T a1 = sa[0], d1 = sd[0];  // a_i, 1/pivot_i of the current row (row 0 divides by b_1)
       for (int i = 0; i < nout; ++i) {
-        w4 = (i + 2 < nin) ? col[(i + 2) * ld] : T(0);
+        w4 = wa;
+        wa = wb;
+        wb = (i + 4 < nin) ? col[(i + 4) * ld] : T(0);
+        const T ai = a1, di = d1;
+        if (i + 1 < nsw) {
+          a1 = sa[i + 1];
+          d1 = sd[i + 1];
+        }
         T r;
         if (i >= P.b_lo && i <= P.b_hi) {
           if (FAM == M1P2C) r = r1 * (w2 + w3) + r2 * (w1 + w4);
@@ -188,15 +199,21 @@ __global__ void __launch_bounds__(256) line_op_kernel(const __grid_constant__ Op
         }
         T y = r;
         if (i < nsw) {
-          y = (i == 0) ? r / b1 : (r - sa[i] * yprev) * sd[i];
+          y = (i == 0) ? r / b1 : (r - ai * yprev) * di;
           yprev = y;
         }
         col[i * ld] = y;
         w0 = w1; w1 = w2; w2 = w3; w3 = w4;
       }
       T xn = col[(nsw - 1) * ld];
+      T cv = nsw >= 2 ? col[(nsw - 2) * ld] : T(0), cc = nsw >= 2 ? sc[nsw - 2] : T(0);
       for (int i = nsw - 2; i >= 0; --i) {
-        const T x = col[i * ld] - sc[i] * xn;
+        const T vi = cv, ci = cc;
+        if (i > 0) {
+          cv = col[(i - 1) * ld];
+          cc = sc[i - 1];
+        }
+        const T x = vi - ci * xn;
         col[i * ld] = x;
         xn = x;
       }
@@ -731,6 +748,9 @@ void launch_line_op_t(int d, const OpPlan& P, const LineIOT<T>& io, const double
   // (32+ warps) stay resident per SM
   int LT = (io.lt_max == 16 || io.lt_max == 32) ? io.lt_max : 64;  // tunable lines per CTA
   while (LT > 16 && ((size_t)nmax * (LT + 1) + 5 * (size_t)nmax) * sizeof(T) > 45 * 1024) LT /= 2;
+  // and fewer while the grid would not give every SM two CTAs (small grids: a CTA's sweep is the
+  // latency of its lines' recurrences, whatever their number)
+  while (LT > 16 && (nlines + LT - 1) / LT < 2 * 148) LT /= 2;
   const size_t shm = ((size_t)nmax * (LT + 1) + 5 * (size_t)nmax) * sizeof(T);
   if (shm > (size_t)kLineSmemMax) throw std::runtime_error("line operator: line too long for the shared-memory tile");
   if (d == 0) launch_dir<T, 0>(P, io, table, st, nlines, LT, shm);
