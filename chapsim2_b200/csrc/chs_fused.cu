@@ -341,7 +341,14 @@ __global__ void __launch_bounds__(256, 4) fz_momentum_kernel(const __grid_consta
       __threadfence();
       __shared__ double acc[256];
       double a = 0.0;
-      for (int q = tid; q < nblk; q += nthr) a += __ldcg(f.part + q);
+      for (int q0 = tid; q0 < nblk; q0 += 8 * nthr) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = q0 + u * nthr < nblk ? __ldcg(f.part + q0 + u * nthr) : 0.0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (q0 + u * nthr < nblk) a += v[u];
+      }
       acc[tid] = a;
       __syncthreads();
       for (int h = nthr / 2; h > 0; h >>= 1) {
