@@ -8,26 +8,54 @@
 
 namespace chs {
 
+// The operands a store mode reads at the output position (the output itself when accumulating or
+// for O_FRAC, the previous right-hand side and q for O_FRAC, the factor of O_DIV / O_MUL), loaded
+// by load_out before any store of the thread: a load behind a store through another pointer of the
+// same struct waits for that store, a full memory round trip per element.
 template <typename T>
-__device__ __forceinline__ void store_out(const LineIOT<T>& io, int64_t a, T g, T v) {
+struct OutPre {
+  T x;     // the factor of O_DIV / O_MUL, else the output's current value
+  T last;  // O_FRAC: the previous right-hand side
+  T q;     // O_FRAC: q
+};
+template <typename T>
+__device__ __forceinline__ OutPre<T> load_out(const LineIOT<T>& io, int64_t a) {
+  OutPre<T> o{T(0), T(0), T(0)};
+  if (io.omode == O_DIV || io.omode == O_MUL) {
+    o.x = io.onum[a];
+  } else if (io.omode == O_FRAC) {
+    o.x = io.out[a];
+    o.last = io.rhs0[a];
+    if (io.qupd) o.q = io.qupd[a];
+  } else if (io.accumulate) {
+    o.x = io.out[a];
+  }
+  return o;
+}
+template <typename T>
+__device__ __forceinline__ void store_out(const LineIOT<T>& io, int64_t a, T g, T v, const OutPre<T>& o) {
   if (io.omode == O_DIV) {
-    io.out[a] = io.onum[a] / (g * v);
+    io.out[a] = o.x / (g * v);
   } else if (io.omode == O_MUL) {
-    io.out[a] = io.onum[a] * (g * v);
+    io.out[a] = o.x * (g * v);
   } else if (io.omode == O_FRAC) {
     // the arithmetic of fractional_step_kernel with pfc = g*v, then update_q_kernel's q += r
     const T tdt = T(io.dt), tg = T(io.gam), tz = T(io.zeta), ta = T(io.alpha);
     const T pfc = g * v;
-    const T cur = io.out[a], last = io.rhs0[a];
+    const T cur = o.x, last = o.last;
     T tot = tg * cur + tz * last;
     io.rhs0[a] = cur;
     tot = tot + ta * pfc;
     const T r = tdt * tot;
     io.out[a] = r;
-    if (io.qupd) io.qupd[a] = io.qupd[a] + (r - T(0));
+    if (io.qupd) io.qupd[a] = o.q + (r - T(0));
   } else {
-    io.out[a] = io.accumulate ? io.out[a] + g * v : g * v;
+    io.out[a] = io.accumulate ? o.x + g * v : g * v;
   }
+}
+template <typename T>
+__device__ __forceinline__ void store_out(const LineIOT<T>& io, int64_t a, T g, T v) {
+  store_out(io, a, g, v, load_out(io, a));
 }
 
 template <int FAM, typename T, typename F>

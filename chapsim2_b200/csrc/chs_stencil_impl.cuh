@@ -237,9 +237,10 @@ __device__ __forceinline__ void stencil_win_body(const OpPlan& P, const LineIOT<
       *reinterpret_cast<VT*>(io.out + a) = *reinterpret_cast<const VT*>(o);
     } else if (frac) {
       // store_out's O_FRAC arithmetic on vectors of the output, the previous right-hand side and q
-      T cur[V], last[V], r[V];
+      T cur[V], last[V], r[V], q[V];
       *reinterpret_cast<VT*>(cur) = *reinterpret_cast<const VT*>(io.out + a);
       *reinterpret_cast<VT*>(last) = *reinterpret_cast<const VT*>(io.rhs0 + a);
+      if (io.qupd) *reinterpret_cast<VT*>(q) = *reinterpret_cast<const VT*>(io.qupd + a);
 #pragma unroll
       for (int e = 0; e < V; ++e) {
         const T pfc = g * v[e];
@@ -250,15 +251,16 @@ __device__ __forceinline__ void stencil_win_body(const OpPlan& P, const LineIOT<
       *reinterpret_cast<VT*>(io.rhs0 + a) = *reinterpret_cast<const VT*>(cur);
       *reinterpret_cast<VT*>(io.out + a) = *reinterpret_cast<const VT*>(r);
       if (io.qupd) {
-        T q[V];
-        *reinterpret_cast<VT*>(q) = *reinterpret_cast<const VT*>(io.qupd + a);
 #pragma unroll
         for (int e = 0; e < V; ++e) q[e] = q[e] + (r[e] - T(0));
         *reinterpret_cast<VT*>(io.qupd + a) = *reinterpret_cast<const VT*>(q);
       }
     } else {
+      OutPre<T> o[V];
 #pragma unroll
-      for (int e = 0; e < V; ++e) store_out(io, a + e, g, v[e]);
+      for (int e = 0; e < V; ++e) o[e] = load_out(io, a + e);
+#pragma unroll
+      for (int e = 0; e < V; ++e) store_out(io, a + e, g, v[e], o[e]);
     }
   }
 }
