@@ -598,10 +598,17 @@ __global__ void __launch_bounds__(256) fz_project_kernel(const __grid_constant__
   const T cf = T(f.coef);
   // every read-modify-write value is loaded before the first store, so that no load waits behind one
   const int b = (k * np1 + j) * n0 + i;
-  const T uy0 = f.uy[b];
+  T uy0 = f.uy[b];
+  if (f.upd) uy0 = uy0 + (f.my[b] - T(0));
   if (j < nc1) {
     const int a = (k * nc1 + j) * n0 + i;
-    const T p0 = f.p[a], ux0 = f.ux[a], uz0 = f.uz[a];
+    const T p0 = f.p[a];
+    T ux0 = f.ux[a], uz0 = f.uz[a];
+    if (f.upd) {
+      const T s = f.bulk ? T(f.bulk[0]) : T(0);
+      ux0 = ux0 + (f.mx[a] - s);
+      uz0 = uz0 + (f.mz[a] - T(0));
+    }
     // p += phi (axpby with unit weights)
     T pv = T(1.0) * p0;
     pv += T(1.0) * phi(i, j, k);
@@ -628,6 +635,43 @@ __global__ void __launch_bounds__(256) fz_project_kernel(const __grid_constant__
     const T ry = fz_row<T>(f.rows, f.in[FP_PY], j, f.fd, nl, L, [&](int q) { return rho(i, q, k); });
     f.qy[b] = gyn / (T(1.0) * ry);
   }
+}
+
+// ---- momentum advance folded into the Poisson right-hand side: thread per cell (i, j, k)
+template <typename T>
+__global__ void __launch_bounds__(256) fz_update_div_kernel(const __grid_constant__ FzUpdateDiv<T> f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  const int n0 = f.n0, nc1 = f.nc1, np1 = f.np1, n2 = f.n2;
+  if (i >= n0 || j >= nc1 || k >= n2) return;
+  const T s = f.bulk ? T(f.bulk[0]) : T(0);
+  // u' at a face (fz_update_kernel's arithmetic)
+  auto gx = [&](int q) {
+    const int a = (k * nc1 + j) * n0 + q;
+    return __ldg(f.ux + a) + (__ldg(f.mx + a) - s);
+  };
+  auto gy = [&](int q) {
+    const int b = (k * np1 + q) * n0 + i;
+    T v = __ldg(f.uy + b) + (__ldg(f.my + b) - T(0));
+    if (f.s0 && q == 0) v = T(f.v0);
+    if (f.s1 && q == np1 - 1) v = T(f.v1);
+    return v;
+  };
+  auto gz = [&](int q) {
+    const int a = (q * nc1 + j) * n0 + i;
+    return __ldg(f.uz + a) + (__ldg(f.mz + a) - T(0));
+  };
+  const T vx = fz_per<D1P2C, T>(f.dx, i, n0, gx);
+  const T vy = fz_row<T>(f.rows, f.dy, j, f.fdy, n0 * n2, i + n0 * k, gy);
+  const T vz = fz_per<D1P2C, T>(f.dz, k, n2, gz);
+  // run_fused's sum of the three terms with their coefficient
+  const T g = T(f.coeff);
+  T sum = T(0);
+  sum = sum + g * vx;
+  sum = sum + g * vy;
+  sum = sum + g * vz;
+  f.out[(k * nc1 + j) * n0 + i] = sum;
 }
 
 }  // namespace
@@ -681,6 +725,13 @@ void launch_fz_energy_walls(const FzEnergy<T>& f, int mode, T* out, cudaStream_t
 }
 
 template <typename T>
+void launch_fz_update_div(const FzUpdateDiv<T>& f, cudaStream_t st) {
+  const dim3 bs(32, 4, 2);
+  const dim3 grid((f.n0 + bs.x - 1) / bs.x, (f.nc1 + bs.y - 1) / bs.y, (f.n2 + bs.z - 1) / bs.z);
+  fz_update_div_kernel<T><<<grid, bs, 0, st>>>(f);
+}
+
+template <typename T>
 void launch_fz_project(const FzProject<T>& f, cudaStream_t st) {
   const dim3 bs(32, 4, 2);
   const dim3 grid((f.n0 + bs.x - 1) / bs.x, (f.np1 + bs.y - 1) / bs.y, (f.n2 + bs.z - 1) / bs.z);
@@ -700,6 +751,8 @@ template void launch_fz_energy<double>(const FzEnergy<double>&, cudaStream_t);
 template void launch_fz_energy<float>(const FzEnergy<float>&, cudaStream_t);
 template void launch_fz_energy_walls<double>(const FzEnergy<double>&, int, double*, cudaStream_t);
 template void launch_fz_energy_walls<float>(const FzEnergy<float>&, int, float*, cudaStream_t);
+template void launch_fz_update_div<double>(const FzUpdateDiv<double>&, cudaStream_t);
+template void launch_fz_update_div<float>(const FzUpdateDiv<float>&, cudaStream_t);
 template void launch_fz_project<double>(const FzProject<double>&, cudaStream_t);
 template void launch_fz_project<float>(const FzProject<float>&, cudaStream_t);
 

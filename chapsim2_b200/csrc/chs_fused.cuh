@@ -153,8 +153,33 @@ struct FzProject {
   int s0, s1;                     // y walls of uy set to v0 / v1
   double v0, v1;
   const FzRow* rows;
+  // upd: the advance of the momentum step (u += m - bulk, fz_update_kernel's arithmetic) is done
+  // here, at each thread's own point, before the correction (the momentum step left u unchanged)
+  int upd;
+  const T *mx, *my, *mz;
+  const double* bulk;
 };
 template <typename T>
 void launch_fz_project(const FzProject<T>& f, cudaStream_t st);
+
+// Poisson right-hand side coeff * (d/dx ux' + d/dy uy' + d/dz uz') of the advanced fields
+// u' = u + m - bulk (y wall rows of uy' set to v0 / v1), formed at each face from u and m without
+// storing u' (the projection stores it): the divergence of the operator path (run_fused on
+// D1P2C of u') with the momentum advance folded in
+template <typename T>
+struct FzUpdateDiv {
+  int n0, nc1, np1, n2;
+  const T *ux, *uy, *uz, *mx, *my, *mz;
+  const double* bulk;  // mass-flux mean subtracted from mx, or null
+  int s0, s1;
+  double v0, v1;
+  FzOp dx, dy, dz;     // D1P2C: x and z periodic, y a row table
+  const T* fdy;        // y wall planes of the y operator (a plan without boundary values never reads them)
+  const FzRow* rows;
+  T* out;
+  double coeff;
+};
+template <typename T>
+void launch_fz_update_div(const FzUpdateDiv<T>& f, cudaStream_t st);
 
 }  // namespace chs

@@ -1275,7 +1275,7 @@ struct FzBuild {
 // launches (wall planes, fused momentum, mean, advance) instead of the ~50 of the operator path.
 // Returns false (nothing launched) when the configuration needs the operator path.
 template <typename T>
-bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz) {
+bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz, bool defer_update) {
   if (!H->kfuse || H->iacc != ACC_CD2 || !H->fz_rows) return false;
   auto A = [](double* p) { return reinterpret_cast<T*>(p); };
   const auto& B = H->ibc;
@@ -1396,10 +1396,43 @@ bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz)
   }
   // the mass-flux mean, written by the x pass's last CTA
   const double* bulk = H->idriven == 1 ? H->scal + 0 : nullptr;
+  if (defer_update) return true;  // the advance is folded into fused_update_div and fused_project
   const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
   PROFD(H, 3, nf * 9.0, bufs(H->mx, H->my, H->mz, bulk), bufs(ux, uy, uz),
         launch_fz_update<T>(A(ux), A(uy), A(uz), A(H->mx), A(H->my), A(H->mz), bulk, nc0, nc1, np1, nc2, w0,
                             H->fbcy[V_QY][0], w1, H->fbcy[V_QY][1], st));
+  H->launches++;
+  return true;
+}
+
+// The Poisson right-hand side with the momentum advance folded in (FzUpdateDiv); launch false:
+// only whether it can run.
+template <typename T>
+bool fused_update_div(chs_handle* H, int isub, double* ux, double* uy, double* uz, int w0, int w1, bool launch) {
+  if (!H->kfuse || H->iacc != ACC_CD2 || !H->fz_rows) return false;
+  auto A = [](double* p) { return reinterpret_cast<T*>(p); };
+  const auto& B = H->ibc;
+  FzBuild b{H};
+  FzUpdateDiv<T> F{};
+  F.n0 = H->nc[0]; F.nc1 = H->nc[1]; F.np1 = H->np[1]; F.n2 = H->nc[2];
+  F.ux = A(ux); F.uy = A(uy); F.uz = A(uz);
+  F.mx = A(H->mx); F.my = A(H->my); F.mz = A(H->mz);
+  F.bulk = H->idriven == 1 ? H->scal + 0 : nullptr;
+  F.s0 = w0; F.s1 = w1;
+  F.v0 = H->fbcy[V_QY][0]; F.v1 = H->fbcy[V_QY][1];
+  // the plans of the operator path's divergence terms
+  F.dx = b.op(0, D1P2C, P2(B[0][V_QX]), true);
+  F.dy = b.op(1, D1P2C, P2(B[1][V_QY]), false);
+  F.dz = b.op(2, D1P2C, P2(B[2][V_QZ]), false);
+  F.fdy = A(H->fb_maxp);
+  F.rows = H->fz_rows;
+  F.out = A(H->pcor);
+  F.coeff = 1.0 / (H->tAlpha[isub] * H->sigma2p * H->dt);
+  if (!b.ok || H->periodic_y) return false;
+  if (!launch) return true;
+  const double nf = (double)sizeof(T) * H->n_ccc;
+  PROFD(H, 4, nf * 7.0, bufs(ux, uy, uz, H->mx, H->my, H->mz, F.bulk), bufs(H->pcor),
+        launch_fz_update_div<T>(F, st));
   H->launches++;
   return true;
 }
@@ -1481,7 +1514,8 @@ bool fused_energy(chs_handle* H, int isub) {
 // Pressure update, projection, wall enforcement and (variable properties) q = g / rho_face in one
 // launch instead of up to nine; false when the configuration needs the operator path.
 template <typename T>
-bool fused_project(chs_handle* H, int isub, double* ux, double* uy, double* uz, int w0, int w1) {
+bool fused_project(chs_handle* H, int isub, double* ux, double* uy, double* uz, int w0, int w1, bool upd,
+                   bool launch) {
   if (!H->kfuse || H->iacc != ACC_CD2 || !H->fz_rows) return false;
   auto A = [](double* p) { return reinterpret_cast<T*>(p); };
   const auto& B = H->ibc;
@@ -1514,8 +1548,14 @@ bool fused_project(chs_handle* H, int isub, double* ux, double* uy, double* uz, 
   F.s0 = w0; F.s1 = w1;
   F.v0 = H->fbcy[V_QY][0]; F.v1 = H->fbcy[V_QY][1];
   F.rows = H->fz_rows;
+  F.upd = upd ? 1 : 0;
+  F.mx = A(H->mx); F.my = A(H->my); F.mz = A(H->mz);
+  F.bulk = H->idriven == 1 ? H->scal + 0 : nullptr;
+  if (!launch) return true;
   const double nf = (double)sizeof(T) * H->n_ccc;
-  PROFD(H, 3, nf * (TH ? 13.0 : 9.0), bufs(H->pcor, H->fb_pr, TH ? H->dDens : nullptr, TH ? H->fb_d : nullptr),
+  PROFD(H, 3, nf * (TH ? 13.0 : 9.0) + (upd ? 3.0 * nf : 0.0),
+        bufs(H->pcor, H->fb_pr, TH ? H->dDens : nullptr, TH ? H->fb_d : nullptr, upd ? H->mx : nullptr,
+             upd ? H->my : nullptr, upd ? H->mz : nullptr, upd ? F.bulk : nullptr),
         bufs(H->pres, ux, uy, uz, TH ? H->qx : nullptr, TH ? H->qy : nullptr, TH ? H->qz : nullptr),
         launch_fz_project<T>(F, st));
   H->launches++;
@@ -1553,7 +1593,13 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
   double* uz = TH ? H->gz : H->qz;
 
   const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
-  if (!fused_momentum<T>(H, isub, ux, uy, uz)) {
+  // fused path: the momentum advance u += m - bulk is not stored by itself but formed where the
+  // Poisson right-hand side and the projection read u (both fused kernels must be available)
+  const bool defer = fused_update_div<T>(H, isub, ux, uy, uz, w0, w1, false) &&
+                     fused_project<T>(H, isub, ux, uy, uz, w0, w1, true, false);
+  const bool mom_fused = fused_momentum<T>(H, isub, ux, uy, uz, defer);
+  const bool upd = defer && mom_fused;
+  if (!mom_fused) {
   // ---- 1. derived quantities (src/eq_momentum2.f90:347-508)
   run_op(H, 0, M1P2C, bx_qx, any, src(A(H->qx)), s_pcc, A(H->qxix), false, 1.0);
   run_op(H, 0, D1P2C, bx_qx, any, src(A(H->qx)), s_pcc, A(H->qxdx), false, 1.0);
@@ -1713,7 +1759,9 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
   // adds (rho - rho_m1)/dt (Calculate_drhodt, src/eq_continuity.f90:26-78), but
   // Update_thermal_properties has already set rho_m1 = rho, so the term is zero and left out.
   const double coeff = 1.0 / (H->tAlpha[isub] * H->sigma2p * H->dt);
-  {
+  if (upd) {
+    fused_update_div<T>(H, isub, ux, uy, uz, w0, w1, true);
+  } else {
     std::vector<OpTerm<T>> t = {term<T>(0, D1P2C, bx_qx, any, src(A(ux)), s_pcc, coeff, 0),
                                 term<T>(1, D1P2C, by_qy, nullptr, src(A(uy)), s_cpc, coeff, 0),
                                 term<T>(2, D1P2C, bz_qz, nullptr, src(A(uz)), s_ccp, coeff, 0)};
@@ -1722,7 +1770,7 @@ void substep_body_t(chs_handle* H, int isub, int parts) {
     run_fused<T>(H, t, A(H->pcor), s_ccc, EP_STORE, nullptr, isub, nullptr, nullptr, false, true);
   }
   poisson_device<T>(H, A(H->pcor));
-  if (fused_project<T>(H, isub, ux, uy, uz, w0, w1)) return;
+  if (fused_project<T>(H, isub, ux, uy, uz, w0, w1, upd, true)) return;
   PROFD(H, 3, 24.0 / 8.0 * sizeof(T) * H->n_ccc, bufs(H->pcor), bufs(H->pres),
         launch_axpby(A(H->pres), A(H->pres), 1.0, A(H->pcor), 1.0, (int64_t)H->n_ccc, st));
   H->launches++;
