@@ -2978,8 +2978,10 @@ int chs_time_steps_host(chs_handle* H, int nsteps, double* qx, double* qy, doubl
   });
 }
 
-int chs_time_steps_host_fields(chs_handle* H, int nsteps, int nfields, const int* ids, double* const* bufs,
-                               float* ms) {
+// nsteps RK3 steps on host-owned fields, copied in and out around every substep (per_substep) or
+// around every RK3 step
+static int time_host_fields(chs_handle* H, int nsteps, int nfields, const int* ids, double* const* bufs, float* ms,
+                            bool per_substep) {
   if (!H || !ms || nsteps < 0 || nfields < 0 || (nfields > 0 && (!ids || !bufs))) return CHS_ERR_ARG;
   return guard(H, [&] {
     std::vector<double*> dev(nfields);
@@ -3049,7 +3051,8 @@ int chs_time_steps_host_fields(chs_handle* H, int nsteps, int nfields, const int
       bool first = true;
       for (int s = 0; s < nsteps; ++s)
         for (int isub = 1; isub <= 3; ++isub) {
-          for (int p = 0; p < nph; ++p) {
+          const bool cin = per_substep || isub == 1, cout = per_substep || isub == 3;
+          for (int p = 0; p < nph && cin; ++p) {
             for (int f = 0; f < nfields; ++f) {
               if (in_ph[f] != p) continue;
               if (!first) CK(cudaStreamWaitEvent(sin, out_done[f], 0));
@@ -3059,12 +3062,12 @@ int chs_time_steps_host_fields(chs_handle* H, int nsteps, int nfields, const int
           }
           first = false;
           for (int p = 0; p < nph; ++p) {
-            CK(cudaStreamWaitEvent(H->st, in_done[p], 0));
+            if (cin) CK(cudaStreamWaitEvent(H->st, in_done[p], 0));
             CK(cudaGraphLaunch(split ? H->gpart[p][isub] : H->gexec[isub], H->st));
             H->launches += split ? H->kernels_per_part[p][isub] : H->kernels_per_sub[isub];
             CK(cudaEventRecord(graph_done[p], H->st));
           }
-          for (int p = 0; p < nph; ++p) {
+          for (int p = 0; p < nph && cout; ++p) {
             CK(cudaStreamWaitEvent(sout, graph_done[p], 0));
             // the fields the next substep copies in first go out first
             for (int q = 0; q < nph; ++q)
@@ -3090,6 +3093,16 @@ int chs_time_steps_host_fields(chs_handle* H, int nsteps, int nfields, const int
     }
     cleanup();
   });
+}
+
+int chs_time_steps_host_fields(chs_handle* H, int nsteps, int nfields, const int* ids, double* const* bufs,
+                               float* ms) {
+  return time_host_fields(H, nsteps, nfields, ids, bufs, ms, true);
+}
+
+int chs_time_rk3_host_fields(chs_handle* H, int nsteps, int nfields, const int* ids, double* const* bufs,
+                             float* ms) {
+  return time_host_fields(H, nsteps, nfields, ids, bufs, ms, false);
 }
 
 void* chs_host_alloc(size_t bytes) {

@@ -66,6 +66,7 @@ EXPORTED = ["chs_create", "chs_destroy", "chs_upload_field", "chs_download_field
             "chs_plan_inspect", "chs_sync", "chs_kernel_launches", "chs_last_error", "chs_momentum_substep_host",
             "chs_time_steps", "chs_time_steps_host", "chs_host_alloc", "chs_host_free", "chs_profile_substep",
             "chs_poisson_periodic_static", "chs_thermo_init", "chs_energy_substep", "chs_time_steps_host_fields",
+            "chs_time_rk3_host_fields",
             "chs_mlp_train", "chs_mlp_set_mode", "chs_mlp_fallbacks", "chs_mlp_params", "chs_mlp_grad",
             "chs_mlp_eval", "chs_mlp_norm", "chs_ensemble_create", "chs_ensemble_step", "chs_ensemble_time_steps",
             "chs_ensemble_kernel_launches", "chs_ensemble_destroy", "chs_autotune", "chs_set_launch_shape",
@@ -148,6 +149,9 @@ def load():
     L.chs_time_steps_host_fields.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D),
                                              ctypes.POINTER(ctypes.c_float)]
+    L.chs_time_rk3_host_fields.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D),
+                                           ctypes.POINTER(ctypes.c_float)]
     L.chs_energy_substep.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.chs_poisson_periodic_static.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_void_p,
@@ -437,14 +441,15 @@ class Solver:
                                                ctypes.byref(ms)), "chs_time_steps_host")
         return float(ms.value)
 
-    def time_steps_host_fields(self, nsteps, fields):
+    def time_steps_host_fields(self, nsteps, fields, per_substep=True):
         """fields: dict {chs_field id: pinned host array}; returns ms of nsteps steps with the arrays
-        copied in and out every substep."""
+        copied in and out every substep (per_substep) or every RK3 step."""
         ids = (ctypes.c_int * len(fields))(*[int(k) for k in fields])
         bufs = (_D * len(fields))(*[_ptr(a) for a in fields.values()])
         ms = ctypes.c_float()
-        self._check(self.L.chs_time_steps_host_fields(self.h, int(nsteps), len(fields), ids, bufs, ctypes.byref(ms)),
-                    "chs_time_steps_host_fields")
+        fn, name = ((self.L.chs_time_steps_host_fields, "chs_time_steps_host_fields") if per_substep else
+                    (self.L.chs_time_rk3_host_fields, "chs_time_rk3_host_fields"))
+        self._check(fn(self.h, int(nsteps), len(fields), ids, bufs, ctypes.byref(ms)), name)
         return float(ms.value)
 
     def profile_substep(self, isub=1, maxk=512):

@@ -144,6 +144,15 @@ int chs_time_steps_host(chs_handle* h, int nsteps, double* qx, double* qy, doubl
 int chs_time_steps_host_fields(chs_handle* h, int nsteps, int nfields, const int* ids, double* const* bufs,
                                float* ms);
 
+/* The same with the host arrays copied in at the start and out at the end of
+ * every RK3 step (src/chapsim.f90:243-391, one pass of the time loop): the
+ * caller that owns the state on the host between time steps.  A field's
+ * copy-in for the next step follows its copy-out, and with variable
+ * properties the energy part of the first substep starts once its fields are
+ * in.  Same buffer rules as chs_time_steps_host_fields. */
+int chs_time_rk3_host_fields(chs_handle* h, int nsteps, int nfields, const int* ids, double* const* bufs,
+                             float* ms);
+
 /* Page-locked host buffers for the host-array entry points. */
 void* chs_host_alloc(size_t bytes);
 void chs_host_free(void* p);

@@ -122,10 +122,12 @@ def test_indexed_table_lookup_matches_oracle(nonuniform):
     g.close()
 
 
+@pytest.mark.parametrize("per_substep", [True, False])
 @pytest.mark.parametrize("precision", [S.CHS_FP64, S.CHS_MIXED])
-def test_host_fields_pipeline_matches_device_steps(precision):
+def test_host_fields_pipeline_matches_device_steps(precision, per_substep):
     """chs_time_steps_host_fields (pinned host state copied in and out around every substep, the two
-    copy directions overlapped per field) gives the same state as device-resident steps."""
+    copy directions overlapped per field) and chs_time_rk3_host_fields (around every RK3 step) give
+    the same state as device-resident steps."""
     cfg, tc = C.heated_channel(nc=(32, 24, 16), iacc=1, dt=0.004, t_ini=0.49)
     f = I.channel_fields(cfg)
     a = S.Solver(cfg, precision=precision)
@@ -142,7 +144,7 @@ def test_host_fields_pipeline_matches_device_steps(precision):
         h[...] = x
         host[k] = h
     a.step(3)
-    b.time_steps_host_fields(3, host)
+    b.time_steps_host_fields(3, host, per_substep=per_substep)
     for k in ids:
         ref = a.download(k)
         assert np.array_equal(host[k], ref), k
