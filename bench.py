@@ -17,7 +17,7 @@ Poisson solver (poisson_000).  --iacc picks another scheme (CP4/CP6 channels run
 the compact operators with their line solves).
 
 `value` is the plain FP64 path (the drop-in).  `forms` adds the mixed form
-(FP32 fields, operators and RHS; FP64 Poisson, mass-flux mean and checks) on
+(FP32 fields, operators, RHS and x/z transforms; FP64 y solves, mass-flux mean and checks) on
 the same workload and step count, with its speed-up and the relative L2 error
 of its x-z-mean u and T profiles against the FP64 path.
 

@@ -773,6 +773,28 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 }
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// complex element type of the transforms: double2 (the FP64 path) or float2 (the FP32 spectrum of the
+// mixed-precision FISHPACK solver); S its scalar, mk its constructor, tw the plan's twiddles
+template <typename C>
+struct Cplx;
+template <>
+struct Cplx<double2> {
+  using S = double;
+  __device__ static double2 mk(double x, double y) { return make_double2(x, y); }
+  __device__ static const double2* tw(const FftPlan& fp) { return fp.tw; }
+};
+template <>
+struct Cplx<float2> {
+  using S = float;
+  __device__ static float2 mk(float x, float y) { return make_float2(x, y); }
+  __device__ static const float2* tw(const FftPlan& fp) { return fp.twf; }
+};
 
 // x / d for 0 <= x < 2^23 from a float reciprocal of d with one correction step (the float
 // estimate is within one of the quotient there); avoids an integer division per butterfly
@@ -786,38 +808,39 @@ __device__ __forceinline__ int fast_div(int x, int d, float inv) {
 
 // one radix-R butterfly column of a Stockham stage: column j = jq * ns + k (k < ns), input stride
 // n / R, twiddle step n / (ns R); k * r * tstep < n, so the twiddle index needs no reduction
-template <int R>
-__device__ __forceinline__ void stockham_bfly(const double2* in, double2* out, int j, int jq, int k, int stride,
-                                              int ns, int tstep, const double2* tw, int sign) {
-  double2 v[R];
+template <int R, typename C>
+__device__ __forceinline__ void stockham_bfly(const C* in, C* out, int j, int jq, int k, int stride, int ns,
+                                              int tstep, const C* tw, int sign) {
+  using S = typename Cplx<C>::S;
+  C v[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    double2 x = in[j + r * stride];
+    C x = in[j + r * stride];
     if (r > 0 && k > 0) {
-      double2 t = tw[k * r * tstep];
+      C t = tw[k * r * tstep];
       if (sign > 0) t.y = -t.y;
       x = cmul(x, t);
     }
     v[r] = x;
   }
-  const double sg = (double)sign;
+  const S sg = (S)sign;
   if (R == 2) {
-    double2 a = v[0], b = v[1];
+    C a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
   } else if (R == 4) {
-    double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-    double2 b0 = cadd(v[1], v[3]), b1 = csub(v[1], v[3]);
-    double2 ib1 = make_double2(-sg * b1.y, sg * b1.x);  // (i*sign) * b1
+    C a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    C b0 = cadd(v[1], v[3]), b1 = csub(v[1], v[3]);
+    C ib1 = Cplx<C>::mk(-sg * b1.y, sg * b1.x);  // (i*sign) * b1
     v[0] = cadd(a0, b0);
     v[2] = csub(a0, b0);
     v[1] = cadd(a1, ib1);
     v[3] = csub(a1, ib1);
   } else {  // R == 3
-    const double h = 0.86602540378443864676;  // sqrt(3)/2
-    double2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
-    double2 m = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
-    double2 it2 = make_double2(-sg * h * t2.y, sg * h * t2.x);
+    const S h = (S)0.86602540378443864676;  // sqrt(3)/2
+    C t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+    C m = Cplx<C>::mk(v[0].x - (S)0.5 * t1.x, v[0].y - (S)0.5 * t1.y);
+    C it2 = Cplx<C>::mk(-sg * h * t2.y, sg * h * t2.x);
     v[0] = cadd(v[0], t1);
     v[1] = cadd(m, it2);
     v[2] = csub(m, it2);
@@ -830,12 +853,14 @@ __device__ __forceinline__ void stockham_bfly(const double2* in, double2* out, i
 // FFT of `nl` lines of length n stored in buf0 with line stride ls (n, or n + 1 where the line
 // loads and stores run across lines: the padding moves consecutive lines to different banks);
 // result in buf0 or buf1 (returned).  All threads of the CTA take part.
-__device__ double2* smem_fft(double2* buf0, double2* buf1, int nl, const FftPlan& fp, int sign, int ls = 0) {
+template <typename C>
+__device__ C* smem_fft(C* buf0, C* buf1, int nl, const FftPlan& fp, int sign, int ls = 0) {
   const int n = fp.n;
   if (ls == 0) ls = n;
   int ns = 1;
-  double2* in = buf0;
-  double2* out = buf1;
+  C* in = buf0;
+  C* out = buf1;
+  const C* tw = Cplx<C>::tw(fp);
   for (int s = 0; s < fp.nst; ++s) {
     const int R = fp.radix[s];
     const int nb = n / R, tstep = n / (ns * R);
@@ -843,15 +868,15 @@ __device__ double2* smem_fft(double2* buf0, double2* buf1, int nl, const FftPlan
     for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
       const int line = fast_div(t, nb, inb), j = t - line * nb;
       const int jq = fast_div(j, ns, ins), k = j - jq * ns;
-      const double2* li = in + line * ls;
-      double2* lo = out + line * ls;
-      if (R == 4) stockham_bfly<4>(li, lo, j, jq, k, nb, ns, tstep, fp.tw, sign);
-      else if (R == 2) stockham_bfly<2>(li, lo, j, jq, k, nb, ns, tstep, fp.tw, sign);
-      else stockham_bfly<3>(li, lo, j, jq, k, nb, ns, tstep, fp.tw, sign);
+      const C* li = in + line * ls;
+      C* lo = out + line * ls;
+      if (R == 4) stockham_bfly<4, C>(li, lo, j, jq, k, nb, ns, tstep, tw, sign);
+      else if (R == 2) stockham_bfly<2, C>(li, lo, j, jq, k, nb, ns, tstep, tw, sign);
+      else stockham_bfly<3, C>(li, lo, j, jq, k, nb, ns, tstep, tw, sign);
     }
     __syncthreads();
     ns *= R;
-    double2* tmp = in; in = out; out = tmp;
+    C* tmp = in; in = out; out = tmp;
   }
   return in;
 }
@@ -864,67 +889,71 @@ static int fft_lines_per_cta(int n) {
 }
 
 // real rows -> half spectra; two real rows per complex transform (rows of type R, FP64 transform)
-template <typename R>
-__global__ void rfft_x_kernel(const __grid_constant__ FftPlan fp, const R* __restrict__ in,
-                              double2* __restrict__ out, int nrows, int lpc) {
-  extern __shared__ double2 sh[];
+template <typename R, typename C>
+__global__ void rfft_x_kernel(const __grid_constant__ FftPlan fp, const R* __restrict__ in, C* __restrict__ out,
+                              int nrows, int lpc) {
+  using S = typename Cplx<C>::S;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  C* sh = reinterpret_cast<C*>(fft_smem);
   const int n = fp.n, nh = n / 2 + 1;
-  double2* b0 = sh;
-  double2* b1 = sh + (size_t)lpc * n;
+  C* b0 = sh;
+  C* b1 = sh + (size_t)lpc * n;
   const int pair0 = blockIdx.x * lpc;
   const float inn = 1.0f / (float)n, innh = 1.0f / (float)nh;
   for (int t0 = threadIdx.x; t0 < lpc * n; t0 += 4 * blockDim.x) {
-    double a[4], b[4];
+    S a[4], b[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int t = t0 + u * blockDim.x;
-      a[u] = 0.0;
-      b[u] = 0.0;
+      a[u] = S(0);
+      b[u] = S(0);
       if (t < lpc * n) {
         const int l = fast_div(t, n, inn), p = t - l * n;
         const int ra = 2 * (pair0 + l), rb = ra + 1;
-        if (ra < nrows) a[u] = (double)in[(int64_t)ra * n + p];
-        if (rb < nrows) b[u] = (double)in[(int64_t)rb * n + p];
+        if (ra < nrows) a[u] = (S)in[(int64_t)ra * n + p];
+        if (rb < nrows) b[u] = (S)in[(int64_t)rb * n + p];
       }
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int t = t0 + u * blockDim.x;
-      if (t < lpc * n) b0[t] = make_double2(a[u], b[u]);
+      if (t < lpc * n) b0[t] = Cplx<C>::mk(a[u], b[u]);
     }
   }
   __syncthreads();
-  double2* r = smem_fft(b0, b1, lpc, fp, -1);
+  C* r = smem_fft(b0, b1, lpc, fp, -1);
   for (int t = threadIdx.x; t < lpc * nh; t += blockDim.x) {
     const int l = fast_div(t, nh, innh), k = t - l * nh;
     const int ra = 2 * (pair0 + l), rb = ra + 1;
-    const double2 z = r[l * n + k];
-    double2 zc = r[l * n + (k == 0 ? 0 : n - k)];
+    const C z = r[l * n + k];
+    C zc = r[l * n + (k == 0 ? 0 : n - k)];
     zc.y = -zc.y;
-    const double2 xa = make_double2(0.5 * (z.x + zc.x), 0.5 * (z.y + zc.y));
-    const double2 d = csub(z, zc);
-    const double2 xb = make_double2(0.5 * d.y, -0.5 * d.x);
+    const C xa = Cplx<C>::mk((S)0.5 * (z.x + zc.x), (S)0.5 * (z.y + zc.y));
+    const C d = csub(z, zc);
+    const C xb = Cplx<C>::mk((S)0.5 * d.y, (S)-0.5 * d.x);
     if (ra < nrows) out[(int64_t)ra * nh + k] = xa;
     if (rb < nrows) out[(int64_t)rb * nh + k] = xb;
   }
 }
 
-template <typename R>
-__global__ void irfft_x_kernel(const __grid_constant__ FftPlan fp, const double2* __restrict__ in,
-                               R* __restrict__ out, int nrows, double scale, int lpc) {
-  extern __shared__ double2 sh[];
+template <typename R, typename C>
+__global__ void irfft_x_kernel(const __grid_constant__ FftPlan fp, const C* __restrict__ in, R* __restrict__ out,
+                               int nrows, double scale, int lpc) {
+  using S = typename Cplx<C>::S;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  C* sh = reinterpret_cast<C*>(fft_smem);
   const int n = fp.n, nh = n / 2 + 1;
-  double2* b0 = sh;
-  double2* b1 = sh + (size_t)lpc * n;
+  C* b0 = sh;
+  C* b1 = sh + (size_t)lpc * n;
   const int pair0 = blockIdx.x * lpc;
   const float inn = 1.0f / (float)n;
   for (int t0 = threadIdx.x; t0 < lpc * n; t0 += 4 * blockDim.x) {
-    double2 xa[4], xb[4];
+    C xa[4], xb[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int t = t0 + u * blockDim.x;
-      xa[u] = make_double2(0.0, 0.0);
-      xb[u] = make_double2(0.0, 0.0);
+      xa[u] = Cplx<C>::mk(S(0), S(0));
+      xb[u] = Cplx<C>::mk(S(0), S(0));
       if (t < lpc * n) {
         const int l = fast_div(t, n, inn), k = t - l * n;
         const int ra = 2 * (pair0 + l), rb = ra + 1;
@@ -940,31 +969,35 @@ __global__ void irfft_x_kernel(const __grid_constant__ FftPlan fp, const double2
         const int k = t - fast_div(t, n, inn) * n;
         const bool hi = k > n / 2;
         const int kk = hi ? n - k : k;
-        double2 A = xa[u], B = xb[u];
-        if (kk == 0 || 2 * kk == n) { A.y = 0.0; B.y = 0.0; }
+        C A = xa[u], B = xb[u];
+        if (kk == 0 || 2 * kk == n) { A.y = S(0); B.y = S(0); }
         if (hi) { A.y = -A.y; B.y = -B.y; }
-        b0[t] = make_double2(A.x - B.y, A.y + B.x);  // xa + i*xb
+        b0[t] = Cplx<C>::mk(A.x - B.y, A.y + B.x);  // xa + i*xb
       }
     }
   }
   __syncthreads();
-  double2* r = smem_fft(b0, b1, lpc, fp, +1);
+  C* r = smem_fft(b0, b1, lpc, fp, +1);
+  const S sc = (S)scale;
   for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
     const int l = fast_div(t, n, inn), p = t - l * n;
     const int ra = 2 * (pair0 + l), rb = ra + 1;
-    const double2 z = r[t];
-    if (ra < nrows) out[(int64_t)ra * n + p] = R(z.x * scale);
-    if (rb < nrows) out[(int64_t)rb * n + p] = R(z.y * scale);
+    const C z = r[t];
+    if (ra < nrows) out[(int64_t)ra * n + p] = R(z.x * sc);
+    if (rb < nrows) out[(int64_t)rb * n + p] = R(z.y * sc);
   }
 }
 
-__global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __restrict__ data, int na, int nb,
+template <typename C>
+__global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, C* __restrict__ data, int na, int nb,
                                  int64_t bstride, int64_t stride, int sign, int lpc) {
-  extern __shared__ double2 sh[];
+  using S = typename Cplx<C>::S;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  C* sh = reinterpret_cast<C*>(fft_smem);
   __shared__ int64_t lbase[32];  // start of each of the CTA's lines (lpc <= 32), -1 past the end
   const int n = fp.n, ls = n + 1;  // padded line stride: the loads and stores run across lines
-  double2* b0 = sh;
-  double2* b1 = sh + (size_t)lpc * ls;
+  C* b0 = sh;
+  C* b1 = sh + (size_t)lpc * ls;
   const int64_t g0 = (int64_t)blockIdx.x * lpc;
   const int64_t nlines = (int64_t)na * nb;
   if (threadIdx.x < lpc) {
@@ -979,11 +1012,11 @@ __global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __
   __syncthreads();
   const float ilpc = 1.0f / (float)lpc;
   for (int t0 = threadIdx.x; t0 < lpc * n; t0 += 4 * blockDim.x) {
-    double2 v[4];
+    C v[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int t = t0 + u * blockDim.x;
-      v[u] = make_double2(0.0, 0.0);
+      v[u] = Cplx<C>::mk(S(0), S(0));
       if (t < lpc * n) {
         const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
         const int64_t base = lbase[l];
@@ -1000,7 +1033,7 @@ __global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __
     }
   }
   __syncthreads();
-  double2* r = smem_fft(b0, b1, lpc, fp, sign, ls);
+  C* r = smem_fft(b0, b1, lpc, fp, sign, ls);
   for (int t = threadIdx.x; t < lpc * n; t += blockDim.x) {
     const int p = fast_div(t, lpc, ilpc), l = t - p * lpc;
     const int64_t base = lbase[l];
@@ -1008,37 +1041,42 @@ __global__ void cfft_axis_kernel(const __grid_constant__ FftPlan fp, double2* __
   }
 }
 
-template <typename R>
-void launch_rfft_x(const FftPlan& fp, const R* in, double2* out, int nrows, cudaStream_t st) {
+template <typename R, typename C>
+void launch_rfft_x(const FftPlan& fp, const R* in, C* out, int nrows, cudaStream_t st) {
   const int lpc = fft_lines_per_cta(fp.n);
   const int npairs = (nrows + 1) / 2;
-  const size_t shm = 2 * (size_t)lpc * fp.n * sizeof(double2);
-  cudaFuncSetAttribute(rfft_x_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-  rfft_x_kernel<R><<<(npairs + lpc - 1) / lpc, 256, shm, st>>>(fp, in, out, nrows, lpc);
+  const size_t shm = 2 * (size_t)lpc * fp.n * sizeof(C);
+  cudaFuncSetAttribute(rfft_x_kernel<R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  rfft_x_kernel<R, C><<<(npairs + lpc - 1) / lpc, 256, shm, st>>>(fp, in, out, nrows, lpc);
 }
 
-template <typename R>
-void launch_irfft_x(const FftPlan& fp, const double2* in, R* out, int nrows, double scale, cudaStream_t st) {
+template <typename R, typename C>
+void launch_irfft_x(const FftPlan& fp, const C* in, R* out, int nrows, double scale, cudaStream_t st) {
   const int lpc = fft_lines_per_cta(fp.n);
   const int npairs = (nrows + 1) / 2;
-  const size_t shm = 2 * (size_t)lpc * fp.n * sizeof(double2);
-  cudaFuncSetAttribute(irfft_x_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-  irfft_x_kernel<R><<<(npairs + lpc - 1) / lpc, 256, shm, st>>>(fp, in, out, nrows, scale, lpc);
+  const size_t shm = 2 * (size_t)lpc * fp.n * sizeof(C);
+  cudaFuncSetAttribute(irfft_x_kernel<R, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  irfft_x_kernel<R, C><<<(npairs + lpc - 1) / lpc, 256, shm, st>>>(fp, in, out, nrows, scale, lpc);
 }
-template void launch_rfft_x<double>(const FftPlan&, const double*, double2*, int, cudaStream_t);
-template void launch_rfft_x<float>(const FftPlan&, const float*, double2*, int, cudaStream_t);
-template void launch_irfft_x<double>(const FftPlan&, const double2*, double*, int, double, cudaStream_t);
-template void launch_irfft_x<float>(const FftPlan&, const double2*, float*, int, double, cudaStream_t);
+template void launch_rfft_x<double, double2>(const FftPlan&, const double*, double2*, int, cudaStream_t);
+template void launch_rfft_x<float, double2>(const FftPlan&, const float*, double2*, int, cudaStream_t);
+template void launch_rfft_x<float, float2>(const FftPlan&, const float*, float2*, int, cudaStream_t);
+template void launch_irfft_x<double, double2>(const FftPlan&, const double2*, double*, int, double, cudaStream_t);
+template void launch_irfft_x<float, double2>(const FftPlan&, const double2*, float*, int, double, cudaStream_t);
+template void launch_irfft_x<float, float2>(const FftPlan&, const float2*, float*, int, double, cudaStream_t);
 
-void launch_cfft_axis(const FftPlan& fp, double2* data, int na, int nb, int64_t bstride, int64_t stride, int sign,
+template <typename C>
+void launch_cfft_axis(const FftPlan& fp, C* data, int na, int nb, int64_t bstride, int64_t stride, int sign,
                       cudaStream_t st) {
   const int lpc = fft_lines_per_cta(fp.n);
   const int64_t nlines = (int64_t)na * nb;
-  const size_t shm = 2 * (size_t)lpc * (fp.n + 1) * sizeof(double2);
-  cudaFuncSetAttribute(cfft_axis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-  cfft_axis_kernel<<<(unsigned)((nlines + lpc - 1) / lpc), 256, shm, st>>>(fp, data, na, nb, bstride, stride, sign,
-                                                                            lpc);
+  const size_t shm = 2 * (size_t)lpc * (fp.n + 1) * sizeof(C);
+  cudaFuncSetAttribute(cfft_axis_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  cfft_axis_kernel<C><<<(unsigned)((nlines + lpc - 1) / lpc), 256, shm, st>>>(fp, data, na, nb, bstride, stride,
+                                                                               sign, lpc);
 }
+template void launch_cfft_axis<double2>(const FftPlan&, double2*, int, int, int64_t, int64_t, int, cudaStream_t);
+template void launch_cfft_axis<float2>(const FftPlan&, float2*, int, int, int64_t, int64_t, int, cudaStream_t);
 
 // ===========================================================================
 // FISHPACK y solve: TRID0 (src/poisson_fishpack.f90:20-57) per (kx, kz) on complex data
@@ -1085,7 +1123,19 @@ void launch_ysolve_factor(double* Zr, double* D, int nxh, int ny, int nz, const 
 // One CTA per `lt` consecutive (kx, kz) columns: the columns and their precomputed factors are
 // staged in shared memory with coalesced row loads by all threads (eight loads in flight per
 // thread), swept by `lt` threads (one column each), and written back.
-__global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data, int nxh, int ny, int nz,
+// The spectrum is double2 (FP64 path) or float2 (the FP32 spectrum of the mixed-precision path); the
+// solve itself always runs in FP64.
+__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.y); }
+template <typename C>
+__device__ __forceinline__ C from_d2(double2 v);
+template <>
+__device__ __forceinline__ double2 from_d2<double2>(double2 v) { return v; }
+template <>
+__device__ __forceinline__ float2 from_d2<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+
+template <typename C>
+__global__ void __launch_bounds__(128) ysolve_kernel(C* __restrict__ data, int nxh, int ny, int nz,
                                                      const double* __restrict__ Zr, const double* __restrict__ D,
                                                      const double* __restrict__ pa, int lt) {
   extern __shared__ __align__(16) double2 sT[];  // [ny][lt] right-hand sides / solution
@@ -1098,7 +1148,7 @@ __global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data,
   const int kz = ok ? (int)(g / nxh) : 0;
   const int kx = ok ? (int)(g - (int64_t)kz * nxh) : 0;
   const int64_t base = (int64_t)kz * ny * nxh + kx;
-  double2* col = data + base;
+  C* col = data + base;
   const int jstep = blockDim.x / lt;
   if (ok) {
     for (int j0 = tid / lt; j0 < ny; j0 += 4 * jstep) {
@@ -1108,7 +1158,7 @@ __global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data,
       for (int u = 0; u < 4; ++u) {
         const int j = j0 + u * jstep;
         if (j < ny) {
-          v[u] = col[(int64_t)j * nxh];
+          v[u] = to_d2(col[(int64_t)j * nxh]);
           z[u] = Zr[base + (int64_t)j * nxh];
           d[u] = D[base + (int64_t)j * nxh];
         }
@@ -1161,7 +1211,7 @@ __global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data,
   }
   __syncthreads();
   if (ok)
-    for (int j = tid / lt; j < ny; j += jstep) col[(int64_t)j * nxh] = sT[j * lt + l];
+    for (int j = tid / lt; j < ny; j += jstep) col[(int64_t)j * nxh] = from_d2<C>(sT[j * lt + l]);
 }
 
 // The same solve with one thread per (kx, kz) line working in place in global memory: at a fixed
@@ -1169,7 +1219,8 @@ __global__ void __launch_bounds__(128) ysolve_kernel(double2* __restrict__ data,
 // loads eight rows ahead of its sweep, so the sequential recurrences of many lines overlap.  The
 // arithmetic and its order are those of ysolve_kernel.
 constexpr int kYsBatch = 8;
-__global__ void __launch_bounds__(128) ysolve_lines_kernel(double2* __restrict__ data, int nxh, int ny, int nz,
+template <typename C>
+__global__ void __launch_bounds__(128) ysolve_lines_kernel(C* __restrict__ data, int nxh, int ny, int nz,
                                                            const double* __restrict__ Zr,
                                                            const double* __restrict__ D,
                                                            const double* __restrict__ pa) {
@@ -1177,22 +1228,22 @@ __global__ void __launch_bounds__(128) ysolve_lines_kernel(double2* __restrict__
   if (g >= (int64_t)nxh * nz) return;
   const int kz = (int)(g / nxh), kx = (int)(g - (int64_t)kz * nxh);
   const int64_t base = (int64_t)kz * ny * nxh + kx;
-  double2* col = data + base;
+  C* col = data + base;
   const double* zr = Zr + base;
   const double* dd = D + base;
   const int64_t s = nxh;
-  double2 tp = col[0];
+  double2 tp = to_d2(col[0]);
   const double Z0 = zr[0];
   tp.x *= Z0;
   tp.y *= Z0;
-  col[0] = tp;
+  col[0] = from_d2<C>(tp);
   for (int j0 = 1; j0 < ny - 1; j0 += kYsBatch) {
     double2 v[kYsBatch];
     double z[kYsBatch];
 #pragma unroll
     for (int u = 0; u < kYsBatch; ++u)
       if (j0 + u < ny - 1) {
-        v[u] = col[(j0 + u) * s];
+        v[u] = to_d2(col[(j0 + u) * s]);
         z[u] = zr[(j0 + u) * s];
       }
 #pragma unroll
@@ -1205,10 +1256,10 @@ __global__ void __launch_bounds__(128) ysolve_lines_kernel(double2* __restrict__
       }
 #pragma unroll
     for (int u = 0; u < kYsBatch; ++u)
-      if (j0 + u < ny - 1) col[(j0 + u) * s] = v[u];
+      if (j0 + u < ny - 1) col[(j0 + u) * s] = from_d2<C>(v[u]);
   }
   const double zl = zr[(ny - 1) * s];
-  double2 v = col[(ny - 1) * s];
+  double2 v = to_d2(col[(ny - 1) * s]);
   // TRID0's singular-pivot pin: the last unknown is zero when the pivot vanishes
   if (zl != 0.0) {
     v.x = (v.x - __ldg(pa + ny - 1) * tp.x) / zl;
@@ -1217,14 +1268,14 @@ __global__ void __launch_bounds__(128) ysolve_lines_kernel(double2* __restrict__
     v.x = 0.0;
     v.y = 0.0;
   }
-  col[(ny - 1) * s] = v;
+  col[(ny - 1) * s] = from_d2<C>(v);
   for (int j0 = ny - 2; j0 >= 0; j0 -= kYsBatch) {
     double2 w[kYsBatch];
     double d[kYsBatch];
 #pragma unroll
     for (int u = 0; u < kYsBatch; ++u)
       if (j0 - u >= 0) {
-        w[u] = col[(j0 - u) * s];
+        w[u] = to_d2(col[(j0 - u) * s]);
         d[u] = dd[(j0 - u) * s];
       }
 #pragma unroll
@@ -1236,17 +1287,18 @@ __global__ void __launch_bounds__(128) ysolve_lines_kernel(double2* __restrict__
       }
 #pragma unroll
     for (int u = 0; u < kYsBatch; ++u)
-      if (j0 - u >= 0) col[(j0 - u) * s] = w[u];
+      if (j0 - u >= 0) col[(j0 - u) * s] = from_d2<C>(w[u]);
   }
 }
 
-void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* Zr, const double* D, const double* pa,
+template <typename C>
+void launch_ysolve(C* data, int nxh, int ny, int nz, const double* Zr, const double* D, const double* pa,
                    cudaStream_t st) {
   if (ny < 2) throw std::runtime_error("ysolve: ny must be at least 2");
   if (ny > 160) {
     // tall columns: the shared-memory tile leaves too few solving threads per SM
     const int64_t n = (int64_t)nxh * nz;
-    ysolve_lines_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(data, nxh, ny, nz, Zr, D, pa);
+    ysolve_lines_kernel<C><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(data, nxh, ny, nz, Zr, D, pa);
     return;
   }
   // 16 columns per CTA: a CTA's load, sweep and store phases run one after another, so several
@@ -1257,12 +1309,16 @@ void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* Zr, con
   if (shm > 200 * 1024) throw std::runtime_error("ysolve: ny too large for the shared-memory tile");
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(ysolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(ysolve_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set = true;
   }
   const int64_t n = (int64_t)nxh * nz;
-  ysolve_kernel<<<(unsigned)((n + lt - 1) / lt), 128, shm, st>>>(data, nxh, ny, nz, Zr, D, pa, lt);
+  ysolve_kernel<C><<<(unsigned)((n + lt - 1) / lt), 128, shm, st>>>(data, nxh, ny, nz, Zr, D, pa, lt);
 }
+template void launch_ysolve<double2>(double2*, int, int, int, const double*, const double*, const double*,
+                                     cudaStream_t);
+template void launch_ysolve<float2>(float2*, int, int, int, const double*, const double*, const double*,
+                                    cudaStream_t);
 
 __global__ void spectral_divide_kernel(double2* __restrict__ data, int nxh, int ny, int nz,
                                        const double* __restrict__ k2x, const double* __restrict__ k2y,

@@ -116,23 +116,28 @@ struct FftPlan {
   int nst;          // number of radix stages
   int radix[16];
   const double2* tw;  // exp(-2 pi i m / n), m = 0..n-1 (device)
+  const float2* twf;  // the same rounded to FP32 (device; the FP32 spectrum of the mixed form), or null
 };
 
-// real x-lines (rows of length nx, R = double or float) -> FP64 half spectra (rows of nx/2+1)
-template <typename R>
-void launch_rfft_x(const FftPlan& fp, const R* in, double2* out, int nrows, cudaStream_t st);
-// FP64 half spectra -> real x-lines, scaled by `scale`
-template <typename R>
-void launch_irfft_x(const FftPlan& fp, const double2* in, R* out, int nrows, double scale, cudaStream_t st);
+// real x-lines (rows of length nx, R = double or float) -> half spectra (rows of nx/2+1) of
+// complex type C (double2: FP64 transforms; float2: FP32 transforms of float rows)
+template <typename R, typename C>
+void launch_rfft_x(const FftPlan& fp, const R* in, C* out, int nrows, cudaStream_t st);
+// half spectra -> real x-lines, scaled by `scale`
+template <typename R, typename C>
+void launch_irfft_x(const FftPlan& fp, const C* in, R* out, int nrows, double scale, cudaStream_t st);
 // complex FFT along a strided axis: element (line, p) at base(line) + p*stride,
 // line = a + na*b with base = a + b*bstride (a fastest); sign -1 forward, +1 backward
-void launch_cfft_axis(const FftPlan& fp, double2* data, int na, int nb, int64_t bstride, int64_t stride, int sign,
+template <typename C>
+void launch_cfft_axis(const FftPlan& fp, C* data, int na, int nb, int64_t bstride, int64_t stride, int sign,
                       cudaStream_t st);
 // forward-sweep factors of the FISHPACK y solve per (kx, kz), computed once (layout (kz, j, kx))
 void launch_ysolve_factor(double* Zr, double* D, int nxh, int ny, int nz, const double* pa, const double* pb,
                           const double* pc, const double* lamx, const double* lamz, cudaStream_t st);
-// y tridiagonal solve per (kx, kz) of the FISHPACK path (TRID0 with the singular-pivot pin)
-void launch_ysolve(double2* data, int nxh, int ny, int nz, const double* Zr, const double* D, const double* pa,
+// y tridiagonal solve per (kx, kz) of the FISHPACK path (TRID0 with the singular-pivot pin), in
+// FP64 on a double2 or float2 spectrum
+template <typename C>
+void launch_ysolve(C* data, int nxh, int ny, int nz, const double* Zr, const double* D, const double* pa,
                    cudaStream_t st);
 // poisson_010 y stage per (kx, kz) column: reordering, y FFT, cosine post-processing, the
 // pentadiagonal solves (ptab: per system s = 0 odd / 1 even cosine modes and row r < ny/2 the

@@ -914,18 +914,22 @@ void setup_device(chs_handle* H, const chs_config* c) {
   // Poisson tables
   std::vector<double2> tw;
   const int nxh = nc0 / 2 + 1;
+  // twiddles in FP64 and, for the FP32 spectrum of the mixed form, rounded to FP32
+  auto upload_tw = [&](FftPlan& fp) {
+    double2* d = H->dalloc<double2>(tw.size());
+    CK(cudaMemcpyAsync(d, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, H->st));
+    fp.tw = d;
+    std::vector<float2> twf(tw.size());
+    for (size_t m = 0; m < tw.size(); ++m) twf[m] = make_float2((float)tw[m].x, (float)tw[m].y);
+    float2* f = H->dalloc<float2>(twf.size());
+    CK(cudaMemcpyAsync(f, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice, H->st));
+    CK(cudaStreamSynchronize(H->st));  // twf is a local vector
+    fp.twf = f;
+  };
   H->fx = make_fft(nc0, tw);
-  {
-    double2* d = H->dalloc<double2>(tw.size());
-    CK(cudaMemcpyAsync(d, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, H->st));
-    H->fx.tw = d;
-  }
+  upload_tw(H->fx);
   H->fz = make_fft(nc2, tw);
-  {
-    double2* d = H->dalloc<double2>(tw.size());
-    CK(cudaMemcpyAsync(d, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, H->st));
-    H->fz.tw = d;
-  }
+  upload_tw(H->fz);
   H->spec = H->dalloc<double2>((size_t)nxh * nc1 * nc2);
   const double pi = 2.0 * std::asin(1.0);
   if (H->ifft == 2) {
@@ -1182,6 +1186,19 @@ void poisson_device(chs_handle* H, T* rhs) {
   const int nxh = nc0 / 2 + 1;
   cudaStream_t st = H->st;
   const double nreal = (double)nc0 * nc1 * nc2, nspec = (double)nxh * nc1 * nc2;
+  if (H->ifft == 2 && sizeof(T) == sizeof(float) && H->fx.twf && H->fz.twf) {
+    // mixed form, FISHPACK: the x and z transforms in FP32 on an FP32 spectrum, the y solve (the
+    // wall-normal tridiagonal systems and the pinned kx = kz = 0 mode) in FP64
+    float2* sp = reinterpret_cast<float2*>(H->spec);
+    const double b_r2c = 4.0 * nreal + 8.0 * nspec, b_c2c = 16.0 * nspec;
+    PROF(H, 1, b_r2c, launch_rfft_x(H->fx, rhs, sp, nc1 * nc2, st));
+    PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, sp, nxh, nc1, nxh, (int64_t)nxh * nc1, -1, st));
+    PROF(H, 2, 32.0 * nspec, launch_ysolve(sp, nxh, nc1, nc2, H->yzr, H->yd, H->pa, st));
+    PROF(H, 1, b_c2c, launch_cfft_axis(H->fz, sp, nxh, nc1, nxh, (int64_t)nxh * nc1, +1, st));
+    PROF(H, 1, b_r2c, launch_irfft_x(H->fx, sp, rhs, nc1 * nc2, 1.0 / ((double)nc0 * (double)nc2), st));
+    H->launches += 5;
+    return;
+  }
   const double b_r2c = (double)sizeof(T) * nreal + 16.0 * nspec, b_c2c = 32.0 * nspec;
   PROF(H, 1, b_r2c, launch_rfft_x(H->fx, rhs, H->spec, nc1 * nc2, st));
   if (H->ifft == 2) {
