@@ -3,7 +3,7 @@ fixtures (tests/golden/*.npz, made by tests/golden/make_long_runs.py).
 
 * heated channel 128x96x128 (the benchmark workload), 500 RK3 steps: x-z-mean u, T, h, rho and p
   profiles, u/v/w rms profiles, bulk velocity and kinetic energy every 50 steps, FP64 and the
-  mixed-precision form (north star: <= 1e-5 relative L2 on the mean u and T profiles);
+  mixed-precision form (its accuracy bound: <= 1e-5 relative L2 on the mean u and T profiles);
 * flow-only channel 128x96x128, 1000 RK3 steps (when its fixture exists);
 * Taylor-Green vortex 64^3, Re 1600, CP6, 200 RK3 steps: kinetic energy (src/io_monitor.f90:209-241)
   after every step;

@@ -44,7 +44,7 @@ def test_channel_mixed_profiles_vs_oracle(acc, ifft):
         pa = xz_mean_profile(a.reshape(sh))
         pb = xz_mean_profile(b.reshape(sh))
         if name == "qx":
-            # mean streamwise velocity profile
+            # mean streamwise velocity profile: the mixed form's accuracy bound
             assert rel(pa, pb) < 1e-5, (name, rel(pa, pb))
         else:
             # the mean wall-normal and spanwise profiles are near zero: absolute check on the bulk scale
