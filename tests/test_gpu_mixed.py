@@ -1,5 +1,6 @@
-"""Mixed-precision form (FP32 fields, operators and RHS; FP64 Poisson, mass-flux mean and
-divergence check) against the FP64 oracle and the FP64 GPU path."""
+"""Mixed-precision form (FP32 fields, operators, RHS and, with the FISHPACK solver, the x and z
+transforms; FP64 wall-normal Poisson solves, mass-flux mean and divergence check) against the FP64
+oracle and the FP64 GPU path."""
 import numpy as np
 import pytest
 
@@ -92,3 +93,27 @@ def test_tgv_mixed_energy_decay():
     rate = (d["bulk_ke"] - e1) / (10 * cfg.dt)
     assert abs(rate + 0.75 / 1600) < 2e-2 * 0.75 / 1600
     g.close()
+
+
+@pytest.mark.parametrize("nc", [(24, 192, 12), (36, 18, 36)])
+def test_mixed_fp32_spectrum_grids(nc):
+    """The FP32 spectrum of the mixed FISHPACK solver on grids that take the other kernel variants:
+    columns taller than 160 rows (the in-place y solve) and radix-3 transform lengths; the mean
+    streamwise profile after three RK3 steps against the FP64 path, and the FP64 divergence check."""
+    cfg = C.channel(nc=nc, iacc=1, dt=0.002)
+    f = I.channel_fields(cfg)
+    out = []
+    for prec in (S.CHS_FP64, S.CHS_MIXED):
+        g = S.Solver(cfg, precision=prec)
+        g.set_fields(*f)
+        g.Solve_momentum_eq(0)
+        g.step(3)
+        out.append((g.get_fields(), g.diagnostics()))
+        g.close()
+    (a, _), (b, db) = out[1], out[0]
+    sh = cfg.shapes()
+    pa = xz_mean_profile(a[0].reshape(sh[0]))
+    pb = xz_mean_profile(b[0].reshape(sh[0]))
+    assert rel(pa, pb) < 1e-5, rel(pa, pb)
+    assert rel(a[0], b[0]) < 1e-4
+    assert out[1][1]["max_div"] < 1e-4 and out[1][1]["nan_flag"] == 0
