@@ -178,10 +178,12 @@ def dist_setup(n_gpus):
 
 
 def max_over_ranks(dist, v):
+    """The maximum of v over the ranks (NCCL on the GPUs; gloo on the host cores)."""
     if dist is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
