@@ -24,9 +24,13 @@ namespace chs {
 namespace {
 
 // Every array of the fused kernels has x extent n0 and z extent n2 (periodic: points = cells) and y
-// extent nc1 (cell rows) or np1 (point rows); index (k, j, i), x fastest, below 2^31 values.
+// extent nc1 (cell rows) or np1 (point rows); index (k, j, i), x fastest, below 2^31 values.  The
+// FP64 kernels form the index as k * (ny * n0) + (j * n0 + i), whose terms the many stencil loads
+// of a thread share (measured 2 % faster per FP64 step; the FP32 kernels keep the nested form,
+// which measured faster for them).
 template <typename T>
 __device__ __forceinline__ T ld(const T* __restrict__ a, int n0, int ny, int i, int j, int k) {
+  if (sizeof(T) == 8) return __ldg(a + (k * (ny * n0) + (j * n0 + i)));
   return __ldg(a + (k * ny + j) * n0 + i);
 }
 
