@@ -36,14 +36,18 @@ __device__ __forceinline__ T ld(const T* __restrict__ a, int n0, int ny, int i, 
 
 // periodic CD2 operator of family FAM at row p: the bulk formula of stencil_op_kernel (bulk_fn with
 // r2 = 0) on wrapped indices, times dd
-template <int FAM, typename T, typename F>
+// W false: the caller's rows p-1 .. p+1 lie inside 0 .. n-1 (a CTA away from the periodic seam), so
+// the neighbours need no wrap
+template <int FAM, typename T, bool W = true, typename F>
 __device__ __forceinline__ T fz_per(const FzOp& o, int p, int n, const F& f) {
   const T r1 = T(o.r1);
+  const int pp = W ? (p + 1 < n ? p + 1 : 0) : p + 1;
+  const int pm = W ? (p > 0 ? p - 1 : n - 1) : p - 1;
   T v;
-  if (FAM == M1P2C) v = r1 * (f(p) + f(p + 1 < n ? p + 1 : 0));
-  else if (FAM == M1C2P) v = r1 * (f(p) + f(p > 0 ? p - 1 : n - 1));
-  else if (FAM == D1C2P) v = r1 * (f(p) - f(p > 0 ? p - 1 : n - 1));
-  else v = r1 * (f(p + 1 < n ? p + 1 : 0) - f(p));  // D1P2C
+  if (FAM == M1P2C) v = r1 * (f(p) + f(pp));
+  else if (FAM == M1C2P) v = r1 * (f(p) + f(pm));
+  else if (FAM == D1C2P) v = r1 * (f(p) - f(pm));
+  else v = r1 * (f(pp) - f(p));  // D1P2C
   return v * T(o.dd);
 }
 
@@ -87,7 +91,7 @@ __device__ __forceinline__ T fz_y(const FzRow* __restrict__ rows, const FzOp& o,
 // op(conv) + w*op(visc) of one direction.  x and z are periodic with one bulk formula for both
 // terms (checked by the host), so one operator runs on conv + (s*w)*visc; a y pair runs on the
 // combined expression when it merges (as the operator path does) and term by term otherwise.
-template <int FAM, int DIR, bool PY, bool E, typename T, typename FC, typename FV>
+template <int FAM, int DIR, bool PY, bool E, typename T, bool WX = true, bool WZ = true, typename FC, typename FV>
 __device__ __forceinline__ T fz_pair(const FzPair<T>& pr, const FzRow* __restrict__ rows, int nl, int n0, int i, int j,
                                      int k, int nin, double sv, double w, const FC& conv, const FV& visc) {
   const double sr = sv * w;
@@ -96,8 +100,8 @@ __device__ __forceinline__ T fz_pair(const FzPair<T>& pr, const FzRow* __restric
     e += visc(sr, q);
     return e;
   };
-  if (DIR == 0) return fz_per<FAM, T>(pr.a, i, nin, comb);
-  if (DIR == 2) return fz_per<FAM, T>(pr.a, k, nin, comb);
+  if (DIR == 0) return fz_per<FAM, T, WX>(pr.a, i, nin, comb);
+  if (DIR == 2) return fz_per<FAM, T, WZ>(pr.a, k, nin, comb);
   if (PY) return fz_per<FAM, T>(pr.a, j, nin, comb);
   const int L = i + n0 * k;
   // interior rows: both terms' plans share the bulk weights (checked by the host)
@@ -116,15 +120,16 @@ __device__ __forceinline__ bool fz_interior_block(int nc1) {
   return j0 >= kFzEdge && j0 + (int)blockDim.y <= nc1 - kFzEdge;
 }
 
-// the inner operators of the momentum equation at one position (E: the row may be near a wall)
-template <typename T, bool TH, bool PY, bool E>
+// the inner operators of the momentum equation at one position (E: the row may be near a wall; WX,
+// WZ: x / z neighbours may wrap around the periodic seam)
+template <typename T, bool TH, bool PY, bool E, bool WX = true, bool WZ = true>
 struct FzCtx {
   const FzMomentum<T>& f;
   int nl;  // lines of a y operator (n0 * n2)
 
   __device__ __forceinline__ T at(const T* a, int ny, int i, int j, int k) const { return ld(a, f.n0, ny, i, j, k); }
-#define FZ_X(FAM, S, A, NY) fz_per<FAM, T>(f.in[S], i, f.n0, [&](int q) { return at(A, NY, q, j, k); })
-#define FZ_Z(FAM, S, A, NY) fz_per<FAM, T>(f.in[S], k, f.n2, [&](int q) { return at(A, NY, i, j, q); })
+#define FZ_X(FAM, S, A, NY) fz_per<FAM, T, WX>(f.in[S], i, f.n0, [&](int q) { return at(A, NY, q, j, k); })
+#define FZ_Z(FAM, S, A, NY) fz_per<FAM, T, WZ>(f.in[S], k, f.n2, [&](int q) { return at(A, NY, i, j, q); })
 #define FZ_Y(FAM, S, A, NY, FB) \
   fz_y<FAM, PY, E, T>(f.rows, f.in[S], j, NY, FB, nl, i + f.n0 * k, [&](int q) { return at(A, NY, i, q, k); })
   // velocity interpolations and derivatives (src/eq_momentum2.f90:347-508)
@@ -161,13 +166,13 @@ struct FzCtx {
   __device__ __forceinline__ T muy(int i, int j, int k) const { return FZ_Y(M1C2P, FI_MU_Y, f.mu, f.nc1, f.fm); }
   __device__ __forceinline__ T mux(int i, int j, int k) const { return FZ_X(M1C2P, FI_MU_X, f.mu, f.nc1); }
   __device__ __forceinline__ T muyx(int i, int j, int k) const {
-    return fz_per<M1C2P, T>(f.in[FI_MU_YX], i, f.n0, [&](int q) { return muy(q, j, k); });
+    return fz_per<M1C2P, T, WX>(f.in[FI_MU_YX], i, f.n0, [&](int q) { return muy(q, j, k); });
   }
   __device__ __forceinline__ T muxz(int i, int j, int k) const {
-    return fz_per<M1C2P, T>(f.in[FI_MU_XZ], k, f.n2, [&](int q) { return mux(i, j, q); });
+    return fz_per<M1C2P, T, WZ>(f.in[FI_MU_XZ], k, f.n2, [&](int q) { return mux(i, j, q); });
   }
   __device__ __forceinline__ T muyz(int i, int j, int k) const {
-    return fz_per<M1C2P, T>(f.in[FI_MU_YZ], k, f.n2, [&](int q) { return muy(i, j, q); });
+    return fz_per<M1C2P, T, WZ>(f.in[FI_MU_YZ], k, f.n2, [&](int q) { return muy(i, j, q); });
   }
 #undef FZ_X
 #undef FZ_Z
@@ -254,10 +259,10 @@ struct FzCtx {
 };
 
 // one momentum component C (0 x, 1 y, 2 z) at (i, j, k)
-template <typename T, bool TH, bool PY, int C, bool E>
+template <typename T, bool TH, bool PY, int C, bool E, bool WX = true, bool WZ = true>
 __device__ __forceinline__ T fz_momentum_body(const FzMomentum<T>& f, int i, int j, int k) {
   const int n0 = f.n0, nc1 = f.nc1, np1 = f.np1, n2 = f.n2;
-  const FzCtx<T, TH, PY, E> c{f, n0 * n2};
+  const FzCtx<T, TH, PY, E, WX, WZ> c{f, n0 * n2};
   const int nl = c.nl, L = i + n0 * k;
   const double r = f.rre;
   const int a = (k * (C == 1 ? np1 : nc1) + j) * n0 + i;
@@ -265,26 +270,26 @@ __device__ __forceinline__ T fz_momentum_body(const FzMomentum<T>& f, int i, int
   T F, v;
   if (C == 0) {
     // x-momentum at (i, j, k) of the qx grid
-    F = fz_pair<D1C2P, 0, PY, E, T>(
+    F = fz_pair<D1C2P, 0, PY, E, T, WX, WZ>(
         f.term[0][0], f.rows, nl, n0, i, j, k, n0, 2.0, r, [&](int q) { return c.template conv_c<0>(q, j, k); },
         [&](double s, int q) { return c.template visc_c<0>(s, q, j, k); });
-    F += fz_pair<D1P2C, 1, PY, E, T>(
+    F += fz_pair<D1P2C, 1, PY, E, T, WX, WZ>(
         f.term[0][1], f.rows, nl, n0, i, j, k, np1, 1.0, r, [&](int q) { return c.template conv_xy<0>(i, q, k); },
         [&](double s, int q) { return c.visc_xy(s, i, q, k); });
-    F += fz_pair<D1P2C, 2, PY, E, T>(
+    F += fz_pair<D1P2C, 2, PY, E, T, WX, WZ>(
         f.term[0][2], f.rows, nl, n0, i, j, k, n2, 1.0, r, [&](int q) { return c.template conv_xz<0>(i, j, q); },
         [&](double s, int q) { return c.visc_xz(s, i, j, q); });
-    v = fz_per<D1C2P, T>(f.pres[0], i, n0, [&](int q) { return T(-1.0) * c.pr(q, j, k); });
+    v = fz_per<D1C2P, T, WX>(f.pres[0], i, n0, [&](int q) { return T(-1.0) * c.pr(q, j, k); });
     return c.frac(0, a, F, v, last);
   } else if (C == 1) {
     // y-momentum at (i, j, k) of the qy grid
-    F = fz_pair<D1P2C, 0, PY, E, T>(
+    F = fz_pair<D1P2C, 0, PY, E, T, WX, WZ>(
         f.term[1][0], f.rows, nl, n0, i, j, k, n0, 1.0, r, [&](int q) { return c.template conv_xy<1>(q, j, k); },
         [&](double s, int q) { return c.visc_xy(s, q, j, k); });
-    F += fz_pair<D1C2P, 1, PY, E, T>(
+    F += fz_pair<D1C2P, 1, PY, E, T, WX, WZ>(
         f.term[1][1], f.rows, nl, n0, i, j, k, nc1, 2.0, r, [&](int q) { return c.template conv_c<1>(i, q, k); },
         [&](double s, int q) { return c.template visc_c<1>(s, i, q, k); });
-    F += fz_pair<D1P2C, 2, PY, E, T>(
+    F += fz_pair<D1P2C, 2, PY, E, T, WX, WZ>(
         f.term[1][2], f.rows, nl, n0, i, j, k, n2, 1.0, r, [&](int q) { return c.template conv_yz<1>(i, j, q); },
         [&](double s, int q) { return c.visc_yz(s, i, j, q); });
     v = fz_y<D1C2P, PY, E, T>(f.rows, f.pres[1], j, nc1, f.fpres[1], nl, L,
@@ -292,16 +297,16 @@ __device__ __forceinline__ T fz_momentum_body(const FzMomentum<T>& f, int i, int
     return c.frac(1, a, F, v, last);
   } else {
     // z-momentum at (i, j, k) of the qz grid
-    F = fz_pair<D1P2C, 0, PY, E, T>(
+    F = fz_pair<D1P2C, 0, PY, E, T, WX, WZ>(
         f.term[2][0], f.rows, nl, n0, i, j, k, n0, 1.0, r, [&](int q) { return c.template conv_xz<2>(q, j, k); },
         [&](double s, int q) { return c.visc_xz(s, q, j, k); });
-    F += fz_pair<D1P2C, 1, PY, E, T>(
+    F += fz_pair<D1P2C, 1, PY, E, T, WX, WZ>(
         f.term[2][1], f.rows, nl, n0, i, j, k, np1, 1.0, r, [&](int q) { return c.template conv_yz<2>(i, q, k); },
         [&](double s, int q) { return c.visc_yz(s, i, q, k); });
-    F += fz_pair<D1C2P, 2, PY, E, T>(
+    F += fz_pair<D1C2P, 2, PY, E, T, WX, WZ>(
         f.term[2][2], f.rows, nl, n0, i, j, k, n2, 2.0, r, [&](int q) { return c.template conv_c<2>(i, j, q); },
         [&](double s, int q) { return c.template visc_c<2>(s, i, j, q); });
-    v = fz_per<D1C2P, T>(f.pres[2], k, n2, [&](int q) { return T(-1.0) * c.pr(i, j, q); });
+    v = fz_per<D1C2P, T, WZ>(f.pres[2], k, n2, [&](int q) { return T(-1.0) * c.pr(i, j, q); });
     return c.frac(2, a, F, v, last);
   }
 }
@@ -316,8 +321,17 @@ __global__ void __launch_bounds__(256, 4) fz_momentum_kernel(const __grid_consta
   const bool valid = i < f.n0 && j < (C == 1 ? f.np1 : f.nc1) && k < f.n2;
   T m = T(0);
   if (valid) {
-    if (PY || fz_interior_block(f.nc1)) m = fz_momentum_body<T, TH, PY, C, false>(f, i, j, k);
-    else m = fz_momentum_body<T, TH, PY, C, true>(f, i, j, k);
+    // CTAs whose x (z) neighbours within two of their rows stay inside the domain skip the wrap
+    const int i0 = blockIdx.x * blockDim.x, k0 = blockIdx.z * blockDim.z;
+    const bool wx = !(i0 >= 2 && i0 + (int)blockDim.x + 2 <= f.n0);
+    const bool wz = !(k0 >= 2 && k0 + (int)blockDim.z + 2 <= f.n2);
+    if (PY || fz_interior_block(f.nc1)) {
+      if (!wx && !wz) m = fz_momentum_body<T, TH, PY, C, false, false, false>(f, i, j, k);
+      else if (!wz) m = fz_momentum_body<T, TH, PY, C, false, true, false>(f, i, j, k);
+      else m = fz_momentum_body<T, TH, PY, C, false, true, true>(f, i, j, k);
+    } else {
+      m = fz_momentum_body<T, TH, PY, C, true>(f, i, j, k);
+    }
   }
   if (C == 0 && f.part) {
     // the CTA's share of the mass-flux mean: sum of wy[j] * m (fixed order, so the mean is
