@@ -342,41 +342,10 @@ __global__ void __launch_bounds__(256, 4) fz_momentum_kernel(const __grid_consta
     const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
     if ((tid & 31) == 0) red[tid >> 5] = s;
     __syncthreads();
-    const int nthr = blockDim.x * blockDim.y * blockDim.z;
-    const int nblk = gridDim.x * gridDim.y * gridDim.z;
-    __shared__ int last;
     if (tid == 0) {
       double t = 0.0;
-      for (int w = 0; w < nthr / 32; ++w) t += red[w];
+      for (int w = 0; w < (int)(blockDim.x * blockDim.y * blockDim.z) / 32; ++w) t += red[w];
       f.part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = t;
-      __threadfence();
-      last = atomicAdd(f.count, 1u) == (unsigned)(nblk - 1);
-    }
-    __syncthreads();
-    if (last) {
-      // every CTA's sum is written: the mean over them in index order (thread t takes t, t + nthr,
-      // ..., then a tree over the threads), read past L1; the counter is left at zero
-      __threadfence();
-      __shared__ double acc[256];
-      double a = 0.0;
-      for (int q0 = tid; q0 < nblk; q0 += 8 * nthr) {
-        double v[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) v[u] = q0 + u * nthr < nblk ? __ldcg(f.part + q0 + u * nthr) : 0.0;
-#pragma unroll
-        for (int u = 0; u < 8; ++u)
-          if (q0 + u * nthr < nblk) a += v[u];
-      }
-      acc[tid] = a;
-      __syncthreads();
-      for (int h = nthr / 2; h > 0; h >>= 1) {
-        if (tid < h) acc[tid] += acc[tid + h];
-        __syncthreads();
-      }
-      if (tid == 0) {
-        f.bulk[0] = acc[0] / f.vol;
-        *f.count = 0u;
-      }
     }
   }
 }
@@ -692,7 +661,35 @@ __global__ void __launch_bounds__(256) fz_update_div_kernel(const __grid_constan
   f.out[(k * nc1 + j) * n0 + i] = sum;
 }
 
+// the mass-flux mean from the x pass's per-CTA sums: one CTA, thread t summing parts t, t + 256, ...
+// (eight loads in flight), then a tree over the threads; a fixed order, so the mean is deterministic
+__global__ void __launch_bounds__(256) fz_finalize_mean_kernel(const double* __restrict__ part, int nblk,
+                                                                double* __restrict__ bulk, double vol) {
+  __shared__ double acc[256];
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  double a = 0.0;
+  for (int q0 = tid; q0 < nblk; q0 += 8 * nthr) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = q0 + u * nthr < nblk ? part[q0 + u * nthr] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (q0 + u * nthr < nblk) a += v[u];
+  }
+  acc[tid] = a;
+  __syncthreads();
+  for (int h = nthr / 2; h > 0; h >>= 1) {
+    if (tid < h) acc[tid] += acc[tid + h];
+    __syncthreads();
+  }
+  if (tid == 0) bulk[0] = acc[0] / vol;
+}
+
 }  // namespace
+
+void launch_fz_finalize_mean(const double* part, int nblk, double* bulk, double vol, cudaStream_t st) {
+  fz_finalize_mean_kernel<<<1, 256, 0, st>>>(part, nblk, bulk, vol);
+}
 
 int fz_momentum_x_blocks(int n0, int nc1, int n2) { return ((n0 + 31) / 32) * ((nc1 + 3) / 4) * ((n2 + 1) / 2); }
 

@@ -79,15 +79,13 @@ struct FzMomentum {
   double rre, dt, gam, zeta, alpha;
   const FzRow* rows;     // row tables of the y operators
   // constant mass flux: the x component also writes, per CTA, the y-weighted sum of its outputs
-  // (wy[j] * m, the numerator of the volume mean), and the last CTA to finish (count, zero between
-  // launches) writes their sum / vol to bulk[0]; part null otherwise
+  // (wy[j] * m, the numerator of the volume mean), for launch_fz_finalize_mean; null otherwise
   const double* wy;
   double* part;
-  unsigned* count;
-  double* bulk;
-  double vol;
 };
 
+// bulk[0] = (sum of the x pass's nblk per-CTA sums) / vol, in a fixed order (one CTA)
+void launch_fz_finalize_mean(const double* part, int nblk, double* bulk, double vol, cudaStream_t st);
 // the right-hand side of momentum component c (0 x, 1 y, 2 z) with the fractional step
 // (m = dt*(gam*F + zeta*m0 + alpha*pfc), m0 = F); the advance q += m is left to launch_fz_update
 template <typename T>

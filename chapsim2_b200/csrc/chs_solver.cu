@@ -130,7 +130,6 @@ struct chs_handle {
   int only_kind = -1;
   FzRow* fz_rows = nullptr;  // device row tables of the y operators (chs_fused.cuh)
   double* fz_part = nullptr;  // per-CTA partial sums of the mass-flux mean from the fused x pass
-  unsigned* fz_count = nullptr;  // CTAs of the fused x pass done (zero between launches)
   // plan key -> first row of its table in fz_rows (-1: no table: periodic, or not representable)
   std::map<std::tuple<int, int, int, int, int>, int> fz_index;
   long long launches = 0;
@@ -908,7 +907,6 @@ void setup_device(chs_handle* H, const chs_config* c) {
   H->npart = 148 * 4;
   H->partial = H->dalloc<double>(2 * H->npart);
   H->fz_part = H->dalloc<double>(fz_momentum_x_blocks(nc0, nc1, nc2));
-  H->fz_count = H->dalloc<unsigned>(1);
   H->scal = H->dalloc<double>(16);
 
   // Poisson tables
@@ -1378,9 +1376,6 @@ bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz,
   if (H->idriven == 1) {
     F.wy = H->wy;
     F.part = H->fz_part;
-    F.count = H->fz_count;
-    F.bulk = H->scal + 0;
-    F.vol = H->vol;
   }
   F.m[0] = A(H->mx); F.m[1] = A(H->my); F.m[2] = A(H->mz);
   F.m0[0] = A(H->mx0); F.m0[1] = A(H->my0); F.m0[2] = A(H->mz0);
@@ -1406,13 +1401,19 @@ bool fused_momentum(chs_handle* H, int isub, double* ux, double* uy, double* uz,
             bufs(H->qx, H->qy, H->qz, H->pres, TH ? H->gx : nullptr, TH ? H->gy : nullptr, TH ? H->gz : nullptr,
                  TH ? H->mVisc : nullptr, c == 1 ? H->fb_comb : nullptr, c == 1 ? H->fb_visc2 : nullptr,
                  H->fb_conv2, H->fb_qx, H->fb_qz, H->fb_qy, TH ? H->fb_m : nullptr),
-            bufs(mo[c], m0[c], c == 0 && F.part ? H->fz_part : nullptr, c == 0 && F.part ? H->scal : nullptr),
-            launch_fz_momentum<T>(F, c, st));
+            bufs(mo[c], m0[c], c == 0 && F.part ? H->fz_part : nullptr), launch_fz_momentum<T>(F, c, st));
       H->launches++;
     }
   }
-  // the mass-flux mean, written by the x pass's last CTA
-  const double* bulk = H->idriven == 1 ? H->scal + 0 : nullptr;
+  const double* bulk = nullptr;
+  if (H->idriven == 1) {
+    // the mass-flux mean from the x pass's per-CTA sums
+    const int nblk = fz_momentum_x_blocks(nc0, nc1, nc2);
+    PROFD(H, 3, 8.0 * nblk, bufs(H->fz_part), bufs(H->scal),
+          launch_fz_finalize_mean(H->fz_part, nblk, H->scal + 0, H->vol, st));
+    bulk = H->scal + 0;
+    H->launches++;
+  }
   if (defer_update) return true;  // the advance is folded into fused_update_div and fused_project
   const int w0 = B[1][V_QY][0] == BC_DIRICHLET, w1 = B[1][V_QY][1] == BC_DIRICHLET;
   PROFD(H, 3, nf * 9.0, bufs(H->mx, H->my, H->mz, bulk), bufs(ux, uy, uz),
